@@ -1,0 +1,155 @@
+/*
+ * shg.h — C ABI of the B200 ShockHash construction engine (libshg.so).
+ *
+ * Plain C types only. Every build entry point reproduces, bit for bit, what the reference's
+ * constructors compute (paths relative to the ShockHash reference project):
+ *   - the Golomb-Rice descriptor words   (RiceBitVector::Builder, include/shockhash/RiceBitVector.h:67-127)
+ *   - bucket_size_acc / bucket_pos_acc   (hash_gen, include/ShockHash.h:616-654; ShockHash2.h:455-494)
+ *   - the retrieval input (key, bit)      (ShockHash.h:425-428; ShockHash2-internal.h:548-572),
+ *     in the reference's push order.
+ * The elias-fano and retrieval structures built from those arrays stay on the host.
+ *
+ * Errors: every entry point returns an shg_status; no C++ exception crosses this boundary. The
+ * message of the last failure on the calling thread is available from shg_last_error().
+ * Threading: an engine owns one CUDA stream and its device buffers and is not thread-safe; use one
+ * engine per host thread. Results are owned by the library until shg_result_free().
+ */
+#ifndef SHG_H
+#define SHG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum shg_status {
+    SHG_OK = 0,
+    SHG_ERR_ARG = 1,          /* invalid argument (leaf size, bucket size, null pointer, n >= 2^32) */
+    SHG_ERR_OOM = 2,          /* device or host allocation failed */
+    SHG_ERR_TRIAL_LIMIT = 3,  /* a seed search exceeded its trial cap (duplicate keys loop forever in the reference) */
+    SHG_ERR_CUDA = 4,         /* a CUDA call failed; see shg_last_error() */
+    SHG_ERR_BUCKET = 5,       /* a bucket holds >= 3000 keys (MAX_BUCKET_SIZE, ShockHash.h:33) */
+    SHG_ERR_NO_DEVICE = 6     /* no CUDA device or the kernels are not loadable on it */
+} shg_status;
+
+/* Which reference class the build reproduces. */
+typedef enum shg_variant {
+    SHG_SHOCKHASH = 1,   /* shockhash::ShockHash<leaf_size, false>            (include/ShockHash.h:134) */
+    SHG_SHOCKHASH2 = 2   /* shockhash::ShockHash2<leaf_size>                  (include/ShockHash2.h:117) */
+} shg_variant;
+
+/* How the search stages are scheduled on the device. All modes give identical results. */
+typedef enum shg_mode {
+    SHG_MODE_PERSISTENT = 0,  /* one persistent kernel drains a device work queue of split and leaf nodes */
+    SHG_MODE_LEVELS = 1,      /* one launch per RecSplit level, then one launch for all leaves */
+    SHG_MODE_PER_LEAF = 2     /* comparison form: per-level split launches and one launch per leaf */
+} shg_mode;
+
+typedef struct shg_params {
+    int variant;              /* shg_variant */
+    int leaf_size;            /* ShockHash: 2..60; ShockHash2: 2..128 */
+    uint64_t bucket_size;     /* expected keys per bucket (the reference's bucket_size argument) */
+    int mode;                 /* shg_mode */
+    uint64_t max_trials;      /* cap on the seeds tried per split node / leaf; 0 = library default (2^40) */
+} shg_params;
+
+typedef struct shg_result {
+    uint64_t n;                  /* number of keys */
+    uint64_t nbuckets;           /* max(1, ceil(n / bucket_size)) (ShockHash.h:616) */
+    uint64_t *bucket_size_acc;   /* [nbuckets + 1] cumulative bucket sizes */
+    uint64_t *bucket_pos_acc;    /* [nbuckets + 1] bit offset of each bucket's codes */
+    uint64_t *descriptors;       /* [desc_words] Golomb-Rice stream incl. the (1,1) sentinel */
+    uint64_t desc_words;         /* ((bits + 7) / 8 + 14) / 8 words, the builder's final size */
+    uint64_t desc_bits;          /* bits written, sentinel included */
+    uint64_t *ribbon_keys;       /* [ribbon_n] retrieval input keys (hash.second), reference push order */
+    uint8_t *ribbon_bits;        /* [ribbon_n] retrieval input values */
+    uint64_t ribbon_n;           /* keys in leaves of size >= 2 */
+    double stage_ms[8];          /* device time per stage: hash, partition, tree, splits, leaves, encode, copy-out, total */
+    uint64_t work[8];            /* split evaluations, leaf evaluations, candidate pairs, filtered pairs,
+                                    pseudoforest edge operations, leaves, split nodes, kernel launches */
+} shg_result;
+
+typedef struct shg_engine shg_engine;
+
+/* Create an engine on CUDA device `device` (its own non-blocking stream). */
+shg_status shg_engine_create(int device, shg_engine **out);
+void shg_engine_destroy(shg_engine *e);
+
+/* Build from 128-bit key fingerprints in HOST memory: first[i], second[i] are the halves of the
+ * reference's hash128_t (ShockHash.h:187, ShockHash2.h:167). The arrays are not modified (the
+ * reference sorts its argument vector in place; this entry point leaves the caller's data alone). */
+shg_status shg_build_hash128(shg_engine *e, const shg_params *p, const uint64_t *first,
+                             const uint64_t *second, uint64_t n, shg_result *out);
+
+/* Build from string keys in HOST memory: bytes + offsets[n+1]; keys are hashed on the device with
+ * SpookyHash V2 seed 0, as the reference's string constructors do (ShockHash.h:159-185). */
+shg_status shg_build_strings(shg_engine *e, const shg_params *p, const char *bytes,
+                             const uint64_t *offsets, uint64_t n, shg_result *out);
+
+/* Build from uint64 keys in HOST memory, each hashed as its 8-byte little-endian string. */
+shg_status shg_build_u64(shg_engine *e, const shg_params *p, const uint64_t *keys, uint64_t n,
+                         shg_result *out);
+
+/* Same as shg_build_hash128 / shg_build_u64 with inputs already in DEVICE memory (device pointers
+ * on the engine's device); outputs are still returned in host memory. */
+shg_status shg_build_hash128_device(shg_engine *e, const shg_params *p, const uint64_t *d_first,
+                                    const uint64_t *d_second, uint64_t n, shg_result *out);
+shg_status shg_build_u64_device(shg_engine *e, const shg_params *p, const uint64_t *d_keys,
+                                uint64_t n, shg_result *out);
+
+void shg_result_free(shg_result *r);
+
+/* Hash n string keys (bytes + offsets[n+1], host memory) to 128-bit fingerprints on the device:
+ * sux spooky(key, len, 0) as used by ShockHash.h:129. */
+shg_status shg_hash_strings(shg_engine *e, const char *bytes, const uint64_t *offsets, uint64_t n,
+                            uint64_t *first, uint64_t *second);
+
+/* Batched bipartite leaf search: the device counterpart of the reference's plugin seam
+ * shockhash2construct (include/shockhash/ShockHash2-precompiled.h:9-10,
+ * src/ShockHash2-precompiled.cpp:24-47), for many leaves in one call. Leaf j holds keys
+ * [leaf_offsets[j], leaf_offsets[j+1]) (2..128 keys each, host memory). Writes seeds[j] and, for
+ * every key in order, the retrieval bit bits[k] that constructRetrieval would push. */
+shg_status shg_sh2_construct_leaves(shg_engine *e, const uint64_t *keys, const uint64_t *leaf_offsets,
+                                    uint64_t nleaves, uint64_t *seeds, uint8_t *bits);
+
+/* Batched original-ShockHash leaf search at tree depth `level` (include/ShockHash.h:404-434):
+ * codes[j] = x - start_seed[level]; keys_by_cell/bits are written per leaf in cell order, as the
+ * reference pushes its retrieval input. Leaves of 2..60 keys. */
+shg_status shg_sh1_construct_leaves(shg_engine *e, const uint64_t *keys, const uint64_t *leaf_offsets,
+                                    uint64_t nleaves, int level, uint64_t *codes, uint64_t *keys_by_cell,
+                                    uint8_t *bits);
+
+/* Leaf query of the bipartite variant: shockhash2query (ShockHash2-precompiled.h:8). */
+uint64_t shg_sh2_query(uint64_t leaf_size, uint64_t seed, uint64_t key, uint64_t retrieved);
+
+/* Host query object over a build result: the reference's operator() (ShockHash.h:199-270,
+ * ShockHash2.h:178-230) and getBits() (ShockHash.h:283-286, ShockHash2.h:243-246). The result's
+ * arrays are copied; the caller still frees the result. */
+typedef struct shg_mphf shg_mphf;
+shg_status shg_mphf_create(const shg_params *p, shg_result *r, shg_mphf **out);
+void shg_mphf_destroy(shg_mphf *f);
+/* operator()(const hash128_t&) for n fingerprints (host memory). */
+shg_status shg_mphf_query_hash(const shg_mphf *f, const uint64_t *first, const uint64_t *second, uint64_t n,
+                               uint64_t *out);
+/* operator()(const string&) for n string keys (bytes + offsets[n+1]). */
+shg_status shg_mphf_query_strings(const shg_mphf *f, const char *bytes, const uint64_t *offsets, uint64_t n,
+                                  uint64_t *out);
+/* getBits(): size estimate in bits, with the same component formulas as the reference classes. */
+uint64_t shg_mphf_bits(const shg_mphf *f);
+/* size(): number of keys. */
+uint64_t shg_mphf_size(const shg_mphf *f);
+
+/* Golomb-Rice memo table of a configuration (ShockHash.h:121-127 / ShockHash2.h:106-115):
+ * out[m] for m < 3000 packs golomb parameter << 27 | subtree nodes << 16 | subtree fixed bits. */
+shg_status shg_memo_table(int variant, int leaf_size, uint64_t *out);
+
+/* Message of the last failure on this thread ("" if none). */
+const char *shg_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SHG_H */

@@ -1,0 +1,243 @@
+"""Test infrastructure only (the oracle): ctypes bindings to the two CPU checkers.
+
+* ``RefLib``  — ``oracle/_ref/libshref.so``: the reference's own headers compiled against the
+  restated third-party stand-ins in ``oracle/shims`` (built by ``make -C oracle ref``).
+* ``PortLib`` — ``oracle/_port/libshgport.so``: the C++ restatement in ``oracle/port``
+  (built by ``make -C oracle port``).
+
+Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` use this
+module. The shipped library never imports it.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_SO = os.path.join(HERE, "_ref", "libshref.so")
+PORT_SO = os.path.join(HERE, "_port", "libshgport.so")
+
+_u64p = ctypes.c_void_p
+_vp = ctypes.c_void_p
+_sz = ctypes.c_size_t
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else ctypes.c_void_p(0)
+
+
+def pack_strings(keys):
+    """bytes keys -> (concatenated bytes, offsets[n+1] uint64)."""
+    data = b"".join(keys)
+    offs = np.zeros(len(keys) + 1, dtype=np.uint64)
+    np.cumsum([len(k) for k in keys], out=offs[1:])
+    return data, offs
+
+
+class Built:
+    """Products of one construction, as numpy arrays."""
+
+    def __init__(self, lib, prefix, h):
+        self.lib, self.prefix, self.h = lib, prefix, h
+        f = lambda name: getattr(lib, prefix + name)
+        self.nbuckets = int(f("nbuckets")(_vp(h)))
+        nw = int(f("desc_words")(_vp(h)))
+        self.desc = np.zeros(nw, dtype=np.uint64)
+        f("get_desc")(_vp(h), _ptr(self.desc))
+        self.size_acc = np.zeros(self.nbuckets + 1, dtype=np.uint64)
+        self.pos_acc = np.zeros(self.nbuckets + 1, dtype=np.uint64)
+        f("get_acc")(_vp(h), _ptr(self.size_acc), _ptr(self.pos_acc))
+        nr = int(f("ribbon_n")(_vp(h)))
+        self.ribbon_keys = np.zeros(nr, dtype=np.uint64)
+        self.ribbon_bits = np.zeros(nr, dtype=np.uint8)
+        f("get_ribbon")(_vp(h), _ptr(self.ribbon_keys), _ptr(self.ribbon_bits))
+
+    def query_hash(self, first, second):
+        first = np.ascontiguousarray(first, dtype=np.uint64)
+        second = np.ascontiguousarray(second, dtype=np.uint64)
+        out = np.zeros(len(first), dtype=np.uint64)
+        getattr(self.lib, self.prefix + "query_hash")(_vp(self.h), _ptr(first), _ptr(second), _sz(len(first)), _ptr(out))
+        return out
+
+    def free(self):
+        if self.h:
+            getattr(self.lib, self.prefix + "free")(_vp(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class _Lib:
+    prefix = ""
+
+    def __init__(self, path):
+        self.path = path
+        self.lib = ctypes.CDLL(path)
+        for name in ("nbuckets", "desc_words", "ribbon_n", "get_bits"):
+            fn = getattr(self.lib, self.prefix + name, None)
+            if fn is not None:
+                fn.restype = ctypes.c_uint64
+                fn.argtypes = [_vp]
+
+
+class RefLib(_Lib):
+    prefix = "ref_"
+
+    def __init__(self, path=REF_SO):
+        super().__init__(path)
+        L = self.lib
+        L.ref_build_hash.restype = _vp
+        L.ref_build_hash.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _vp, _sz, _sz, _sz]
+        L.ref_build_strings.restype = _vp
+        L.ref_build_strings.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_char_p, _vp, _sz, _sz, _sz]
+        L.ref_sh2_leaf.restype = ctypes.c_uint64
+        L.ref_sh2_leaf.argtypes = [_sz, _vp, _vp, _vp]
+        L.ref_sh2_leaf_query.restype = ctypes.c_uint64
+        L.ref_sh2_leaf_query.argtypes = [_sz, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64]
+        L.ref_sh1_leaf.restype = ctypes.c_uint64
+        L.ref_sh1_leaf.argtypes = [ctypes.c_int, _vp, _sz, ctypes.c_int, _vp, _vp]
+        L.ref_memo.restype = ctypes.c_int
+        L.ref_memo.argtypes = [ctypes.c_int, ctypes.c_int, _vp]
+        L.ref_query_strings.argtypes = [_vp, ctypes.c_char_p, _vp, _sz, _vp]
+
+    def build_hash(self, variant, leaf, first, second, bucket_size=2000, threads=1):
+        first = np.ascontiguousarray(first, dtype=np.uint64)
+        second = np.ascontiguousarray(second, dtype=np.uint64)
+        h = self.lib.ref_build_hash(variant, leaf, _ptr(first), _ptr(second), len(first), bucket_size, threads)
+        if not h:
+            raise ValueError(f"leaf size {leaf} not instantiated in the reference oracle")
+        b = Built(self.lib, "ref_", h)
+        b.bits = int(self.lib.ref_get_bits(_vp(h)))
+        return b
+
+    def build_strings(self, variant, leaf, keys, bucket_size=2000, threads=1):
+        data, offs = pack_strings(keys)
+        h = self.lib.ref_build_strings(variant, leaf, data, _ptr(offs), len(keys), bucket_size, threads)
+        if not h:
+            raise ValueError(f"leaf size {leaf} not instantiated in the reference oracle")
+        b = Built(self.lib, "ref_", h)
+        b.bits = int(self.lib.ref_get_bits(_vp(h)))
+        b._strings = (data, offs)
+        return b
+
+    def query_strings(self, built, keys):
+        data, offs = pack_strings(keys)
+        out = np.zeros(len(keys), dtype=np.uint64)
+        self.lib.ref_query_strings(_vp(built.h), data, _ptr(offs), len(keys), _ptr(out))
+        return out
+
+    def memo(self, variant, leaf):
+        out = np.zeros(3000, dtype=np.uint64)
+        if not self.lib.ref_memo(variant, leaf, _ptr(out)):
+            return None
+        return out
+
+    def sh2_leaf(self, keys):
+        keys = np.ascontiguousarray(keys, dtype=np.uint64)
+        m = len(keys)
+        rk = np.zeros(m, np.uint64)
+        rb = np.zeros(m, np.uint8)
+        seed = self.lib.ref_sh2_leaf(m, _ptr(keys), _ptr(rk), _ptr(rb))
+        return int(seed), rk, rb
+
+    def sh1_leaf(self, leaf, keys, level=0):
+        keys = np.ascontiguousarray(keys, dtype=np.uint64)
+        m = len(keys)
+        rk = np.zeros(m, np.uint64)
+        rb = np.zeros(m, np.uint8)
+        code = self.lib.ref_sh1_leaf(leaf, _ptr(keys), m, level, _ptr(rk), _ptr(rb))
+        return int(code), rk, rb
+
+    def spooky128(self, keys):
+        data, offs = pack_strings(keys)
+        f = np.zeros(len(keys), np.uint64)
+        s = np.zeros(len(keys), np.uint64)
+        self.lib.ref_spooky128.argtypes = [ctypes.c_char_p, _vp, _sz, _vp, _vp]
+        self.lib.ref_spooky128(data, _ptr(offs), len(keys), _ptr(f), _ptr(s))
+        return f, s
+
+    def murmur64(self, keys):
+        data, offs = pack_strings(keys)
+        out = np.zeros(len(keys), np.uint64)
+        self.lib.ref_murmur64.argtypes = [ctypes.c_char_p, _vp, _sz, _vp]
+        self.lib.ref_murmur64(data, _ptr(offs), len(keys), _ptr(out))
+        return out
+
+
+class PortLib(_Lib):
+    prefix = "port_"
+
+    def __init__(self, path=PORT_SO):
+        super().__init__(path)
+        L = self.lib
+        L.port_build.restype = _vp
+        L.port_build.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_uint64, ctypes.c_uint64]
+        L.port_node_count.restype = ctypes.c_uint64
+        L.port_node_count.argtypes = [_vp]
+        L.port_sh2_leaf.restype = ctypes.c_uint64
+        L.port_sh2_leaf.argtypes = [ctypes.c_uint32, _vp, _vp, _vp, _vp]
+        L.port_sh2_leaf_query.restype = ctypes.c_uint64
+        L.port_sh2_leaf_query.argtypes = [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64]
+        L.port_sh1_leaf.restype = ctypes.c_uint64
+        L.port_sh1_leaf.argtypes = [ctypes.c_uint32, ctypes.c_int, _vp, _vp, _vp]
+        L.port_memo.argtypes = [ctypes.c_int, ctypes.c_int, _vp]
+
+    def build_hash(self, variant, leaf, first, second, bucket_size=2000):
+        first = np.ascontiguousarray(first, dtype=np.uint64)
+        second = np.ascontiguousarray(second, dtype=np.uint64)
+        h = self.lib.port_build(variant, leaf, _ptr(first), _ptr(second), len(first), bucket_size)
+        if not h:
+            raise ValueError("port build failed")
+        b = Built(self.lib, "port_", h)
+        nn = int(self.lib.port_node_count(_vp(h)))
+        b.node_codes = np.zeros(nn, np.uint64)
+        self.lib.port_get_node_codes(_vp(h), _ptr(b.node_codes))
+        b.sorted_keys = np.zeros(len(first), np.uint64)
+        self.lib.port_get_sorted_keys(_vp(h), _ptr(b.sorted_keys))
+        b.work = np.zeros(7, np.uint64)
+        self.lib.port_get_work(_vp(h), _ptr(b.work))
+        return b
+
+    def memo(self, variant, leaf):
+        out = np.zeros(3000, dtype=np.uint64)
+        self.lib.port_memo(variant, leaf, _ptr(out))
+        return out
+
+    def spooky128(self, keys):
+        data, offs = pack_strings(keys)
+        f = np.zeros(len(keys), np.uint64)
+        s = np.zeros(len(keys), np.uint64)
+        self.lib.port_spooky128.argtypes = [ctypes.c_char_p, _vp, _sz, _vp, _vp]
+        self.lib.port_spooky128(data, _ptr(offs), len(keys), _ptr(f), _ptr(s))
+        return f, s
+
+    def sh2_leaf(self, keys, with_work=False):
+        keys = np.ascontiguousarray(keys, dtype=np.uint64)
+        m = len(keys)
+        rk = np.zeros(m, np.uint64)
+        rb = np.zeros(m, np.uint8)
+        w = np.zeros(7, np.uint64)
+        seed = self.lib.port_sh2_leaf(m, _ptr(keys), _ptr(rk), _ptr(rb), _ptr(w))
+        if with_work:
+            return int(seed), rk, rb, w
+        return int(seed), rk, rb
+
+    def sh1_leaf(self, keys, level=0):
+        keys = np.ascontiguousarray(keys, dtype=np.uint64)
+        m = len(keys)
+        rk = np.zeros(m, np.uint64)
+        rb = np.zeros(m, np.uint8)
+        code = self.lib.port_sh1_leaf(m, level, _ptr(keys), _ptr(rk), _ptr(rb))
+        return int(code), rk, rb
+
+
+def ref_available():
+    return os.path.exists(REF_SO)
+
+
+def port_available():
+    return os.path.exists(PORT_SO)

@@ -1,0 +1,295 @@
+// Test infrastructure only (the oracle). Never linked into the shipped library.
+//
+// C entry points over the UNMODIFIED reference headers (include/ShockHash.h, ShockHash2.h,
+// ShockHash2Flat.h, src/ShockHash2-precompiled.cpp, src/Sorter.cpp), compiled against the
+// restated third-party stand-ins in oracle/shims/. Used by the tests to pin the C restatement
+// (oracle/port) and the CUDA path, to dump the construction products (Golomb-Rice words,
+// bucket_size_acc, bucket_pos_acc, retrieval input) and as the timed CPU baseline.
+//
+// Private members are reached with `#define private public`, applied only after every standard
+// and stand-in header has been included, so the reference sources themselves stay untouched.
+#include <array>
+#include <atomic>
+#include <cassert>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstdint>
+#include <cstring>
+#include <experimental/simd>
+#include <fstream>
+#include <iostream>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <span>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <variant>
+#include <vector>
+#include <sux/util/Vector.hpp>
+#include <sux/support/common.hpp>
+#include <sux/function/RecSplit.hpp>
+#include <sux/function/DoubleEF.hpp>
+#include <sux/function/RiceBitVector.hpp>
+#include <SimpleRibbon.h>
+#include <bytehamster/util/Function.h>
+#include <bytehamster/util/MurmurHash64.h>
+#include <bytehamster/util/IntVector.h>
+#include <bytehamster/util/EliasFano.h>
+#include <tlx/math/integer_log2.hpp>
+
+#define private public
+#include <ShockHash.h>
+#include <ShockHash2.h>
+#include <ShockHash2Flat.h>
+#undef private
+
+using shockhash::hash128_t;
+
+namespace {
+
+struct RefBase {
+    virtual ~RefBase() {}
+    virtual size_t desc_words() = 0;
+    virtual const uint64_t *desc_data() = 0;
+    virtual const std::vector<uint64_t> &size_acc() = 0;
+    virtual const std::vector<uint64_t> &pos_acc() = 0;
+    virtual const std::vector<std::pair<uint64_t, uint8_t>> &ribbon_input() = 0;
+    virtual uint64_t query_hash(uint64_t first, uint64_t second) = 0;
+    virtual uint64_t query_str(const char *p, size_t len) = 0;
+    virtual uint64_t bits() = 0;
+    virtual uint64_t nbuckets() = 0;
+};
+
+// Reaching the implicitly private data members of the reference classes (declared before any
+// access specifier, so `#define private public` does not cover them): an explicit template
+// instantiation may name private members, and it defines a friend accessor for each.
+template <class Tag, typename Tag::type M> struct Rob {
+    friend typename Tag::type get(Tag) { return M; }
+};
+template <class C, class T, int K> struct MemberTag {
+    using type = T C::*;
+    friend type get(MemberTag);
+};
+using RBV = shockhash::RiceBitVector<sux::util::AllocType::MALLOC>;
+using EF = sux::function::DoubleEF<sux::util::AllocType::MALLOC>;
+template <size_t L> using RibbonOf = SimpleRibbon<1, (L > 24) ? 128 : 64>;
+template <class C> using DescTag = MemberTag<C, RBV, 0>;
+template <class C> using EfTag = MemberTag<C, EF, 1>;
+template <class C, size_t L> using RibbonTag = MemberTag<C, RibbonOf<L>, 2>;
+template <class C> using NbTag = MemberTag<C, size_t, 3>;
+using RecSplitFn = void(std::vector<uint64_t> &, std::vector<uint64_t> &, size_t, size_t, RBV::Builder &,
+                        std::vector<uint32_t> &, const int, shockhash::TinyBinaryCuckooHashTable &,
+                        std::vector<std::pair<uint64_t, uint8_t>> &);
+template <class C> using RecSplitTag = MemberTag<C, RecSplitFn, 4>;
+
+#define SHG_ROB_CLASS(C, L)                                                   \
+    template struct Rob<DescTag<C>, &C::descriptors>;                         \
+    template struct Rob<EfTag<C>, &C::ef>;                                    \
+    template struct Rob<RibbonTag<C, L>, &C::ribbon>;                         \
+    template struct Rob<NbTag<C>, &C::nbuckets>;
+
+template <class T, size_t L> struct RefRS : RefBase {
+    T obj;
+    template <class... A> explicit RefRS(A &&...a) : obj(std::forward<A>(a)...) {}
+    RBV &desc() { return obj.*get(DescTag<T>()); }
+    size_t desc_words() override { return desc().data.size(); }
+    const uint64_t *desc_data() override { return &desc().data; }
+    const std::vector<uint64_t> &size_acc() override { return (obj.*get(EfTag<T>())).cum_keys; }
+    const std::vector<uint64_t> &pos_acc() override { return (obj.*get(EfTag<T>())).position; }
+    const std::vector<std::pair<uint64_t, uint8_t>> &ribbon_input() override { return (obj.*get(RibbonTag<T, L>())).input; }
+    uint64_t query_hash(uint64_t first, uint64_t second) override { return obj(hash128_t(first, second)); }
+    uint64_t query_str(const char *p, size_t len) override { return obj(std::string(p, len)); }
+    uint64_t bits() override { return obj.getBits(); }
+    uint64_t nbuckets() override { return obj.*get(NbTag<T>()); }
+};
+
+std::vector<std::string> make_strings(const char *bytes, const uint64_t *offsets, size_t n) {
+    std::vector<std::string> keys;
+    keys.reserve(n);
+    for (size_t i = 0; i < n; i++) keys.emplace_back(bytes + offsets[i], offsets[i + 1] - offsets[i]);
+    return keys;
+}
+
+#define SHG_SH1_LEAVES(X) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(10) X(12) X(13) X(16) X(20) X(24) X(25) X(30) X(32) X(33) X(40) X(48) X(60)
+#define SHG_SH2_LEAVES(X) X(2) X(3) X(4) X(5) X(6) X(8) X(9) X(10) X(11) X(12) X(16) X(20) X(24) X(32) X(33) X(40) X(48) X(64) X(100) X(128)
+
+#define X(L) SHG_ROB_CLASS(shockhash::ShockHash<L COMMA false>, L) template struct Rob<RecSplitTag<shockhash::ShockHash<L COMMA false>>, &shockhash::ShockHash<L COMMA false>::recSplit>;
+#define COMMA ,
+SHG_SH1_LEAVES(X)
+#undef X
+#define X(L) SHG_ROB_CLASS(shockhash::ShockHash2<L>, L)
+SHG_SH2_LEAVES(X)
+#undef X
+#undef COMMA
+
+RefBase *make_sh1(int leaf, std::vector<hash128_t> &keys, size_t b, size_t threads) {
+    switch (leaf) {
+#define X(L) case L: return new RefRS<shockhash::ShockHash<L, false>, L>(keys, b, threads);
+        SHG_SH1_LEAVES(X)
+#undef X
+        default: return nullptr;
+    }
+}
+RefBase *make_sh1_str(int leaf, const std::vector<std::string> &keys, size_t b, size_t threads) {
+    switch (leaf) {
+#define X(L) case L: return new RefRS<shockhash::ShockHash<L, false>, L>(keys, b, threads);
+        SHG_SH1_LEAVES(X)
+#undef X
+        default: return nullptr;
+    }
+}
+RefBase *make_sh2(int leaf, std::vector<hash128_t> &keys, size_t b, size_t threads) {
+    switch (leaf) {
+#define X(L) case L: return new RefRS<shockhash::ShockHash2<L>, L>(std::span<hash128_t>(keys), b, threads);
+        SHG_SH2_LEAVES(X)
+#undef X
+        default: return nullptr;
+    }
+}
+RefBase *make_sh2_str(int leaf, const std::vector<std::string> &keys, size_t b, size_t threads) {
+    switch (leaf) {
+#define X(L) case L: return new RefRS<shockhash::ShockHash2<L>, L>(std::span<const std::string>(keys), b, threads);
+        SHG_SH2_LEAVES(X)
+#undef X
+        default: return nullptr;
+    }
+}
+
+// Single original-ShockHash leaf through the reference's own recSplit leaf branch
+// (ShockHash.h:404-439): returns the stored code x - start_seed[level] and the retrieval input.
+template <size_t L>
+uint64_t sh1_leaf(const uint64_t *keys, size_t m, int level, uint64_t *rkeys, uint8_t *rbits) {
+    using C = shockhash::ShockHash<L, false>;
+    C obj;
+    std::vector<uint64_t> bucket(keys, keys + m), temp(shockhash::MAX_BUCKET_SIZE);
+    RBV::Builder builder;
+    std::vector<uint32_t> unary;
+    shockhash::TinyBinaryCuckooHashTable table(L);
+    std::vector<std::pair<uint64_t, uint8_t>> ribbon;
+    (obj.*get(RecSplitTag<C>()))(bucket, temp, 0, m, builder, unary, level, table, ribbon);
+    const int g = shockhash::bij_memo[m];
+    RBV built = builder.build();
+    uint64_t fixed = g ? ((&built.data)[0] & ((uint64_t(1) << g) - 1)) : 0;
+    for (size_t i = 0; i < ribbon.size(); i++) { rkeys[i] = ribbon[i].first; rbits[i] = ribbon[i].second; }
+    return ((uint64_t)unary.at(0) << g) | fixed;
+}
+
+template <size_t L> void memo1(uint64_t *out) {
+    static constexpr auto memo = shockhash::fill_golomb_rice<L>();  // evaluated at compile time, as ShockHash.h:145
+    for (size_t i = 0; i < memo.size(); i++) out[i] = memo[i];
+}
+template <size_t L> void memo2(uint64_t *out) {
+    static constexpr auto memo = shockhash::fill_golomb_rice2<L>();  // as ShockHash2.h:127
+    for (size_t i = 0; i < memo.size(); i++) out[i] = memo[i];
+}
+
+} // namespace
+
+extern "C" {
+
+// The compile-time Golomb-Rice memo table (3000 entries) of ShockHash<leaf> (variant 1) or
+// ShockHash2<leaf> (variant 2). Returns 0 when the leaf size is not instantiated here.
+int ref_memo(int variant, int leaf, uint64_t *out) {
+    if (variant == 1) {
+        switch (leaf) {
+#define X(L) case L: memo1<L>(out); return 1;
+            SHG_SH1_LEAVES(X)
+#undef X
+        }
+    } else {
+        switch (leaf) {
+#define X(L) case L: memo2<L>(out); return 1;
+            SHG_SH2_LEAVES(X)
+#undef X
+        }
+    }
+    return 0;
+}
+
+// 128-bit key fingerprint as the reference computes it (ShockHash.h:129 first_hash).
+void ref_spooky128(const char *bytes, const uint64_t *offsets, size_t n, uint64_t *first, uint64_t *second) {
+    for (size_t i = 0; i < n; i++) {
+        auto h = sux::function::spooky(bytes + offsets[i], offsets[i + 1] - offsets[i], 0);
+        first[i] = h.first;
+        second[i] = h.second;
+    }
+}
+
+void ref_murmur64(const char *bytes, const uint64_t *offsets, size_t n, uint64_t *out) {
+    for (size_t i = 0; i < n; i++) out[i] = bytehamster::util::MurmurHash64(bytes + offsets[i], offsets[i + 1] - offsets[i]);
+}
+
+// variant: 1 = ShockHash<leaf,false>, 2 = ShockHash2<leaf>. Keys given as 128-bit hashes
+// (the hash128_t constructors, ShockHash.h:187 / ShockHash2.h:167; the arrays are not modified).
+void *ref_build_hash(int variant, int leaf, const uint64_t *first, const uint64_t *second, size_t n,
+                     size_t bucket_size, size_t threads) {
+    std::vector<hash128_t> keys(n);
+    for (size_t i = 0; i < n; i++) keys[i] = hash128_t(first[i], second[i]);
+    if (variant == 1) return make_sh1(leaf, keys, bucket_size, threads);
+    if (variant == 2) return make_sh2(leaf, keys, bucket_size, threads);
+    return nullptr;
+}
+
+// Same, from string keys (ShockHash.h:159 / ShockHash2.h:140); offsets has n+1 entries.
+void *ref_build_strings(int variant, int leaf, const char *bytes, const uint64_t *offsets, size_t n,
+                        size_t bucket_size, size_t threads) {
+    auto keys = make_strings(bytes, offsets, n);
+    if (variant == 1) return make_sh1_str(leaf, keys, bucket_size, threads);
+    if (variant == 2) return make_sh2_str(leaf, keys, bucket_size, threads);
+    return nullptr;
+}
+
+void ref_free(void *h) { delete (RefBase *)h; }
+uint64_t ref_nbuckets(void *h) { return ((RefBase *)h)->nbuckets(); }
+uint64_t ref_desc_words(void *h) { return ((RefBase *)h)->desc_words(); }
+void ref_get_desc(void *h, uint64_t *out) {
+    auto *r = (RefBase *)h;
+    std::memcpy(out, r->desc_data(), r->desc_words() * 8);
+}
+void ref_get_acc(void *h, uint64_t *size_acc, uint64_t *pos_acc) {
+    auto *r = (RefBase *)h;
+    std::memcpy(size_acc, r->size_acc().data(), r->size_acc().size() * 8);
+    std::memcpy(pos_acc, r->pos_acc().data(), r->pos_acc().size() * 8);
+}
+uint64_t ref_ribbon_n(void *h) { return ((RefBase *)h)->ribbon_input().size(); }
+void ref_get_ribbon(void *h, uint64_t *keys, uint8_t *bits) {
+    auto &v = ((RefBase *)h)->ribbon_input();
+    for (size_t i = 0; i < v.size(); i++) { keys[i] = v[i].first; bits[i] = v[i].second; }
+}
+void ref_query_hash(void *h, const uint64_t *first, const uint64_t *second, size_t n, uint64_t *out) {
+    auto *r = (RefBase *)h;
+    for (size_t i = 0; i < n; i++) out[i] = r->query_hash(first[i], second[i]);
+}
+void ref_query_strings(void *h, const char *bytes, const uint64_t *offsets, size_t n, uint64_t *out) {
+    auto *r = (RefBase *)h;
+    for (size_t i = 0; i < n; i++) out[i] = r->query_str(bytes + offsets[i], offsets[i + 1] - offsets[i]);
+}
+uint64_t ref_get_bits(void *h) { return ((RefBase *)h)->bits(); }
+
+// One bipartite leaf through the reference's plugin seam (ShockHash2-precompiled.cpp:44-47).
+// Returns the leaf seed; writes m retrieval pairs in the reference's push order.
+uint64_t ref_sh2_leaf(size_t m, const uint64_t *keys, uint64_t *rkeys, uint8_t *rbits) {
+    std::vector<uint64_t> leaf(keys, keys + m);
+    std::vector<std::pair<uint64_t, uint8_t>> ribbon;
+    size_t seed = shockhash::shockhash2construct(m, leaf, ribbon);
+    for (size_t i = 0; i < ribbon.size(); i++) { rkeys[i] = ribbon[i].first; rbits[i] = ribbon[i].second; }
+    return seed;
+}
+uint64_t ref_sh2_leaf_query(size_t m, uint64_t seed, uint64_t key, uint64_t retrieved) {
+    return shockhash::shockhash2query(m, seed, key, retrieved);
+}
+
+// One original-ShockHash leaf (m <= leaf) at tree depth `level`; returns the stored code.
+uint64_t ref_sh1_leaf(int leaf, const uint64_t *keys, size_t m, int level, uint64_t *rkeys, uint8_t *rbits) {
+    switch (leaf) {
+#define X(L) case L: return sh1_leaf<L>(keys, m, level, rkeys, rbits);
+        SHG_SH1_LEAVES(X)
+#undef X
+        default: return ~0ull;
+    }
+}
+
+} // extern "C"

@@ -1,0 +1,334 @@
+"""B200 ShockHash construction engine — Python host interface over ``libshg.so`` (include/shg.h).
+
+Mirrors the reference's public classes (paths relative to the ShockHash reference project):
+
+* ``ShockHash[l](keys, bucket_size, num_threads=1)``  — ``shockhash::ShockHash<l, false>``
+  (include/ShockHash.h:134-191)
+* ``ShockHash2[l](keys, bucket_size, num_threads=1)`` — ``shockhash::ShockHash2<l>``
+  (include/ShockHash2.h:117-170)
+
+with ``obj(key)`` (operator()), ``obj.size()``, ``obj.getBits()`` and ``obj.printBits()``. ``keys``
+is a list of ``str``/``bytes`` (hashed with SpookyHash V2 on the device, as the reference's string
+constructors do), or a pair of uint64 arrays ``(first, second)`` standing for ``hash128_t`` values.
+``num_threads`` is accepted for signature compatibility; construction runs on the GPU.
+
+The CUDA library must be built (``python -m shockhash_b200.build``); there is no CPU fallback:
+every entry point raises ``ShgError`` when the library or a CUDA device is missing.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = ["ShgError", "Engine", "BuildResult", "ShockHash", "ShockHash2", "lib", "LIB_PATH",
+           "SHOCKHASH", "SHOCKHASH2", "MODE_PERSISTENT", "MODE_LEVELS", "MODE_PER_LEAF"]
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libshg.so")
+
+SHOCKHASH, SHOCKHASH2 = 1, 2
+MODE_PERSISTENT, MODE_LEVELS, MODE_PER_LEAF = 0, 1, 2
+_STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_OOM", 3: "ERR_TRIAL_LIMIT", 4: "ERR_CUDA", 5: "ERR_BUCKET",
+           6: "ERR_NO_DEVICE"}
+STAGES = ("hash", "partition", "plan", "splits", "leaves", "encode", "copy_out", "total")
+WORK = ("split_evals", "leaf_evals", "pairs", "pairs_filtered", "uf_edges", "leaves", "split_nodes", "launches")
+
+
+class ShgError(RuntimeError):
+    def __init__(self, status, msg):
+        self.status = status
+        super().__init__(f"shg {_STATUS.get(status, status)}: {msg}")
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [("variant", ctypes.c_int), ("leaf_size", ctypes.c_int), ("bucket_size", ctypes.c_uint64),
+                ("mode", ctypes.c_int), ("max_trials", ctypes.c_uint64)]
+
+
+class _Result(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_uint64), ("nbuckets", ctypes.c_uint64),
+                ("bucket_size_acc", ctypes.POINTER(ctypes.c_uint64)),
+                ("bucket_pos_acc", ctypes.POINTER(ctypes.c_uint64)),
+                ("descriptors", ctypes.POINTER(ctypes.c_uint64)), ("desc_words", ctypes.c_uint64),
+                ("desc_bits", ctypes.c_uint64), ("ribbon_keys", ctypes.POINTER(ctypes.c_uint64)),
+                ("ribbon_bits", ctypes.POINTER(ctypes.c_uint8)), ("ribbon_n", ctypes.c_uint64),
+                ("stage_ms", ctypes.c_double * 8), ("work", ctypes.c_uint64 * 8)]
+
+
+_lib = None
+_vp = ctypes.c_void_p
+_u64 = ctypes.c_uint64
+
+
+def lib():
+    """The loaded ``libshg.so``; raises ShgError when it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ShgError(6, f"{LIB_PATH} is missing; build it with `python -m shockhash_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    P, R = ctypes.POINTER(_Params), ctypes.POINTER(_Result)
+    sig = {
+        "shg_engine_create": ([ctypes.c_int, ctypes.POINTER(_vp)], ctypes.c_int),
+        "shg_engine_destroy": ([_vp], None),
+        "shg_build_hash128": ([_vp, P, _vp, _vp, _u64, R], ctypes.c_int),
+        "shg_build_hash128_device": ([_vp, P, _vp, _vp, _u64, R], ctypes.c_int),
+        "shg_build_u64": ([_vp, P, _vp, _u64, R], ctypes.c_int),
+        "shg_build_u64_device": ([_vp, P, _vp, _u64, R], ctypes.c_int),
+        "shg_build_strings": ([_vp, P, ctypes.c_char_p, _vp, _u64, R], ctypes.c_int),
+        "shg_result_free": ([R], None),
+        "shg_hash_strings": ([_vp, ctypes.c_char_p, _vp, _u64, _vp, _vp], ctypes.c_int),
+        "shg_sh2_construct_leaves": ([_vp, _vp, _vp, _u64, _vp, _vp], ctypes.c_int),
+        "shg_sh1_construct_leaves": ([_vp, _vp, _vp, _u64, ctypes.c_int, _vp, _vp, _vp], ctypes.c_int),
+        "shg_sh2_query": ([_u64, _u64, _u64, _u64], _u64),
+        "shg_memo_table": ([ctypes.c_int, ctypes.c_int, _vp], ctypes.c_int),
+        "shg_last_error": ([], ctypes.c_char_p),
+        "shg_mphf_create": ([P, R, ctypes.POINTER(_vp)], ctypes.c_int),
+        "shg_mphf_destroy": ([_vp], None),
+        "shg_mphf_query_hash": ([_vp, _vp, _vp, _u64, _vp], ctypes.c_int),
+        "shg_mphf_query_strings": ([_vp, ctypes.c_char_p, _vp, _u64, _vp], ctypes.c_int),
+        "shg_mphf_bits": ([_vp], _u64),
+        "shg_mphf_size": ([_vp], _u64),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = L
+    return L
+
+
+def _check(st):
+    if st != 0:
+        raise ShgError(st, lib().shg_last_error().decode())
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def pack_strings(keys):
+    """list of str/bytes -> (bytes, offsets[n+1] uint64)."""
+    bs = [k.encode() if isinstance(k, str) else bytes(k) for k in keys]
+    data = b"".join(bs)
+    offs = np.zeros(len(bs) + 1, dtype=np.uint64)
+    if bs:
+        np.cumsum(np.fromiter((len(k) for k in bs), dtype=np.uint64, count=len(bs)), out=offs[1:])
+    return data, offs
+
+
+def memo_table(variant, leaf_size):
+    out = np.zeros(3000, dtype=np.uint64)
+    _check(lib().shg_memo_table(variant, leaf_size, _ptr(out)))
+    return out
+
+
+def sh2_query(leaf_size, seed, key, retrieved):
+    return int(lib().shg_sh2_query(leaf_size, seed, key, retrieved))
+
+
+class BuildResult:
+    """Products of one device build, copied into numpy arrays."""
+
+    def __init__(self, params, res):
+        self.params = params
+        n, nb = res.n, res.nbuckets
+        self.n, self.nbuckets = n, nb
+        self.bucket_size_acc = np.ctypeslib.as_array(res.bucket_size_acc, (nb + 1,)).copy()
+        self.bucket_pos_acc = np.ctypeslib.as_array(res.bucket_pos_acc, (nb + 1,)).copy()
+        self.descriptors = np.ctypeslib.as_array(res.descriptors, (res.desc_words,)).copy()
+        self.desc_bits = res.desc_bits
+        rn = res.ribbon_n
+        self.ribbon_keys = np.ctypeslib.as_array(res.ribbon_keys, (max(rn, 1),))[:rn].copy()
+        self.ribbon_bits = np.ctypeslib.as_array(res.ribbon_bits, (max(rn, 1),))[:rn].copy()
+        self.stage_ms = dict(zip(STAGES, list(res.stage_ms)))
+        self.work = dict(zip(WORK, [int(x) for x in res.work]))
+
+
+class Engine:
+    """One CUDA device + stream with resident buffers (shg_engine)."""
+
+    def __init__(self, device=0):
+        h = _vp()
+        _check(lib().shg_engine_create(device, ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().shg_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def params(variant, leaf_size, bucket_size=2000, mode=MODE_PERSISTENT, max_trials=0):
+        return _Params(variant, leaf_size, bucket_size, mode, max_trials)
+
+    def _finish(self, p, st, res, keep_raw=False):
+        if st != 0:
+            _check(st)
+        try:
+            out = BuildResult(p, res)
+            if keep_raw:
+                out._mphf = _Mphf(p, res)
+        finally:
+            lib().shg_result_free(ctypes.byref(res))
+        return out
+
+    def build_hash128(self, variant, leaf_size, first, second, bucket_size=2000, mode=MODE_PERSISTENT, max_trials=0,
+                      query=False):
+        first = np.ascontiguousarray(first, dtype=np.uint64)
+        second = np.ascontiguousarray(second, dtype=np.uint64)
+        p, res = self.params(variant, leaf_size, bucket_size, mode, max_trials), _Result()
+        st = lib().shg_build_hash128(self._h, ctypes.byref(p), _ptr(first), _ptr(second), len(first), ctypes.byref(res))
+        return self._finish(p, st, res, query)
+
+    def build_u64(self, variant, leaf_size, keys, bucket_size=2000, mode=MODE_PERSISTENT, max_trials=0, query=False):
+        keys = np.ascontiguousarray(keys, dtype=np.uint64)
+        p, res = self.params(variant, leaf_size, bucket_size, mode, max_trials), _Result()
+        st = lib().shg_build_u64(self._h, ctypes.byref(p), _ptr(keys), len(keys), ctypes.byref(res))
+        return self._finish(p, st, res, query)
+
+    def build_u64_device(self, variant, leaf_size, d_keys_ptr, n, bucket_size=2000, mode=MODE_PERSISTENT):
+        p, res = self.params(variant, leaf_size, bucket_size, mode, 0), _Result()
+        st = lib().shg_build_u64_device(self._h, ctypes.byref(p), _vp(d_keys_ptr), n, ctypes.byref(res))
+        return self._finish(p, st, res)
+
+    def build_strings(self, variant, leaf_size, keys, bucket_size=2000, mode=MODE_PERSISTENT, max_trials=0,
+                      query=False):
+        data, offs = pack_strings(keys)
+        p, res = self.params(variant, leaf_size, bucket_size, mode, max_trials), _Result()
+        st = lib().shg_build_strings(self._h, ctypes.byref(p), data, _ptr(offs), len(offs) - 1, ctypes.byref(res))
+        return self._finish(p, st, res, query)
+
+    def hash_strings(self, keys):
+        data, offs = pack_strings(keys)
+        n = len(offs) - 1
+        f = np.zeros(n, np.uint64)
+        s = np.zeros(n, np.uint64)
+        _check(lib().shg_hash_strings(self._h, data, _ptr(offs), n, _ptr(f), _ptr(s)))
+        return f, s
+
+    def sh2_construct_leaves(self, keys, leaf_offsets):
+        keys = np.ascontiguousarray(keys, dtype=np.uint64)
+        offs = np.ascontiguousarray(leaf_offsets, dtype=np.uint64)
+        nl = len(offs) - 1
+        seeds = np.zeros(max(nl, 1), np.uint64)
+        bits = np.zeros(max(len(keys), 1), np.uint8)
+        _check(lib().shg_sh2_construct_leaves(self._h, _ptr(keys), _ptr(offs), nl, _ptr(seeds), _ptr(bits)))
+        return seeds[:nl], bits[:len(keys)]
+
+    def sh1_construct_leaves(self, keys, leaf_offsets, level=0):
+        keys = np.ascontiguousarray(keys, dtype=np.uint64)
+        offs = np.ascontiguousarray(leaf_offsets, dtype=np.uint64)
+        nl = len(offs) - 1
+        codes = np.zeros(max(nl, 1), np.uint64)
+        kc = np.zeros(max(len(keys), 1), np.uint64)
+        bits = np.zeros(max(len(keys), 1), np.uint8)
+        _check(lib().shg_sh1_construct_leaves(self._h, _ptr(keys), _ptr(offs), nl, level, _ptr(codes), _ptr(kc),
+                                              _ptr(bits)))
+        return codes[:nl], kc[:len(keys)], bits[:len(keys)]
+
+
+class _Mphf:
+    def __init__(self, p, res):
+        h = _vp()
+        _check(lib().shg_mphf_create(ctypes.byref(p), ctypes.byref(res), ctypes.byref(h)))
+        self._h = h
+
+    def query_hash(self, first, second):
+        first = np.ascontiguousarray(first, dtype=np.uint64)
+        second = np.ascontiguousarray(second, dtype=np.uint64)
+        out = np.zeros(len(first), np.uint64)
+        _check(lib().shg_mphf_query_hash(self._h, _ptr(first), _ptr(second), len(first), _ptr(out)))
+        return out
+
+    def query_strings(self, keys):
+        data, offs = pack_strings(keys)
+        out = np.zeros(len(offs) - 1, np.uint64)
+        _check(lib().shg_mphf_query_strings(self._h, data, _ptr(offs), len(offs) - 1, _ptr(out)))
+        return out
+
+    def bits(self):
+        return int(lib().shg_mphf_bits(self._h))
+
+    def __del__(self):
+        try:
+            if self._h:
+                lib().shg_mphf_destroy(self._h)
+        except Exception:
+            pass
+
+
+_default_engines = {}
+
+
+def default_engine(device=0):
+    if device not in _default_engines:
+        _default_engines[device] = Engine(device)
+    return _default_engines[device]
+
+
+class _RecSplitBase:
+    VARIANT = None
+    LEAF = None
+
+    def __init__(self, keys, bucket_size, num_threads=1, mode=MODE_PERSISTENT, engine=None):
+        if self.LEAF is None:
+            raise TypeError("pick a leaf size first, e.g. ShockHash2[64](keys, 2000)")
+        eng = engine or default_engine()
+        if isinstance(keys, tuple) and len(keys) == 2:
+            self._strings = False
+            r = eng.build_hash128(self.VARIANT, self.LEAF, keys[0], keys[1], bucket_size, mode, query=True)
+        else:
+            self._strings = True
+            r = eng.build_strings(self.VARIANT, self.LEAF, keys, bucket_size, mode, query=True)
+        self.result = r
+        self._mphf = r._mphf
+        self.keys_count = r.n
+
+    def __call__(self, key):
+        """operator(): a str/bytes key, or a (first, second) hash128 pair."""
+        if isinstance(key, tuple):
+            return int(self._mphf.query_hash(np.array([key[0]], np.uint64), np.array([key[1]], np.uint64))[0])
+        return int(self._mphf.query_strings([key])[0])
+
+    def query_many(self, keys):
+        if isinstance(keys, tuple):
+            return self._mphf.query_hash(keys[0], keys[1])
+        return self._mphf.query_strings(keys)
+
+    def size(self):
+        return self.keys_count
+
+    def getBits(self):
+        return self._mphf.bits()
+
+    def printBits(self):
+        r, n = self.result, max(self.keys_count, 1)
+        print("trees:  ", r.descriptors.size * 64 / n)
+        print("ribbon: ", 8 * ((len(r.ribbon_keys) + 7) // 8) / n)
+
+
+class _Templated(type):
+    _cache = {}
+
+    def __getitem__(cls, leaf):
+        key = (cls.__name__, int(leaf))
+        if key not in _Templated._cache:
+            _Templated._cache[key] = type(f"{cls.__name__}[{leaf}]", (cls,), {"LEAF": int(leaf)})
+        return _Templated._cache[key]
+
+
+class ShockHash(_RecSplitBase, metaclass=_Templated):
+    """shockhash::ShockHash<LEAF_SIZE, false> (include/ShockHash.h:134); use ShockHash[l](keys, b)."""
+    VARIANT = SHOCKHASH
+
+
+class ShockHash2(_RecSplitBase, metaclass=_Templated):
+    """shockhash::ShockHash2<LEAF_SIZE> (include/ShockHash2.h:117); use ShockHash2[l](keys, b)."""
+    VARIANT = SHOCKHASH2

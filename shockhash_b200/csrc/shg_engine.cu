@@ -1,0 +1,623 @@
+// Engine: device buffers, the build pipeline and the C ABI (include/shg.h).
+//
+// Pipeline of one build (all on the engine's stream):
+//   hash (optional) -> bucket count/scan -> scatter + per-bucket sort  [partition, Sorter.hpp:15-36]
+//   -> host plan of the RecSplit trees from bucket_size_acc            [shapes, ShockHash.h:303-555]
+//   -> split-seed search per tree level                                 [ShockHash.h:451-547]
+//   -> leaf searches                                                    [ShockHash.h:404-434 / ShockHash2.h:267-285]
+//   -> Golomb-Rice encode                                               [RiceBitVector.h:67-127]
+//   -> copy-out of descriptors, accumulators and retrieval input.
+#include <algorithm>
+#include <chrono>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+#include "shg.h"
+#include "shg_common.cuh"
+#include "shg_internal.h"
+
+namespace shg {
+uint64_t sh2_scratch_bytes(uint32_t smax, uint32_t cmax);
+void launch_leaves_sh1_ctr(const Node *nodes, const uint32_t *ids, uint32_t count, const uint64_t *keys, uint64_t *codes,
+                           uint64_t *rib_keys, uint8_t *rib_bits, uint64_t max_trials, uint32_t *err,
+                           unsigned long long *work, unsigned int *ctr, int grid, cudaStream_t s);
+void launch_leaves_sh2_ctr(const Node *nodes, const uint32_t *ids, uint32_t count, const uint64_t *keys, uint64_t *codes,
+                           uint8_t *rib_bits, uint8_t *scratch, uint64_t scratch_per_warp, uint32_t smax, uint32_t cmax,
+                           uint32_t *err, unsigned long long *work, unsigned int *ctr, int grid, cudaStream_t s);
+} // namespace shg
+
+using namespace shg;
+
+static thread_local std::string g_last_error;
+
+static shg_status fail(shg_status st, const std::string &msg) {
+    g_last_error = msg;
+    return st;
+}
+
+#define CU(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) return fail(SHG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+namespace {
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes) {
+        if (bytes <= cap) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = std::max<size_t>(bytes, 256);
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e == cudaSuccess) cap = want;
+        return e;
+    }
+    template <class T> T *as() const { return (T *)p; }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+
+} // namespace
+
+struct shg_engine {
+    int device = 0;
+    int sms = 148;
+    cudaStream_t stream = nullptr;
+    DevBuf in_keys, in_bytes, in_offsets, first, second, sfirst, sidx, counts, cursor, acc, keys, nodes, ids, codes,
+        fixed_off, bnb, bucket_bits, pos_acc, words, rib_keys, rib_bits, skip_bits, scratch, misc;
+    cudaEvent_t ev[8] = {};
+    ~shg_engine() {
+        DevBuf *all[] = {&in_keys, &in_bytes, &in_offsets, &first, &second, &sfirst, &sidx, &counts, &cursor,
+                         &acc, &keys, &nodes, &ids, &codes, &fixed_off, &bnb, &bucket_bits, &pos_acc, &words,
+                         &rib_keys, &rib_bits, &skip_bits, &scratch, &misc};
+        for (DevBuf *b : all) b->release();
+        for (auto &e : ev)
+            if (e) cudaEventDestroy(e);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+struct Misc {  // small device-side counters, one allocation
+    uint32_t err;
+    uint32_t maxsz;
+    unsigned int leaf_ctr;
+    unsigned int pad;
+    unsigned long long work[8];
+};
+
+// Memo tables are cached per configuration (they cost ~3000 transcendental evaluations).
+const Config &config_of(int variant, int leaf) {
+    static std::mutex mu;
+    static std::vector<Config *> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    for (Config *c : cache)
+        if (c->variant == variant && c->leaf == leaf) return *c;
+    cache.push_back(new Config(variant, leaf));
+    return *cache.back();
+}
+
+shg_status check_params(const shg_params *p, uint64_t n) {
+    if (!p) return fail(SHG_ERR_ARG, "null params");
+    if (p->variant != SHG_SHOCKHASH && p->variant != SHG_SHOCKHASH2) return fail(SHG_ERR_ARG, "unknown variant");
+    const int maxleaf = p->variant == SHG_SHOCKHASH ? kMaxLeaf1 : kMaxLeaf2;
+    if (p->leaf_size < 2 || p->leaf_size > maxleaf) return fail(SHG_ERR_ARG, "leaf size out of range");
+    if (p->bucket_size < 1) return fail(SHG_ERR_ARG, "bucket size must be >= 1");
+    if (n >= (1ull << 32)) return fail(SHG_ERR_ARG, "at most 2^32 - 1 keys per build");
+    if (p->mode < SHG_MODE_PERSISTENT || p->mode > SHG_MODE_PER_LEAF) return fail(SHG_ERR_ARG, "unknown mode");
+    return SHG_OK;
+}
+
+// The core build from 128-bit fingerprints already in device memory (e->first / e->second).
+shg_status build_core(shg_engine *e, const shg_params *p, const uint64_t *d_first, const uint64_t *d_second, uint64_t n,
+                      shg_result *out, float hash_ms) {
+    const Config &cfg = config_of(p->variant, p->leaf_size);
+    cudaStream_t s = e->stream;
+    const uint64_t nb = std::max<uint64_t>(1, (n + p->bucket_size - 1) / p->bucket_size);  // ShockHash.h:616
+    memset(out, 0, sizeof(*out));
+    out->n = n;
+    out->nbuckets = nb;
+
+    CU(e->misc.ensure(sizeof(Misc)));
+    Misc *misc = e->misc.as<Misc>();
+    CU(cudaMemsetAsync(misc, 0, sizeof(Misc), s));
+    CU(e->counts.ensure(nb * 4));
+    CU(e->cursor.ensure(nb * 4));
+    CU(e->acc.ensure((nb + 1) * 8));
+    CU(e->sfirst.ensure(std::max<uint64_t>(n, 1) * 8));
+    CU(e->sidx.ensure(std::max<uint64_t>(n, 1) * 4));
+    CU(e->keys.ensure(std::max<uint64_t>(n, 1) * 8));
+
+    // ---- partition
+    CU(cudaEventRecord(e->ev[0], s));
+    launch_bucket_count(d_first, n, nb, e->counts.as<uint32_t>(), s);
+    launch_scan_counts(e->counts.as<uint32_t>(), nb, e->acc.as<uint64_t>(), e->cursor.as<uint32_t>(), &misc->maxsz, s);
+    std::vector<uint64_t> acc(nb + 1);
+    uint32_t maxsz = 0;
+    CU(cudaMemcpyAsync(acc.data(), e->acc.p, (nb + 1) * 8, cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(&maxsz, &misc->maxsz, 4, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    if (maxsz >= (uint32_t)kMaxBucket)
+        return fail(SHG_ERR_BUCKET, "a bucket holds " + std::to_string(maxsz) + " keys (MAX_BUCKET_SIZE is 3000)");
+    launch_bucket_scatter(d_first, n, nb, e->cursor.as<uint32_t>(), e->sfirst.as<uint64_t>(), e->sidx.as<uint32_t>(), s);
+    launch_bucket_sort(e->acc.as<uint64_t>(), nb, e->sfirst.as<uint64_t>(), e->sidx.as<uint32_t>(), d_second,
+                       e->keys.as<uint64_t>(), s);
+    CU(cudaEventRecord(e->ev[1], s));
+
+    // ---- plan (host)
+    Plan plan;
+    try {
+        make_plan(cfg, acc, plan);
+    } catch (const std::exception &ex) {
+        return fail(SHG_ERR_ARG, ex.what());
+    }
+    const uint64_t nn = plan.nodes.size();
+    uint64_t nids = plan.leaves.size();
+    for (auto &l : plan.split_levels) nids += l.size();
+    std::vector<uint32_t> ids;
+    ids.reserve(nids);
+    std::vector<uint64_t> level_off;
+    for (auto &l : plan.split_levels) {
+        level_off.push_back(ids.size());
+        ids.insert(ids.end(), l.begin(), l.end());
+    }
+    const uint64_t leaf_off = ids.size();
+    ids.insert(ids.end(), plan.leaves.begin(), plan.leaves.end());
+    std::vector<uint32_t> skip(kMaxBucket);
+    for (int m = 0; m < kMaxBucket; m++) skip[m] = cfg.skip_bits(m);
+
+    CU(e->nodes.ensure(std::max<uint64_t>(nn, 1) * sizeof(Node)));
+    CU(e->fixed_off.ensure(std::max<uint64_t>(nn, 1) * 2));
+    CU(e->codes.ensure(std::max<uint64_t>(nn, 1) * 8));
+    CU(e->ids.ensure(std::max<uint64_t>(nids, 1) * 4));
+    CU(e->bnb.ensure((nb + 1) * 4));
+    CU(e->skip_bits.ensure(kMaxBucket * 4));
+    CU(e->bucket_bits.ensure(nb * 8));
+    CU(e->pos_acc.ensure((nb + 1) * 8));
+    CU(e->rib_bits.ensure(std::max<uint64_t>(n, 1)));
+    if (p->variant == SHG_SHOCKHASH) CU(e->rib_keys.ensure(std::max<uint64_t>(n, 1) * 8));
+    if (nn) {
+        CU(cudaMemcpyAsync(e->nodes.p, plan.nodes.data(), nn * sizeof(Node), cudaMemcpyHostToDevice, s));
+        CU(cudaMemcpyAsync(e->fixed_off.p, plan.fixed_off.data(), nn * 2, cudaMemcpyHostToDevice, s));
+    }
+    if (nids) CU(cudaMemcpyAsync(e->ids.p, ids.data(), nids * 4, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(e->bnb.p, plan.bucket_node_begin.data(), (nb + 1) * 4, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(e->skip_bits.p, skip.data(), kMaxBucket * 4, cudaMemcpyHostToDevice, s));
+    CU(cudaEventRecord(e->ev[2], s));
+
+    // ---- splits, level by level
+    uint64_t launches = 0;
+    const uint32_t *d_ids = e->ids.as<uint32_t>();
+    for (size_t lv = 0; lv < plan.split_levels.size(); lv++) {
+        const uint32_t cnt = (uint32_t)plan.split_levels[lv].size();
+        if (!cnt) continue;
+        launch_split_level(e->nodes.as<Node>(), d_ids + level_off[lv], cnt, e->keys.as<uint64_t>(), e->codes.as<uint64_t>(),
+                           p->max_trials, &misc->err, &misc->work[0], s);
+        launches++;
+    }
+    CU(cudaGetLastError());
+    CU(cudaEventRecord(e->ev[3], s));
+
+    // ---- leaves
+    const uint32_t nleaves = (uint32_t)plan.leaves.size();
+    const int wpb = leaves_sh2_warps_per_block();
+    const int grid = std::max(1, std::min<int>(e->sms * 8, (int)((nleaves + wpb - 1) / wpb)));
+    if (p->variant == SHG_SHOCKHASH2) {
+        const uint32_t smax = p->leaf_size > 64 ? 16384 : 4096;
+        const uint32_t cmax = p->leaf_size > 64 ? 8192 : 1024;
+        const uint64_t per_warp = (sh2_scratch_bytes(smax, cmax) + 255) & ~255ull;
+        const int grid2 = p->mode == SHG_MODE_PER_LEAF ? 1 : grid;
+        CU(e->scratch.ensure(per_warp * (uint64_t)grid2 * wpb));
+        if (p->mode == SHG_MODE_PER_LEAF) {
+            for (uint32_t l = 0; l < nleaves; l++) {
+                launch_leaves_sh2_ctr(e->nodes.as<Node>(), d_ids + leaf_off + l, 1, e->keys.as<uint64_t>(),
+                                      e->codes.as<uint64_t>(), e->rib_bits.as<uint8_t>(), e->scratch.as<uint8_t>(), per_warp,
+                                      smax, cmax, &misc->err, misc->work, &misc->leaf_ctr, 1, s);
+                launches++;
+            }
+        } else if (nleaves) {
+            launch_leaves_sh2_ctr(e->nodes.as<Node>(), d_ids + leaf_off, nleaves, e->keys.as<uint64_t>(),
+                                  e->codes.as<uint64_t>(), e->rib_bits.as<uint8_t>(), e->scratch.as<uint8_t>(), per_warp, smax,
+                                  cmax, &misc->err, misc->work, &misc->leaf_ctr, grid2, s);
+            launches++;
+        }
+    } else {
+        if (p->mode == SHG_MODE_PER_LEAF) {
+            for (uint32_t l = 0; l < nleaves; l++) {
+                launch_leaves_sh1_ctr(e->nodes.as<Node>(), d_ids + leaf_off + l, 1, e->keys.as<uint64_t>(),
+                                      e->codes.as<uint64_t>(), e->rib_keys.as<uint64_t>(), e->rib_bits.as<uint8_t>(),
+                                      p->max_trials, &misc->err, misc->work, &misc->leaf_ctr, 1, s);
+                launches++;
+            }
+        } else if (nleaves) {
+            launch_leaves_sh1_ctr(e->nodes.as<Node>(), d_ids + leaf_off, nleaves, e->keys.as<uint64_t>(),
+                                  e->codes.as<uint64_t>(), e->rib_keys.as<uint64_t>(), e->rib_bits.as<uint8_t>(), p->max_trials,
+                                  &misc->err, misc->work, &misc->leaf_ctr, grid, s);
+            launches++;
+        }
+    }
+    CU(cudaGetLastError());
+    CU(cudaEventRecord(e->ev[4], s));
+
+    // ---- Golomb-Rice encode
+    launch_gr_bucket_bits(e->nodes.as<Node>(), e->bnb.as<uint32_t>(), nb, e->acc.as<uint64_t>(), e->codes.as<uint64_t>(),
+                          e->skip_bits.as<uint32_t>(), e->bucket_bits.as<uint64_t>(), s);
+    launch_scan_u64(e->bucket_bits.as<uint64_t>(), nb, e->pos_acc.as<uint64_t>(), s);
+    uint64_t total_bits = 0;
+    CU(cudaMemcpyAsync(&total_bits, e->pos_acc.as<uint64_t>() + nb, 8, cudaMemcpyDeviceToHost, s));
+    uint32_t err = 0;
+    CU(cudaMemcpyAsync(&err, &misc->err, 4, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    if (err & kErrTrialLimit) return fail(SHG_ERR_TRIAL_LIMIT, "a seed search exceeded its trial cap (duplicate keys?)");
+    if (err & kErrScratch) return fail(SHG_ERR_TRIAL_LIMIT, "a bipartite leaf exceeded its candidate capacity (duplicate keys?)");
+    if (err) return fail(SHG_ERR_CUDA, "internal device error flag " + std::to_string(err));
+    const uint64_t bits = total_bits + 1;  // + sentinel (ShockHash.h:652)
+    const uint64_t words = ((bits + 7) / 8 + 7 + 7) / 8;
+    CU(e->words.ensure(words * 8));
+    CU(cudaMemsetAsync(e->words.p, 0, words * 8, s));
+    launch_gr_write(e->nodes.as<Node>(), e->fixed_off.as<uint16_t>(), e->bnb.as<uint32_t>(), nb, e->acc.as<uint64_t>(),
+                    e->pos_acc.as<uint64_t>(), e->codes.as<uint64_t>(), e->skip_bits.as<uint32_t>(),
+                    e->words.as<unsigned long long>(), s);
+    launch_set_bit(e->words.as<unsigned long long>(), total_bits, s);
+    launches += 4;
+    CU(cudaGetLastError());
+    CU(cudaEventRecord(e->ev[5], s));
+
+    // ---- copy-out
+    out->bucket_size_acc = (uint64_t *)malloc((nb + 1) * 8);
+    out->bucket_pos_acc = (uint64_t *)malloc((nb + 1) * 8);
+    out->descriptors = (uint64_t *)malloc(words * 8);
+    std::vector<uint64_t> rk(n);
+    std::vector<uint8_t> rb(n);
+    if (!out->bucket_size_acc || !out->bucket_pos_acc || !out->descriptors) {
+        shg_result_free(out);
+        return fail(SHG_ERR_OOM, "host allocation failed");
+    }
+    memcpy(out->bucket_size_acc, acc.data(), (nb + 1) * 8);
+    CU(cudaMemcpyAsync(out->bucket_pos_acc, e->pos_acc.p, (nb + 1) * 8, cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(out->descriptors, e->words.p, words * 8, cudaMemcpyDeviceToHost, s));
+    if (n) {
+        CU(cudaMemcpyAsync(rk.data(), p->variant == SHG_SHOCKHASH ? e->rib_keys.p : e->keys.p, n * 8, cudaMemcpyDeviceToHost, s));
+        CU(cudaMemcpyAsync(rb.data(), e->rib_bits.p, n, cudaMemcpyDeviceToHost, s));
+    }
+    unsigned long long work[8];
+    CU(cudaMemcpyAsync(work, misc->work, sizeof(work), cudaMemcpyDeviceToHost, s));
+    CU(cudaEventRecord(e->ev[6], s));
+    CU(cudaStreamSynchronize(s));
+    out->desc_words = words;
+    out->desc_bits = bits;
+    // Retrieval input: every position except keys of size-1 children and size-1 buckets.
+    const uint64_t rn = n - plan.singles.size();
+    out->ribbon_n = rn;
+    out->ribbon_keys = (uint64_t *)malloc(std::max<uint64_t>(rn, 1) * 8);
+    out->ribbon_bits = (uint8_t *)malloc(std::max<uint64_t>(rn, 1));
+    if (!out->ribbon_keys || !out->ribbon_bits) {
+        shg_result_free(out);
+        return fail(SHG_ERR_OOM, "host allocation failed");
+    }
+    {
+        uint64_t j = 0, si = 0;
+        for (uint64_t i = 0; i < n; i++) {
+            if (si < plan.singles.size() && plan.singles[si] == i) {
+                si++;
+                continue;
+            }
+            out->ribbon_keys[j] = rk[i];
+            out->ribbon_bits[j] = rb[i];
+            j++;
+        }
+    }
+    float ms[6] = {};
+    cudaEventElapsedTime(&ms[0], e->ev[0], e->ev[1]);
+    cudaEventElapsedTime(&ms[1], e->ev[1], e->ev[2]);
+    cudaEventElapsedTime(&ms[2], e->ev[2], e->ev[3]);
+    cudaEventElapsedTime(&ms[3], e->ev[3], e->ev[4]);
+    cudaEventElapsedTime(&ms[4], e->ev[4], e->ev[5]);
+    cudaEventElapsedTime(&ms[5], e->ev[5], e->ev[6]);
+    out->stage_ms[0] = hash_ms;
+    out->stage_ms[1] = ms[0];
+    out->stage_ms[2] = ms[1];
+    out->stage_ms[3] = ms[2];
+    out->stage_ms[4] = ms[3];
+    out->stage_ms[5] = ms[4];
+    out->stage_ms[6] = ms[5];
+    out->stage_ms[7] = hash_ms + ms[0] + ms[1] + ms[2] + ms[3] + ms[4] + ms[5];
+    for (int i = 0; i < 7; i++) out->work[i] = work[i];
+    out->work[5] = nleaves;
+    out->work[6] = nn - nleaves;
+    out->work[7] = launches + 5;
+    return SHG_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+shg_status shg_engine_create(int device, shg_engine **out) {
+    if (!out) return fail(SHG_ERR_ARG, "null output");
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return fail(SHG_ERR_NO_DEVICE, "no CUDA device");
+    if (device < 0 || device >= count) return fail(SHG_ERR_ARG, "device index out of range");
+    CU(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    CU(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10) return fail(SHG_ERR_NO_DEVICE, "libshg is built for sm_100a (B200); found sm_" + std::to_string(prop.major) + std::to_string(prop.minor));
+    auto *e = new shg_engine();
+    e->device = device;
+    e->sms = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete e;
+        return fail(SHG_ERR_CUDA, "stream creation failed");
+    }
+    for (auto &ev : e->ev) cudaEventCreate(&ev);
+    *out = e;
+    return SHG_OK;
+}
+
+void shg_engine_destroy(shg_engine *e) {
+    if (!e) return;
+    cudaSetDevice(e->device);
+    delete e;
+}
+
+static shg_status timed_hash_u64(shg_engine *e, const uint64_t *d_keys, uint64_t n, float &ms) {
+    CU(e->first.ensure(std::max<uint64_t>(n, 1) * 8));
+    CU(e->second.ensure(std::max<uint64_t>(n, 1) * 8));
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, e->stream);
+    launch_spooky_u64(d_keys, n, e->first.as<uint64_t>(), e->second.as<uint64_t>(), e->stream);
+    cudaEventRecord(b, e->stream);
+    cudaEventSynchronize(b);
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    CU(cudaGetLastError());
+    return SHG_OK;
+}
+
+shg_status shg_build_hash128_device(shg_engine *e, const shg_params *p, const uint64_t *d_first, const uint64_t *d_second,
+                                    uint64_t n, shg_result *out) {
+    if (!e || !out) return fail(SHG_ERR_ARG, "null engine or result");
+    shg_status st = check_params(p, n);
+    if (st) return st;
+    CU(cudaSetDevice(e->device));
+    return build_core(e, p, d_first, d_second, n, out, 0.f);
+}
+
+shg_status shg_build_hash128(shg_engine *e, const shg_params *p, const uint64_t *first, const uint64_t *second, uint64_t n,
+                             shg_result *out) {
+    if (!e || !out || (n && (!first || !second))) return fail(SHG_ERR_ARG, "null argument");
+    shg_status st = check_params(p, n);
+    if (st) return st;
+    CU(cudaSetDevice(e->device));
+    CU(e->first.ensure(std::max<uint64_t>(n, 1) * 8));
+    CU(e->second.ensure(std::max<uint64_t>(n, 1) * 8));
+    if (n) {
+        CU(cudaMemcpyAsync(e->first.p, first, n * 8, cudaMemcpyHostToDevice, e->stream));
+        CU(cudaMemcpyAsync(e->second.p, second, n * 8, cudaMemcpyHostToDevice, e->stream));
+    }
+    return build_core(e, p, e->first.as<uint64_t>(), e->second.as<uint64_t>(), n, out, 0.f);
+}
+
+shg_status shg_build_u64_device(shg_engine *e, const shg_params *p, const uint64_t *d_keys, uint64_t n, shg_result *out) {
+    if (!e || !out) return fail(SHG_ERR_ARG, "null engine or result");
+    shg_status st = check_params(p, n);
+    if (st) return st;
+    CU(cudaSetDevice(e->device));
+    float ms = 0;
+    st = timed_hash_u64(e, d_keys, n, ms);
+    if (st) return st;
+    return build_core(e, p, e->first.as<uint64_t>(), e->second.as<uint64_t>(), n, out, ms);
+}
+
+shg_status shg_build_u64(shg_engine *e, const shg_params *p, const uint64_t *keys, uint64_t n, shg_result *out) {
+    if (!e || !out || (n && !keys)) return fail(SHG_ERR_ARG, "null argument");
+    shg_status st = check_params(p, n);
+    if (st) return st;
+    CU(cudaSetDevice(e->device));
+    CU(e->in_keys.ensure(std::max<uint64_t>(n, 1) * 8));
+    if (n) CU(cudaMemcpyAsync(e->in_keys.p, keys, n * 8, cudaMemcpyHostToDevice, e->stream));
+    float ms = 0;
+    st = timed_hash_u64(e, e->in_keys.as<uint64_t>(), n, ms);
+    if (st) return st;
+    return build_core(e, p, e->first.as<uint64_t>(), e->second.as<uint64_t>(), n, out, ms);
+}
+
+static shg_status hash_strings_dev(shg_engine *e, const char *bytes, const uint64_t *offsets, uint64_t n, float &ms) {
+    const uint64_t nbytes = n ? offsets[n] : 0;
+    CU(e->in_bytes.ensure(std::max<uint64_t>(nbytes, 1)));
+    CU(e->in_offsets.ensure((n + 1) * 8));
+    CU(e->first.ensure(std::max<uint64_t>(n, 1) * 8));
+    CU(e->second.ensure(std::max<uint64_t>(n, 1) * 8));
+    if (nbytes) CU(cudaMemcpyAsync(e->in_bytes.p, bytes, nbytes, cudaMemcpyHostToDevice, e->stream));
+    CU(cudaMemcpyAsync(e->in_offsets.p, offsets, (n + 1) * 8, cudaMemcpyHostToDevice, e->stream));
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, e->stream);
+    launch_spooky_strings(e->in_bytes.as<uint8_t>(), e->in_offsets.as<uint64_t>(), n, e->first.as<uint64_t>(),
+                          e->second.as<uint64_t>(), e->stream);
+    cudaEventRecord(b, e->stream);
+    cudaEventSynchronize(b);
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    CU(cudaGetLastError());
+    return SHG_OK;
+}
+
+shg_status shg_build_strings(shg_engine *e, const shg_params *p, const char *bytes, const uint64_t *offsets, uint64_t n,
+                             shg_result *out) {
+    if (!e || !out || !offsets || (n && !bytes)) return fail(SHG_ERR_ARG, "null argument");
+    shg_status st = check_params(p, n);
+    if (st) return st;
+    CU(cudaSetDevice(e->device));
+    float ms = 0;
+    st = hash_strings_dev(e, bytes, offsets, n, ms);
+    if (st) return st;
+    return build_core(e, p, e->first.as<uint64_t>(), e->second.as<uint64_t>(), n, out, ms);
+}
+
+shg_status shg_hash_strings(shg_engine *e, const char *bytes, const uint64_t *offsets, uint64_t n, uint64_t *first,
+                            uint64_t *second) {
+    if (!e || !offsets || !first || !second || (n && !bytes)) return fail(SHG_ERR_ARG, "null argument");
+    CU(cudaSetDevice(e->device));
+    float ms = 0;
+    shg_status st = hash_strings_dev(e, bytes, offsets, n, ms);
+    if (st) return st;
+    if (n) {
+        CU(cudaMemcpyAsync(first, e->first.p, n * 8, cudaMemcpyDeviceToHost, e->stream));
+        CU(cudaMemcpyAsync(second, e->second.p, n * 8, cudaMemcpyDeviceToHost, e->stream));
+    }
+    CU(cudaStreamSynchronize(e->stream));
+    return SHG_OK;
+}
+
+void shg_result_free(shg_result *r) {
+    if (!r) return;
+    free(r->bucket_size_acc);
+    free(r->bucket_pos_acc);
+    free(r->descriptors);
+    free(r->ribbon_keys);
+    free(r->ribbon_bits);
+    r->bucket_size_acc = r->bucket_pos_acc = r->descriptors = r->ribbon_keys = nullptr;
+    r->ribbon_bits = nullptr;
+}
+
+static shg_status leaves_common(shg_engine *e, const uint64_t *keys, const uint64_t *leaf_offsets, uint64_t nleaves,
+                                int max_leaf, int level, std::vector<Node> &nodes) {
+    if (!e || !keys || !leaf_offsets) return fail(SHG_ERR_ARG, "null argument");
+    nodes.resize(nleaves);
+    for (uint64_t j = 0; j < nleaves; j++) {
+        const uint64_t m = leaf_offsets[j + 1] - leaf_offsets[j];
+        if (m < 2 || m > (uint64_t)max_leaf) return fail(SHG_ERR_ARG, "leaf size out of range");
+        if (leaf_offsets[j + 1] >= (1ull << 32)) return fail(SHG_ERR_ARG, "too many keys");
+        Node &n = nodes[j];
+        memset(&n, 0, sizeof n);
+        n.start = (uint32_t)leaf_offsets[j];
+        n.m = (uint16_t)m;
+        n.level = (uint8_t)level;
+        n.kind = kLeaf;
+        const Config &c = config_of(max_leaf == kMaxLeaf1 ? SHG_SHOCKHASH : SHG_SHOCKHASH2, max_leaf);
+        n.g = (uint8_t)c.golomb((uint32_t)m);
+    }
+    return SHG_OK;
+}
+
+shg_status shg_sh2_construct_leaves(shg_engine *e, const uint64_t *keys, const uint64_t *leaf_offsets, uint64_t nleaves,
+                                    uint64_t *seeds, uint8_t *bits) {
+    std::vector<Node> nodes;
+    shg_status st = leaves_common(e, keys, leaf_offsets, nleaves, kMaxLeaf2, 0, nodes);
+    if (st) return st;
+    if (!seeds || !bits) return fail(SHG_ERR_ARG, "null output");
+    if (!nleaves) return SHG_OK;
+    CU(cudaSetDevice(e->device));
+    cudaStream_t s = e->stream;
+    const uint64_t n = leaf_offsets[nleaves];
+    std::vector<uint32_t> ids(nleaves);
+    for (uint64_t j = 0; j < nleaves; j++) ids[j] = (uint32_t)j;
+    CU(e->keys.ensure(n * 8));
+    CU(e->nodes.ensure(nleaves * sizeof(Node)));
+    CU(e->ids.ensure(nleaves * 4));
+    CU(e->codes.ensure(nleaves * 8));
+    CU(e->rib_bits.ensure(n));
+    CU(e->misc.ensure(sizeof(Misc)));
+    Misc *misc = e->misc.as<Misc>();
+    CU(cudaMemsetAsync(misc, 0, sizeof(Misc), s));
+    CU(cudaMemcpyAsync(e->keys.p, keys, n * 8, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(e->nodes.p, nodes.data(), nleaves * sizeof(Node), cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(e->ids.p, ids.data(), nleaves * 4, cudaMemcpyHostToDevice, s));
+    uint64_t maxm = 0;
+    for (auto &nd : nodes) maxm = std::max<uint64_t>(maxm, nd.m);
+    const uint32_t smax = maxm > 64 ? 16384 : 4096, cmax = maxm > 64 ? 8192 : 1024;
+    const uint64_t per_warp = (sh2_scratch_bytes(smax, cmax) + 255) & ~255ull;
+    const int wpb = leaves_sh2_warps_per_block();
+    const int grid = std::max(1, std::min<int>(e->sms * 8, (int)((nleaves + wpb - 1) / wpb)));
+    CU(e->scratch.ensure(per_warp * (uint64_t)grid * wpb));
+    launch_leaves_sh2_ctr(e->nodes.as<Node>(), e->ids.as<uint32_t>(), (uint32_t)nleaves, e->keys.as<uint64_t>(),
+                          e->codes.as<uint64_t>(), e->rib_bits.as<uint8_t>(), e->scratch.as<uint8_t>(), per_warp, smax, cmax,
+                          &misc->err, misc->work, &misc->leaf_ctr, grid, s);
+    CU(cudaGetLastError());
+    uint32_t err = 0;
+    CU(cudaMemcpyAsync(seeds, e->codes.p, nleaves * 8, cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(bits, e->rib_bits.p, n, cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(&err, &misc->err, 4, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    if (err) return fail(SHG_ERR_TRIAL_LIMIT, "leaf search failed (error flags " + std::to_string(err) + ")");
+    return SHG_OK;
+}
+
+shg_status shg_sh1_construct_leaves(shg_engine *e, const uint64_t *keys, const uint64_t *leaf_offsets, uint64_t nleaves,
+                                    int level, uint64_t *codes, uint64_t *keys_by_cell, uint8_t *bits) {
+    if (level < 0 || level >= kMaxLevels) return fail(SHG_ERR_ARG, "level out of range");
+    std::vector<Node> nodes;
+    shg_status st = leaves_common(e, keys, leaf_offsets, nleaves, kMaxLeaf1, level, nodes);
+    if (st) return st;
+    if (!codes || !keys_by_cell || !bits) return fail(SHG_ERR_ARG, "null output");
+    if (!nleaves) return SHG_OK;
+    CU(cudaSetDevice(e->device));
+    cudaStream_t s = e->stream;
+    const uint64_t n = leaf_offsets[nleaves];
+    std::vector<uint32_t> ids(nleaves);
+    for (uint64_t j = 0; j < nleaves; j++) ids[j] = (uint32_t)j;
+    CU(e->keys.ensure(n * 8));
+    CU(e->nodes.ensure(nleaves * sizeof(Node)));
+    CU(e->ids.ensure(nleaves * 4));
+    CU(e->codes.ensure(nleaves * 8));
+    CU(e->rib_bits.ensure(n));
+    CU(e->rib_keys.ensure(n * 8));
+    CU(e->misc.ensure(sizeof(Misc)));
+    Misc *misc = e->misc.as<Misc>();
+    CU(cudaMemsetAsync(misc, 0, sizeof(Misc), s));
+    CU(cudaMemcpyAsync(e->keys.p, keys, n * 8, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(e->nodes.p, nodes.data(), nleaves * sizeof(Node), cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(e->ids.p, ids.data(), nleaves * 4, cudaMemcpyHostToDevice, s));
+    const int wpb = leaves_sh1_warps_per_block();
+    const int grid = std::max(1, std::min<int>(e->sms * 8, (int)((nleaves + wpb - 1) / wpb)));
+    launch_leaves_sh1_ctr(e->nodes.as<Node>(), e->ids.as<uint32_t>(), (uint32_t)nleaves, e->keys.as<uint64_t>(),
+                          e->codes.as<uint64_t>(), e->rib_keys.as<uint64_t>(), e->rib_bits.as<uint8_t>(), 0, &misc->err,
+                          misc->work, &misc->leaf_ctr, grid, s);
+    CU(cudaGetLastError());
+    uint32_t err = 0;
+    CU(cudaMemcpyAsync(codes, e->codes.p, nleaves * 8, cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(keys_by_cell, e->rib_keys.p, n * 8, cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(bits, e->rib_bits.p, n, cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(&err, &misc->err, 4, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    if (err) return fail(SHG_ERR_TRIAL_LIMIT, "leaf search failed (error flags " + std::to_string(err) + ")");
+    return SHG_OK;
+}
+
+uint64_t shg_sh2_query(uint64_t leaf_size, uint64_t seed, uint64_t key, uint64_t retrieved) {
+    return sh2_leaf_query((uint32_t)leaf_size, seed, key, retrieved);
+}
+
+shg_status shg_memo_table(int variant, int leaf_size, uint64_t *out) {
+    if (!out) return fail(SHG_ERR_ARG, "null output");
+    if (variant != SHG_SHOCKHASH && variant != SHG_SHOCKHASH2) return fail(SHG_ERR_ARG, "unknown variant");
+    const int maxleaf = variant == SHG_SHOCKHASH ? kMaxLeaf1 : kMaxLeaf2;
+    if (leaf_size < 2 || leaf_size > maxleaf) return fail(SHG_ERR_ARG, "leaf size out of range");
+    const Config &c = config_of(variant, leaf_size);
+    memcpy(out, c.memo.data(), kMaxBucket * 8);
+    return SHG_OK;
+}
+
+const char *shg_last_error(void) { return g_last_error.c_str(); }
+
+} // extern "C"

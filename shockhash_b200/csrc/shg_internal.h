@@ -1,0 +1,98 @@
+// Internal declarations shared by the engine's translation units (not part of the C ABI).
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+#include "shg.h"
+
+namespace shg {
+
+// Node kinds of the RecSplit tree.
+enum NodeKind : uint8_t { kLeaf = 0, kSplit2 = 1, kSplitK = 2 };
+
+// One tree node as the device sees it (16 bytes). `start` is the global offset of the node's first
+// key in the bucket-ordered key array; `unit` is the split point (fanout 2) or the part size.
+struct __align__(16) Node {
+    uint32_t start;
+    uint16_t m;
+    uint8_t level;
+    uint8_t kind;
+    uint32_t bucket;
+    uint16_t unit;
+    uint8_t fanout;
+    uint8_t g;  // Golomb-Rice parameter of the node's code
+};
+static_assert(sizeof(Node) == 16, "Node must stay 16 bytes");
+
+// Splitting thresholds and the Golomb-Rice memo of one configuration.
+// ShockHash<l>: lower = l*(l>24?4:2), upper = lower*(l>24?3:2) (ShockHash.h:63-72);
+// ShockHash2<l>: lower = 4l, upper = 12l (ShockHash2.h:49-56).
+struct Config {
+    int variant = 0, leaf = 0;
+    uint32_t lower = 0, upper = 0;
+    std::vector<uint64_t> memo;  // kMaxBucket entries, fill_golomb_rice(2) layout
+    Config() {}
+    Config(int variant, int leaf);
+    int golomb(uint32_t m) const { return (int)(memo[m] >> 27); }
+    uint32_t skip_bits(uint32_t m) const { return (uint32_t)(memo[m] & 0xFFFF); }
+    uint32_t skip_nodes(uint32_t m) const { return (uint32_t)((memo[m] >> 16) & 0x7FF); }
+};
+
+// Tree of one bucket size, in preorder (the order the reference appends codes, ShockHash.h:303-555).
+struct TNode {
+    uint16_t rel;        // first key relative to the bucket start
+    uint16_t m;
+    uint8_t level, kind, fanout, g;
+    uint16_t unit;
+    uint16_t fixed_off;  // bit offset of the node's fixed part within the bucket
+};
+struct Shape {
+    std::vector<TNode> nodes;
+    std::vector<uint16_t> singles;  // relative positions of size-1 children (no code, no retrieval bit)
+    int depth = 0;
+};
+const Shape &shape_of(const Config &c, uint32_t m, std::vector<Shape> &cache, std::vector<char> &have);
+
+// Expanded plan of a whole build.
+struct Plan {
+    std::vector<Node> nodes;                      // all nodes, buckets in order, preorder within a bucket
+    std::vector<uint16_t> fixed_off;              // per node
+    std::vector<uint32_t> bucket_node_begin;      // [nbuckets + 1]
+    std::vector<std::vector<uint32_t>> split_levels;  // split node ids per level
+    std::vector<uint32_t> leaves;                 // leaf node ids
+    std::vector<uint32_t> leaf_sizes_hist;        // count of leaves per size
+    std::vector<uint64_t> singles;                // global positions of keys in size-1 children or buckets
+    uint64_t leaf_keys = 0;
+};
+void make_plan(const Config &c, const std::vector<uint64_t> &bucket_size_acc, Plan &plan);
+
+// Device error flag bits.
+enum : uint32_t { kErrTrialLimit = 1, kErrScratch = 2, kErrBucket = 4, kErrInternal = 8 };
+
+// ----------------------------------------------------------------- kernels (shg_kernels.cu)
+void launch_spooky_u64(const uint64_t *keys, uint64_t n, uint64_t *first, uint64_t *second, cudaStream_t s);
+void launch_spooky_strings(const uint8_t *bytes, const uint64_t *offsets, uint64_t n, uint64_t *first,
+                           uint64_t *second, cudaStream_t s);
+void launch_bucket_count(const uint64_t *first, uint64_t n, uint64_t nb, uint32_t *counts, cudaStream_t s);
+void launch_scan_counts(const uint32_t *counts, uint64_t nb, uint64_t *acc, uint32_t *cursor, uint32_t *maxsz,
+                        cudaStream_t s);
+void launch_bucket_scatter(const uint64_t *first, uint64_t n, uint64_t nb, uint32_t *cursor, uint64_t *sfirst,
+                           uint32_t *sidx, cudaStream_t s);
+void launch_bucket_sort(const uint64_t *acc, uint64_t nb, const uint64_t *sfirst, const uint32_t *sidx,
+                        const uint64_t *second, uint64_t *keys, cudaStream_t s);
+void launch_split_level(const Node *nodes, const uint32_t *ids, uint32_t count, uint64_t *keys,
+                        uint64_t *codes, uint64_t max_trials, uint32_t *err, unsigned long long *work,
+                        cudaStream_t s);
+int leaves_sh2_warps_per_block();
+int leaves_sh1_warps_per_block();
+void launch_gr_bucket_bits(const Node *nodes, const uint32_t *bnb, uint64_t nb, const uint64_t *acc,
+                           const uint64_t *codes, const uint32_t *memo_skip_bits, uint64_t *bucket_bits,
+                           cudaStream_t s);
+void launch_scan_u64(const uint64_t *in, uint64_t n, uint64_t *out_excl_plus_total, cudaStream_t s);
+void launch_gr_write(const Node *nodes, const uint16_t *fixed_off, const uint32_t *bnb, uint64_t nb,
+                     const uint64_t *acc, const uint64_t *pos_acc, const uint64_t *codes,
+                     const uint32_t *memo_skip_bits, unsigned long long *words, cudaStream_t s);
+void launch_set_bit(unsigned long long *words, uint64_t bit, cudaStream_t s);
+
+} // namespace shg

@@ -1,0 +1,180 @@
+// Host-side planning of a build: the Golomb-Rice memo of a configuration and the RecSplit tree
+// of every bucket, laid out in preorder. The tree's shape depends only on the bucket size, so one
+// shape per distinct size is derived (mirroring the recursion of ShockHash.h:303-555 /
+// ShockHash2.h:259-394) and then stamped out for every bucket of that size.
+#include <cmath>
+#include <cstdint>
+#include <stdexcept>
+#include <vector>
+#include "shg_common.cuh"
+#include "shg_internal.h"
+
+namespace shg {
+
+// ShockHash.h:53-61
+static const uint8_t kBijMemo[61] = {0,  0,  0,  0,  0,  0,  1,  1,  2,  2,  2,  3,  3,  4,  4,  4,  5,  5,  6,  6,  7,
+                                     7,  8,  8,  9,  9,  9,  10, 10, 10, 11, 11, 12, 12, 13, 13, 13, 14, 15, 15, 15,
+                                     16, 16, 16, 17, 17, 18, 18, 19, 19, 19, 20, 20, 20, 21, 21, 22, 22, 23, 23, 23};
+// ShockHash2.h:33-47
+static const uint8_t kBijMemo2[129] = {
+    0,  0,  0,  0,  0,  0,  1,  3,  2,  4,  4,  6,  5,  7,  6,  8,  7,  8,  7,  9,  8,  10, 9,  11, 10, 11,
+    11, 12, 11, 13, 12, 14, 13, 14, 14, 15, 14, 16, 15, 17, 16, 18, 17, 18, 17, 19, 18, 20, 19, 21, 20, 22,
+    21, 22, 22, 23, 22, 24, 23, 25, 24, 26, 25, 27, 26, 27, 27, 28, 27, 29, 28, 30, 29, 31, 30, 32, 31, 33,
+    32, 33, 33, 34, 33, 35, 34, 36, 35, 37, 36, 38, 37, 39, 38, 40, 38, 40, 40, 41, 40, 42, 41, 43, 42, 44,
+    43, 45, 44, 45, 45, 47, 46, 47, 46, 48, 47, 49, 48, 50, 49, 51, 50, 52, 51, 53, 52, 54, 53, 54, 54};
+
+Config::Config(int variant_, int leaf_) : variant(variant_), leaf(leaf_) {
+    if (variant == SHG_SHOCKHASH) {
+        lower = leaf * (leaf > 24 ? 4 : 2);
+        upper = lower * (leaf > 24 ? 3 : 2);
+    } else {
+        lower = leaf * 4;
+        upper = lower * 3;
+    }
+    memo.assign(kMaxBucket, 0);
+    uint32_t s = 0;
+    // fill_golomb_rice (ShockHash.h:121-127) / fill_golomb_rice2 (ShockHash2.h:106-115)
+    for (; s <= (uint32_t)leaf; ++s) {
+        const uint64_t b = variant == SHG_SHOCKHASH ? kBijMemo[s] : kBijMemo2[s];
+        memo[s] = b << 27 | (uint64_t)(s > 1) << 16 | b;
+    }
+    // _fill_golomb_rice (ShockHash.h:79-119) / _fill_golomb_rice2 (ShockHash2.h:63-104): the Rice
+    // parameter of a split is ceil(log2(-ln(phi) / ln(1 - p))) with p the probability that a
+    // random seed yields the exact part sizes.
+    for (; s < (uint32_t)kMaxBucket; ++s) {
+        const uint32_t m = s;
+        long k[32] = {0};
+        uint32_t fanout, unit;
+        if (m > upper) {
+            unit = upper * (uint16_t(m / 2 + upper - 1) / upper);
+            fanout = 2;
+        } else if (m > lower) {
+            unit = lower;
+            fanout = uint16_t(m + lower - 1) / lower;
+        } else {
+            unit = leaf;
+            fanout = uint16_t(m + leaf - 1) / leaf;
+        }
+        k[fanout - 1] = m;
+        for (uint32_t i = 0; i < fanout - 1; ++i) { k[i] = unit; k[fanout - 1] -= k[i]; }
+        double sqrt_prod = 1;
+        for (uint32_t i = 0; i < fanout; ++i) sqrt_prod *= std::sqrt((double)k[i]);
+        const double p = std::sqrt((double)m) / (std::pow(2 * M_PI, (fanout - 1.) / 2) * sqrt_prod);
+        uint64_t grl = (uint64_t)std::ceil(std::log2(-std::log((std::sqrt(5) + 1) / 2) / std::log1p(-p)));
+        memo[m] = grl << 27;
+        for (uint32_t i = 0; i < fanout; ++i) grl += memo[k[i]] & 0xFFFF;
+        memo[m] |= grl;
+        uint64_t nodes = 1;
+        for (uint32_t i = 0; i < fanout; ++i) nodes += (memo[k[i]] >> 16) & 0x7FF;
+        memo[m] |= nodes << 16;
+    }
+}
+
+namespace {
+struct ShapeBuilder {
+    const Config &c;
+    Shape &sh;
+    uint32_t fixed = 0;
+    void rec(uint32_t rel, uint32_t m, int level) {
+        if (level >= kMaxLevels) throw std::runtime_error("tree deeper than the start-seed table");
+        if (level + 1 > sh.depth) sh.depth = level + 1;
+        TNode t{};
+        t.rel = (uint16_t)rel;
+        t.m = (uint16_t)m;
+        t.level = (uint8_t)level;
+        t.g = (uint8_t)c.golomb(m);
+        t.fixed_off = (uint16_t)fixed;
+        fixed += t.g;
+        if (m <= (uint32_t)c.leaf) {
+            t.kind = kLeaf;
+            sh.nodes.push_back(t);
+            return;
+        }
+        if (m > c.upper) {
+            const uint32_t sp = (uint16_t(m / 2 + c.upper - 1) / c.upper) * c.upper;
+            t.kind = kSplit2;
+            t.unit = (uint16_t)sp;
+            t.fanout = 2;
+            sh.nodes.push_back(t);
+            rec(rel, sp, level + 1);
+            if (m - sp > 1) rec(rel + sp, m - sp, level + 1);
+            else sh.singles.push_back((uint16_t)(rel + sp));
+        } else {
+            const uint32_t unit = m > c.lower ? c.lower : (uint32_t)c.leaf;
+            t.kind = kSplitK;
+            t.unit = (uint16_t)unit;
+            t.fanout = (uint8_t)(uint16_t(m + unit - 1) / unit);
+            sh.nodes.push_back(t);
+            uint32_t i;
+            for (i = 0; i < m - unit; i += unit) rec(rel + i, unit, level + 1);
+            if (m - i > 1) rec(rel + i, m - i, level + 1);
+            else sh.singles.push_back((uint16_t)(rel + i));
+        }
+    }
+};
+} // namespace
+
+const Shape &shape_of(const Config &c, uint32_t m, std::vector<Shape> &cache, std::vector<char> &have) {
+    if (!have[m]) {
+        Shape &sh = cache[m];
+        sh = Shape();
+        if (m == 1) sh.singles.push_back(0);
+        if (m > 1) {
+            ShapeBuilder b{c, sh};
+            b.rec(0, m, 0);
+        }
+        have[m] = 1;
+    }
+    return cache[m];
+}
+
+void make_plan(const Config &c, const std::vector<uint64_t> &acc, Plan &plan) {
+    const uint64_t nb = acc.size() - 1;
+    std::vector<Shape> cache(kMaxBucket);
+    std::vector<char> have(kMaxBucket, 0);
+    uint64_t total = 0;
+    for (uint64_t b = 0; b < nb; b++) {
+        const uint64_t m = acc[b + 1] - acc[b];
+        if (m >= (uint64_t)kMaxBucket) throw std::runtime_error("bucket too large");
+        total += shape_of(c, (uint32_t)m, cache, have).nodes.size();
+    }
+    plan.nodes.resize(total);
+    plan.fixed_off.resize(total);
+    plan.bucket_node_begin.assign(nb + 1, 0);
+    plan.split_levels.clear();
+    plan.leaves.clear();
+    plan.singles.clear();
+    plan.leaf_sizes_hist.assign(kMaxLeaf2 + 1, 0);
+    plan.leaf_keys = 0;
+    uint64_t id = 0;
+    for (uint64_t b = 0; b < nb; b++) {
+        plan.bucket_node_begin[b] = (uint32_t)id;
+        const uint32_t m = (uint32_t)(acc[b + 1] - acc[b]);
+        const Shape &sh = shape_of(c, m, cache, have);
+        for (uint16_t s : sh.singles) plan.singles.push_back(acc[b] + s);
+        for (const TNode &t : sh.nodes) {
+            Node &n = plan.nodes[id];
+            n.start = (uint32_t)(acc[b] + t.rel);
+            n.m = t.m;
+            n.level = t.level;
+            n.kind = t.kind;
+            n.bucket = (uint32_t)b;
+            n.unit = t.unit;
+            n.fanout = t.fanout;
+            n.g = t.g;
+            plan.fixed_off[id] = t.fixed_off;
+            if (t.kind == kLeaf) {
+                plan.leaves.push_back((uint32_t)id);
+                plan.leaf_sizes_hist[t.m]++;
+                plan.leaf_keys += t.m;
+            } else {
+                if (plan.split_levels.size() <= t.level) plan.split_levels.resize(t.level + 1);
+                plan.split_levels[t.level].push_back((uint32_t)id);
+            }
+            id++;
+        }
+    }
+    plan.bucket_node_begin[nb] = (uint32_t)id;
+}
+
+} // namespace shg

@@ -1,0 +1,218 @@
+// RecSplit split-seed search and stable partition (ShockHash.h:451-547, ShockHash2.h:290-386).
+//
+// One thread block per split node. The node's keys (<= 3000 x 8 B) sit in shared memory and are
+// read as warp-wide broadcasts; each lane owns kSeedsPerLane consecutive-in-round seeds and keeps
+// per-seed part counts in registers. A seed x is valid when every part but the last receives
+// exactly its size under  part(k) = remap16(remix(k + x), m) / unit  (fanout 2: h >= split).
+//
+// The part test never multiplies: h = (r16 * m) >> 16 < K  <=>  r16 < ceil(K * 65536 / m) with
+// r16 the low 16 bits of remix, so each part boundary becomes one 16-bit threshold and only the
+// low 47 bits of remix's second product are needed.
+//
+// Rounds: the block evaluates 64*G seeds per round (G warp groups; a group's warps split the
+// node's keys and merge counts in shared memory). G is picked from the node's expected trial count
+// 1/p (the same p the Golomb-Rice memo uses) so the overshoot past the answer stays small. The
+// smallest valid seed of the first round that has one is the answer, identical to the reference's
+// sequential `for (;;) x++` search.
+#include <cmath>
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "shg_common.cuh"
+#include "shg_internal.h"
+
+namespace shg {
+
+constexpr int kSplitThreads = 256;
+constexpr int kSplitWarps = kSplitThreads / 32;
+constexpr int kSeedsPerLane = 2;
+constexpr int kSeedsPerWarp = 32 * kSeedsPerLane;
+
+struct SplitSmem {
+    uint64_t keys[kMaxBucket];
+    uint32_t part_counts[kSplitWarps][kSeedsPerWarp][3];
+    uint64_t scan[kSplitWarps];
+    uint32_t best;
+};
+
+// Counts of keys below each of NT thresholds, for kSeedsPerLane seeds, over keys [lo, hi).
+template <int NT>
+__device__ __forceinline__ void count_range(const uint64_t *__restrict__ sk, uint32_t lo, uint32_t hi, uint64_t x0,
+                                            const uint32_t T0, const uint32_t T1, const uint32_t T2,
+                                            uint32_t (&c)[kSeedsPerLane][3]) {
+    const uint32_t T[3] = {T0, T1, T2};
+    uint32_t i = lo;
+    for (; i + 2 <= hi; i += 2) {
+        const uint64_t k0 = sk[i], k1 = sk[i + 1];
+#pragma unroll
+        for (int s = 0; s < kSeedsPerLane; s++) {
+            const uint64_t x = x0 + (uint64_t)(s * 32);
+            const uint32_t r0 = remix_low16(k0 + x);
+            const uint32_t r1 = remix_low16(k1 + x);
+#pragma unroll
+            for (int t = 0; t < NT; t++) c[s][t] += (r0 < T[t]) + (r1 < T[t]);
+        }
+    }
+    for (; i < hi; i++) {
+        const uint64_t k0 = sk[i];
+#pragma unroll
+        for (int s = 0; s < kSeedsPerLane; s++) {
+            const uint32_t r0 = remix_low16(k0 + x0 + (uint64_t)(s * 32));
+#pragma unroll
+            for (int t = 0; t < NT; t++) c[s][t] += (r0 < T[t]);
+        }
+    }
+}
+
+// Smallest valid trial index (seed - seed0), or ~0 when `cap` trials were exhausted.
+template <int NT>
+__device__ uint64_t search_seeds(SplitSmem &sm, uint32_t m, uint64_t seed0, const uint32_t T0, const uint32_t T1,
+                                 const uint32_t T2, const uint32_t N0, const uint32_t N1, const uint32_t N2, int G,
+                                 uint64_t cap) {
+    const uint32_t need[3] = {N0, N1, N2};
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wpg = kSplitWarps / G;  // warps per group
+    const int group = warp / wpg, sub = warp % wpg;
+    const uint32_t lo = (uint32_t)((uint64_t)m * sub / wpg), hi = (uint32_t)((uint64_t)m * (sub + 1) / wpg);
+    const uint32_t per_round = (uint32_t)(kSeedsPerWarp * G);
+    for (uint64_t base = 0; base < cap; base += per_round) {
+        const uint32_t slot0 = (uint32_t)group * kSeedsPerWarp + lane;  // seed slot s is slot0 + 32 s
+        uint32_t c[kSeedsPerLane][3] = {};
+        count_range<NT>(sm.keys, lo, hi, seed0 + base + slot0, T0, T1, T2, c);
+        if (wpg > 1) {
+#pragma unroll
+            for (int s = 0; s < kSeedsPerLane; s++)
+#pragma unroll
+                for (int t = 0; t < NT; t++) sm.part_counts[warp][s * 32 + lane][t] = c[s][t];
+            __syncthreads();
+            if (sub == 0) {
+#pragma unroll
+                for (int s = 0; s < kSeedsPerLane; s++)
+#pragma unroll
+                    for (int t = 0; t < NT; t++) {
+                        uint32_t tot = 0;
+                        for (int w = 0; w < wpg; w++) tot += sm.part_counts[warp + w][s * 32 + lane][t];
+                        c[s][t] = tot;
+                    }
+            }
+        }
+        if (sub == 0) {
+#pragma unroll
+            for (int s = 0; s < kSeedsPerLane; s++) {
+                bool ok = true;
+#pragma unroll
+                for (int t = 0; t < NT; t++) ok &= c[s][t] == need[t];
+                if (ok) atomicMin(&sm.best, slot0 + 32u * s);
+            }
+        }
+        __syncthreads();
+        const uint32_t b = sm.best;
+        if (b != 0xffffffffu) return base + b;
+    }
+    return ~0ull;
+}
+
+__global__ void __launch_bounds__(kSplitThreads) k_split(const Node *__restrict__ nodes, const uint32_t *__restrict__ ids,
+                                                         uint64_t *__restrict__ keys, uint64_t *__restrict__ codes,
+                                                         uint64_t max_trials, uint32_t *__restrict__ err,
+                                                         unsigned long long *__restrict__ work) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    SplitSmem &sm = *reinterpret_cast<SplitSmem *>(smem_raw);
+    const uint32_t id = ids[blockIdx.x];
+    const Node nd = nodes[id];
+    const uint32_t m = nd.m;
+    for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) sm.keys[i] = keys[nd.start + i];
+
+    // Part boundaries as thresholds on the low 16 bits of remix (see header).
+    uint32_t T[3] = {65536u, 65536u, 65536u}, need[3] = {m, m, m};
+    int NT;
+    double p;
+    if (nd.kind == kSplit2) {
+        NT = 1;
+        T[0] = (uint32_t)(((uint64_t)nd.unit * 65536u + m - 1) / m);
+        need[0] = nd.unit;
+        const double k0 = nd.unit, k1 = m - nd.unit;
+        p = sqrt((double)m) / (sqrt(2 * M_PI) * sqrt(k0) * sqrt(k1));
+    } else {
+        NT = nd.fanout - 1;
+        double sp = 1;
+        for (int t = 0; t < NT; t++) {
+            const uint64_t K = (uint64_t)(t + 1) * nd.unit;
+            T[t] = (uint32_t)((K * 65536u + m - 1) / m);
+            need[t] = (uint32_t)K;
+            sp *= sqrt((double)nd.unit);
+        }
+        sp *= sqrt((double)(m - (uint32_t)NT * nd.unit));
+        p = sqrt((double)m) / (pow(2 * M_PI, NT / 2.0) * sp);
+    }
+    // Warp groups: aim for a round of ~1/8 of the expected trials.
+    const double expect = 1.0 / p;
+    int G = 1;
+    while (G < kSplitWarps && (double)(kSeedsPerWarp * G * 2) * 8.0 <= expect) G <<= 1;
+    if (threadIdx.x == 0) sm.best = 0xffffffffu;
+    __syncthreads();
+
+    const uint64_t seed0 = start_seed(nd.level);
+    // Trial cap: 2^(g+12) is ~2000 expected searches (g ~ log2(0.48 / p)), so only duplicate keys
+    // or a caller-set max_trials can reach it.
+    uint64_t cap = 1ull << min(nd.g + 12, 40);
+    if (max_trials && max_trials < cap) cap = max_trials;
+    uint64_t trial;
+    switch (NT) {
+        case 1: trial = search_seeds<1>(sm, m, seed0, T[0], T[1], T[2], need[0], need[1], need[2], G, cap); break;
+        case 2: trial = search_seeds<2>(sm, m, seed0, T[0], T[1], T[2], need[0], need[1], need[2], G, cap); break;
+        default: trial = search_seeds<3>(sm, m, seed0, T[0], T[1], T[2], need[0], need[1], need[2], G, cap); break;
+    }
+    if (trial == ~0ull) {
+        if (threadIdx.x == 0) atomicOr(err, kErrTrialLimit);
+        return;
+    }
+    const uint64_t x = seed0 + trial;
+
+    // Stable partition (counting sort by part, original order inside a part). Each thread owns a
+    // contiguous chunk; per-part counts are packed 16 bits per part into one 64-bit word and
+    // exclusive-scanned across the block.
+    const uint32_t chunk = (m + kSplitThreads - 1) / kSplitThreads;
+    const uint32_t lo = min(m, threadIdx.x * chunk), hi = min(m, lo + chunk);
+    uint64_t mine = 0;
+    for (uint32_t i = lo; i < hi; i++) {
+        const uint32_t r = remix_low16(sm.keys[i] + x);
+        const uint32_t part = (r >= T[0]) + (r >= T[1]) + (r >= T[2]);
+        mine += 1ull << (16 * part);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint64_t incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint64_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    __syncthreads();  // sm.scan reuse
+    if (lane == 31) sm.scan[warp] = incl;
+    __syncthreads();
+    uint64_t before = 0;
+    for (int w = 0; w < warp; w++) before += sm.scan[w];
+    uint64_t run = before + incl - mine;  // exclusive prefix, packed
+    const uint32_t unit = nd.unit;
+    for (uint32_t i = lo; i < hi; i++) {
+        const uint64_t k = sm.keys[i];
+        const uint32_t r = remix_low16(k + x);
+        const uint32_t part = (r >= T[0]) + (r >= T[1]) + (r >= T[2]);
+        const uint32_t dest = part * unit + (uint32_t)((run >> (16 * part)) & 0xFFFF);
+        run += 1ull << (16 * part);
+        keys[nd.start + dest] = k;
+    }
+    if (threadIdx.x == 0) {
+        codes[id] = trial;  // x - start_seed[level]
+        atomicAdd(work, (unsigned long long)(trial + 1) * m);
+    }
+}
+
+void launch_split_level(const Node *nodes, const uint32_t *ids, uint32_t count, uint64_t *keys, uint64_t *codes,
+                        uint64_t max_trials, uint32_t *err, unsigned long long *work, cudaStream_t s) {
+    if (!count) return;
+    const size_t smem = sizeof(SplitSmem);
+    cudaFuncSetAttribute(k_split, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_split<<<count, kSplitThreads, smem, s>>>(nodes, ids, keys, codes, max_trials, err, work);
+}
+
+} // namespace shg

@@ -1,0 +1,121 @@
+"""Generates the golden fixtures in this folder by running the reference itself.
+
+The reference (its unmodified headers and src/ShockHash2-precompiled.cpp, compiled with the
+restated third-party stand-ins in oracle/shims) is built as oracle/_ref/libshref.so by
+``make -C oracle ref`` in the container that holds the reference sources. This script seeds the
+inputs, runs the reference constructors and stores inputs and products as .npz files together with
+a SHA-256 manifest. The tests compare the CPU restatement (oracle/port) and the CUDA path against
+these files; they never need the reference sources at run time.
+
+Usage:  python tests/golden/make_golden.py
+"""
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+from oracle.bindings import RefLib  # noqa: E402
+
+# (name, variant, leaf, n, bucket_size, seed)
+BUILDS = [
+    ("sh1_l30_b2000", 1, 30, 20000, 2000, 101),
+    ("sh1_l8_b100", 1, 8, 5000, 100, 102),
+    ("sh1_l40_b2000", 1, 40, 6000, 2000, 103),
+    ("sh1_l5_b7", 1, 5, 1500, 7, 104),
+    ("sh1_l60_b500", 1, 60, 1500, 500, 105),
+    ("sh2_l64_b2000", 2, 64, 20000, 2000, 201),
+    ("sh2_l10_b100", 2, 10, 5000, 100, 202),
+    ("sh2_l9_b50", 2, 9, 3000, 50, 203),
+    ("sh2_l33_b500", 2, 33, 8000, 500, 204),
+    ("sh2_l3_b5", 2, 3, 1000, 5, 205),
+    ("sh2_l100_b1000", 2, 100, 2000, 1000, 206),
+    ("sh2_l64_tiny", 2, 64, 3, 2000, 207),
+    ("sh1_l30_tiny", 1, 30, 2, 2000, 208),
+]
+LEAVES_SH2 = [(m, 40 if m <= 64 else 4) for m in list(range(2, 65)) + [80, 100, 128]]
+LEAVES_SH1 = [(m, 20) for m in range(2, 41)] + [(48, 3), (60, 2)]
+
+
+def sha(path):
+    h = hashlib.sha256()
+    with open(path, "rb") as f:
+        h.update(f.read())
+    return h.hexdigest()
+
+
+def main():
+    R = RefLib()
+    manifest = {}
+    for name, variant, leaf, n, b, seed in BUILDS:
+        rng = np.random.default_rng(seed)
+        first = rng.integers(0, 2**64, size=n, dtype=np.uint64)
+        second = np.unique(rng.integers(0, 2**64, size=n + 8, dtype=np.uint64))[:n]
+        rng.shuffle(second)
+        r = R.build_hash(variant, leaf, first, second, b, 1)
+        q = r.query_hash(first, second)
+        path = os.path.join(HERE, name + ".npz")
+        np.savez_compressed(path, variant=variant, leaf=leaf, bucket_size=b, first=first, second=second,
+                            desc=r.desc, size_acc=r.size_acc, pos_acc=r.pos_acc, ribbon_keys=r.ribbon_keys,
+                            ribbon_bits=r.ribbon_bits, query=q, bits=r.bits)
+        manifest[name + ".npz"] = sha(path)
+        r.free()
+    # single leaves through the reference's leaf seams
+    rng = np.random.default_rng(301)
+    keys, offs, seeds, bits = [], [0], [], []
+    for m, cnt in LEAVES_SH2:
+        for _ in range(cnt):
+            k = np.unique(rng.integers(0, 2**64, size=m + 4, dtype=np.uint64))[:m]
+            rng.shuffle(k)
+            s, rk, rb = R.sh2_leaf(k)
+            assert np.array_equal(rk, k)
+            keys.append(k)
+            offs.append(offs[-1] + m)
+            seeds.append(s)
+            bits.append(rb)
+    path = os.path.join(HERE, "sh2_leaves.npz")
+    np.savez_compressed(path, keys=np.concatenate(keys), offsets=np.array(offs, np.uint64),
+                        seeds=np.array(seeds, np.uint64), bits=np.concatenate(bits))
+    manifest["sh2_leaves.npz"] = sha(path)
+    rng = np.random.default_rng(302)
+    keys, offs, codes, kc, bits, levels = [], [0], [], [], [], []
+    for m, cnt in LEAVES_SH1:
+        for t in range(cnt):
+            k = np.unique(rng.integers(0, 2**64, size=m + 4, dtype=np.uint64))[:m]
+            rng.shuffle(k)
+            level = t % 3
+            c, rk, rb = R.sh1_leaf(60, k, level)
+            keys.append(k)
+            offs.append(offs[-1] + m)
+            codes.append(c)
+            kc.append(rk)
+            bits.append(rb)
+            levels.append(level)
+    path = os.path.join(HERE, "sh1_leaves.npz")
+    np.savez_compressed(path, keys=np.concatenate(keys), offsets=np.array(offs, np.uint64),
+                        codes=np.array(codes, np.uint64), keys_by_cell=np.concatenate(kc),
+                        bits=np.concatenate(bits), levels=np.array(levels, np.int32))
+    manifest["sh1_leaves.npz"] = sha(path)
+    # string hashing (short and long SpookyHash paths) and the README example
+    rng = np.random.default_rng(303)
+    strs = [bytes(rng.integers(0, 256, size=L, dtype=np.uint8)) for L in list(range(0, 260)) + [300, 511, 1000]]
+    f, s = R.spooky128(strs)
+    readme = [b"abc", b"def", b"123", b"456"]
+    rb = R.build_strings(1, 30, readme, 2000, 1)
+    readme_out = R.query_strings(rb, readme)
+    path = os.path.join(HERE, "strings.npz")
+    np.savez_compressed(path, data=np.frombuffer(b"".join(strs), np.uint8),
+                        lengths=np.array([len(x) for x in strs], np.uint64), first=f, second=s,
+                        murmur=R.murmur64(strs), readme_out=readme_out)
+    manifest["strings.npz"] = sha(path)
+    with open(os.path.join(HERE, "MANIFEST.json"), "w") as fh:
+        json.dump(manifest, fh, indent=1, sort_keys=True)
+    print(json.dumps(manifest, indent=1))
+
+
+if __name__ == "__main__":
+    main()

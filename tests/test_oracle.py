@@ -1,0 +1,123 @@
+"""The CPU oracle, pinned: the C++ restatement (oracle/port) and the compiled reference
+(oracle/_ref) against the golden fixtures generated by the reference itself (tests/golden)."""
+import glob
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import rand_u64, unique_u64
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+BUILD_FIXTURES = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "sh*_*.npz"))
+                        if "leaves" not in p)
+
+
+def load(name):
+    return np.load(os.path.join(GOLDEN, name + ".npz"))
+
+
+def test_manifest_hashes():
+    with open(os.path.join(GOLDEN, "MANIFEST.json")) as f:
+        manifest = json.load(f)
+    for name, digest in manifest.items():
+        with open(os.path.join(GOLDEN, name), "rb") as fh:
+            assert hashlib.sha256(fh.read()).hexdigest() == digest, name
+
+
+def test_readme_vector_golden():
+    # README.md:42-46 — ShockHash<30,false>({"abc","def","123","456"}, 2000) maps them to 1 3 2 0.
+    assert list(load("strings")["readme_out"]) == [1, 3, 2, 0]
+
+
+@pytest.mark.parametrize("name", BUILD_FIXTURES)
+def test_port_matches_golden(port, name):
+    g = load(name)
+    r = port.build_hash(int(g["variant"]), int(g["leaf"]), g["first"], g["second"], int(g["bucket_size"]))
+    assert np.array_equal(r.desc, g["desc"])
+    assert np.array_equal(r.size_acc, g["size_acc"])
+    assert np.array_equal(r.pos_acc, g["pos_acc"])
+    assert np.array_equal(r.ribbon_keys, g["ribbon_keys"])
+    assert np.array_equal(r.ribbon_bits, g["ribbon_bits"])
+    assert np.array_equal(r.query_hash(g["first"], g["second"]), g["query"])
+
+
+def test_port_leaves_match_golden(port):
+    g = load("sh2_leaves")
+    offs = g["offsets"]
+    for j in range(len(offs) - 1):
+        k = g["keys"][offs[j]:offs[j + 1]]
+        seed, rk, rb = port.sh2_leaf(k)
+        assert seed == g["seeds"][j]
+        assert np.array_equal(rb, g["bits"][offs[j]:offs[j + 1]])
+    g = load("sh1_leaves")
+    offs = g["offsets"]
+    for j in range(len(offs) - 1):
+        k = g["keys"][offs[j]:offs[j + 1]]
+        code, rk, rb = port.sh1_leaf(k, int(g["levels"][j]))
+        assert code == g["codes"][j]
+        assert np.array_equal(rk, g["keys_by_cell"][offs[j]:offs[j + 1]])
+        assert np.array_equal(rb, g["bits"][offs[j]:offs[j + 1]])
+
+
+def test_port_spooky_matches_golden(port):
+    g = load("strings")
+    data = g["data"].tobytes()
+    offs = np.concatenate([[0], np.cumsum(g["lengths"])]).astype(np.uint64)
+    keys = [data[offs[i]:offs[i + 1]] for i in range(len(offs) - 1)]
+    f, s = port.spooky128(keys)
+    assert np.array_equal(f, g["first"]) and np.array_equal(s, g["second"])
+
+
+def test_ref_matches_golden(ref):
+    for name in ("sh2_l64_b2000", "sh1_l30_b2000", "sh2_l9_b50"):
+        g = load(name)
+        r = ref.build_hash(int(g["variant"]), int(g["leaf"]), g["first"], g["second"], int(g["bucket_size"]), 1)
+        assert np.array_equal(r.desc, g["desc"])
+        assert np.array_equal(r.ribbon_bits, g["ribbon_bits"])
+
+
+def test_ref_readme_vector(ref):
+    keys = [b"abc", b"def", b"123", b"456"]
+    b = ref.build_strings(1, 30, keys, 2000, 1)
+    assert list(ref.query_strings(b, keys)) == [1, 3, 2, 0]
+
+
+@pytest.mark.parametrize("variant,leaf,n,b,threads", [(2, 64, 12000, 2000, 4), (1, 24, 8000, 300, 3)])
+def test_ref_thread_count_invariance(ref, variant, leaf, n, b, threads):
+    rng = np.random.default_rng(leaf)
+    f, s = rand_u64(rng, n), unique_u64(rng, n)
+    r1 = ref.build_hash(variant, leaf, f, s, b, 1)
+    rt = ref.build_hash(variant, leaf, f, s, b, threads)
+    assert np.array_equal(r1.desc, rt.desc) and np.array_equal(r1.pos_acc, rt.pos_acc)
+
+
+@pytest.mark.parametrize("variant,leaf,n,b", [(1, 12, 4000, 150), (2, 16, 4000, 150), (2, 48, 9000, 1200),
+                                              (1, 32, 6000, 900), (2, 5, 500, 9), (1, 2, 300, 4)])
+def test_port_matches_ref_random(port, ref, variant, leaf, n, b):
+    rng = np.random.default_rng(n + leaf)
+    f, s = rand_u64(rng, n), unique_u64(rng, n)
+    r = ref.build_hash(variant, leaf, f, s, b, 2)
+    p = port.build_hash(variant, leaf, f, s, b)
+    assert np.array_equal(p.desc, r.desc)
+    assert np.array_equal(p.size_acc, r.size_acc) and np.array_equal(p.pos_acc, r.pos_acc)
+    assert np.array_equal(p.ribbon_keys, r.ribbon_keys) and np.array_equal(p.ribbon_bits, r.ribbon_bits)
+
+
+def test_memo_tables_port_vs_ref(port, ref):
+    for variant, leaves in ((1, [2, 3, 4, 5, 6, 7, 8, 10, 12, 13, 16, 20, 24, 25, 30, 32, 33, 40, 48, 60]),
+                            (2, [2, 3, 4, 5, 6, 8, 9, 10, 11, 12, 16, 20, 24, 32, 33, 40, 48, 64, 100, 128])):
+        for leaf in leaves:
+            assert np.array_equal(port.memo(variant, leaf), ref.memo(variant, leaf)), (variant, leaf)
+
+
+def test_mphf_property_port(port):
+    rng = np.random.default_rng(9)
+    n = 30000
+    f, s = rand_u64(rng, n), unique_u64(rng, n)
+    for variant, leaf in ((1, 20), (2, 24)):
+        r = port.build_hash(variant, leaf, f, s, 1000)
+        q = r.query_hash(f, s)
+        assert np.array_equal(np.sort(q), np.arange(n, dtype=np.uint64))
