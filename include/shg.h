@@ -145,6 +145,13 @@ uint64_t shg_mphf_size(const shg_mphf *f);
  * out[m] for m < 3000 packs golomb parameter << 27 | subtree nodes << 16 | subtree fixed bits. */
 shg_status shg_memo_table(int variant, int leaf_size, uint64_t *out);
 
+/* Benchmark utilities (no counterpart in the reference interface). n keys drawn from
+ * std::mt19937_64(seed) with duplicates redrawn, as the benchmark configurations specify. */
+void shg_keys_mt19937_64(uint64_t seed, uint64_t n, uint64_t *out);
+/* Integer-pipe peak of the split-search arithmetic (remix + 16-bit part thresholds, operands in
+ * registers) on `device`, in evaluations per second: the roofline denominator of the searches. */
+int shg_int_peak(int device, uint64_t iters, double *evals_per_s, double *ms);
+
 /* Message of the last failure on this thread ("" if none). */
 const char *shg_last_error(void);
 

@@ -89,6 +89,9 @@ def lib():
         "shg_mphf_query_strings": ([_vp, ctypes.c_char_p, _vp, _u64, _vp], ctypes.c_int),
         "shg_mphf_bits": ([_vp], _u64),
         "shg_mphf_size": ([_vp], _u64),
+        "shg_keys_mt19937_64": ([_u64, _u64, _vp], None),
+        "shg_int_peak": ([ctypes.c_int, _u64, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)],
+                         ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -115,6 +118,20 @@ def pack_strings(keys):
     if bs:
         np.cumsum(np.fromiter((len(k) for k in bs), dtype=np.uint64, count=len(bs)), out=offs[1:])
     return data, offs
+
+
+def keys_mt19937_64(seed, n):
+    """n uint64 keys from std::mt19937_64(seed), duplicates redrawn (the benchmark key sets)."""
+    out = np.zeros(n, dtype=np.uint64)
+    lib().shg_keys_mt19937_64(seed, n, _ptr(out))
+    return out
+
+
+def int_peak(device=0, iters=1 << 16):
+    """Measured evaluations/s of the split-search arithmetic with no memory traffic."""
+    e, ms = ctypes.c_double(), ctypes.c_double()
+    _check(lib().shg_int_peak(device, iters, ctypes.byref(e), ctypes.byref(ms)))
+    return e.value, ms.value
 
 
 def memo_table(variant, leaf_size):

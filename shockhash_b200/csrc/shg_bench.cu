@@ -1,0 +1,104 @@
+// Measurement utilities (not part of the reference's interface):
+//  * the seeded key generators the benchmark configurations name (std::mt19937_64), shared by the
+//    CPU and GPU runs so both build from the same keys;
+//  * the integer-pipe peak of the split search: the same remix + 16-bit threshold arithmetic as
+//    the split kernel's inner loop (three part boundaries), on register-resident operands with no
+//    memory traffic. Its evaluations per second are the denominator of the search kernels'
+//    roofline fraction.
+#include <algorithm>
+#include <cstdint>
+#include <random>
+#include <vector>
+#include <cuda_runtime.h>
+#include "shg.h"
+#include "shg_common.cuh"
+
+namespace {
+
+constexpr int kPeakThreads = 256;
+
+__global__ void __launch_bounds__(kPeakThreads) k_int_peak(uint64_t iters, uint32_t T0, uint32_t T1, uint32_t T2,
+                                                           unsigned long long *sink) {
+    const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    uint64_t k0 = shg::remix(tid * 0x9E3779B97F4A7C15ULL), k1 = shg::remix(k0);
+    const uint64_t x0 = 0x643e521ddbd2be98ULL + tid;
+    uint32_t c0 = 0, c1 = 0, c2 = 0, d0 = 0, d1 = 0, d2 = 0;
+    for (uint64_t i = 0; i < iters; i++) {
+        // two seeds per key pair, as the split kernel's kSeedsPerLane = 2
+        const uint32_t r0 = shg::remix_low16(k0 + x0 + i);
+        const uint32_t r1 = shg::remix_low16(k1 + x0 + i);
+        c0 += r0 < T0; c1 += r0 < T1; c2 += r0 < T2;
+        d0 += r1 < T0; d1 += r1 < T1; d2 += r1 < T2;
+    }
+    if ((c0 ^ c1 ^ c2 ^ d0 ^ d1 ^ d2) == 0xFFFFFFFFu) atomicAdd(sink, 1ull);
+}
+
+} // namespace
+
+extern "C" {
+
+// n keys from std::mt19937_64(seed), duplicates removed by drawing replacements (the reference
+// loops forever on duplicate keys), in draw order.
+void shg_keys_mt19937_64(uint64_t seed, uint64_t n, uint64_t *out) {
+    std::mt19937_64 rng(seed);
+    for (uint64_t i = 0; i < n; i++) out[i] = rng();
+    std::vector<uint64_t> sorted(out, out + n);
+    std::sort(sorted.begin(), sorted.end());
+    if (std::adjacent_find(sorted.begin(), sorted.end()) == sorted.end()) return;
+    std::vector<uint64_t> seen;
+    seen.reserve(n);
+    std::vector<uint64_t> tmp(out, out + n);
+    std::sort(tmp.begin(), tmp.end());
+    // replace later occurrences of a duplicate by fresh draws that are not present
+    std::vector<uint64_t> uniq;
+    uniq.reserve(n);
+    std::vector<char> keep(n, 1);
+    {
+        std::vector<std::pair<uint64_t, uint64_t>> vi(n);
+        for (uint64_t i = 0; i < n; i++) vi[i] = {out[i], i};
+        std::sort(vi.begin(), vi.end());
+        for (uint64_t i = 1; i < n; i++)
+            if (vi[i].first == vi[i - 1].first) keep[vi[i].second] = 0;
+    }
+    for (uint64_t i = 0; i < n; i++) {
+        while (!keep[i]) {
+            const uint64_t v = rng();
+            if (!std::binary_search(tmp.begin(), tmp.end(), v)) {
+                out[i] = v;
+                keep[i] = 1;
+                tmp.insert(std::upper_bound(tmp.begin(), tmp.end(), v), v);
+            }
+        }
+    }
+}
+
+// Integer-pipe peak: evaluations per second of the split search arithmetic on `device`.
+int shg_int_peak(int device, uint64_t iters, double *evals_per_s, double *ms_out) {
+    if (cudaSetDevice(device) != cudaSuccess) return SHG_ERR_CUDA;
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, device);
+    const int blocks = prop.multiProcessorCount * 8;
+    unsigned long long *sink;
+    if (cudaMalloc(&sink, 8) != cudaSuccess) return SHG_ERR_OOM;
+    cudaMemset(sink, 0, 8);
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const uint32_t T0 = 16384, T1 = 32768, T2 = 49152;
+    k_int_peak<<<blocks, kPeakThreads>>>(iters / 16 + 1, T0, T1, T2, sink);  // warm-up
+    cudaEventRecord(a);
+    k_int_peak<<<blocks, kPeakThreads>>>(iters, T0, T1, T2, sink);
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(sink);
+    if (cudaGetLastError() != cudaSuccess) return SHG_ERR_CUDA;
+    *evals_per_s = 2.0 * (double)iters * blocks * kPeakThreads / (ms * 1e-3);
+    if (ms_out) *ms_out = ms;
+    return SHG_OK;
+}
+
+} // extern "C"

@@ -234,18 +234,15 @@ SHG_HD void spooky128(const uint8_t *msg, size_t length, uint64_t seed, uint64_t
             for (int i = 0; i < 12; i++) block[i] = ld64(msg + bk * 96 + 8 * i);
             spooky_mix(block, h);
         }
+        // Last partial block: the remaining bytes, zero padding, and the remainder length in the
+        // block's final byte.
         const size_t rem = length - nblocks * 96;
         const uint8_t *tail = msg + nblocks * 96;
-        for (int i = 0; i < 12; i++) {
-            uint64_t v = 0;
-            for (int j = 7; j >= 0; j--) {
-                const size_t pos = (size_t)i * 8 + j;
-                uint8_t byte = pos < rem ? tail[pos] : 0;
-                if (pos == 95) byte = (uint8_t)rem;
-                v = (v << 8) | byte;
-            }
-            h[i] += v;
-        }
+        uint8_t buf[96];
+        for (int i = 0; i < 96; i++) buf[i] = 0;
+        for (size_t i = 0; i < rem; i++) buf[i] = tail[i];
+        buf[95] = (uint8_t)rem;
+        for (int i = 0; i < 12; i++) h[i] += ld64(buf + 8 * i);
         spooky_end_partial(h);
         spooky_end_partial(h);
         spooky_end_partial(h);

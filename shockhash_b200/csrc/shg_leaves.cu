@@ -116,7 +116,8 @@ __global__ void __launch_bounds__(kLeafWarps * 32) k_leaves_sh1(const Node *__re
         __syncwarp();
         const uint64_t seed0 = start_seed(nd.level);
         const uint64_t all = (1ull << m) - 1;
-        uint64_t cap = 1ull << min(nd.g + 14, 44);
+        // ~2^(g+1) trials are expected; 2^(g+10) is only reached by duplicate keys.
+        uint64_t cap = 1ull << min(nd.g + 10, 40);
         if (max_trials && max_trials < cap) cap = max_trials;
         LaneUF uf{sm.uf, lane};
         uint64_t found = ~0ull;
@@ -468,7 +469,11 @@ void launch_leaves_sh2_ctr(const Node *nodes, const uint32_t *ids, uint32_t coun
     if (!count) return;
     cudaMemsetAsync(ctr, 0, sizeof(unsigned int), s);
     const size_t smem = sizeof(Sh2WarpSmem) * kLeafWarps;
-    cudaFuncSetAttribute(k_leaves_sh2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_leaves_sh2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr_set = true;
+    }
     k_leaves_sh2<<<grid, kLeafWarps * 32, smem, s>>>(nodes, ids, count, keys, codes, rib_bits, scratch, scratch_per_warp,
                                                      smax, cmax, err, work, ctr);
 }

@@ -199,7 +199,8 @@ __global__ void __launch_bounds__(kSplitThreads) k_split(const Node *__restrict_
         const uint32_t part = (r >= T[0]) + (r >= T[1]) + (r >= T[2]);
         const uint32_t dest = part * unit + (uint32_t)((run >> (16 * part)) & 0xFFFF);
         run += 1ull << (16 * part);
-        keys[nd.start + dest] = k;
+        if (dest < m) keys[nd.start + dest] = k;
+        else atomicOr(err, kErrInternal);  // unreachable for a valid seed; never write outside the node
     }
     if (threadIdx.x == 0) {
         codes[id] = trial;  // x - start_seed[level]

@@ -74,7 +74,8 @@ def test_string_hashing_matches_golden(engine):
     offs = np.concatenate([[0], np.cumsum(g["lengths"])]).astype(np.uint64)
     keys = [data[offs[i]:offs[i + 1]] for i in range(len(offs) - 1)]
     f, s = engine.hash_strings(keys)
-    assert np.array_equal(f, g["first"]) and np.array_equal(s, g["second"])
+    bad = np.nonzero((f != g["first"]) | (s != g["second"]))[0]
+    assert len(bad) == 0, f"lengths that differ: {g['lengths'][bad].tolist()}"
 
 
 def test_readme_vector():
@@ -128,15 +129,23 @@ def test_large_build_is_a_minimal_perfect_hash(engine):
     assert np.array_equal(np.sort(q), np.arange(n, dtype=np.uint64))
 
 
-def test_duplicate_keys_report_trial_limit(engine):
-    # Duplicate keys make the original leaf search loop forever in the reference; here the trial
-    # cap turns that into SHG_ERR_TRIAL_LIMIT.
-    rng = np.random.default_rng(3)
-    f, s = rand_u64(rng, 500), unique_u64(rng, 500)
-    s[10], f[10] = s[11], f[11]
-    with pytest.raises(shg.ShgError) as ei:
-        engine.build_hash128(1, 8, f, s, 100, max_trials=1 << 16)
-    assert ei.value.status == 3
-    # the engine stays usable after the error
+def test_trial_cap_reports_error_and_engine_recovers(engine):
+    # A trial cap below the answer turns a search into SHG_ERR_TRIAL_LIMIT (the reference has no cap
+    # and would keep searching); the engine must stay usable afterwards.
     g = load("sh2_l10_b100")
+    with pytest.raises(shg.ShgError) as ei:
+        engine.build_hash128(1, 8, g["first"], g["second"], 100, max_trials=1)
+    assert ei.value.status == 3
     assert_same(engine.build_hash128(2, 10, g["first"], g["second"], 100), g)
+
+
+def test_duplicate_keys_match_oracle(engine, port):
+    # Equal keys form a double edge (a 2-cycle), which a pseudoforest admits; the reference then
+    # builds a structure that maps both copies to one value. The device must build the same one.
+    rng = np.random.default_rng(3)
+    f, s = rand_u64(rng, 3000), unique_u64(rng, 3000)
+    s[10], f[10] = s[11], f[11]
+    for variant, leaf in ((1, 8), (2, 12)):
+        p = port.build_hash(variant, leaf, f, s, 100)
+        r = engine.build_hash128(variant, leaf, f, s, 100)
+        assert np.array_equal(r.descriptors, p.desc) and np.array_equal(r.ribbon_bits, p.ribbon_bits)
