@@ -149,7 +149,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_KEYS)
     ap.add_argument("--mode", type=int, default=0)
-    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-forms", action="store_true", help="skip the per-leaf-launch comparison form")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -234,8 +235,8 @@ def main():
             cpu = {"value": round(dt * 1e9 / sample, 3), "unit": "ns/key", "cores": cores, "kind": kind,
                    "sample": f"first {sample} keys of the same stream, constructor only, all host threads"}
         forms = {"persistent_or_levels_ns_per_key": round(ms * 1e6 / n, 3)}
-        if ws == 1:
-            pl_n = int(os.environ.get("SHG_PER_LEAF_SAMPLE", "200000"))
+        if ws == 1 and not args.no_forms:
+            pl_n = int(os.environ.get("SHG_PER_LEAF_SAMPLE", "100000"))
             rp = eng.build_u64_device(VARIANT, LEAF, d_keys.data_ptr(), pl_n, BUCKET, shg.MODE_PER_LEAF)
             rl = eng.build_u64_device(VARIANT, LEAF, d_keys.data_ptr(), pl_n, BUCKET, shg.MODE_LEVELS)
             forms["per_leaf_launch_ns_per_key_at_%d" % pl_n] = round(rp.stage_ms["total"] * 1e6 / pl_n, 3)

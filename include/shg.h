@@ -12,7 +12,8 @@
  * Errors: every entry point returns an shg_status; no C++ exception crosses this boundary. The
  * message of the last failure on the calling thread is available from shg_last_error().
  * Threading: an engine owns one CUDA stream and its device buffers and is not thread-safe; use one
- * engine per host thread. Results are owned by the library until shg_result_free().
+ * engine per host thread. Result arrays live in pinned host memory owned by the engine that built
+ * them; they stay valid until shg_result_free() or shg_engine_destroy(), whichever comes first.
  */
 #ifndef SHG_H
 #define SHG_H
@@ -52,7 +53,9 @@ typedef struct shg_params {
     int leaf_size;            /* ShockHash: 2..60; ShockHash2: 2..128 */
     uint64_t bucket_size;     /* expected keys per bucket (the reference's bucket_size argument) */
     int mode;                 /* shg_mode */
-    uint64_t max_trials;      /* cap on the seeds tried per split node / leaf; 0 = library default (2^40) */
+    uint64_t max_trials;      /* seeds tried at most per split node / original leaf; 0 = library default,
+                                 2^(g+12) per split and 2^(g+10) per leaf (g = the node's Rice parameter),
+                                 about a thousand times the expected count */
 } shg_params;
 
 typedef struct shg_result {
@@ -69,6 +72,7 @@ typedef struct shg_result {
     double stage_ms[8];          /* device time per stage: hash, partition, tree, splits, leaves, encode, copy-out, total */
     uint64_t work[8];            /* split evaluations, leaf evaluations, candidate pairs, filtered pairs,
                                     pseudoforest edge operations, leaves, split nodes, kernel launches */
+    void *owner;                 /* library-internal: the pinned host block the arrays live in */
 } shg_result;
 
 typedef struct shg_engine shg_engine;

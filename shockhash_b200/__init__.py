@@ -51,7 +51,7 @@ class _Result(ctypes.Structure):
                 ("descriptors", ctypes.POINTER(ctypes.c_uint64)), ("desc_words", ctypes.c_uint64),
                 ("desc_bits", ctypes.c_uint64), ("ribbon_keys", ctypes.POINTER(ctypes.c_uint64)),
                 ("ribbon_bits", ctypes.POINTER(ctypes.c_uint8)), ("ribbon_n", ctypes.c_uint64),
-                ("stage_ms", ctypes.c_double * 8), ("work", ctypes.c_uint64 * 8)]
+                ("stage_ms", ctypes.c_double * 8), ("work", ctypes.c_uint64 * 8), ("owner", ctypes.c_void_p)]
 
 
 _lib = None
@@ -145,21 +145,35 @@ def sh2_query(leaf_size, seed, key, retrieved):
 
 
 class BuildResult:
-    """Products of one device build, copied into numpy arrays."""
+    """Products of one device build. The arrays are numpy views of the engine's pinned host block
+    (no copy); they stay valid until ``free()`` (also called on garbage collection) or until the
+    engine is destroyed."""
 
-    def __init__(self, params, res):
-        self.params = params
+    def __init__(self, params, res, engine):
+        self.params, self._res, self._engine = params, res, engine
         n, nb = res.n, res.nbuckets
         self.n, self.nbuckets = n, nb
-        self.bucket_size_acc = np.ctypeslib.as_array(res.bucket_size_acc, (nb + 1,)).copy()
-        self.bucket_pos_acc = np.ctypeslib.as_array(res.bucket_pos_acc, (nb + 1,)).copy()
-        self.descriptors = np.ctypeslib.as_array(res.descriptors, (res.desc_words,)).copy()
+        view = np.ctypeslib.as_array
+        self.bucket_size_acc = view(res.bucket_size_acc, (nb + 1,))
+        self.bucket_pos_acc = view(res.bucket_pos_acc, (nb + 1,))
+        self.descriptors = view(res.descriptors, (res.desc_words,))
         self.desc_bits = res.desc_bits
         rn = res.ribbon_n
-        self.ribbon_keys = np.ctypeslib.as_array(res.ribbon_keys, (max(rn, 1),))[:rn].copy()
-        self.ribbon_bits = np.ctypeslib.as_array(res.ribbon_bits, (max(rn, 1),))[:rn].copy()
+        self.ribbon_keys = view(res.ribbon_keys, (max(rn, 1),))[:rn]
+        self.ribbon_bits = view(res.ribbon_bits, (max(rn, 1),))[:rn]
         self.stage_ms = dict(zip(STAGES, list(res.stage_ms)))
         self.work = dict(zip(WORK, [int(x) for x in res.work]))
+
+    def free(self):
+        if self._res is not None:
+            lib().shg_result_free(ctypes.byref(self._res))
+            self._res = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
 
 
 class Engine:
@@ -188,12 +202,9 @@ class Engine:
     def _finish(self, p, st, res, keep_raw=False):
         if st != 0:
             _check(st)
-        try:
-            out = BuildResult(p, res)
-            if keep_raw:
-                out._mphf = _Mphf(p, res)
-        finally:
-            lib().shg_result_free(ctypes.byref(res))
+        out = BuildResult(p, res, self)
+        if keep_raw:
+            out._mphf = _Mphf(p, res)
         return out
 
     def build_hash128(self, variant, leaf_size, first, second, bucket_size=2000, mode=MODE_PERSISTENT, max_trials=0,

@@ -28,7 +28,10 @@ void launch_leaves_sh1_ctr(const Node *nodes, const uint32_t *ids, uint32_t coun
                            unsigned long long *work, unsigned int *ctr, int grid, cudaStream_t s);
 void launch_leaves_sh2_ctr(const Node *nodes, const uint32_t *ids, uint32_t count, const uint64_t *keys, uint64_t *codes,
                            uint8_t *rib_bits, uint8_t *scratch, uint64_t scratch_per_warp, uint32_t smax, uint32_t cmax,
-                           uint32_t *err, unsigned long long *work, unsigned int *ctr, int grid, cudaStream_t s);
+                           uint32_t *err, unsigned long long *work, unsigned int *ctr, int grid, cudaStream_t s,
+                           int max_leaf);
+int sh2_smem_per_warp(int max_leaf);
+int leaves_sh1_warps_per_block();
 } // namespace shg
 
 using namespace shg;
@@ -71,18 +74,32 @@ struct DevBuf {
 
 } // namespace
 
+// Pinned host block that a result's arrays live in; reused across builds once released.
+struct PinnedBlock {
+    void *p = nullptr;
+    size_t cap = 0;
+    bool in_use = false;
+    shg_engine *eng = nullptr;
+};
+
 struct shg_engine {
+    std::mutex pool_mu;
+    std::vector<PinnedBlock *> pool;
     int device = 0;
     int sms = 148;
     cudaStream_t stream = nullptr;
     DevBuf in_keys, in_bytes, in_offsets, first, second, sfirst, sidx, counts, cursor, acc, keys, nodes, ids, codes,
-        fixed_off, bnb, bucket_bits, pos_acc, words, rib_keys, rib_bits, skip_bits, scratch, misc;
+        fixed_off, bnb, bucket_bits, pos_acc, words, rib_keys, rib_bits, skip_bits, scratch, misc, singles, ckeys, cbits;
     cudaEvent_t ev[8] = {};
     ~shg_engine() {
         DevBuf *all[] = {&in_keys, &in_bytes, &in_offsets, &first, &second, &sfirst, &sidx, &counts, &cursor,
                          &acc, &keys, &nodes, &ids, &codes, &fixed_off, &bnb, &bucket_bits, &pos_acc, &words,
-                         &rib_keys, &rib_bits, &skip_bits, &scratch, &misc};
+                         &rib_keys, &rib_bits, &skip_bits, &scratch, &misc, &singles, &ckeys, &cbits};
         for (DevBuf *b : all) b->release();
+        for (PinnedBlock *b : pool) {
+            if (b->p) cudaFreeHost(b->p);
+            delete b;
+        }
         for (auto &e : ev)
             if (e) cudaEventDestroy(e);
         if (stream) cudaStreamDestroy(stream);
@@ -90,6 +107,25 @@ struct shg_engine {
 };
 
 namespace {
+
+PinnedBlock *acquire_pinned(shg_engine *e, size_t bytes) {
+    std::lock_guard<std::mutex> lock(e->pool_mu);
+    PinnedBlock *best = nullptr;
+    for (PinnedBlock *b : e->pool)
+        if (!b->in_use && b->cap >= bytes && (!best || b->cap < best->cap)) best = b;
+    if (!best) {
+        best = new PinnedBlock();
+        best->eng = e;
+        best->cap = bytes + bytes / 8 + 4096;
+        if (cudaMallocHost(&best->p, best->cap) != cudaSuccess) {
+            delete best;
+            return nullptr;
+        }
+        e->pool.push_back(best);
+    }
+    best->in_use = true;
+    return best;
+}
 
 struct Misc {  // small device-side counters, one allocation
     uint32_t err;
@@ -213,28 +249,32 @@ shg_status build_core(shg_engine *e, const shg_params *p, const uint64_t *d_firs
 
     // ---- leaves
     const uint32_t nleaves = (uint32_t)plan.leaves.size();
-    const int wpb = leaves_sh2_warps_per_block();
-    const int grid = std::max(1, std::min<int>(e->sms * 8, (int)((nleaves + wpb - 1) / wpb)));
     if (p->variant == SHG_SHOCKHASH2) {
-        const uint32_t smax = p->leaf_size > 64 ? 16384 : 4096;
-        const uint32_t cmax = p->leaf_size > 64 ? 8192 : 1024;
+        const int maxm = p->leaf_size;
+        const uint32_t smax = maxm > 64 ? 16384 : 4096;
+        const uint32_t cmax = maxm > 64 ? 16384 : 2048;
         const uint64_t per_warp = (sh2_scratch_bytes(smax, cmax) + 255) & ~255ull;
-        const int grid2 = p->mode == SHG_MODE_PER_LEAF ? 1 : grid;
-        CU(e->scratch.ensure(per_warp * (uint64_t)grid2 * wpb));
+        const int per_block_smem = 4 * sh2_smem_per_warp(maxm);
+        const int blocks_per_sm = std::max(1, std::min(8, (228 * 1024) / (per_block_smem + 1024)));
+        const int grid = p->mode == SHG_MODE_PER_LEAF ? 1
+                         : std::max(1, std::min<int>(e->sms * blocks_per_sm, (int)((nleaves + 3) / 4)));
+        CU(e->scratch.ensure(per_warp * (uint64_t)grid * 4));
         if (p->mode == SHG_MODE_PER_LEAF) {
             for (uint32_t l = 0; l < nleaves; l++) {
                 launch_leaves_sh2_ctr(e->nodes.as<Node>(), d_ids + leaf_off + l, 1, e->keys.as<uint64_t>(),
                                       e->codes.as<uint64_t>(), e->rib_bits.as<uint8_t>(), e->scratch.as<uint8_t>(), per_warp,
-                                      smax, cmax, &misc->err, misc->work, &misc->leaf_ctr, 1, s);
+                                      smax, cmax, &misc->err, misc->work, &misc->leaf_ctr, 1, s, maxm);
                 launches++;
             }
         } else if (nleaves) {
             launch_leaves_sh2_ctr(e->nodes.as<Node>(), d_ids + leaf_off, nleaves, e->keys.as<uint64_t>(),
                                   e->codes.as<uint64_t>(), e->rib_bits.as<uint8_t>(), e->scratch.as<uint8_t>(), per_warp, smax,
-                                  cmax, &misc->err, misc->work, &misc->leaf_ctr, grid2, s);
+                                  cmax, &misc->err, misc->work, &misc->leaf_ctr, grid, s, maxm);
             launches++;
         }
     } else {
+        const int wpb = leaves_sh1_warps_per_block();
+        const int grid = std::max(1, std::min<int>(e->sms * 8, (int)((nleaves + wpb - 1) / wpb)));
         if (p->mode == SHG_MODE_PER_LEAF) {
             for (uint32_t l = 0; l < nleaves; l++) {
                 launch_leaves_sh1_ctr(e->nodes.as<Node>(), d_ids + leaf_off + l, 1, e->keys.as<uint64_t>(),
@@ -276,22 +316,34 @@ shg_status build_core(shg_engine *e, const shg_params *p, const uint64_t *d_firs
     CU(cudaGetLastError());
     CU(cudaEventRecord(e->ev[5], s));
 
-    // ---- copy-out
-    out->bucket_size_acc = (uint64_t *)malloc((nb + 1) * 8);
-    out->bucket_pos_acc = (uint64_t *)malloc((nb + 1) * 8);
-    out->descriptors = (uint64_t *)malloc(words * 8);
-    std::vector<uint64_t> rk(n);
-    std::vector<uint8_t> rb(n);
-    if (!out->bucket_size_acc || !out->bucket_pos_acc || !out->descriptors) {
-        shg_result_free(out);
-        return fail(SHG_ERR_OOM, "host allocation failed");
-    }
-    memcpy(out->bucket_size_acc, acc.data(), (nb + 1) * 8);
-    CU(cudaMemcpyAsync(out->bucket_pos_acc, e->pos_acc.p, (nb + 1) * 8, cudaMemcpyDeviceToHost, s));
+    // ---- copy-out: compact the retrieval input on the device (drop keys of size-1 children), then
+    // copy every product into one pinned host block owned by the engine.
+    const uint64_t nsingles = plan.singles.size();
+    const uint64_t rn = n - nsingles;
+    CU(e->singles.ensure(std::max<uint64_t>(nsingles, 1) * 8));
+    CU(e->ckeys.ensure(std::max<uint64_t>(rn, 1) * 8));
+    CU(e->cbits.ensure(std::max<uint64_t>(rn, 1)));
+    if (nsingles) CU(cudaMemcpyAsync(e->singles.p, plan.singles.data(), nsingles * 8, cudaMemcpyHostToDevice, s));
+    launch_compact_ribbon(p->variant == SHG_SHOCKHASH ? e->rib_keys.as<uint64_t>() : e->keys.as<uint64_t>(),
+                          e->rib_bits.as<uint8_t>(), n, e->singles.as<uint64_t>(), nsingles, e->ckeys.as<uint64_t>(),
+                          e->cbits.as<uint8_t>(), s);
+    const size_t acc_bytes = (nb + 1) * 8;
+    const size_t block_bytes = 2 * acc_bytes + words * 8 + rn * 8 + rn + 64;
+    PinnedBlock *blk = acquire_pinned(e, block_bytes);
+    if (!blk) return fail(SHG_ERR_OOM, "pinned host allocation failed");
+    uint8_t *hp = (uint8_t *)blk->p;
+    out->owner = blk;
+    out->bucket_size_acc = (uint64_t *)hp;
+    out->bucket_pos_acc = (uint64_t *)(hp + acc_bytes);
+    out->descriptors = (uint64_t *)(hp + 2 * acc_bytes);
+    out->ribbon_keys = (uint64_t *)(hp + 2 * acc_bytes + words * 8);
+    out->ribbon_bits = hp + 2 * acc_bytes + words * 8 + rn * 8;
+    memcpy(out->bucket_size_acc, acc.data(), acc_bytes);
+    CU(cudaMemcpyAsync(out->bucket_pos_acc, e->pos_acc.p, acc_bytes, cudaMemcpyDeviceToHost, s));
     CU(cudaMemcpyAsync(out->descriptors, e->words.p, words * 8, cudaMemcpyDeviceToHost, s));
-    if (n) {
-        CU(cudaMemcpyAsync(rk.data(), p->variant == SHG_SHOCKHASH ? e->rib_keys.p : e->keys.p, n * 8, cudaMemcpyDeviceToHost, s));
-        CU(cudaMemcpyAsync(rb.data(), e->rib_bits.p, n, cudaMemcpyDeviceToHost, s));
+    if (rn) {
+        CU(cudaMemcpyAsync(out->ribbon_keys, e->ckeys.p, rn * 8, cudaMemcpyDeviceToHost, s));
+        CU(cudaMemcpyAsync(out->ribbon_bits, e->cbits.p, rn, cudaMemcpyDeviceToHost, s));
     }
     unsigned long long work[8];
     CU(cudaMemcpyAsync(work, misc->work, sizeof(work), cudaMemcpyDeviceToHost, s));
@@ -299,27 +351,7 @@ shg_status build_core(shg_engine *e, const shg_params *p, const uint64_t *d_firs
     CU(cudaStreamSynchronize(s));
     out->desc_words = words;
     out->desc_bits = bits;
-    // Retrieval input: every position except keys of size-1 children and size-1 buckets.
-    const uint64_t rn = n - plan.singles.size();
     out->ribbon_n = rn;
-    out->ribbon_keys = (uint64_t *)malloc(std::max<uint64_t>(rn, 1) * 8);
-    out->ribbon_bits = (uint8_t *)malloc(std::max<uint64_t>(rn, 1));
-    if (!out->ribbon_keys || !out->ribbon_bits) {
-        shg_result_free(out);
-        return fail(SHG_ERR_OOM, "host allocation failed");
-    }
-    {
-        uint64_t j = 0, si = 0;
-        for (uint64_t i = 0; i < n; i++) {
-            if (si < plan.singles.size() && plan.singles[si] == i) {
-                si++;
-                continue;
-            }
-            out->ribbon_keys[j] = rk[i];
-            out->ribbon_bits[j] = rb[i];
-            j++;
-        }
-    }
     float ms[6] = {};
     cudaEventElapsedTime(&ms[0], e->ev[0], e->ev[1]);
     cudaEventElapsedTime(&ms[1], e->ev[1], e->ev[2]);
@@ -491,11 +523,12 @@ shg_status shg_hash_strings(shg_engine *e, const char *bytes, const uint64_t *of
 
 void shg_result_free(shg_result *r) {
     if (!r) return;
-    free(r->bucket_size_acc);
-    free(r->bucket_pos_acc);
-    free(r->descriptors);
-    free(r->ribbon_keys);
-    free(r->ribbon_bits);
+    if (r->owner) {
+        PinnedBlock *b = (PinnedBlock *)r->owner;
+        std::lock_guard<std::mutex> lock(b->eng->pool_mu);
+        b->in_use = false;
+    }
+    r->owner = nullptr;
     r->bucket_size_acc = r->bucket_pos_acc = r->descriptors = r->ribbon_keys = nullptr;
     r->ribbon_bits = nullptr;
 }
@@ -545,14 +578,15 @@ shg_status shg_sh2_construct_leaves(shg_engine *e, const uint64_t *keys, const u
     CU(cudaMemcpyAsync(e->ids.p, ids.data(), nleaves * 4, cudaMemcpyHostToDevice, s));
     uint64_t maxm = 0;
     for (auto &nd : nodes) maxm = std::max<uint64_t>(maxm, nd.m);
-    const uint32_t smax = maxm > 64 ? 16384 : 4096, cmax = maxm > 64 ? 8192 : 1024;
+    const uint32_t smax = maxm > 64 ? 16384 : 4096, cmax = maxm > 64 ? 16384 : 2048;
     const uint64_t per_warp = (sh2_scratch_bytes(smax, cmax) + 255) & ~255ull;
-    const int wpb = leaves_sh2_warps_per_block();
-    const int grid = std::max(1, std::min<int>(e->sms * 8, (int)((nleaves + wpb - 1) / wpb)));
-    CU(e->scratch.ensure(per_warp * (uint64_t)grid * wpb));
+    const int per_block_smem = 4 * sh2_smem_per_warp((int)maxm);
+    const int blocks_per_sm = std::max(1, std::min(8, (228 * 1024) / (per_block_smem + 1024)));
+    const int grid = std::max(1, std::min<int>(e->sms * blocks_per_sm, (int)((nleaves + 3) / 4)));
+    CU(e->scratch.ensure(per_warp * (uint64_t)grid * 4));
     launch_leaves_sh2_ctr(e->nodes.as<Node>(), e->ids.as<uint32_t>(), (uint32_t)nleaves, e->keys.as<uint64_t>(),
                           e->codes.as<uint64_t>(), e->rib_bits.as<uint8_t>(), e->scratch.as<uint8_t>(), per_warp, smax, cmax,
-                          &misc->err, misc->work, &misc->leaf_ctr, grid, s);
+                          &misc->err, misc->work, &misc->leaf_ctr, grid, s, (int)maxm);
     CU(cudaGetLastError());
     uint32_t err = 0;
     CU(cudaMemcpyAsync(seeds, e->codes.p, nleaves * 8, cudaMemcpyDeviceToHost, s));

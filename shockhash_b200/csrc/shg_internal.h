@@ -84,7 +84,6 @@ void launch_bucket_sort(const uint64_t *acc, uint64_t nb, const uint64_t *sfirst
 void launch_split_level(const Node *nodes, const uint32_t *ids, uint32_t count, uint64_t *keys,
                         uint64_t *codes, uint64_t max_trials, uint32_t *err, unsigned long long *work,
                         cudaStream_t s);
-int leaves_sh2_warps_per_block();
 int leaves_sh1_warps_per_block();
 void launch_gr_bucket_bits(const Node *nodes, const uint32_t *bnb, uint64_t nb, const uint64_t *acc,
                            const uint64_t *codes, const uint32_t *memo_skip_bits, uint64_t *bucket_bits,
@@ -94,5 +93,7 @@ void launch_gr_write(const Node *nodes, const uint16_t *fixed_off, const uint32_
                      const uint64_t *acc, const uint64_t *pos_acc, const uint64_t *codes,
                      const uint32_t *memo_skip_bits, unsigned long long *words, cudaStream_t s);
 void launch_set_bit(unsigned long long *words, uint64_t bit, cudaStream_t s);
+void launch_compact_ribbon(const uint64_t *keys, const uint8_t *bits, uint64_t n, const uint64_t *singles,
+                           uint64_t nsingles, uint64_t *out_keys, uint8_t *out_bits, cudaStream_t s);
 
 } // namespace shg

@@ -158,6 +158,28 @@ __global__ void __launch_bounds__(kSortThreads) k_bucket_sort(const uint64_t *__
     }
 }
 
+// Retrieval input without the keys of size-1 children (they get no retrieval bit,
+// ShockHash.h:480,514,547): out[i - #singles before i] = in[i] for every non-single position i.
+__global__ void k_compact_ribbon(const uint64_t *__restrict__ keys, const uint8_t *__restrict__ bits, uint64_t n,
+                                 const uint64_t *__restrict__ singles, uint64_t nsingles, uint64_t *__restrict__ out_keys,
+                                 uint8_t *__restrict__ out_bits) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t lo = 0, hi = nsingles;  // count of singles < i
+        while (lo < hi) {
+            const uint64_t mid = (lo + hi) >> 1;
+            if (singles[mid] < i) lo = mid + 1; else hi = mid;
+        }
+        if (lo < nsingles && singles[lo] == i) continue;
+        out_keys[i - lo] = keys[i];
+        out_bits[i - lo] = bits[i];
+    }
+}
+
+void launch_compact_ribbon(const uint64_t *keys, const uint8_t *bits, uint64_t n, const uint64_t *singles,
+                           uint64_t nsingles, uint64_t *out_keys, uint8_t *out_bits, cudaStream_t s) {
+    if (n) k_compact_ribbon<<<grid_for(n, 256), 256, 0, s>>>(keys, bits, n, singles, nsingles, out_keys, out_bits);
+}
+
 void launch_bucket_count(const uint64_t *first, uint64_t n, uint64_t nb, uint32_t *counts, cudaStream_t s) {
     cudaMemsetAsync(counts, 0, nb * sizeof(uint32_t), s);
     if (n) k_bucket_count<<<grid_for(n, 256), 256, 0, s>>>(first, n, nb, counts);

@@ -1,0 +1,454 @@
+// Bipartite ShockHash leaf search (ShockHash2-internal.h:34-107, 386-572; ShockHash2-precompiled.cpp:24-47),
+// one warp per leaf, leaves pulled from a device counter.
+//
+// The reference finds the first pair, in lexicographic order of (new candidate j, earlier
+// candidate i), that passes the isolated-key filter and the pseudoforest test, where candidates
+// arrive in ascending candidate-seed order. This kernel computes the same pair with the work laid
+// out for a warp:
+//   1. raw seeds are hashed 32 at a time (one seed per lane): coverage masks of set A / set B;
+//   2. the candidates whose larger raw seed lies in that block of 32 are listed in the reference's
+//      order (lane L owns raw seed s0+L; its candidates (a<s, s) by a, then (s, b<=s) by b; lanes in
+//      order) with a count pass, a warp prefix sum and a write pass;
+//   3. every new candidate's isolated-key mask is computed (one candidate per lane);
+//   4. all pairs (j, i) of the new batch are filtered lane-parallel in lexicographic order; the
+//      survivors go through a queue, 32 pseudoforest tests at a time (one per lane, union-find with
+//      a cycle flag per root; the cells are recomputed, nothing per key is stored); the first
+//      passing survivor in queue order is the answer (all pairs of earlier batches failed).
+// Candidate and raw-seed state live in shared memory; indices past its capacity spill to a
+// per-warp slice of global scratch.
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "shg_common.cuh"
+#include "shg_internal.h"
+
+namespace shg {
+
+namespace {
+
+template <int MAXM> struct Sh2Cfg;
+template <> struct Sh2Cfg<64> {
+    static constexpr int SMS = 256;  // raw seeds whose masks stay in shared memory
+    static constexpr int CMS = 256;  // candidates held in shared memory
+    static constexpr int ISO_WORDS = 1;
+};
+template <> struct Sh2Cfg<128> {
+    static constexpr int SMS = 512;
+    static constexpr int CMS = 384;
+    static constexpr int ISO_WORDS = 2;
+};
+
+template <int MAXM> struct Sh2Smem {
+    using C = Sh2Cfg<MAXM>;
+    uint64_t keys[MAXM];  // finder order (QuadSplit: even keys in order, odd keys from the back)
+    uint64_t orig[MAXM];  // leaf order
+    uint64_t maskA[C::SMS], maskB[C::SMS];
+    uint32_t csa[C::CMS], csb[C::CMS];           // raw seeds (seedA, seedB) of each candidate
+    uint64_t iso[C::CMS][C::ISO_WORDS];          // isolated-key masks
+    uint8_t uf[MAXM * 32];                       // per-lane union-find parents / per-lane hash rows
+    uint32_t surv[64];                           // survivor queue: j << 16 | i
+    uint32_t nsurv;
+    uint8_t c1[MAXM], c2[MAXM];                  // retrieval cuckoo insertion
+    int16_t cell[MAXM];
+    uint8_t xr[MAXM];
+};
+
+struct Sh2Global {
+    uint64_t *maskA, *maskB;  // [smax]
+    uint32_t *csa, *csb;      // [cmax]
+    uint64_t *iso;            // [cmax][2]
+};
+
+// Per-lane union-find over at most MAXM vertices: parents in shared memory (byte per vertex,
+// [vertex][lane]), cycle flags of roots in registers.
+template <int MAXM> struct LaneUF2 {
+    uint8_t *par;
+    int lane;
+    uint64_t cyc0, cyc1;
+    __device__ __forceinline__ void init(uint32_t n) {
+        for (uint32_t v = 0; v < n; v++) par[v * 32 + lane] = (uint8_t)v;
+        cyc0 = cyc1 = 0;
+    }
+    __device__ __forceinline__ uint32_t find(uint32_t x) {
+        for (;;) {
+            const uint32_t p = par[x * 32 + lane];
+            if (p == x) return x;
+            const uint32_t gp = par[p * 32 + lane];
+            par[x * 32 + lane] = (uint8_t)gp;
+            x = gp;
+        }
+    }
+    __device__ __forceinline__ bool cyc(uint32_t r) const {
+        if (MAXM <= 64) return (cyc0 >> r) & 1;
+        return ((r < 64 ? cyc0 : cyc1) >> (r & 63)) & 1;
+    }
+    __device__ __forceinline__ void set_cyc(uint32_t r) {
+        if (MAXM <= 64 || r < 64) cyc0 |= 1ull << (r & 63);
+        else cyc1 |= 1ull << (r & 63);
+    }
+    // Adds edge (u, v); false when a component would get a second cycle.
+    __device__ __forceinline__ bool add(uint32_t u, uint32_t v) {
+        const uint32_t ru = find(u), rv = find(v);
+        if (ru == rv) {
+            if (cyc(ru)) return false;
+            set_cyc(ru);
+            return true;
+        }
+        const bool cu = cyc(ru), cv = cyc(rv);
+        if (cu && cv) return false;
+        par[ru * 32 + lane] = (uint8_t)rv;
+        if (cu) set_cyc(rv);
+        return true;
+    }
+};
+
+__device__ bool cuckoo_insert2(int16_t *cell, uint8_t *xr, int e, uint32_t c1, uint32_t c2, int limit) {
+    xr[e] = (uint8_t)(c1 ^ c2);
+    if (cell[c1] < 0) { cell[c1] = (int16_t)e; return true; }
+    if (cell[c2] < 0) { cell[c2] = (int16_t)e; return true; }
+    uint32_t cur = c1;
+    const uint32_t orig_cell = cur;
+    int entry = e;
+    for (int step = 0; step < limit; step++) {
+        const uint32_t alt = xr[entry] ^ cur;
+        const int displaced = cell[alt];
+        cell[alt] = (int16_t)entry;
+        entry = displaced;
+        if (entry < 0) return true;
+        cur = alt;
+        if (cur == orig_cell && entry == e) return false;
+    }
+    return false;
+}
+
+template <int MAXM> struct LeafCtx {
+    Sh2Smem<MAXM> &sm;
+    Sh2Global g;
+    uint32_t m, half, sizeA, smax, cmax;
+    uint64_t full;
+    bool quad;
+    __device__ __forceinline__ uint64_t &maskA(uint64_t s) { return s < Sh2Cfg<MAXM>::SMS ? sm.maskA[s] : g.maskA[s]; }
+    __device__ __forceinline__ uint64_t &maskB(uint64_t s) { return s < Sh2Cfg<MAXM>::SMS ? sm.maskB[s] : g.maskB[s]; }
+    __device__ __forceinline__ uint32_t &csa(uint32_t j) { return j < Sh2Cfg<MAXM>::CMS ? sm.csa[j] : g.csa[j]; }
+    __device__ __forceinline__ uint32_t &csb(uint32_t j) { return j < Sh2Cfg<MAXM>::CMS ? sm.csb[j] : g.csb[j]; }
+    __device__ __forceinline__ uint64_t &iso(uint32_t j, int w) {
+        return j < Sh2Cfg<MAXM>::CMS ? sm.iso[j][w] : g.iso[2 * (uint64_t)j + w];
+    }
+    __device__ __forceinline__ uint64_t cseed(uint32_t j) {
+        const uint32_t a = csa(j), b = csb(j);
+        return quad ? pair_elegant(a, b) : a;
+    }
+    // candidate pair test on the edges (h_j + m/2, h_i), recomputing the cells
+    __device__ __forceinline__ bool pair_ok(LaneUF2<MAXM> &uf, uint32_t j, uint32_t i, unsigned long long &edges) {
+        const uint64_t ja = csa(j), jb = csb(j), ia = csa(i), ib = csb(i);
+        uf.init(m);
+        const uint32_t off = m / 2;
+        for (uint32_t k = 0; k < m; k++) {
+            const uint64_t key = sm.keys[k];
+            const bool inA = k < sizeA;
+            const uint32_t u = half_hash(key, inA ? ja : jb, half) + off;
+            const uint32_t v = half_hash(key, inA ? ia : ib, half);
+            edges++;
+            if (!uf.add(u, v)) return false;
+        }
+        return true;
+    }
+};
+
+template <int MAXM>
+__global__ void __launch_bounds__(128) k_leaves_sh2_v2(const Node *__restrict__ nodes, const uint32_t *__restrict__ ids,
+                                                       uint32_t count, const uint64_t *__restrict__ keys,
+                                                       uint64_t *__restrict__ codes, uint8_t *__restrict__ rib_bits,
+                                                       uint8_t *__restrict__ scratch, uint64_t scratch_per_warp,
+                                                       uint32_t smax, uint32_t cmax, uint32_t *__restrict__ err,
+                                                       unsigned long long *__restrict__ work,
+                                                       unsigned int *__restrict__ next_leaf) {
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    constexpr int WPB = 4;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    Sh2Smem<MAXM> &sm = reinterpret_cast<Sh2Smem<MAXM> *>(smem_raw)[warp];
+    const uint64_t gw = (uint64_t)blockIdx.x * WPB + warp;
+    uint8_t *gbase = scratch + gw * scratch_per_warp;
+    Sh2Global g;
+    g.maskA = (uint64_t *)gbase;
+    g.maskB = g.maskA + smax;
+    g.iso = g.maskB + smax;
+    g.csa = (uint32_t *)(g.iso + 2 * (uint64_t)cmax);
+    g.csb = g.csa + cmax;
+    LaneUF2<MAXM> uf{sm.uf, lane, 0, 0};
+    unsigned long long w_evals = 0, w_pairs = 0, w_filtered = 0, w_edges = 0;
+    const unsigned below = (1u << lane) - 1;
+
+    for (;;) {
+        uint32_t li = 0;
+        if (lane == 0) li = atomicAdd(next_leaf, 1u);
+        li = __shfl_sync(0xffffffffu, li, 0);
+        if (li >= count) break;
+        const uint32_t id = ids[li];
+        const Node nd = nodes[id];
+        LeafCtx<MAXM> cx{sm, g};
+        cx.m = nd.m;
+        cx.half = (cx.m + 1) / 2;
+        cx.full = cx.half >= 64 ? ~0ull : (1ull << cx.half) - 1;
+        cx.quad = cx.m >= 10;
+        cx.smax = smax;
+        cx.cmax = cmax;
+        const uint32_t m = cx.m, half = cx.half;
+
+        // keys in finder order (QuadSplitCandidateFinder ctor, ShockHash2-internal.h:397-407)
+        {
+            uint32_t evens = 0, odds = 0;
+            for (uint32_t k0 = 0; k0 < m; k0 += 32) {
+                const uint32_t k = k0 + lane;
+                const uint64_t key = k < m ? keys[nd.start + k] : 0;
+                const bool even = (key & 1) == 0;
+                const unsigned be = __ballot_sync(0xffffffffu, k < m && even);
+                const unsigned bo = __ballot_sync(0xffffffffu, k < m && !even);
+                if (k < m) {
+                    sm.orig[k] = key;
+                    uint32_t pos = k;
+                    if (cx.quad) pos = even ? evens + __popc(be & below) : m - 1 - (odds + __popc(bo & below));
+                    sm.keys[pos] = key;
+                }
+                evens += __popc(be);
+                odds += __popc(bo);
+            }
+            cx.sizeA = cx.quad ? evens : m;
+        }
+        if (lane == 0) sm.nsurv = 0;
+        __syncwarp();
+
+        uint32_t J = 0;             // candidates stored so far
+        uint64_t S = 0;             // raw seeds hashed so far
+        uint64_t answer = ~0ull;
+        bool overflow = false;
+        // survivor queue: run pseudoforest tests 32 at a time; returns true when a pair passed
+        auto drain = [&](uint32_t upto) -> bool {
+            const uint32_t cnt = min(upto, sm.nsurv);
+            bool ok = false;
+            uint32_t j = 0, i = 0;
+            if ((uint32_t)lane < cnt) {
+                const uint32_t e = sm.surv[lane];
+                j = e >> 16;
+                i = e & 0xFFFF;
+                ok = cx.pair_ok(uf, j, i, w_edges);
+            }
+            unsigned pass = __ballot_sync(0xffffffffu, ok);
+            while (pass) {
+                const int src = __ffs(pass) - 1;
+                const uint32_t jj = __shfl_sync(0xffffffffu, j, src), ii = __shfl_sync(0xffffffffu, i, src);
+                const uint64_t sj = cx.cseed(jj), si = cx.cseed(ii);
+                if (float_accurate_triangular(sj, si)) {
+                    answer = pair_triangular(sj, si);
+                    return true;
+                }
+                pass &= pass - 1;
+            }
+            // drop the tested entries, keep the rest in order
+            const uint32_t rest = sm.nsurv - cnt;
+            __syncwarp();
+            uint32_t v0 = (uint32_t)lane < rest ? sm.surv[cnt + lane] : 0;
+            uint32_t v1 = (uint32_t)lane + 32 < rest ? sm.surv[cnt + lane + 32] : 0;
+            __syncwarp();
+            if ((uint32_t)lane < rest) sm.surv[lane] = v0;
+            if ((uint32_t)lane + 32 < rest) sm.surv[lane + 32] = v1;
+            if (lane == 0) sm.nsurv = rest;
+            __syncwarp();
+            return false;
+        };
+
+        while (answer == ~0ull && !overflow) {
+            // 1. hash raw seeds S..S+31
+            if (S + 32 > smax) {
+                overflow = true;
+                break;
+            }
+            {
+                const uint64_t s = S + lane;
+                uint64_t tA = 0, tB = 0;
+                for (uint32_t k = 0; k < m; k++) {
+                    const uint64_t bit = 1ull << half_hash(sm.keys[k], s, half);
+                    if (k < cx.sizeA) tA |= bit; else tB |= bit;
+                }
+                cx.maskA(s) = tA;
+                cx.maskB(s) = tB;
+                w_evals += m;
+            }
+            __syncwarp();
+            const uint64_t s = S + lane;
+            // 2. candidates whose larger raw seed is s, in the reference's order
+            uint32_t mine = 0;
+            if (cx.quad) {
+                const uint64_t tA = cx.maskA(s), tB = cx.maskB(s);
+                for (uint64_t a = 0; a < s; a++)
+                    mine += (cx.maskA(a) | tB) == cx.full && float_accurate_elegant(a, s);
+                for (uint64_t b = 0; b <= s; b++)
+                    mine += (cx.maskB(b) | tA) == cx.full && float_accurate_elegant(s, b);
+            } else {
+                mine = cx.maskA(s) == cx.full;
+            }
+            uint32_t incl = mine;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const uint32_t T = __shfl_sync(0xffffffffu, incl, 31);
+            if (J + T > cmax || J + T > 0xFFFF) {
+                overflow = true;
+                break;
+            }
+            {
+                uint32_t pos = J + incl - mine;
+                if (cx.quad) {
+                    const uint64_t tA = cx.maskA(s), tB = cx.maskB(s);
+                    for (uint64_t a = 0; a < s && mine; a++)
+                        if ((cx.maskA(a) | tB) == cx.full && float_accurate_elegant(a, s)) {
+                            cx.csa(pos) = (uint32_t)a;
+                            cx.csb(pos) = (uint32_t)s;
+                            pos++;
+                        }
+                    for (uint64_t b = 0; b <= s && mine; b++)
+                        if ((cx.maskB(b) | tA) == cx.full && float_accurate_elegant(s, b)) {
+                            cx.csa(pos) = (uint32_t)s;
+                            cx.csb(pos) = (uint32_t)b;
+                            pos++;
+                        }
+                } else if (mine) {
+                    cx.csa(pos) = (uint32_t)s;
+                    cx.csb(pos) = (uint32_t)s;
+                }
+            }
+            S += 32;
+            __syncwarp();
+            if (T == 0) continue;
+            // 3. isolated-key masks of the new candidates (calculateIsolatedVertices), one per lane
+            for (uint32_t c0 = J; c0 < J + T; c0 += 32) {
+                const uint32_t c = c0 + lane;
+                if (c < J + T) {
+                    const uint64_t sa = cx.csa(c), sb = cx.csb(c);
+                    uint64_t seen1 = 0, seen2 = 0;
+                    for (uint32_t k = 0; k < m; k++) {
+                        const uint32_t h = half_hash(sm.keys[k], k < cx.sizeA ? sa : sb, half);
+                        sm.uf[k * 32 + lane] = (uint8_t)h;
+                        const uint64_t bit = 1ull << h;
+                        seen2 |= seen1 & bit;
+                        seen1 |= bit;
+                    }
+                    const uint64_t single = seen1 & ~seen2;
+                    uint64_t iso0 = 0, iso1 = 0;
+                    for (uint32_t k = 0; k < m; k++) {
+                        const uint32_t h = sm.uf[k * 32 + lane];
+                        const uint64_t b = (single >> h) & 1;
+                        if (k < 64) iso0 |= b << k; else iso1 |= b << (k - 64);
+                    }
+                    cx.iso(c, 0) = iso0;
+                    if (Sh2Cfg<MAXM>::ISO_WORDS > 1) cx.iso(c, 1) = iso1;
+                    w_evals += m;
+                }
+            }
+            __syncwarp();
+            // 4. all pairs (j, i), J <= j < J+T, i < j, in lexicographic order
+            const uint64_t q0 = (uint64_t)J * (J - 1) / 2, q1 = (uint64_t)(J + T) * (J + T - 1) / 2;
+            bool done = false;
+            for (uint64_t qb = q0; qb < q1 && !done; qb += 32) {
+                const uint64_t q = qb + lane;
+                bool filt = false;
+                uint32_t j = 0, i = 0;
+                if (q < q1) {
+                    // j = largest with j(j-1)/2 <= q
+                    uint64_t jj = (uint64_t)((1.0 + sqrt(1.0 + 8.0 * (double)q)) * 0.5);
+                    while (jj * (jj - 1) / 2 > q) jj--;
+                    while ((jj + 1) * jj / 2 <= q) jj++;
+                    j = (uint32_t)jj;
+                    i = (uint32_t)(q - jj * (jj - 1) / 2);
+                    uint64_t x = cx.iso(j, 0) & cx.iso(i, 0);
+                    if (Sh2Cfg<MAXM>::ISO_WORDS > 1) x |= cx.iso(j, 1) & cx.iso(i, 1);
+                    filt = x == 0;
+                    w_pairs++;
+                    w_filtered += filt;
+                }
+                const unsigned bal = __ballot_sync(0xffffffffu, filt);
+                const uint32_t base = sm.nsurv;
+                __syncwarp();
+                if (filt) sm.surv[base + __popc(bal & below)] = j << 16 | i;
+                __syncwarp();
+                if (lane == 0) sm.nsurv = base + __popc(bal);
+                __syncwarp();
+                if (sm.nsurv >= 32) done = drain(32);
+            }
+            while (!done && sm.nsurv > 0) done = drain(32);
+            J += T;
+        }
+        if (overflow || answer == ~0ull) {
+            if (lane == 0) atomicOr(err, kErrScratch);
+            continue;
+        }
+
+        // Retrieval bits (constructRetrieval, ShockHash2-internal.h:548-572): ordered cuckoo
+        // insertion of the leaf keys in leaf order; bit 1 when a key rests in its seed2 cell.
+        uint64_t s1, s2;
+        unpair_triangular(answer, s1, s2);
+        for (uint32_t k = lane; k < m; k += 32) {
+            sm.c1[k] = (uint8_t)(sh2_cand_hash(sm.orig[k], s1, m) + m / 2);
+            sm.c2[k] = (uint8_t)sh2_cand_hash(sm.orig[k], s2, m);
+            sm.cell[k] = -1;
+        }
+        __syncwarp();
+        if (lane == 0) {
+            bool okc = true;
+            for (uint32_t k = 0; k < m && okc; k++) okc = cuckoo_insert2(sm.cell, sm.xr, (int)k, sm.c1[k], sm.c2[k], 8 * (int)m + 16);
+            if (!okc) atomicOr(err, kErrInternal);
+            codes[id] = answer;
+        }
+        __syncwarp();
+        for (uint32_t k = lane; k < m; k += 32) rib_bits[nd.start + k] = sm.cell[sm.c2[k]] == (int16_t)k ? 1 : 0;
+        __syncwarp();
+    }
+    for (int o = 16; o; o >>= 1) {
+        w_evals += __shfl_xor_sync(0xffffffffu, w_evals, o);
+        w_pairs += __shfl_xor_sync(0xffffffffu, w_pairs, o);
+        w_filtered += __shfl_xor_sync(0xffffffffu, w_filtered, o);
+        w_edges += __shfl_xor_sync(0xffffffffu, w_edges, o);
+    }
+    if (lane == 0) {
+        atomicAdd(&work[1], w_evals);
+        atomicAdd(&work[2], w_pairs);
+        atomicAdd(&work[3], w_filtered);
+        atomicAdd(&work[4], w_edges);
+    }
+}
+
+template <int MAXM>
+void launch_v2(const Node *nodes, const uint32_t *ids, uint32_t count, const uint64_t *keys, uint64_t *codes,
+               uint8_t *rib_bits, uint8_t *scratch, uint64_t scratch_per_warp, uint32_t smax, uint32_t cmax,
+               uint32_t *err, unsigned long long *work, unsigned int *ctr, int grid, cudaStream_t s) {
+    const size_t smem = sizeof(Sh2Smem<MAXM>) * 4;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_leaves_sh2_v2<MAXM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    k_leaves_sh2_v2<MAXM><<<grid, 128, smem, s>>>(nodes, ids, count, keys, codes, rib_bits, scratch, scratch_per_warp,
+                                                 smax, cmax, err, work, ctr);
+}
+
+} // namespace
+
+// Bytes of global scratch per warp for the given capacities (raw seeds, candidates).
+uint64_t sh2_scratch_bytes(uint32_t smax, uint32_t cmax) { return 16ull * smax + 16ull * cmax + 8ull * cmax; }
+
+void launch_leaves_sh2_ctr(const Node *nodes, const uint32_t *ids, uint32_t count, const uint64_t *keys, uint64_t *codes,
+                           uint8_t *rib_bits, uint8_t *scratch, uint64_t scratch_per_warp, uint32_t smax, uint32_t cmax,
+                           uint32_t *err, unsigned long long *work, unsigned int *ctr, int grid, cudaStream_t s,
+                           int max_leaf) {
+    if (!count) return;
+    cudaMemsetAsync(ctr, 0, sizeof(unsigned int), s);
+    if (max_leaf <= 64)
+        launch_v2<64>(nodes, ids, count, keys, codes, rib_bits, scratch, scratch_per_warp, smax, cmax, err, work, ctr, grid, s);
+    else
+        launch_v2<128>(nodes, ids, count, keys, codes, rib_bits, scratch, scratch_per_warp, smax, cmax, err, work, ctr, grid, s);
+}
+
+int sh2_smem_per_warp(int max_leaf) { return max_leaf <= 64 ? (int)sizeof(Sh2Smem<64>) : (int)sizeof(Sh2Smem<128>); }
+
+} // namespace shg

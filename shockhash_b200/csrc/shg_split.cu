@@ -106,7 +106,7 @@ __device__ uint64_t search_seeds(SplitSmem &sm, uint32_t m, uint64_t seed0, cons
         }
         __syncthreads();
         const uint32_t b = sm.best;
-        if (b != 0xffffffffu) return base + b;
+        if (b != 0xffffffffu) return base + b < cap ? base + b : ~0ull;  // at most `cap` seeds count
     }
     return ~0ull;
 }
