@@ -35,6 +35,13 @@ METRIC = "build ns/key on 1 B200, batched vs per-leaf GPU vs CPU, bit-exact; p99
 CONFIG_NAME = "ShockHash2<64> b=2000, 10M uint64 keys (mt19937_64 seed 7) hashed to 128-bit"
 
 
+class _Summary:
+    """What the report needs from one build, kept after its result block is released."""
+
+    def __init__(self, r):
+        self.stage_ms, self.work = dict(r.stage_ms), dict(r.work)
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -186,23 +193,29 @@ def main():
         step_device()
     # ---- device-resident timed steps (value)
     results, step_ms = [], []
+    r = None
     barrier()
     with ClockSampler(local) as clocks:
         for _ in range(args.steps):
             flush.zero_()
             torch.cuda.synchronize()
+            if r is not None:
+                r.free()  # the previous step's pinned result block is reused
             t0 = time.perf_counter()
             r = step_device()
             step_ms.append(1e3 * (time.perf_counter() - t0))
-            results.append(r)
+            results.append(_Summary(r))
         barrier()
     dev_ms = [r.stage_ms["total"] for r in results]
     # ---- end to end through the public API, host (pinned) input, host outputs (e2e)
     e2e_ms = []
+    r2 = None
     barrier()
     for _ in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
+        if r2 is not None:
+            r2.free()
         t0 = time.perf_counter()
         r2 = eng.build_u64(VARIANT, LEAF, h_keys.numpy().view(np.uint64), BUCKET, args.mode)
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
@@ -220,10 +233,10 @@ def main():
     ms_e2e = maxed(statistics.mean(e2e_ms))
     p99 = maxed(float(np.percentile(e2e_ms, 99)))
     total_keys = n * ws
-    r = results[-1]
     split_ms = statistics.mean(x.stage_ms["splits"] for x in results)
     leaf_ms = statistics.mean(x.stage_ms["leaves"] for x in results)
-    achieved = r.work["split_evals"] / (split_ms * 1e-3)
+    last = results[-1]
+    achieved = last.work["split_evals"] / (split_ms * 1e-3)
     bits_per_key = (r.descriptors.size * 64) / n
 
     line = None
@@ -262,10 +275,10 @@ def main():
                          "note": "useful split evaluations (the reference's sequential count) / device time of "
                                  "the split stage; peak = measured integer microbenchmark of the same "
                                  "arithmetic (no memory traffic)"},
-            "leaf_stage": {"ms": round(leaf_ms, 3), "leaf_evals": r.work["leaf_evals"], "pairs": r.work["pairs"],
-                           "uf_edges": r.work["uf_edges"]},
-            "work": r.work, "bits_per_key_trees": round(bits_per_key, 4),
-            "gpu_launches": int(r.work["launches"] * args.steps),
+            "leaf_stage": {"ms": round(leaf_ms, 3), "leaf_evals": last.work["leaf_evals"],
+                           "pairs": last.work["pairs"], "uf_edges": last.work["uf_edges"]},
+            "work": last.work, "bits_per_key_trees": round(bits_per_key, 4),
+            "gpu_launches": int(last.work["launches"] * args.steps),
             "clocks": clocks.summary(),
             "cpu_baseline": cpu, "forms": forms,
         }
