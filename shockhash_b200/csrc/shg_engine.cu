@@ -43,6 +43,10 @@ static shg_status fail(shg_status st, const std::string &msg) {
     return st;
 }
 
+namespace shg {
+shg_status shg_set_error(shg_status st, const std::string &msg) { return fail(st, msg); }
+} // namespace shg
+
 #define CU(call)                                                                                   \
     do {                                                                                           \
         cudaError_t e_ = (call);                                                                   \

@@ -67,8 +67,11 @@ struct Plan {
 };
 void make_plan(const Config &c, const std::vector<uint64_t> &bucket_size_acc, Plan &plan);
 
+// Records the message returned by shg_last_error() on this thread and passes the status through.
+shg_status shg_set_error(shg_status st, const std::string &msg);
+
 // Device error flag bits.
-enum : uint32_t { kErrTrialLimit = 1, kErrScratch = 2, kErrBucket = 4, kErrInternal = 8 };
+enum : uint32_t { kErrTrialLimit = 1, kErrScratch = 2, kErrBucket = 4, kErrInternal = 8, kErrArg = 16 };
 
 // ----------------------------------------------------------------- kernels (shg_kernels.cu)
 void launch_spooky_u64(const uint64_t *keys, uint64_t n, uint64_t *first, uint64_t *second, cudaStream_t s);

@@ -154,10 +154,23 @@ template <int MAXM> struct LeafCtx {
     }
 };
 
-template <int MAXM>
-__global__ void __launch_bounds__(128) k_leaves_sh2_v2(const Node *__restrict__ nodes, const uint32_t *__restrict__ ids,
-                                                       uint32_t count, const uint64_t *__restrict__ keys,
-                                                       uint64_t *__restrict__ codes, uint8_t *__restrict__ rib_bits,
+// Where a leaf's keys and its output seed are: the engine's planned tree nodes...
+struct NodeLeaves {
+    const Node *nodes;
+    const uint32_t *ids;
+    uint64_t *codes;
+    __device__ __forceinline__ bool get(uint32_t li, uint32_t &start, uint32_t &m, uint64_t *&code) const {
+        const uint32_t id = ids[li];
+        const Node nd = nodes[id];
+        start = nd.start;
+        m = nd.m;
+        code = codes + id;
+        return true;
+    }
+};
+template <int MAXM, class Src>
+__global__ void __launch_bounds__(128) k_leaves_sh2_v2(Src src, uint32_t count, const uint64_t *__restrict__ keys,
+                                                       uint8_t *__restrict__ rib_bits,
                                                        uint8_t *__restrict__ scratch, uint64_t scratch_per_warp,
                                                        uint32_t smax, uint32_t cmax, uint32_t *__restrict__ err,
                                                        unsigned long long *__restrict__ work,
@@ -183,10 +196,14 @@ __global__ void __launch_bounds__(128) k_leaves_sh2_v2(const Node *__restrict__ 
         if (lane == 0) li = atomicAdd(next_leaf, 1u);
         li = __shfl_sync(0xffffffffu, li, 0);
         if (li >= count) break;
-        const uint32_t id = ids[li];
-        const Node nd = nodes[id];
+        uint32_t start = 0, m_leaf = 0;
+        uint64_t *code_out = nullptr;
+        if (!src.get(li, start, m_leaf, code_out)) {
+            if (lane == 0) atomicOr(err, kErrArg);
+            continue;
+        }
         LeafCtx<MAXM> cx{sm, g};
-        cx.m = nd.m;
+        cx.m = m_leaf;
         cx.half = (cx.m + 1) / 2;
         cx.full = cx.half >= 64 ? ~0ull : (1ull << cx.half) - 1;
         cx.quad = cx.m >= 10;
@@ -199,7 +216,7 @@ __global__ void __launch_bounds__(128) k_leaves_sh2_v2(const Node *__restrict__ 
             uint32_t evens = 0, odds = 0;
             for (uint32_t k0 = 0; k0 < m; k0 += 32) {
                 const uint32_t k = k0 + lane;
-                const uint64_t key = k < m ? keys[nd.start + k] : 0;
+                const uint64_t key = k < m ? keys[start + k] : 0;
                 const bool even = (key & 1) == 0;
                 const unsigned be = __ballot_sync(0xffffffffu, k < m && even);
                 const unsigned bo = __ballot_sync(0xffffffffu, k < m && !even);
@@ -256,13 +273,14 @@ __global__ void __launch_bounds__(128) k_leaves_sh2_v2(const Node *__restrict__ 
             return false;
         };
 
+        uint64_t S_proc = 0;  // raw seeds whose candidates are listed
         while (answer == ~0ull && !overflow) {
-            // 1. hash raw seeds S..S+31
-            if (S + 32 > smax) {
-                overflow = true;
-                break;
-            }
-            {
+            // 1. hash raw seeds S..S+31 once the listed ones have caught up
+            if (S_proc == S) {
+                if (S + 32 > smax) {
+                    overflow = true;
+                    break;
+                }
                 const uint64_t s = S + lane;
                 uint64_t tA = 0, tB = 0;
                 for (uint32_t k = 0; k < m; k++) {
@@ -272,19 +290,23 @@ __global__ void __launch_bounds__(128) k_leaves_sh2_v2(const Node *__restrict__ 
                 cx.maskA(s) = tA;
                 cx.maskB(s) = tB;
                 w_evals += m;
+                S += 32;
+                __syncwarp();
             }
-            __syncwarp();
-            const uint64_t s = S + lane;
-            // 2. candidates whose larger raw seed is s, in the reference's order
+            // 2. candidates whose larger raw seed is s (lane L: s = S_proc + L), in the reference's order
+            const uint64_t s = S_proc + lane;
+            const bool live = s < S;
             uint32_t mine = 0;
-            if (cx.quad) {
-                const uint64_t tA = cx.maskA(s), tB = cx.maskB(s);
-                for (uint64_t a = 0; a < s; a++)
-                    mine += (cx.maskA(a) | tB) == cx.full && float_accurate_elegant(a, s);
-                for (uint64_t b = 0; b <= s; b++)
-                    mine += (cx.maskB(b) | tA) == cx.full && float_accurate_elegant(s, b);
-            } else {
-                mine = cx.maskA(s) == cx.full;
+            if (live) {
+                if (cx.quad) {
+                    const uint64_t tA = cx.maskA(s), tB = cx.maskB(s);
+                    for (uint64_t a = 0; a < s; a++)
+                        mine += (cx.maskA(a) | tB) == cx.full && float_accurate_elegant(a, s);
+                    for (uint64_t b = 0; b <= s; b++)
+                        mine += (cx.maskB(b) | tA) == cx.full && float_accurate_elegant(s, b);
+                } else {
+                    mine = cx.maskA(s) == cx.full;
+                }
             }
             uint32_t incl = mine;
 #pragma unroll
@@ -292,12 +314,16 @@ __global__ void __launch_bounds__(128) k_leaves_sh2_v2(const Node *__restrict__ 
                 const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
                 if (lane >= o) incl += y;
             }
-            const uint32_t T = __shfl_sync(0xffffffffu, incl, 31);
-            if (J + T > cmax || J + T > 0xFFFF) {
+            // take the longest prefix of raw seeds whose candidates fit the candidate capacity
+            const uint32_t cap = min(cmax, 0xFFFFu);
+            const unsigned fits = __ballot_sync(0xffffffffu, live && J + incl <= cap);
+            const int take = fits == 0xffffffffu ? 32 : __ffs(~fits) - 1;  // fits is a prefix of lanes
+            if (take == 0) {
                 overflow = true;
                 break;
             }
-            {
+            const uint32_t T = __shfl_sync(0xffffffffu, incl, take - 1);
+            if (lane < take) {
                 uint32_t pos = J + incl - mine;
                 if (cx.quad) {
                     const uint64_t tA = cx.maskA(s), tB = cx.maskB(s);
@@ -318,7 +344,7 @@ __global__ void __launch_bounds__(128) k_leaves_sh2_v2(const Node *__restrict__ 
                     cx.csb(pos) = (uint32_t)s;
                 }
             }
-            S += 32;
+            S_proc += take;
             __syncwarp();
             if (T == 0) continue;
             // 3. isolated-key masks of the new candidates (calculateIsolatedVertices), one per lane
@@ -398,10 +424,10 @@ __global__ void __launch_bounds__(128) k_leaves_sh2_v2(const Node *__restrict__ 
             bool okc = true;
             for (uint32_t k = 0; k < m && okc; k++) okc = cuckoo_insert2(sm.cell, sm.xr, (int)k, sm.c1[k], sm.c2[k], 8 * (int)m + 16);
             if (!okc) atomicOr(err, kErrInternal);
-            codes[id] = answer;
+            *code_out = answer;
         }
         __syncwarp();
-        for (uint32_t k = lane; k < m; k += 32) rib_bits[nd.start + k] = sm.cell[sm.c2[k]] == (int16_t)k ? 1 : 0;
+        for (uint32_t k = lane; k < m; k += 32) rib_bits[start + k] = sm.cell[sm.c2[k]] == (int16_t)k ? 1 : 0;
         __syncwarp();
     }
     for (int o = 16; o; o >>= 1) {
@@ -425,11 +451,11 @@ void launch_v2(const Node *nodes, const uint32_t *ids, uint32_t count, const uin
     const size_t smem = sizeof(Sh2Smem<MAXM>) * 4;
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_leaves_sh2_v2<MAXM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_leaves_sh2_v2<MAXM, NodeLeaves>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
-    k_leaves_sh2_v2<MAXM><<<grid, 128, smem, s>>>(nodes, ids, count, keys, codes, rib_bits, scratch, scratch_per_warp,
-                                                 smax, cmax, err, work, ctr);
+    k_leaves_sh2_v2<MAXM, NodeLeaves><<<grid, 128, smem, s>>>(NodeLeaves{nodes, ids, codes}, count, keys, rib_bits, scratch,
+                                                              scratch_per_warp, smax, cmax, err, work, ctr);
 }
 
 } // namespace
