@@ -118,6 +118,21 @@ shg_status shg_hash_strings(shg_engine *e, const char *bytes, const uint64_t *of
 shg_status shg_sh2_construct_leaves(shg_engine *e, const uint64_t *keys, const uint64_t *leaf_offsets,
                                     uint64_t nleaves, uint64_t *seeds, uint8_t *bits);
 
+/* No counterpart in the reference. The bipartite leaf search of shg_sh2_construct_leaves for callers
+ * that cannot allocate device memory (a framework-owned memory pool that forbids cudaMalloc, a
+ * real-time host path, code that must not grow its footprint): it calls no cudaMalloc, cudaFree or
+ * allocating library routine, and no engine is needed. Inputs and outputs are DEVICE pointers on
+ * the current device: keys, leaf_offsets[nleaves+1] (leaves of 2..64 keys, at most 2^32 - 1 keys),
+ * seeds[nleaves], bits[total keys]; `stream` is a cudaStream_t (NULL = default stream). The call
+ * synchronizes that stream to report errors. Scratch is a fixed 16 MiB array in the library's own
+ * device image, held by every GPU that loads the library until the process exits; a leaf needing
+ * more than 512 raw seeds or 512 candidates fails with SHG_ERR_TRIAL_LIMIT, a leaf outside 2..64
+ * keys with SHG_ERR_ARG. The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture. All calls share the
+ * array, so calls that overlap on the GPU (other streams, other host threads) race. */
+shg_status shg_sh2_construct_leaves_noalloc(const uint64_t *d_keys, const uint64_t *d_leaf_offsets, uint64_t nleaves,
+                                            uint64_t *d_seeds, uint8_t *d_bits, void *stream);
+
 /* Batched original-ShockHash leaf search at tree depth `level` (include/ShockHash.h:404-434):
  * codes[j] = x - start_seed[level]; keys_by_cell/bits are written per leaf in cell order, as the
  * reference pushes its retrieval input. Leaves of 2..60 keys. */

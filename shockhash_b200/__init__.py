@@ -89,6 +89,7 @@ def lib():
         "shg_mphf_query_strings": ([_vp, ctypes.c_char_p, _vp, _u64, _vp], ctypes.c_int),
         "shg_mphf_bits": ([_vp], _u64),
         "shg_mphf_size": ([_vp], _u64),
+        "shg_sh2_construct_leaves_noalloc": ([_vp, _vp, _u64, _vp, _vp, _vp], ctypes.c_int),
         "shg_keys_mt19937_64": ([_u64, _u64, _vp], None),
         "shg_int_peak": ([ctypes.c_int, _u64, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)],
                          ctypes.c_int),
@@ -132,6 +133,15 @@ def int_peak(device=0, iters=1 << 16):
     e, ms = ctypes.c_double(), ctypes.c_double()
     _check(lib().shg_int_peak(device, iters, ctypes.byref(e), ctypes.byref(ms)))
     return e.value, ms.value
+
+
+def sh2_construct_leaves_noalloc(d_keys, d_leaf_offsets, nleaves, d_seeds, d_bits, stream=0):
+    """Bipartite leaf search without any device allocation (fixed 16 MiB library scratch).
+
+    All arguments are device addresses (ints) on the current device: keys, leaf_offsets[nleaves+1]
+    (leaves of 2..64 keys), seeds[nleaves], bits[total keys]; ``stream`` a cudaStream_t handle."""
+    _check(lib().shg_sh2_construct_leaves_noalloc(_vp(d_keys), _vp(d_leaf_offsets), nleaves, _vp(d_seeds),
+                                                   _vp(d_bits), _vp(stream)))
 
 
 def memo_table(variant, leaf_size):

@@ -16,7 +16,10 @@
 //      passing survivor in queue order is the answer (all pairs of earlier batches failed).
 // Candidate and raw-seed state live in shared memory; indices past its capacity spill to a
 // per-warp slice of global scratch.
+#include <algorithm>
 #include <cstdint>
+#include <mutex>
+#include <string>
 #include <cuda_runtime.h>
 #include "shg_common.cuh"
 #include "shg_internal.h"
@@ -168,6 +171,20 @@ struct NodeLeaves {
         return true;
     }
 };
+// ...or a caller's leaf offsets (leaf j = keys [offs[j], offs[j+1])), validated on the device.
+template <int MAXM> struct OffsetLeaves {
+    const uint64_t *offs;
+    uint64_t *seeds;
+    __device__ __forceinline__ bool get(uint32_t li, uint32_t &start, uint32_t &m, uint64_t *&code) const {
+        const uint64_t b = offs[li], e = offs[li + 1];
+        if (e < b + 2 || e - b > (uint64_t)MAXM || e > 0xFFFFFFFFull) return false;
+        start = (uint32_t)b;
+        m = (uint32_t)(e - b);
+        code = seeds + li;
+        return true;
+    }
+};
+
 template <int MAXM, class Src>
 __global__ void __launch_bounds__(128) k_leaves_sh2_v2(Src src, uint32_t count, const uint64_t *__restrict__ keys,
                                                        uint8_t *__restrict__ rib_bits,
@@ -477,4 +494,82 @@ void launch_leaves_sh2_ctr(const Node *nodes, const uint32_t *ids, uint32_t coun
 
 int sh2_smem_per_warp(int max_leaf) { return max_leaf <= 64 ? (int)sizeof(Sh2Smem<64>) : (int)sizeof(Sh2Smem<128>); }
 
+// ------------------------------------------------------------------ no-allocation variant
+// Some callers cannot allocate device memory at the moment they need leaf seeds: code running
+// under a host-side allocator that forbids cudaMalloc (a memory pool owned by another framework,
+// a region being captured, a real-time or embedded host path), or code that already owns every
+// buffer it may touch. For them the bipartite leaf search also runs from a fixed scratch area that
+// lives in this library's own device image: kNoAllocScratchBytes (16 MiB) per device that loads the
+// library, held until the process exits. Its layout: 256 bytes of counters (error flags, the leaf
+// counter, work counters), then a spill slice per warp for raw-seed masks and candidates beyond
+// what fits in shared memory (512 raw seeds and 512 candidates per leaf in this variant).
+constexpr uint64_t kNoAllocScratchBytes = 16ull << 20;
+constexpr uint32_t kNoAllocSmax = 512, kNoAllocCmax = 512;
+static __device__ __align__(256) uint8_t g_noalloc_scratch[kNoAllocScratchBytes];
+
+struct NoAllocCounters {
+    uint32_t err;
+    unsigned int leaf_ctr;
+    unsigned long long work[8];
+};
+
+// Device address of g_noalloc_scratch on the current device, looked up once per device.
+static uint8_t *noalloc_base(int device, cudaError_t &st) {
+    static std::mutex mu;
+    static uint8_t *addr[64] = {};
+    std::lock_guard<std::mutex> lock(mu);
+    st = cudaSuccess;
+    if (device < 0 || device >= 64) {
+        st = cudaErrorInvalidDevice;
+        return nullptr;
+    }
+    if (!addr[device]) {
+        void *p = nullptr;
+        st = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (st != cudaSuccess) return nullptr;
+        addr[device] = (uint8_t *)p;
+    }
+    return addr[device];
+}
+
 } // namespace shg
+
+extern "C" shg_status shg_sh2_construct_leaves_noalloc(const uint64_t *d_keys, const uint64_t *d_leaf_offsets,
+                                                       uint64_t nleaves, uint64_t *d_seeds, uint8_t *d_bits,
+                                                       void *stream) {
+    using namespace shg;
+    if (nleaves == 0) return SHG_OK;
+    if (!d_keys || !d_leaf_offsets || !d_seeds || !d_bits) return shg_set_error(SHG_ERR_ARG, "null device pointer");
+    if (nleaves >= (1ull << 32)) return shg_set_error(SHG_ERR_ARG, "at most 2^32 - 1 leaves per call");
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) return shg_set_error(SHG_ERR_NO_DEVICE, "no current CUDA device");
+    cudaError_t st;
+    uint8_t *base = noalloc_base(device, st);
+    if (!base) return shg_set_error(SHG_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(st));
+    cudaStream_t s = (cudaStream_t)stream;
+    NoAllocCounters *ctr = (NoAllocCounters *)base;
+    // counters start at zero on every call; the spill slices need no clearing (written before read)
+    if ((st = cudaMemsetAsync(ctr, 0, sizeof(NoAllocCounters), s)) != cudaSuccess)
+        return shg_set_error(SHG_ERR_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(st));
+    const uint64_t per_warp = (sh2_scratch_bytes(kNoAllocSmax, kNoAllocCmax) + 255) & ~255ull;
+    const uint64_t warps = (kNoAllocScratchBytes - 256) / per_warp;
+    const uint64_t blocks = std::min<uint64_t>(warps / 4, (nleaves + 3) / 4);
+    const size_t smem = sizeof(Sh2Smem<64>) * 4;
+    k_leaves_sh2_v2<64, OffsetLeaves<64>><<<(int)blocks, 128, smem, s>>>(
+        OffsetLeaves<64>{d_leaf_offsets, d_seeds}, (uint32_t)nleaves, d_keys, d_bits, base + 256, per_warp,
+        kNoAllocSmax, kNoAllocCmax, &ctr->err, ctr->work, &ctr->leaf_ctr);
+    if ((st = cudaGetLastError()) != cudaSuccess)
+        return shg_set_error(SHG_ERR_CUDA, std::string("leaf kernel launch: ") + cudaGetErrorString(st));
+    uint32_t err = 0;
+    if ((st = cudaMemcpyAsync(&err, &ctr->err, sizeof(err), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (st = cudaStreamSynchronize(s)) != cudaSuccess)
+        return shg_set_error(SHG_ERR_CUDA, std::string("leaf kernel: ") + cudaGetErrorString(st));
+    if (err & kErrArg)
+        return shg_set_error(SHG_ERR_ARG, "a leaf has fewer than 2 or more than 64 keys, or keys past 2^32 - 1 "
+                                          "(limits of the no-allocation entry point)");
+    if (err & kErrScratch)
+        return shg_set_error(SHG_ERR_TRIAL_LIMIT, "a leaf needed more than 512 raw seeds or 512 candidates (the "
+                                                  "no-allocation scratch limit; duplicate keys?)");
+    if (err) return shg_set_error(SHG_ERR_CUDA, "internal device error flag " + std::to_string(err));
+    return SHG_OK;
+}
