@@ -1,10 +1,10 @@
 // Measurement utilities (not part of the reference's interface):
 //  * the seeded key generators the benchmark configurations name (std::mt19937_64), shared by the
 //    CPU and GPU runs so both build from the same keys;
-//  * the integer-pipe peak of the split search: the same remix + 16-bit threshold arithmetic as
-//    the split kernel's inner loop (three part boundaries), on register-resident operands with no
-//    memory traffic. Its evaluations per second are the denominator of the search kernels'
-//    roofline fraction.
+//  * the integer-pipe peak of the split search: the arithmetic of the split kernel's dominant inner
+//    loop (remix to 16 bits, quarter-split part, moment sums; two seeds per lane) on
+//    register-resident operands with no memory traffic. Its evaluations per second are the
+//    denominator of the search kernels' roofline fraction.
 #include <algorithm>
 #include <cstdint>
 #include <random>
@@ -17,6 +17,8 @@ namespace {
 
 constexpr int kPeakThreads = 256;
 
+// The arithmetic of the split kernel's dominant loop (quarter splits): remix to 16 bits, part
+// p = r >> 14, moments sum p, sum p^2, sum p^3; two seeds per key pair.
 __global__ void __launch_bounds__(kPeakThreads) k_int_peak(uint64_t iters, uint32_t T0, uint32_t T1, uint32_t T2,
                                                            unsigned long long *sink) {
     const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
@@ -24,13 +26,13 @@ __global__ void __launch_bounds__(kPeakThreads) k_int_peak(uint64_t iters, uint3
     const uint64_t x0 = 0x643e521ddbd2be98ULL + tid;
     uint32_t c0 = 0, c1 = 0, c2 = 0, d0 = 0, d1 = 0, d2 = 0;
     for (uint64_t i = 0; i < iters; i++) {
-        // two seeds per key pair, as the split kernel's kSeedsPerLane = 2
-        const uint32_t r0 = shg::remix_low16(k0 + x0 + i);
-        const uint32_t r1 = shg::remix_low16(k1 + x0 + i);
-        c0 += r0 < T0; c1 += r0 < T1; c2 += r0 < T2;
-        d0 += r1 < T0; d1 += r1 < T1; d2 += r1 < T2;
+        const uint32_t p0 = shg::remix_low16(k0 + x0 + i) >> 14;
+        const uint32_t p1 = shg::remix_low16(k1 + x0 + i) >> 14;
+        const uint32_t q0 = p0 * p0, q1 = p1 * p1;
+        c0 += p0; c1 += q0; c2 += q0 * p0;
+        d0 += p1; d1 += q1; d2 += q1 * p1;
     }
-    if ((c0 ^ c1 ^ c2 ^ d0 ^ d1 ^ d2) == 0xFFFFFFFFu) atomicAdd(sink, 1ull);
+    if ((c0 ^ c1 ^ c2 ^ d0 ^ d1 ^ d2 ^ T0 ^ T1 ^ T2) == 0xFFFFFFFFu) atomicAdd(sink, 1ull);
 }
 
 } // namespace

@@ -63,7 +63,41 @@ __device__ __forceinline__ void count_range(const uint64_t *__restrict__ sk, uin
     }
 }
 
+// Quarter split (fanout 4 with m = 4 * unit, every full first-level node): the thresholds are
+// k * 16384, so a key's part is p = r16 >> 14. Instead of three compare-and-count chains the lane
+// accumulates the moments sum p, sum p^2, sum p^3 (multiply-adds); part counts (u, u, u, u) are the
+// only counts with moments (6u, 14u, 36u) because the system matrix [[1,2,3],[1,4,9],[1,8,27]] is
+// invertible.
+__device__ __forceinline__ void moments_range(const uint64_t *__restrict__ sk, uint32_t lo, uint32_t hi, uint64_t x0,
+                                              uint32_t (&c)[kSeedsPerLane][3]) {
+    uint32_t i = lo;
+    for (; i + 2 <= hi; i += 2) {
+        const uint64_t k0 = sk[i], k1 = sk[i + 1];
+#pragma unroll
+        for (int s = 0; s < kSeedsPerLane; s++) {
+            const uint64_t x = x0 + (uint64_t)(s * 32);
+            const uint32_t p0 = remix_low16(k0 + x) >> 14;
+            const uint32_t p1 = remix_low16(k1 + x) >> 14;
+            const uint32_t q0 = p0 * p0, q1 = p1 * p1;
+            c[s][0] += p0 + p1;
+            c[s][1] += q0 + q1;
+            c[s][2] += q0 * p0 + q1 * p1;
+        }
+    }
+    for (; i < hi; i++) {
+        const uint64_t k0 = sk[i];
+#pragma unroll
+        for (int s = 0; s < kSeedsPerLane; s++) {
+            const uint32_t p0 = remix_low16(k0 + x0 + (uint64_t)(s * 32)) >> 14;
+            c[s][0] += p0;
+            c[s][1] += p0 * p0;
+            c[s][2] += p0 * p0 * p0;
+        }
+    }
+}
+
 // Smallest valid trial index (seed - seed0), or ~0 when `cap` trials were exhausted.
+// NT = number of part thresholds compared (1..3); NT = 4 selects the quarter-split moments.
 template <int NT>
 __device__ uint64_t search_seeds(SplitSmem &sm, uint32_t m, uint64_t seed0, const uint32_t T0, const uint32_t T1,
                                  const uint32_t T2, const uint32_t N0, const uint32_t N1, const uint32_t N2, int G,
@@ -77,18 +111,20 @@ __device__ uint64_t search_seeds(SplitSmem &sm, uint32_t m, uint64_t seed0, cons
     for (uint64_t base = 0; base < cap; base += per_round) {
         const uint32_t slot0 = (uint32_t)group * kSeedsPerWarp + lane;  // seed slot s is slot0 + 32 s
         uint32_t c[kSeedsPerLane][3] = {};
-        count_range<NT>(sm.keys, lo, hi, seed0 + base + slot0, T0, T1, T2, c);
+        if (NT == 4) moments_range(sm.keys, lo, hi, seed0 + base + slot0, c);
+        else count_range<NT>(sm.keys, lo, hi, seed0 + base + slot0, T0, T1, T2, c);
+        constexpr int NC = NT == 4 ? 3 : NT;  // counters per seed
         if (wpg > 1) {
 #pragma unroll
             for (int s = 0; s < kSeedsPerLane; s++)
 #pragma unroll
-                for (int t = 0; t < NT; t++) sm.part_counts[warp][s * 32 + lane][t] = c[s][t];
+                for (int t = 0; t < NC; t++) sm.part_counts[warp][s * 32 + lane][t] = c[s][t];
             __syncthreads();
             if (sub == 0) {
 #pragma unroll
                 for (int s = 0; s < kSeedsPerLane; s++)
 #pragma unroll
-                    for (int t = 0; t < NT; t++) {
+                    for (int t = 0; t < NC; t++) {
                         uint32_t tot = 0;
                         for (int w = 0; w < wpg; w++) tot += sm.part_counts[warp + w][s * 32 + lane][t];
                         c[s][t] = tot;
@@ -100,7 +136,7 @@ __device__ uint64_t search_seeds(SplitSmem &sm, uint32_t m, uint64_t seed0, cons
             for (int s = 0; s < kSeedsPerLane; s++) {
                 bool ok = true;
 #pragma unroll
-                for (int t = 0; t < NT; t++) ok &= c[s][t] == need[t];
+                for (int t = 0; t < NC; t++) ok &= c[s][t] == need[t];
                 if (ok) atomicMin(&sm.best, slot0 + 32u * s);
             }
         }
@@ -157,10 +193,18 @@ __global__ void __launch_bounds__(kSplitThreads) k_split(const Node *__restrict_
     uint64_t cap = 1ull << min(nd.g + 12, 40);
     if (max_trials && max_trials < cap) cap = max_trials;
     uint64_t trial;
+    const bool quarter = nd.kind == kSplitK && nd.fanout == 4 && m == 4u * nd.unit;
+    if (quarter) {
+        NT = 4;  // moments: sum p = 6u, sum p^2 = 14u, sum p^3 = 36u
+        need[0] = 6u * nd.unit;
+        need[1] = 14u * nd.unit;
+        need[2] = 36u * nd.unit;
+    }
     switch (NT) {
         case 1: trial = search_seeds<1>(sm, m, seed0, T[0], T[1], T[2], need[0], need[1], need[2], G, cap); break;
         case 2: trial = search_seeds<2>(sm, m, seed0, T[0], T[1], T[2], need[0], need[1], need[2], G, cap); break;
-        default: trial = search_seeds<3>(sm, m, seed0, T[0], T[1], T[2], need[0], need[1], need[2], G, cap); break;
+        case 3: trial = search_seeds<3>(sm, m, seed0, T[0], T[1], T[2], need[0], need[1], need[2], G, cap); break;
+        default: trial = search_seeds<4>(sm, m, seed0, T[0], T[1], T[2], need[0], need[1], need[2], G, cap); break;
     }
     if (trial == ~0ull) {
         if (threadIdx.x == 0) atomicOr(err, kErrTrialLimit);
