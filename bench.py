@@ -251,7 +251,12 @@ def main():
             dt, kind, cores = cpu_reference(keys[:sample], os.cpu_count() or 1)
             cpu = {"value": round(dt * 1e9 / sample, 3), "unit": "ns/key", "cores": cores, "kind": kind,
                    "sample": f"first {sample} keys of the same stream, constructor only, all host threads"}
-        forms = {"persistent_or_levels_ns_per_key": round(ms * 1e6 / n, 3)}
+        forms = {"default_ns_per_key": round(ms * 1e6 / n, 3)}
+        if ws == 1 and not args.no_forms:
+            for name, mode in (("levels", shg.MODE_LEVELS), ("pipelined", shg.MODE_PIPELINED)):
+                rm = eng.build_u64_device(VARIANT, LEAF, d_keys.data_ptr(), n, BUCKET, mode)
+                forms[f"{name}_device_ns_per_key"] = round(rm.stage_ms["total"] * 1e6 / n, 3)
+                rm.free()
         if ws == 1 and not args.no_forms:
             pl_n = int(os.environ.get("SHG_PER_LEAF_SAMPLE", "100000"))
             rp = eng.build_u64_device(VARIANT, LEAF, d_keys.data_ptr(), pl_n, BUCKET, shg.MODE_PER_LEAF)
@@ -266,7 +271,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
             "config": {"workload": CONFIG_NAME, "keys_per_gpu": n, "leaf_size": LEAF, "bucket_size": BUCKET,
-                       "variant": "ShockHash2", "mode": ["persistent", "levels", "per_leaf"][args.mode],
+                       "variant": "ShockHash2", "mode": ["default (levels)", "levels", "per_leaf", "pipelined"][args.mode],
                        "l2": "flushed (256 MB write) before every timed step, outside the timing",
                        "parallelism": f"{ws} independent bucket shards, no data-path collective"},
             "device_ms_per_step": round(ms_dev, 3),

@@ -43,9 +43,12 @@ typedef enum shg_variant {
 
 /* How the search stages are scheduled on the device. All modes give identical results. */
 typedef enum shg_mode {
-    SHG_MODE_PERSISTENT = 0,  /* one persistent kernel drains a device work queue of split and leaf nodes */
-    SHG_MODE_LEVELS = 1,      /* one launch per RecSplit level, then one launch for all leaves */
-    SHG_MODE_PER_LEAF = 2     /* comparison form: per-level split launches and one launch per leaf */
+    SHG_MODE_DEFAULT = 0,     /* the fastest measured schedule: currently SHG_MODE_LEVELS */
+    SHG_MODE_LEVELS = 1,      /* one launch per RecSplit level (a block per split node), then one persistent
+                                 leaf launch whose warps drain all leaves from a device counter */
+    SHG_MODE_PER_LEAF = 2,    /* comparison form: per-level split launches and one launch per leaf */
+    SHG_MODE_PIPELINED = 3    /* buckets in chunks; a chunk's leaf launch (second stream) overlaps the next
+                                 chunk's split launches (measured slower on B200: both compete for issue slots) */
 } shg_mode;
 
 typedef struct shg_params {

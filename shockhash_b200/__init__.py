@@ -21,12 +21,13 @@ import os
 import numpy as np
 
 __all__ = ["ShgError", "Engine", "BuildResult", "ShockHash", "ShockHash2", "lib", "LIB_PATH",
-           "SHOCKHASH", "SHOCKHASH2", "MODE_PERSISTENT", "MODE_LEVELS", "MODE_PER_LEAF"]
+           "SHOCKHASH", "SHOCKHASH2", "MODE_DEFAULT", "MODE_LEVELS", "MODE_PER_LEAF",
+           "MODE_PIPELINED"]
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libshg.so")
 
 SHOCKHASH, SHOCKHASH2 = 1, 2
-MODE_PERSISTENT, MODE_LEVELS, MODE_PER_LEAF = 0, 1, 2
+MODE_DEFAULT, MODE_LEVELS, MODE_PER_LEAF, MODE_PIPELINED = 0, 1, 2, 3
 _STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_OOM", 3: "ERR_TRIAL_LIMIT", 4: "ERR_CUDA", 5: "ERR_BUCKET",
            6: "ERR_NO_DEVICE"}
 STAGES = ("hash", "partition", "plan", "splits", "leaves", "encode", "copy_out", "total")
@@ -206,7 +207,7 @@ class Engine:
             pass
 
     @staticmethod
-    def params(variant, leaf_size, bucket_size=2000, mode=MODE_PERSISTENT, max_trials=0):
+    def params(variant, leaf_size, bucket_size=2000, mode=MODE_DEFAULT, max_trials=0):
         return _Params(variant, leaf_size, bucket_size, mode, max_trials)
 
     def _finish(self, p, st, res, keep_raw=False):
@@ -217,7 +218,7 @@ class Engine:
             out._mphf = _Mphf(p, res)
         return out
 
-    def build_hash128(self, variant, leaf_size, first, second, bucket_size=2000, mode=MODE_PERSISTENT, max_trials=0,
+    def build_hash128(self, variant, leaf_size, first, second, bucket_size=2000, mode=MODE_DEFAULT, max_trials=0,
                       query=False):
         first = np.ascontiguousarray(first, dtype=np.uint64)
         second = np.ascontiguousarray(second, dtype=np.uint64)
@@ -225,18 +226,18 @@ class Engine:
         st = lib().shg_build_hash128(self._h, ctypes.byref(p), _ptr(first), _ptr(second), len(first), ctypes.byref(res))
         return self._finish(p, st, res, query)
 
-    def build_u64(self, variant, leaf_size, keys, bucket_size=2000, mode=MODE_PERSISTENT, max_trials=0, query=False):
+    def build_u64(self, variant, leaf_size, keys, bucket_size=2000, mode=MODE_DEFAULT, max_trials=0, query=False):
         keys = np.ascontiguousarray(keys, dtype=np.uint64)
         p, res = self.params(variant, leaf_size, bucket_size, mode, max_trials), _Result()
         st = lib().shg_build_u64(self._h, ctypes.byref(p), _ptr(keys), len(keys), ctypes.byref(res))
         return self._finish(p, st, res, query)
 
-    def build_u64_device(self, variant, leaf_size, d_keys_ptr, n, bucket_size=2000, mode=MODE_PERSISTENT):
+    def build_u64_device(self, variant, leaf_size, d_keys_ptr, n, bucket_size=2000, mode=MODE_DEFAULT):
         p, res = self.params(variant, leaf_size, bucket_size, mode, 0), _Result()
         st = lib().shg_build_u64_device(self._h, ctypes.byref(p), _vp(d_keys_ptr), n, ctypes.byref(res))
         return self._finish(p, st, res)
 
-    def build_strings(self, variant, leaf_size, keys, bucket_size=2000, mode=MODE_PERSISTENT, max_trials=0,
+    def build_strings(self, variant, leaf_size, keys, bucket_size=2000, mode=MODE_DEFAULT, max_trials=0,
                       query=False):
         data, offs = pack_strings(keys)
         p, res = self.params(variant, leaf_size, bucket_size, mode, max_trials), _Result()
@@ -315,7 +316,7 @@ class _RecSplitBase:
     VARIANT = None
     LEAF = None
 
-    def __init__(self, keys, bucket_size, num_threads=1, mode=MODE_PERSISTENT, engine=None):
+    def __init__(self, keys, bucket_size, num_threads=1, mode=MODE_DEFAULT, engine=None):
         if self.LEAF is None:
             raise TypeError("pick a leaf size first, e.g. ShockHash2[64](keys, 2000)")
         eng = engine or default_engine()

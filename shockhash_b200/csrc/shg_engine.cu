@@ -95,6 +95,11 @@ struct shg_engine {
     DevBuf in_keys, in_bytes, in_offsets, first, second, sfirst, sidx, counts, cursor, acc, keys, nodes, ids, codes,
         fixed_off, bnb, bucket_bits, pos_acc, words, rib_keys, rib_bits, skip_bits, scratch, misc, singles, ckeys, cbits;
     cudaEvent_t ev[8] = {};
+    cudaStream_t stream2 = nullptr;  // leaves of the pipelined mode
+    static constexpr int kMaxChunks = 64;
+    cudaEvent_t chunk_ev[kMaxChunks] = {};
+    cudaEvent_t join_ev = nullptr;
+    int pipe_chunks = 8;
     ~shg_engine() {
         DevBuf *all[] = {&in_keys, &in_bytes, &in_offsets, &first, &second, &sfirst, &sidx, &counts, &cursor,
                          &acc, &keys, &nodes, &ids, &codes, &fixed_off, &bnb, &bucket_bits, &pos_acc, &words,
@@ -106,6 +111,10 @@ struct shg_engine {
         }
         for (auto &e : ev)
             if (e) cudaEventDestroy(e);
+        for (auto &e : chunk_ev)
+            if (e) cudaEventDestroy(e);
+        if (join_ev) cudaEventDestroy(join_ev);
+        if (stream2) cudaStreamDestroy(stream2);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -157,7 +166,7 @@ shg_status check_params(const shg_params *p, uint64_t n) {
     if (p->leaf_size < 2 || p->leaf_size > maxleaf) return fail(SHG_ERR_ARG, "leaf size out of range");
     if (p->bucket_size < 1) return fail(SHG_ERR_ARG, "bucket size must be >= 1");
     if (n >= (1ull << 32)) return fail(SHG_ERR_ARG, "at most 2^32 - 1 keys per build");
-    if (p->mode < SHG_MODE_PERSISTENT || p->mode > SHG_MODE_PER_LEAF) return fail(SHG_ERR_ARG, "unknown mode");
+    if (p->mode < SHG_MODE_DEFAULT || p->mode > SHG_MODE_PIPELINED) return fail(SHG_ERR_ARG, "unknown mode");
     return SHG_OK;
 }
 
@@ -236,62 +245,90 @@ shg_status build_core(shg_engine *e, const shg_params *p, const uint64_t *d_firs
     if (nids) CU(cudaMemcpyAsync(e->ids.p, ids.data(), nids * 4, cudaMemcpyHostToDevice, s));
     CU(cudaMemcpyAsync(e->bnb.p, plan.bucket_node_begin.data(), (nb + 1) * 4, cudaMemcpyHostToDevice, s));
     CU(cudaMemcpyAsync(e->skip_bits.p, skip.data(), kMaxBucket * 4, cudaMemcpyHostToDevice, s));
+    if (p->variant == SHG_SHOCKHASH2) {
+        // bipartite leaf scratch for the widest leaf grid any schedule uses (grown once, then reused)
+        const uint32_t sm_ = p->leaf_size > 64 ? 16384 : 4096, cm_ = p->leaf_size > 64 ? 16384 : 2048;
+        const uint64_t pw = (sh2_scratch_bytes(sm_, cm_) + 255) & ~255ull;
+        const int bps = std::max(1, std::min(8, (228 * 1024) / (4 * sh2_smem_per_warp(p->leaf_size) + 1024)));
+        CU(e->scratch.ensure(pw * (uint64_t)e->sms * bps * 4));
+    }
     CU(cudaEventRecord(e->ev[2], s));
 
-    // ---- splits, level by level
+    // ---- splits and leaves
     uint64_t launches = 0;
     const uint32_t *d_ids = e->ids.as<uint32_t>();
-    for (size_t lv = 0; lv < plan.split_levels.size(); lv++) {
-        const uint32_t cnt = (uint32_t)plan.split_levels[lv].size();
-        if (!cnt) continue;
-        launch_split_level(e->nodes.as<Node>(), d_ids + level_off[lv], cnt, e->keys.as<uint64_t>(), e->codes.as<uint64_t>(),
-                           p->max_trials, &misc->err, &misc->work[0], s);
-        launches++;
-    }
-    CU(cudaGetLastError());
-    CU(cudaEventRecord(e->ev[3], s));
-
-    // ---- leaves
     const uint32_t nleaves = (uint32_t)plan.leaves.size();
-    if (p->variant == SHG_SHOCKHASH2) {
-        const int maxm = p->leaf_size;
-        const uint32_t smax = maxm > 64 ? 16384 : 4096;
-        const uint32_t cmax = maxm > 64 ? 16384 : 2048;
-        const uint64_t per_warp = (sh2_scratch_bytes(smax, cmax) + 255) & ~255ull;
+    const bool sh2 = p->variant == SHG_SHOCKHASH2;
+    const bool pipelined = p->mode == SHG_MODE_PIPELINED;
+    // leaf kernel launch shape and scratch
+    const int maxm = p->leaf_size;
+    const uint32_t smax = maxm > 64 ? 16384 : 4096, cmax = maxm > 64 ? 16384 : 2048;
+    const uint64_t per_warp = (sh2_scratch_bytes(smax, cmax) + 255) & ~255ull;
+    int leaf_grid;
+    if (sh2) {
         const int per_block_smem = 4 * sh2_smem_per_warp(maxm);
         const int blocks_per_sm = std::max(1, std::min(8, (228 * 1024) / (per_block_smem + 1024)));
-        const int grid = p->mode == SHG_MODE_PER_LEAF ? 1
-                         : std::max(1, std::min<int>(e->sms * blocks_per_sm, (int)((nleaves + 3) / 4)));
-        CU(e->scratch.ensure(per_warp * (uint64_t)grid * 4));
-        if (p->mode == SHG_MODE_PER_LEAF) {
-            for (uint32_t l = 0; l < nleaves; l++) {
-                launch_leaves_sh2_ctr(e->nodes.as<Node>(), d_ids + leaf_off + l, 1, e->keys.as<uint64_t>(),
-                                      e->codes.as<uint64_t>(), e->rib_bits.as<uint8_t>(), e->scratch.as<uint8_t>(), per_warp,
-                                      smax, cmax, &misc->err, misc->work, &misc->leaf_ctr, 1, s, maxm);
-                launches++;
-            }
-        } else if (nleaves) {
-            launch_leaves_sh2_ctr(e->nodes.as<Node>(), d_ids + leaf_off, nleaves, e->keys.as<uint64_t>(),
-                                  e->codes.as<uint64_t>(), e->rib_bits.as<uint8_t>(), e->scratch.as<uint8_t>(), per_warp, smax,
-                                  cmax, &misc->err, misc->work, &misc->leaf_ctr, grid, s, maxm);
-            launches++;
-        }
+        // next to running split launches, leaves take part of each SM (the splits are ALU bound,
+        // the leaves latency bound, so the two interleave)
+        const int bps = pipelined ? std::max(1, blocks_per_sm / 2) : blocks_per_sm;
+        leaf_grid = p->mode == SHG_MODE_PER_LEAF ? 1 : std::max(1, std::min<int>(e->sms * bps, (int)((nleaves + 3) / 4)));
     } else {
         const int wpb = leaves_sh1_warps_per_block();
-        const int grid = std::max(1, std::min<int>(e->sms * 8, (int)((nleaves + wpb - 1) / wpb)));
-        if (p->mode == SHG_MODE_PER_LEAF) {
-            for (uint32_t l = 0; l < nleaves; l++) {
-                launch_leaves_sh1_ctr(e->nodes.as<Node>(), d_ids + leaf_off + l, 1, e->keys.as<uint64_t>(),
-                                      e->codes.as<uint64_t>(), e->rib_keys.as<uint64_t>(), e->rib_bits.as<uint8_t>(),
-                                      p->max_trials, &misc->err, misc->work, &misc->leaf_ctr, 1, s);
-                launches++;
-            }
-        } else if (nleaves) {
-            launch_leaves_sh1_ctr(e->nodes.as<Node>(), d_ids + leaf_off, nleaves, e->keys.as<uint64_t>(),
+        leaf_grid = std::max(1, std::min<int>(e->sms * (pipelined ? 4 : 8), (int)((nleaves + wpb - 1) / wpb)));
+    }
+    auto split_range = [&](size_t lv, uint64_t a, uint64_t b, cudaStream_t st) {
+        if (b <= a) return;
+        launch_split_level(e->nodes.as<Node>(), d_ids + level_off[lv] + a, (uint32_t)(b - a), e->keys.as<uint64_t>(),
+                           e->codes.as<uint64_t>(), p->max_trials, &misc->err, &misc->work[0], st);
+        launches++;
+    };
+    auto leaf_range = [&](uint64_t a, uint64_t b, cudaStream_t st, int grid) {
+        if (b <= a) return;
+        if (sh2)
+            launch_leaves_sh2_ctr(e->nodes.as<Node>(), d_ids + leaf_off + a, (uint32_t)(b - a), e->keys.as<uint64_t>(),
+                                  e->codes.as<uint64_t>(), e->rib_bits.as<uint8_t>(), e->scratch.as<uint8_t>(), per_warp, smax,
+                                  cmax, &misc->err, misc->work, &misc->leaf_ctr, grid, st, maxm);
+        else
+            launch_leaves_sh1_ctr(e->nodes.as<Node>(), d_ids + leaf_off + a, (uint32_t)(b - a), e->keys.as<uint64_t>(),
                                   e->codes.as<uint64_t>(), e->rib_keys.as<uint64_t>(), e->rib_bits.as<uint8_t>(), p->max_trials,
-                                  &misc->err, misc->work, &misc->leaf_ctr, grid, s);
-            launches++;
+                                  &misc->err, misc->work, &misc->leaf_ctr, grid, st);
+        launches++;
+    };
+    if (pipelined) {
+        // Buckets in chunks: chunk c's split levels run on the engine stream, its leaves on the
+        // second stream as soon as those splits are done, overlapping the next chunk's splits.
+        // Node and leaf lists are in bucket order, so a chunk is a contiguous range of each list.
+        const int C = (int)std::max<uint64_t>(1, std::min<uint64_t>(nb, (uint64_t)e->pipe_chunks));
+        auto chunk_bounds = [&](const std::vector<uint32_t> &list, std::vector<uint64_t> &bounds) {
+            bounds.assign(C + 1, list.size());
+            bounds[0] = 0;
+            uint64_t j = 0;
+            for (int c = 1; c < C; c++) {
+                const uint64_t bucket_lo = nb * (uint64_t)c / C;
+                while (j < list.size() && plan.nodes[list[j]].bucket < bucket_lo) j++;
+                bounds[c] = j;
+            }
+        };
+        std::vector<std::vector<uint64_t>> lvb(plan.split_levels.size());
+        for (size_t lv = 0; lv < plan.split_levels.size(); lv++) chunk_bounds(plan.split_levels[lv], lvb[lv]);
+        std::vector<uint64_t> lb;
+        chunk_bounds(plan.leaves, lb);
+        for (int c = 0; c < C; c++) {
+            for (size_t lv = 0; lv < plan.split_levels.size(); lv++) split_range(lv, lvb[lv][c], lvb[lv][c + 1], s);
+            CU(cudaEventRecord(e->chunk_ev[c], s));
+            CU(cudaStreamWaitEvent(e->stream2, e->chunk_ev[c], 0));
+            leaf_range(lb[c], lb[c + 1], e->stream2, leaf_grid);
         }
+        CU(cudaEventRecord(e->ev[3], s));  // last split launch done
+        CU(cudaEventRecord(e->join_ev, e->stream2));
+        CU(cudaStreamWaitEvent(s, e->join_ev, 0));
+    } else {
+        for (size_t lv = 0; lv < plan.split_levels.size(); lv++) split_range(lv, 0, plan.split_levels[lv].size(), s);
+        CU(cudaEventRecord(e->ev[3], s));
+        if (p->mode == SHG_MODE_PER_LEAF)
+            for (uint32_t l = 0; l < nleaves; l++) leaf_range(l, l + 1, s, 1);
+        else
+            leaf_range(0, nleaves, s, leaf_grid);
     }
     CU(cudaGetLastError());
     CU(cudaEventRecord(e->ev[4], s));
@@ -400,6 +437,13 @@ shg_status shg_engine_create(int device, shg_engine **out) {
         return fail(SHG_ERR_CUDA, "stream creation failed");
     }
     for (auto &ev : e->ev) cudaEventCreate(&ev);
+    for (auto &ev : e->chunk_ev) cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&e->join_ev, cudaEventDisableTiming);
+    if (cudaStreamCreateWithFlags(&e->stream2, cudaStreamNonBlocking) != cudaSuccess) {
+        delete e;
+        return fail(SHG_ERR_CUDA, "stream creation failed");
+    }
+    if (const char *c = getenv("SHG_PIPE_CHUNKS")) e->pipe_chunks = std::max(1, std::min(shg_engine::kMaxChunks, atoi(c)));
     *out = e;
     return SHG_OK;
 }

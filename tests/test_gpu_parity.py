@@ -12,7 +12,7 @@ pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 BUILD_FIXTURES = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "sh*_*.npz"))
                         if "leaves" not in p)
-MODES = [shg.MODE_PERSISTENT, shg.MODE_LEVELS]
+MODES = [shg.MODE_DEFAULT, shg.MODE_LEVELS]
 
 
 def load(name):
@@ -40,12 +40,30 @@ def test_build_matches_golden(engine, name):
 def test_modes_identical(engine):
     g = load("sh2_l64_b2000")
     outs = [engine.build_hash128(2, 64, g["first"], g["second"], 2000, mode=m) for m in
-            (shg.MODE_PERSISTENT, shg.MODE_LEVELS, shg.MODE_PER_LEAF)]
+            (shg.MODE_DEFAULT, shg.MODE_LEVELS, shg.MODE_PER_LEAF, shg.MODE_PIPELINED)]
     for r in outs:
         assert_same(r, g)
     g = load("sh1_l30_b2000")
-    r = engine.build_hash128(1, 30, g["first"], g["second"], 2000, mode=shg.MODE_PER_LEAF)
-    assert_same(r, g)
+    for m in (shg.MODE_PER_LEAF, shg.MODE_LEVELS, shg.MODE_PIPELINED):
+        assert_same(engine.build_hash128(1, 30, g["first"], g["second"], 2000, mode=m), g)
+
+
+def test_pipelined_chunk_counts_identical(port):
+    # the bucket chunking of the pipelined schedule must not change any product
+    rng = np.random.default_rng(21)
+    n = 30000
+    f, s = rand_u64(rng, n), unique_u64(rng, n)
+    p = port.build_hash(2, 24, f, s, 700)
+    for chunks in ("1", "3", "64"):
+        os.environ["SHG_PIPE_CHUNKS"] = chunks
+        try:
+            eng = shg.Engine(0)
+        finally:
+            del os.environ["SHG_PIPE_CHUNKS"]
+        r = eng.build_hash128(2, 24, f, s, 700, mode=shg.MODE_PIPELINED)
+        assert np.array_equal(r.descriptors, p.desc) and np.array_equal(r.ribbon_bits, p.ribbon_bits), chunks
+        r.free()
+        eng.close()
 
 
 def test_sh2_leaves_match_golden(engine):
