@@ -163,6 +163,39 @@ uint64_t shg_mphf_bits(const shg_mphf *f);
 /* size(): number of keys. */
 uint64_t shg_mphf_size(const shg_mphf *f);
 
+/* ------------------------------------------------------------------ ShockHash2Flat<k>
+ * k-perfect "flat" variant (include/ShockHash2Flat.h:37-302): MurmurHash64 keys, two threshold
+ * layers of k-key buckets, a fallback ShockHash2<k> for bumped keys, one bipartite leaf search per
+ * bucket. k in 4..128. */
+typedef struct shg_flat_result {
+    uint64_t n, k, nbuckets, layers;
+    uint64_t layer_bases[3];           /* layerBases (ShockHash2Flat.h:49) */
+    uint32_t threshold_bits, seed_bits;
+    uint64_t *thresholds_and_seeds;    /* [nbuckets] seed << threshold_bits | compact threshold (:173-192) */
+    uint64_t nfallback_seeds;          /* seedsFallback (:48): buckets whose seed is 0 or >= 2^seed_bits */
+    uint64_t *fallback_seed_buckets;   /* ascending */
+    uint64_t *fallback_seeds;
+    uint64_t nfree;
+    uint64_t *free_positions;          /* freePositions (:71, 129-146) */
+    uint64_t nfallback_keys;           /* keys of the fallback PHF */
+    shg_result fallback;               /* ShockHash2<k>(to_string(mhc) of the bumped keys, 2000) (:124-128) */
+    uint64_t *ribbon_keys;             /* [ribbon_n] retrieval input (mhc, bit), bucket order (:159-170) */
+    uint8_t *ribbon_bits;
+    uint64_t ribbon_n;
+    double stage_ms[8];                /* hash, layers, fallback build, assign, leaves, copy-out, -, total */
+    void *owner;
+} shg_flat_result;
+shg_status shg_build_flat_strings(shg_engine *e, uint64_t k, const char *bytes, const uint64_t *offsets, uint64_t n,
+                                  shg_flat_result *out);
+void shg_flat_result_free(shg_flat_result *r);
+/* Query object: operator()(const string&) / operator()(uint64_t) and getBits() (ShockHash2Flat.h:236-277). */
+typedef struct shg_flat shg_flat;
+shg_status shg_flat_create(const shg_flat_result *r, shg_flat **out);
+void shg_flat_destroy(shg_flat *f);
+shg_status shg_flat_query_strings(const shg_flat *f, const char *bytes, const uint64_t *offsets, uint64_t n, uint64_t *out);
+shg_status shg_flat_query_hash(const shg_flat *f, const uint64_t *mhc, uint64_t n, uint64_t *out);
+uint64_t shg_flat_bits(const shg_flat *f);
+
 /* Golomb-Rice memo table of a configuration (ShockHash.h:121-127 / ShockHash2.h:106-115):
  * out[m] for m < 3000 packs golomb parameter << 27 | subtree nodes << 16 | subtree fixed bits. */
 shg_status shg_memo_table(int variant, int leaf_size, uint64_t *out);

@@ -144,6 +144,33 @@ class RefLib(_Lib):
         seed = self.lib.ref_sh2_leaf(m, _ptr(keys), _ptr(rk), _ptr(rb))
         return int(seed), rk, rb
 
+    def flat_build_strings(self, k, keys):
+        """ShockHash2Flat<k>(keys) (ShockHash2Flat.h:66-171); returns a dict of its internals."""
+        L = self.lib
+        L.ref_flat_build_strings.restype = _vp
+        L.ref_flat_build_strings.argtypes = [ctypes.c_int, ctypes.c_char_p, _vp, _sz]
+        L.ref_flat_bits.restype = ctypes.c_uint64
+        L.ref_flat_bits.argtypes = [_vp]
+        L.ref_flat_dump.argtypes = [_vp] + [_vp] * 8
+        L.ref_flat_query_strings.argtypes = [_vp, ctypes.c_char_p, _vp, _sz, _vp]
+        L.ref_flat_free.argtypes = [_vp]
+        data, offs = pack_strings(keys)
+        h = L.ref_flat_build_strings(k, data, _ptr(offs), len(keys))
+        if not h:
+            raise ValueError(f"k={k} not instantiated")
+        sizes = np.zeros(6, np.uint64)
+        L.ref_flat_dump(_vp(h), _ptr(sizes), *([_vp(0)] * 7))
+        lb, tas, fbb, fbs, fp = (np.zeros(int(sizes[i]), np.uint64) for i in (0, 1, 2, 2, 3))
+        rk, rb = np.zeros(int(sizes[4]), np.uint64), np.zeros(int(sizes[4]), np.uint8)
+        L.ref_flat_dump(_vp(h), _ptr(sizes), _ptr(lb), _ptr(tas), _ptr(fbb), _ptr(fbs), _ptr(fp), _ptr(rk), _ptr(rb))
+        q = np.zeros(len(keys), np.uint64)
+        L.ref_flat_query_strings(_vp(h), data, _ptr(offs), len(keys), _ptr(q))
+        out = dict(layer_bases=lb, thresholds_and_seeds=tas, fallback_buckets=fbb, fallback_seeds=fbs,
+                   free_positions=fp, ribbon_keys=rk, ribbon_bits=rb, layers=int(sizes[5]), query=q,
+                   bits=int(L.ref_flat_bits(_vp(h))))
+        L.ref_flat_free(_vp(h))
+        return out
+
     def sh1_leaf(self, leaf, keys, level=0):
         keys = np.ascontiguousarray(keys, dtype=np.uint64)
         m = len(keys)

@@ -177,6 +177,65 @@ uint64_t sh1_leaf(const uint64_t *keys, size_t m, int level, uint64_t *rkeys, ui
     return ((uint64_t)unary.at(0) << g) | fixed;
 }
 
+// ShockHash2Flat<k> (ShockHash2Flat.h:37-302): private members reached the same way.
+#define SHG_FLAT_KS(X) X(8) X(16) X(24) X(32) X(48) X(64) X(100)
+template <class C> using LayerTag = MemberTag<C, std::vector<size_t>, 10>;
+template <class C> using FallbackMapTag = MemberTag<C, std::map<size_t, size_t>, 11>;
+template <class C, size_t K> using FallbackPhfTag = MemberTag<C, shockhash::ShockHash2<K>, 12>;
+template <class C, size_t K> using FlatRibbonTag = MemberTag<C, RibbonOf<K>, 13>;
+template <class C> using FreeBvTag = MemberTag<C, pasta::BitVector, 14>;
+template <class C> using LayersTag = MemberTag<C, size_t, 15>;
+template <class C, size_t W> using TasTag = MemberTag<C, bytehamster::util::IntVector<W>, 16>;
+template <class C> using FlatNbTag = MemberTag<C, size_t, 17>;
+template <size_t K> struct FlatW {
+    static constexpr size_t TB = tlx::integer_log2_floor(K) - 1;
+    static constexpr size_t SB = std::ceil(0.442 * K - 0.2);
+    static constexpr size_t W = TB + SB;
+};
+#define X(K)                                                                                                            \
+    template struct Rob<LayerTag<shockhash::ShockHash2Flat<K>>, &shockhash::ShockHash2Flat<K>::layerBases>;             \
+    template struct Rob<FallbackMapTag<shockhash::ShockHash2Flat<K>>, &shockhash::ShockHash2Flat<K>::seedsFallback>;     \
+    template struct Rob<FallbackPhfTag<shockhash::ShockHash2Flat<K>, K>, &shockhash::ShockHash2Flat<K>::fallbackPhf>;   \
+    template struct Rob<FlatRibbonTag<shockhash::ShockHash2Flat<K>, K>, &shockhash::ShockHash2Flat<K>::ribbon>;         \
+    template struct Rob<FreeBvTag<shockhash::ShockHash2Flat<K>>, &shockhash::ShockHash2Flat<K>::freePositionsBv>;       \
+    template struct Rob<LayersTag<shockhash::ShockHash2Flat<K>>, &shockhash::ShockHash2Flat<K>::layers>;                \
+    template struct Rob<FlatNbTag<shockhash::ShockHash2Flat<K>>, &shockhash::ShockHash2Flat<K>::nbuckets>;              \
+    template struct Rob<TasTag<shockhash::ShockHash2Flat<K>, FlatW<K>::W>, &shockhash::ShockHash2Flat<K>::thresholdsAndSeeds>;
+SHG_FLAT_KS(X)
+#undef X
+
+struct FlatBase {
+    virtual ~FlatBase() {}
+    virtual uint64_t query_str(const char *p, size_t len) = 0;
+    virtual uint64_t bits() = 0;
+    virtual void dump(std::vector<uint64_t> &layer_bases, std::vector<uint64_t> &tas, std::vector<uint64_t> &fb_buckets,
+                      std::vector<uint64_t> &fb_seeds, std::vector<uint64_t> &free_positions,
+                      std::vector<std::pair<uint64_t, uint8_t>> &ribbon, RefBase *&fallback, uint64_t &layers) = 0;
+};
+template <size_t K> struct FlatRS : FlatBase {
+    using C = shockhash::ShockHash2Flat<K>;
+    C obj;
+    explicit FlatRS(std::span<const std::string> keys) : obj(keys) {}
+    uint64_t query_str(const char *p, size_t len) override { return obj(std::string(p, len)); }
+    uint64_t bits() override { return obj.getBits(); }
+    void dump(std::vector<uint64_t> &layer_bases, std::vector<uint64_t> &tas, std::vector<uint64_t> &fb_buckets,
+              std::vector<uint64_t> &fb_seeds, std::vector<uint64_t> &free_positions,
+              std::vector<std::pair<uint64_t, uint8_t>> &ribbon, RefBase *&fallback, uint64_t &layers) override {
+        for (size_t v : obj.*get(LayerTag<C>())) layer_bases.push_back(v);
+        auto &iv = obj.*get(TasTag<C, FlatW<K>::W>());
+        for (size_t i = 0; i < obj.*get(FlatNbTag<C>()); i++) tas.push_back(iv.at(i));
+        for (auto &kv : obj.*get(FallbackMapTag<C>())) { fb_buckets.push_back(kv.first); fb_seeds.push_back(kv.second); }
+        auto &bv = obj.*get(FreeBvTag<C>());
+        // freePositions[i] = (position of the i-th set bit) - i  (ShockHash2Flat.h:141-144)
+        for (size_t i = 0, ones = 0; i < bv.size(); i++)
+            if (bv[i]) { free_positions.push_back(i - ones); ones++; }
+        ribbon = (obj.*get(FlatRibbonTag<C, K>())).input;
+        fallback = nullptr;
+        layers = obj.*get(LayersTag<C>());
+        (void)fallback;
+    }
+};
+
 template <size_t L> void memo1(uint64_t *out) {
     static constexpr auto memo = shockhash::fill_golomb_rice<L>();  // evaluated at compile time, as ShockHash.h:145
     for (size_t i = 0; i < memo.size(); i++) out[i] = memo[i];
@@ -192,6 +251,52 @@ extern "C" {
 
 // The compile-time Golomb-Rice memo table (3000 entries) of ShockHash<leaf> (variant 1) or
 // ShockHash2<leaf> (variant 2). Returns 0 when the leaf size is not instantiated here.
+void *ref_flat_build_strings(int k, const char *bytes, const uint64_t *offsets, size_t n) {
+    auto keys = make_strings(bytes, offsets, n);
+    switch (k) {
+#define X(K) case K: return new FlatRS<K>(std::span<const std::string>(keys));
+        SHG_FLAT_KS(X)
+#undef X
+        default: return nullptr;
+    }
+}
+void ref_flat_free(void *h) { delete (FlatBase *)h; }
+uint64_t ref_flat_sizeof(int k) {
+    switch (k) {
+#define X(K) case K: return sizeof(shockhash::ShockHash2Flat<K>);
+        SHG_FLAT_KS(X)
+#undef X
+        default: return 0;
+    }
+}
+uint64_t ref_sizeof(int variant, int leaf) {
+    if (variant == 1) return sizeof(shockhash::ShockHash<30, false>);
+    return sizeof(shockhash::ShockHash2<64>);
+}
+uint64_t ref_flat_bits(void *h) { return ((FlatBase *)h)->bits(); }
+void ref_flat_query_strings(void *h, const char *bytes, const uint64_t *offsets, size_t n, uint64_t *out) {
+    auto *f = (FlatBase *)h;
+    for (size_t i = 0; i < n; i++) out[i] = f->query_str(bytes + offsets[i], offsets[i + 1] - offsets[i]);
+}
+// Sizes first (sizes[0..5] = layer bases, buckets, fallback map, free positions, ribbon, layers),
+// then the arrays when the pointers are non-null.
+void ref_flat_dump(void *h, uint64_t *sizes, uint64_t *layer_bases, uint64_t *tas, uint64_t *fb_buckets,
+                   uint64_t *fb_seeds, uint64_t *free_positions, uint64_t *rkeys, uint8_t *rbits) {
+    std::vector<uint64_t> lb, t, fbb, fbs, fp;
+    std::vector<std::pair<uint64_t, uint8_t>> rb;
+    RefBase *fb = nullptr;
+    uint64_t layers = 0;
+    ((FlatBase *)h)->dump(lb, t, fbb, fbs, fp, rb, fb, layers);
+    sizes[0] = lb.size(); sizes[1] = t.size(); sizes[2] = fbb.size(); sizes[3] = fp.size(); sizes[4] = rb.size();
+    sizes[5] = layers;
+    if (layer_bases) std::memcpy(layer_bases, lb.data(), lb.size() * 8);
+    if (tas) std::memcpy(tas, t.data(), t.size() * 8);
+    if (fb_buckets) std::memcpy(fb_buckets, fbb.data(), fbb.size() * 8);
+    if (fb_seeds) std::memcpy(fb_seeds, fbs.data(), fbs.size() * 8);
+    if (free_positions) std::memcpy(free_positions, fp.data(), fp.size() * 8);
+    if (rkeys) for (size_t i = 0; i < rb.size(); i++) { rkeys[i] = rb[i].first; rbits[i] = rb[i].second; }
+}
+
 int ref_memo(int variant, int leaf, uint64_t *out) {
     if (variant == 1) {
         switch (leaf) {

@@ -20,7 +20,7 @@ import os
 
 import numpy as np
 
-__all__ = ["ShgError", "Engine", "BuildResult", "ShockHash", "ShockHash2", "lib", "LIB_PATH",
+__all__ = ["ShgError", "Engine", "BuildResult", "ShockHash", "ShockHash2", "ShockHash2Flat", "lib", "LIB_PATH",
            "SHOCKHASH", "SHOCKHASH2", "MODE_DEFAULT", "MODE_LEVELS", "MODE_PER_LEAF",
            "MODE_PIPELINED"]
 
@@ -53,6 +53,18 @@ class _Result(ctypes.Structure):
                 ("desc_bits", ctypes.c_uint64), ("ribbon_keys", ctypes.POINTER(ctypes.c_uint64)),
                 ("ribbon_bits", ctypes.POINTER(ctypes.c_uint8)), ("ribbon_n", ctypes.c_uint64),
                 ("stage_ms", ctypes.c_double * 8), ("work", ctypes.c_uint64 * 8), ("owner", ctypes.c_void_p)]
+
+
+class _FlatResult(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_uint64), ("k", ctypes.c_uint64), ("nbuckets", ctypes.c_uint64), ("layers", ctypes.c_uint64),
+                ("layer_bases", ctypes.c_uint64 * 3), ("threshold_bits", ctypes.c_uint32), ("seed_bits", ctypes.c_uint32),
+                ("thresholds_and_seeds", ctypes.POINTER(ctypes.c_uint64)), ("nfallback_seeds", ctypes.c_uint64),
+                ("fallback_seed_buckets", ctypes.POINTER(ctypes.c_uint64)),
+                ("fallback_seeds", ctypes.POINTER(ctypes.c_uint64)), ("nfree", ctypes.c_uint64),
+                ("free_positions", ctypes.POINTER(ctypes.c_uint64)), ("nfallback_keys", ctypes.c_uint64),
+                ("fallback", _Result), ("ribbon_keys", ctypes.POINTER(ctypes.c_uint64)),
+                ("ribbon_bits", ctypes.POINTER(ctypes.c_uint8)), ("ribbon_n", ctypes.c_uint64),
+                ("stage_ms", ctypes.c_double * 8), ("owner", ctypes.c_void_p)]
 
 
 _lib = None
@@ -91,6 +103,13 @@ def lib():
         "shg_mphf_bits": ([_vp], _u64),
         "shg_mphf_size": ([_vp], _u64),
         "shg_sh2_construct_leaves_noalloc": ([_vp, _vp, _u64, _vp, _vp, _vp], ctypes.c_int),
+        "shg_build_flat_strings": ([_vp, _u64, ctypes.c_char_p, _vp, _u64, ctypes.POINTER(_FlatResult)], ctypes.c_int),
+        "shg_flat_result_free": ([ctypes.POINTER(_FlatResult)], None),
+        "shg_flat_create": ([ctypes.POINTER(_FlatResult), ctypes.POINTER(_vp)], ctypes.c_int),
+        "shg_flat_destroy": ([_vp], None),
+        "shg_flat_query_strings": ([_vp, ctypes.c_char_p, _vp, _u64, _vp], ctypes.c_int),
+        "shg_flat_query_hash": ([_vp, _vp, _u64, _vp], ctypes.c_int),
+        "shg_flat_bits": ([_vp], _u64),
         "shg_keys_mt19937_64": ([_u64, _u64, _vp], None),
         "shg_int_peak": ([ctypes.c_int, _u64, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)],
                          ctypes.c_int),
@@ -244,6 +263,13 @@ class Engine:
         st = lib().shg_build_strings(self._h, ctypes.byref(p), data, _ptr(offs), len(offs) - 1, ctypes.byref(res))
         return self._finish(p, st, res, query)
 
+    def build_flat_strings(self, k, keys):
+        """ShockHash2Flat<k>(keys) on the device (include/ShockHash2Flat.h:66-171)."""
+        data, offs = pack_strings(keys)
+        res = _FlatResult()
+        _check(lib().shg_build_flat_strings(self._h, k, data, _ptr(offs), len(offs) - 1, ctypes.byref(res)))
+        return FlatBuild(res, self)
+
     def hash_strings(self, keys):
         data, offs = pack_strings(keys)
         n = len(offs) - 1
@@ -271,6 +297,60 @@ class Engine:
         _check(lib().shg_sh1_construct_leaves(self._h, _ptr(keys), _ptr(offs), nl, level, _ptr(codes), _ptr(kc),
                                               _ptr(bits)))
         return codes[:nl], kc[:len(keys)], bits[:len(keys)]
+
+
+class FlatBuild:
+    """Products of a ShockHash2Flat<k> build (views of the engine's pinned block) plus its query
+    object: ``query_strings(keys)`` is operator()(const string&), ``bits()`` getBits()."""
+
+    def __init__(self, res, engine):
+        self._res, self._engine = res, engine
+        v = np.ctypeslib.as_array
+        self.n, self.k, self.nbuckets, self.layers = res.n, res.k, res.nbuckets, res.layers
+        self.layer_bases = np.array(list(res.layer_bases)[:res.layers + 1], np.uint64)
+        nb = max(res.nbuckets, 1)
+        self.thresholds_and_seeds = v(res.thresholds_and_seeds, (nb,))[:res.nbuckets]
+        nfs = max(res.nfallback_seeds, 1)
+        self.fallback_seed_buckets = v(res.fallback_seed_buckets, (nfs,))[:res.nfallback_seeds]
+        self.fallback_seeds = v(res.fallback_seeds, (nfs,))[:res.nfallback_seeds]
+        self.free_positions = v(res.free_positions, (max(res.nfree, 1),))[:res.nfree]
+        rn = max(res.ribbon_n, 1)
+        self.ribbon_keys = v(res.ribbon_keys, (rn,))[:res.ribbon_n]
+        self.ribbon_bits = v(res.ribbon_bits, (rn,))[:res.ribbon_n]
+        self.nfallback_keys = res.nfallback_keys
+        self.stage_ms = list(res.stage_ms)
+        h = _vp()
+        _check(lib().shg_flat_create(ctypes.byref(res), ctypes.byref(h)))
+        self._q = h
+
+    def query_strings(self, keys):
+        data, offs = pack_strings(keys)
+        out = np.zeros(len(offs) - 1, np.uint64)
+        _check(lib().shg_flat_query_strings(self._q, data, _ptr(offs), len(offs) - 1, _ptr(out)))
+        return out
+
+    def query_hash(self, mhc):
+        mhc = np.ascontiguousarray(mhc, dtype=np.uint64)
+        out = np.zeros(len(mhc), np.uint64)
+        _check(lib().shg_flat_query_hash(self._q, _ptr(mhc), len(mhc), _ptr(out)))
+        return out
+
+    def bits(self):
+        return int(lib().shg_flat_bits(self._q))
+
+    def free(self):
+        if getattr(self, "_q", None):
+            lib().shg_flat_destroy(self._q)
+            self._q = None
+        if self._res is not None:
+            lib().shg_flat_result_free(ctypes.byref(self._res))
+            self._res = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
 
 
 class _Mphf:
@@ -371,3 +451,31 @@ class ShockHash(_RecSplitBase, metaclass=_Templated):
 class ShockHash2(_RecSplitBase, metaclass=_Templated):
     """shockhash::ShockHash2<LEAF_SIZE> (include/ShockHash2.h:117); use ShockHash2[l](keys, b)."""
     VARIANT = SHOCKHASH2
+
+
+class ShockHash2Flat(metaclass=_Templated):
+    """shockhash::ShockHash2Flat<k> (include/ShockHash2Flat.h:37); use ShockHash2Flat[k](keys).
+
+    The two extra constructor arguments of the reference (ShockHash2Flat.h:60-64) are accepted and
+    ignored, as there."""
+    LEAF = None
+
+    def __init__(self, keys, ignore=0, ignore2=0, engine=None):
+        if self.LEAF is None:
+            raise TypeError("pick k first, e.g. ShockHash2Flat[100](keys)")
+        self.result = (engine or default_engine()).build_flat_strings(self.LEAF, keys)
+        self.keys_count = self.result.n
+
+    def __call__(self, key):
+        if isinstance(key, int):
+            return int(self.result.query_hash(np.array([key], np.uint64))[0])
+        return int(self.result.query_strings([key])[0])
+
+    def query_many(self, keys):
+        return self.result.query_strings(keys)
+
+    def getBits(self):
+        return self.result.bits()
+
+    def size(self):
+        return self.keys_count

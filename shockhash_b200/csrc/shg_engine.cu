@@ -94,6 +94,10 @@ struct shg_engine {
     cudaStream_t stream = nullptr;
     DevBuf in_keys, in_bytes, in_offsets, first, second, sfirst, sidx, counts, cursor, acc, keys, nodes, ids, codes,
         fixed_off, bnb, bucket_bits, pos_acc, words, rib_keys, rib_bits, skip_bits, scratch, misc, singles, ckeys, cbits;
+    // ShockHash2Flat state kept across its nested fallback build
+    DevBuf f_bytes, f_offs, f_mhc0, f_cur, f_sorted, f_next, f_thr, f_counts, f_cursor, f_acc, f_free_cnt, f_bump_cnt,
+        f_first, f_free_off, f_bump_off, f_free_out, f_bucket, f_last, f_list, f_slot, f_leaf_keys, f_nodes, f_ids, f_codes,
+        f_bits, f_mapping, f_lb, f_tmp, f_tmp2;
     cudaEvent_t ev[8] = {};
     cudaStream_t stream2 = nullptr;  // leaves of the pipelined mode
     static constexpr int kMaxChunks = 64;
@@ -103,7 +107,10 @@ struct shg_engine {
     ~shg_engine() {
         DevBuf *all[] = {&in_keys, &in_bytes, &in_offsets, &first, &second, &sfirst, &sidx, &counts, &cursor,
                          &acc, &keys, &nodes, &ids, &codes, &fixed_off, &bnb, &bucket_bits, &pos_acc, &words,
-                         &rib_keys, &rib_bits, &skip_bits, &scratch, &misc, &singles, &ckeys, &cbits};
+                         &rib_keys, &rib_bits, &skip_bits, &scratch, &misc, &singles, &ckeys, &cbits, &f_bytes, &f_offs,
+                         &f_mhc0, &f_cur, &f_sorted, &f_next, &f_thr, &f_counts, &f_cursor, &f_acc, &f_free_cnt,
+                         &f_bump_cnt, &f_first, &f_free_off, &f_bump_off, &f_free_out, &f_bucket, &f_last, &f_list,
+                         &f_slot, &f_leaf_keys, &f_nodes, &f_ids, &f_codes, &f_bits, &f_mapping, &f_lb, &f_tmp, &f_tmp2};
         for (DevBuf *b : all) b->release();
         for (PinnedBlock *b : pool) {
             if (b->p) cudaFreeHost(b->p);
@@ -118,6 +125,8 @@ struct shg_engine {
         if (stream) cudaStreamDestroy(stream);
     }
 };
+
+shg_status hash_strings_into(shg_engine *e, const char *bytes, const uint64_t *offsets, uint64_t n, float &ms);
 
 namespace {
 
@@ -415,6 +424,287 @@ shg_status build_core(shg_engine *e, const shg_params *p, const uint64_t *d_firs
     return SHG_OK;
 }
 
+extern "C" shg_status shg_mphf_create(const shg_params *p, shg_result *r, shg_mphf **out);
+extern "C" void shg_mphf_destroy(shg_mphf *f);
+extern "C" shg_status shg_mphf_query_strings(const shg_mphf *f, const char *bytes, const uint64_t *offsets, uint64_t n,
+                                             uint64_t *out);
+
+// ------------------------------------------------------------------ ShockHash2Flat<k>
+double ms_since(std::chrono::steady_clock::time_point t) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
+}
+
+shg_status build_flat(shg_engine *e, uint64_t k, const char *bytes, const uint64_t *offsets, uint64_t n,
+                      shg_flat_result *out) {
+    using clk = std::chrono::steady_clock;
+    const auto t_start = clk::now();
+    cudaStream_t s = e->stream;
+    const FlatConsts fc = flat_consts((uint32_t)k);
+    memset(out, 0, sizeof(*out));
+    out->n = n;
+    out->k = k;
+    out->threshold_bits = fc.threshold_bits;
+    out->seed_bits = fc.seed_bits;
+    const uint64_t nbuckets = n / k;                   // ShockHash2Flat.h:68
+    const uint64_t keys_in_end_bucket = n - nbuckets * k;
+    out->nbuckets = nbuckets;
+    CU(e->misc.ensure(sizeof(Misc)));
+    Misc *misc = e->misc.as<Misc>();
+    CU(cudaMemsetAsync(misc, 0, sizeof(Misc), s));
+
+    // ---- MurmurHash64 of every key
+    const uint64_t nbytes = n ? offsets[n] : 0;
+    const uint64_t nn = std::max<uint64_t>(n, 1);
+    CU(e->f_bytes.ensure(std::max<uint64_t>(nbytes, 1)));
+    CU(e->f_offs.ensure((n + 1) * 8));
+    CU(e->f_mhc0.ensure(nn * 8));
+    CU(e->f_cur.ensure(nn * 8));
+    CU(e->f_sorted.ensure(nn * 8));
+    CU(e->f_next.ensure(nn * 8));
+    CU(e->f_thr.ensure(std::max<uint64_t>(nbuckets, 1)));
+    CU(e->f_mapping.ensure(fc.threshold_range * 4 + 4));
+    CU(e->f_lb.ensure(4 * 8));
+    if (nbytes) CU(cudaMemcpyAsync(e->f_bytes.p, bytes, nbytes, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(e->f_offs.p, offsets, (n + 1) * 8, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(e->f_mapping.p, fc.mapping.data(), fc.threshold_range * 4, cudaMemcpyHostToDevice, s));
+    CU(cudaMemsetAsync(e->f_thr.p, 0, std::max<uint64_t>(nbuckets, 1), s));  // thresholdsAndSeeds starts zeroed
+    flat_launch_murmur(e->f_bytes.as<uint8_t>(), e->f_offs.as<uint64_t>(), n, e->f_mhc0.as<uint64_t>(), s);
+    if (n) CU(cudaMemcpyAsync(e->f_cur.p, e->f_mhc0.p, n * 8, cudaMemcpyDeviceToDevice, s));
+    CU(cudaStreamSynchronize(s));
+    out->stage_ms[0] = ms_since(t_start);
+    auto t = clk::now();
+
+    // ---- threshold layers (ShockHash2Flat.h:86-122)
+    std::vector<uint64_t> layer_bases{0};
+    std::vector<uint64_t> free_positions;
+    uint64_t layers = 2, cur_n = n;
+    uint64_t buckets_this_layer = (uint64_t)std::ceil(0.9 * (double)nbuckets);  // :70
+    if (buckets_this_layer == 0) layers = 0;
+    for (uint64_t layer = 0; layer < layers; layer++) {
+        const uint64_t base = layer_bases.back();
+        if (layer != 0) {
+            buckets_this_layer = (uint64_t)(0.9 * (double)(cur_n / k));  // :89-90
+            buckets_this_layer = std::min(buckets_this_layer, nbuckets - base);
+            if (buckets_this_layer == 0) {
+                layers = 1;
+                break;
+            }
+        }
+        const uint32_t B = (uint32_t)buckets_this_layer;
+        layer_bases.push_back(base + B);
+        CU(e->f_counts.ensure(B * 4ull));
+        CU(e->f_cursor.ensure(B * 4ull));
+        CU(e->f_acc.ensure((B + 1ull) * 8));
+        CU(e->f_free_cnt.ensure(B * 8ull));
+        CU(e->f_bump_cnt.ensure(B * 8ull));
+        CU(e->f_first.ensure(B * 4ull));
+        CU(e->f_free_off.ensure((B + 1ull) * 8));
+        CU(e->f_bump_off.ensure((B + 1ull) * 8));
+        flat_launch_count(e->f_cur.as<uint64_t>(), cur_n, B, layer != 0, e->f_counts.as<uint32_t>(), s);
+        launch_scan_counts(e->f_counts.as<uint32_t>(), B, e->f_acc.as<uint64_t>(), e->f_cursor.as<uint32_t>(), &misc->maxsz, s);
+        flat_launch_scatter(e->f_cur.as<uint64_t>(), cur_n, B, e->f_cursor.as<uint32_t>(), e->f_sorted.as<uint64_t>(), s);
+        flat_launch_sort_flush(e->f_sorted.as<uint64_t>(), e->f_acc.as<uint64_t>(), B, (uint32_t)k, e->f_mapping.as<uint32_t>(),
+                               fc.threshold_range, base, e->f_thr.as<uint8_t>(), e->f_free_cnt.as<uint64_t>(),
+                               e->f_bump_cnt.as<uint64_t>(), e->f_first.as<uint32_t>(), &misc->err, s);
+        launch_scan_u64(e->f_free_cnt.as<uint64_t>(), B, e->f_free_off.as<uint64_t>(), s);
+        launch_scan_u64(e->f_bump_cnt.as<uint64_t>(), B, e->f_bump_off.as<uint64_t>(), s);
+        uint64_t tot[2];
+        CU(cudaMemcpyAsync(&tot[0], e->f_free_off.as<uint64_t>() + B, 8, cudaMemcpyDeviceToHost, s));
+        CU(cudaMemcpyAsync(&tot[1], e->f_bump_off.as<uint64_t>() + B, 8, cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        CU(e->f_free_out.ensure(std::max<uint64_t>(tot[0], 1) * 8));
+        flat_launch_emit(e->f_sorted.as<uint64_t>(), e->f_acc.as<uint64_t>(), B, base, e->f_free_cnt.as<uint64_t>(),
+                         e->f_free_off.as<uint64_t>(), e->f_bump_cnt.as<uint64_t>(), e->f_bump_off.as<uint64_t>(),
+                         e->f_first.as<uint32_t>(), e->f_free_out.as<uint64_t>(), e->f_next.as<uint64_t>(), s);
+        const size_t old = free_positions.size();
+        free_positions.resize(old + tot[0]);
+        if (tot[0]) CU(cudaMemcpyAsync(free_positions.data() + old, e->f_free_out.p, tot[0] * 8, cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        std::swap(e->f_cur, e->f_next);
+        cur_n = tot[1];
+    }
+    uint32_t err0 = 0;
+    CU(cudaMemcpy(&err0, &misc->err, 4, cudaMemcpyDeviceToHost));
+    if (err0) return fail(SHG_ERR_BUCKET, "a threshold-layer bucket holds more than 1024 keys");
+    out->layers = layers;
+    for (size_t i = 0; i < layer_bases.size() && i < 3; i++) out->layer_bases[i] = layer_bases[i];
+    out->stage_ms[1] = ms_since(t);
+    t = clk::now();
+
+    // ---- fallback PHF over the keys bumped from the last layer (:124-128)
+    std::vector<uint64_t> bumped(cur_n);
+    if (cur_n) CU(cudaMemcpy(bumped.data(), e->f_cur.p, cur_n * 8, cudaMemcpyDeviceToHost));
+    std::string fb_bytes;
+    std::vector<uint64_t> fb_offs{0};
+    for (uint64_t h : bumped) {
+        fb_bytes += std::to_string(h);
+        fb_offs.push_back(fb_bytes.size());
+    }
+    out->nfallback_keys = cur_n;
+    shg_params fp{SHG_SHOCKHASH2, (int)k, 2000, SHG_MODE_DEFAULT, 0};
+    {
+        float hms = 0;
+        shg_status st = hash_strings_into(e, fb_bytes.data(), fb_offs.data(), cur_n, hms);
+        if (st) return st;
+        st = build_core(e, &fp, e->first.as<uint64_t>(), e->second.as<uint64_t>(), cur_n, &out->fallback, hms);
+        if (st) return st;
+    }
+    shg_mphf *fbq = nullptr;
+    {
+        shg_status st = shg_mphf_create(&fp, &out->fallback, &fbq);
+        if (st) return fail(st, "fallback query object");
+    }
+    // free positions of the fallback keys (:129-139)
+    const uint64_t additional = cur_n - free_positions.size();
+    const uint64_t handled = layer_bases.back();
+    {
+        uint64_t i = 0;
+        for (; i < additional - keys_in_end_bucket; i++) free_positions.push_back(handled + i / k);
+        for (; i < additional; i++) free_positions.push_back(nbuckets + i);
+    }
+    out->stage_ms[2] = ms_since(t);
+    t = clk::now();
+
+    // ---- every key's bucket (evaluateKPerfect), fallback keys through the fallback PHF
+    CU(e->f_bucket.ensure(nn * 8));
+    CU(e->f_last.ensure(nn * 8));
+    CU(e->f_list.ensure(nn * 8));
+    CU(cudaMemcpyAsync(e->f_lb.p, layer_bases.data(), layer_bases.size() * 8, cudaMemcpyHostToDevice, s));
+    flat_launch_assign(e->f_mhc0.as<uint64_t>(), n, (uint32_t)layers, e->f_lb.as<uint64_t>(), e->f_thr.as<uint8_t>(),
+                       e->f_mapping.as<uint32_t>(), e->f_bucket.as<uint64_t>(), e->f_last.as<uint64_t>(), s);
+    unsigned long long *cnt = &misc->work[7];
+    flat_launch_fallback_list(e->f_bucket.as<uint64_t>(), n, cnt, e->f_list.as<uint64_t>(), s);
+    unsigned long long nfb = 0;
+    CU(cudaMemcpyAsync(&nfb, cnt, 8, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    if (nfb) {
+        std::vector<uint64_t> idx(nfb), last(nfb), vals(nfb);
+        CU(cudaMemcpy(idx.data(), e->f_list.p, nfb * 8, cudaMemcpyDeviceToHost));
+        std::sort(idx.begin(), idx.end());
+        // re-mixed hashes of the fallback keys, gathered on the device
+        CU(e->f_tmp.ensure(nfb * 8));
+        CU(e->f_tmp2.ensure(nfb * 8));
+        CU(cudaMemcpyAsync(e->f_tmp.p, idx.data(), nfb * 8, cudaMemcpyHostToDevice, s));
+        flat_launch_gather(e->f_tmp.as<uint64_t>(), e->f_last.as<uint64_t>(), nfb, e->f_tmp2.as<uint64_t>(), s);
+        CU(cudaMemcpyAsync(last.data(), e->f_tmp2.p, nfb * 8, cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        std::string qb;
+        std::vector<uint64_t> qo{0};
+        for (uint64_t h : last) {
+            qb += std::to_string(h);
+            qo.push_back(qb.size());
+        }
+        std::vector<uint64_t> phf(nfb);
+        shg_status st = shg_mphf_query_strings(fbq, qb.data(), qo.data(), nfb, phf.data());
+        if (st) return fail(st, "fallback query");
+        for (uint64_t j = 0; j < nfb; j++) {
+            if (phf[j] >= free_positions.size()) return fail(SHG_ERR_CUDA, "fallback value outside the free positions");
+            const uint64_t b = free_positions[phf[j]];  // select1(phf + 1) - phf (:295)
+            vals[j] = b < nbuckets ? b : ~1ull;         // keys past the last full bucket are not searched
+        }
+        CU(cudaMemcpyAsync(e->f_tmp2.p, vals.data(), nfb * 8, cudaMemcpyHostToDevice, s));
+        flat_launch_set_buckets(e->f_tmp.as<uint64_t>(), e->f_tmp2.as<uint64_t>(), nfb, e->f_bucket.as<uint64_t>(), s);
+    }
+    shg_mphf_destroy(fbq);
+    // keys grouped k per bucket, input order inside a bucket (:149-158)
+    const uint64_t leaf_n = nbuckets * k;
+    CU(e->f_slot.ensure(std::max<uint64_t>(leaf_n, 1) * 4));
+    CU(e->f_leaf_keys.ensure(std::max<uint64_t>(leaf_n, 1) * 8));
+    CU(e->f_cursor.ensure(std::max<uint64_t>(nbuckets, 1) * 4));
+    flat_launch_group(e->f_bucket.as<uint64_t>(), n, nbuckets, (uint32_t)k, e->f_cursor.as<uint32_t>(), e->f_slot.as<uint32_t>(),
+                      e->f_mhc0.as<uint64_t>(), e->f_leaf_keys.as<uint64_t>(), &misc->err, s);
+    out->stage_ms[3] = ms_since(t);
+    t = clk::now();
+
+    // ---- one bipartite leaf search per bucket (:160-168)
+    std::vector<Node> nodes(nbuckets);
+    std::vector<uint32_t> ids(nbuckets);
+    const Config &c2 = config_of(SHG_SHOCKHASH2, kMaxLeaf2);
+    for (uint64_t b = 0; b < nbuckets; b++) {
+        Node &nd = nodes[b];
+        memset(&nd, 0, sizeof nd);
+        nd.start = (uint32_t)(b * k);
+        nd.m = (uint16_t)k;
+        nd.kind = kLeaf;
+        nd.g = (uint8_t)c2.golomb((uint32_t)k);
+        ids[b] = (uint32_t)b;
+    }
+    CU(e->f_nodes.ensure(std::max<uint64_t>(nbuckets, 1) * sizeof(Node)));
+    CU(e->f_ids.ensure(std::max<uint64_t>(nbuckets, 1) * 4));
+    CU(e->f_codes.ensure(std::max<uint64_t>(nbuckets, 1) * 8));
+    CU(e->f_bits.ensure(std::max<uint64_t>(leaf_n, 1)));
+    if (nbuckets) {
+        CU(cudaMemcpyAsync(e->f_nodes.p, nodes.data(), nbuckets * sizeof(Node), cudaMemcpyHostToDevice, s));
+        CU(cudaMemcpyAsync(e->f_ids.p, ids.data(), nbuckets * 4, cudaMemcpyHostToDevice, s));
+        const uint32_t smax = k > 64 ? 16384 : 4096, cmax = k > 64 ? 16384 : 2048;
+        const uint64_t per_warp = (sh2_scratch_bytes(smax, cmax) + 255) & ~255ull;
+        const int bps = std::max(1, std::min(8, (228 * 1024) / (4 * sh2_smem_per_warp((int)k) + 1024)));
+        const int grid = std::max(1, std::min<int>(e->sms * bps, (int)((nbuckets + 3) / 4)));
+        CU(e->scratch.ensure(per_warp * (uint64_t)grid * 4));
+        launch_leaves_sh2_ctr(e->f_nodes.as<Node>(), e->f_ids.as<uint32_t>(), (uint32_t)nbuckets, e->f_leaf_keys.as<uint64_t>(),
+                              e->f_codes.as<uint64_t>(), e->f_bits.as<uint8_t>(), e->scratch.as<uint8_t>(), per_warp, smax, cmax,
+                              &misc->err, misc->work, &misc->leaf_ctr, grid, s, (int)k);
+        CU(cudaGetLastError());
+    }
+    uint32_t err = 0;
+    CU(cudaMemcpyAsync(&err, &misc->err, 4, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    if (err & kErrInternal) return fail(SHG_ERR_CUDA, "a bucket did not receive exactly k keys");
+    if (err) return fail(SHG_ERR_TRIAL_LIMIT, "a bucket's leaf search exceeded its capacity (duplicate keys?)");
+    out->stage_ms[4] = ms_since(t);
+    t = clk::now();
+
+    // ---- products: packed thresholds and seeds, seed fallback map, free positions, retrieval input
+    std::vector<uint64_t> seeds(nbuckets);
+    std::vector<uint8_t> thr(nbuckets);
+    if (nbuckets) {
+        CU(cudaMemcpyAsync(seeds.data(), e->f_codes.p, nbuckets * 8, cudaMemcpyDeviceToHost, s));
+        CU(cudaMemcpyAsync(thr.data(), e->f_thr.p, nbuckets, cudaMemcpyDeviceToHost, s));
+    }
+    CU(cudaStreamSynchronize(s));
+    std::vector<uint64_t> fbb, fbs;
+    const uint64_t max_seed = fc.seed_bits >= 64 ? ~0ull : (1ull << fc.seed_bits);
+    const size_t block_bytes = nbuckets * 8 + 2 * nbuckets * 8 + free_positions.size() * 8 + leaf_n * 9 + 256;
+    PinnedBlock *blk = acquire_pinned(e, block_bytes);
+    if (!blk) return fail(SHG_ERR_OOM, "pinned host allocation failed");
+    uint8_t *hp = (uint8_t *)blk->p;
+    out->owner = blk;
+    out->thresholds_and_seeds = (uint64_t *)hp;
+    hp += nbuckets * 8;
+    for (uint64_t b = 0; b < nbuckets; b++) {
+        uint64_t sd = seeds[b];
+        if (sd >= max_seed || sd == 0) {  // :163-166
+            fbb.push_back(b);
+            fbs.push_back(sd);
+            sd = 0;
+        }
+        out->thresholds_and_seeds[b] = sd << fc.threshold_bits | thr[b];
+    }
+    out->nfallback_seeds = fbb.size();
+    out->fallback_seed_buckets = (uint64_t *)hp;
+    memcpy(hp, fbb.data(), fbb.size() * 8);
+    hp += nbuckets * 8;
+    out->fallback_seeds = (uint64_t *)hp;
+    memcpy(hp, fbs.data(), fbs.size() * 8);
+    hp += nbuckets * 8;
+    out->nfree = free_positions.size();
+    out->free_positions = (uint64_t *)hp;
+    memcpy(hp, free_positions.data(), free_positions.size() * 8);
+    hp += free_positions.size() * 8;
+    out->ribbon_n = leaf_n;
+    out->ribbon_keys = (uint64_t *)hp;
+    hp += leaf_n * 8;
+    out->ribbon_bits = hp;
+    if (leaf_n) {
+        CU(cudaMemcpyAsync(out->ribbon_keys, e->f_leaf_keys.p, leaf_n * 8, cudaMemcpyDeviceToHost, s));
+        CU(cudaMemcpyAsync(out->ribbon_bits, e->f_bits.p, leaf_n, cudaMemcpyDeviceToHost, s));
+    }
+    CU(cudaStreamSynchronize(s));
+    out->stage_ms[5] = ms_since(t);
+    out->stage_ms[7] = ms_since(t_start);
+    return SHG_OK;
+}
+
 } // namespace
 
 extern "C" {
@@ -520,6 +810,10 @@ shg_status shg_build_u64(shg_engine *e, const shg_params *p, const uint64_t *key
 }
 
 static shg_status hash_strings_dev(shg_engine *e, const char *bytes, const uint64_t *offsets, uint64_t n, float &ms) {
+    return hash_strings_into(e, bytes, offsets, n, ms);
+}
+}  // extern "C"
+shg_status hash_strings_into(shg_engine *e, const char *bytes, const uint64_t *offsets, uint64_t n, float &ms) {
     const uint64_t nbytes = n ? offsets[n] : 0;
     CU(e->in_bytes.ensure(std::max<uint64_t>(nbytes, 1)));
     CU(e->in_offsets.ensure((n + 1) * 8));
@@ -542,6 +836,7 @@ static shg_status hash_strings_dev(shg_engine *e, const char *bytes, const uint6
     return SHG_OK;
 }
 
+extern "C" {
 shg_status shg_build_strings(shg_engine *e, const shg_params *p, const char *bytes, const uint64_t *offsets, uint64_t n,
                              shg_result *out) {
     if (!e || !out || !offsets || (n && !bytes)) return fail(SHG_ERR_ARG, "null argument");
@@ -684,6 +979,30 @@ shg_status shg_sh1_construct_leaves(shg_engine *e, const uint64_t *keys, const u
     CU(cudaStreamSynchronize(s));
     if (err) return fail(SHG_ERR_TRIAL_LIMIT, "leaf search failed (error flags " + std::to_string(err) + ")");
     return SHG_OK;
+}
+
+shg_status shg_build_flat_strings(shg_engine *e, uint64_t k, const char *bytes, const uint64_t *offsets, uint64_t n,
+                                  shg_flat_result *out) {
+    if (!e || !out || !offsets || (n && !bytes)) return fail(SHG_ERR_ARG, "null argument");
+    if (k < 4 || k > (uint64_t)kMaxLeaf2) return fail(SHG_ERR_ARG, "ShockHash2Flat needs 4 <= k <= 128");
+    if (n >= (1ull << 32)) return fail(SHG_ERR_ARG, "at most 2^32 - 1 keys per build");
+    CU(cudaSetDevice(e->device));
+    shg_status st = build_flat(e, k, bytes, offsets, n, out);
+    if (st) shg_flat_result_free(out);
+    return st;
+}
+
+void shg_flat_result_free(shg_flat_result *r) {
+    if (!r) return;
+    shg_result_free(&r->fallback);
+    if (r->owner) {
+        PinnedBlock *b = (PinnedBlock *)r->owner;
+        std::lock_guard<std::mutex> lock(b->eng->pool_mu);
+        b->in_use = false;
+    }
+    r->owner = nullptr;
+    r->thresholds_and_seeds = r->fallback_seed_buckets = r->fallback_seeds = r->free_positions = r->ribbon_keys = nullptr;
+    r->ribbon_bits = nullptr;
 }
 
 uint64_t shg_sh2_query(uint64_t leaf_size, uint64_t seed, uint64_t key, uint64_t retrieved) {

@@ -67,6 +67,29 @@ struct Plan {
 };
 void make_plan(const Config &c, const std::vector<uint64_t> &bucket_size_acc, Plan &plan);
 
+// ShockHash2Flat<k> constants (ShockHash2Flat.h:16-46).
+struct FlatConsts {
+    uint32_t k = 0, threshold_bits = 0, threshold_range = 0, seed_bits = 0;
+    std::vector<uint32_t> mapping;  // THRESHOLD_MAPPING
+};
+FlatConsts flat_consts(uint32_t k);
+void flat_launch_murmur(const uint8_t *bytes, const uint64_t *offsets, uint64_t n, uint64_t *out, cudaStream_t s);
+void flat_launch_count(uint64_t *mhc, uint64_t n, uint32_t nb, bool rehash, uint32_t *counts, cudaStream_t s);
+void flat_launch_scatter(const uint64_t *mhc, uint64_t n, uint32_t nb, uint32_t *cursor, uint64_t *out, cudaStream_t s);
+void flat_launch_sort_flush(uint64_t *keys, const uint64_t *acc, uint32_t nb, uint32_t k, const uint32_t *mapping,
+                            uint32_t range, uint64_t layer_base, uint8_t *thr, uint64_t *free_cnt, uint64_t *bump_cnt,
+                            uint32_t *bump_first, uint32_t *err, cudaStream_t s);
+void flat_launch_emit(const uint64_t *keys, const uint64_t *acc, uint32_t nb, uint64_t layer_base, const uint64_t *free_cnt,
+                      const uint64_t *free_off, const uint64_t *bump_cnt, const uint64_t *bump_off, const uint32_t *bump_first,
+                      uint64_t *free_out, uint64_t *bump_out, cudaStream_t s);
+void flat_launch_assign(const uint64_t *mhc0, uint64_t n, uint32_t layers, const uint64_t *layer_bases, const uint8_t *thr,
+                        const uint32_t *mapping, uint64_t *bucket, uint64_t *last_mhc, cudaStream_t s);
+void flat_launch_fallback_list(const uint64_t *bucket, uint64_t n, unsigned long long *count, uint64_t *list, cudaStream_t s);
+void flat_launch_gather(const uint64_t *idx, const uint64_t *src, uint64_t cnt, uint64_t *out, cudaStream_t s);
+void flat_launch_set_buckets(const uint64_t *idx, const uint64_t *val, uint64_t cnt, uint64_t *bucket, cudaStream_t s);
+void flat_launch_group(const uint64_t *bucket, uint64_t n, uint64_t nbuckets, uint32_t k, uint32_t *cursor,
+                       uint32_t *slot_idx, const uint64_t *mhc0, uint64_t *leaf_keys, uint32_t *err, cudaStream_t s);
+
 // Records the message returned by shg_last_error() on this thread and passes the status through.
 shg_status shg_set_error(shg_status st, const std::string &msg);
 

@@ -19,6 +19,8 @@
 
 using namespace shg;
 
+extern "C" uint64_t shg_mphf_bits(const shg_mphf *f);
+
 struct shg_mphf {
     int variant = 0, leaf = 0;
     Config cfg;
@@ -227,5 +229,135 @@ uint64_t shg_mphf_bits(const shg_mphf *f) {
 }
 
 uint64_t shg_mphf_size(const shg_mphf *f) { return f ? f->n : 0; }
+
+} // extern "C"
+
+// ------------------------------------------------------------------ ShockHash2Flat<k> queries
+struct shg_flat {
+    uint64_t n = 0, k = 0, nbuckets = 0, layers = 0;
+    std::vector<uint64_t> layer_bases, tas, free_positions;
+    std::vector<std::pair<uint64_t, uint64_t>> seed_fallback;  // sorted by bucket
+    FlatConsts fc;
+    shg_mphf *fallback = nullptr;
+    uint64_t nfallback_keys = 0;
+    // retrieval map
+    std::vector<uint64_t> rkey;
+    std::vector<uint8_t> rval;
+    uint64_t rmask = 0, ribbon_n = 0;
+    ~shg_flat() {
+        if (fallback) shg_mphf_destroy(fallback);
+    }
+};
+
+namespace {
+
+uint64_t flat_retrieve(const shg_flat *f, uint64_t key) {
+    uint64_t s = slot_of(key, f->rmask);
+    for (;;) {
+        if (f->rval[s] == 2) return 0;
+        if (f->rkey[s] == key) return f->rval[s];
+        s = (s + 1) & f->rmask;
+    }
+}
+
+// evaluateKPerfect (ShockHash2Flat.h:280-301): (bucket, seed)
+std::pair<uint64_t, uint64_t> flat_eval(const shg_flat *f, uint64_t mhc) {
+    const uint64_t tb = f->fc.threshold_bits, rmask = f->fc.threshold_range - 1;
+    for (uint64_t layer = 0; layer < f->layers; layer++) {
+        if (layer) mhc = remix(mhc);
+        const uint64_t base = f->layer_bases[layer];
+        const uint32_t size = (uint32_t)(f->layer_bases[layer + 1] - base);
+        const uint64_t bucket = base + fastrange32((uint32_t)mhc, size);
+        const uint64_t stored = f->tas[bucket];
+        if ((uint32_t)(mhc >> 32) <= f->fc.mapping[stored & rmask]) return {bucket, stored >> tb};
+    }
+    const std::string s = std::to_string(mhc);
+    const uint64_t offs[2] = {0, s.size()};
+    uint64_t phf = 0;
+    shg_mphf_query_strings(f->fallback, s.data(), offs, 1, &phf);
+    const uint64_t bucket = phf < f->free_positions.size() ? f->free_positions[phf] : 0;  // select1(phf+1) - phf
+    if (bucket >= f->nbuckets) return {bucket - f->nbuckets + f->k * f->nbuckets, 1};
+    return {bucket, f->tas[bucket] >> tb};
+}
+
+// operator()(uint64_t) (ShockHash2Flat.h:266-277)
+uint64_t flat_query(const shg_flat *f, uint64_t hash) {
+    auto [bucket, seed] = flat_eval(f, hash);
+    if (bucket >= f->nbuckets) return bucket;
+    if (seed == 0) {
+        auto it = std::lower_bound(f->seed_fallback.begin(), f->seed_fallback.end(), std::make_pair(bucket, (uint64_t)0));
+        seed = (it != f->seed_fallback.end() && it->first == bucket) ? it->second : 0;
+    }
+    const uint64_t retrieved = flat_retrieve(f, hash);
+    return bucket * f->k + sh2_leaf_query((uint32_t)f->k, seed, hash, retrieved);
+}
+
+} // namespace
+
+extern "C" {
+
+shg_status shg_flat_create(const shg_flat_result *r, shg_flat **out) {
+    if (!r || !out) return SHG_ERR_ARG;
+    auto *f = new shg_flat();
+    f->n = r->n;
+    f->k = r->k;
+    f->nbuckets = r->nbuckets;
+    f->layers = r->layers;
+    f->layer_bases.assign(r->layer_bases, r->layer_bases + r->layers + 1);
+    f->tas.assign(r->thresholds_and_seeds, r->thresholds_and_seeds + r->nbuckets);
+    f->free_positions.assign(r->free_positions, r->free_positions + r->nfree);
+    for (uint64_t i = 0; i < r->nfallback_seeds; i++) f->seed_fallback.emplace_back(r->fallback_seed_buckets[i], r->fallback_seeds[i]);
+    f->fc = flat_consts((uint32_t)r->k);
+    f->nfallback_keys = r->nfallback_keys;
+    shg_params fp{SHG_SHOCKHASH2, (int)r->k, 2000, SHG_MODE_DEFAULT, 0};
+    shg_status st = shg_mphf_create(&fp, const_cast<shg_result *>(&r->fallback), &f->fallback);
+    if (st) {
+        delete f;
+        return st;
+    }
+    f->ribbon_n = r->ribbon_n;
+    uint64_t cap = 16;
+    while (cap < r->ribbon_n * 3 / 2 + 1) cap <<= 1;
+    f->rkey.assign(cap, 0);
+    f->rval.assign(cap, 2);
+    f->rmask = cap - 1;
+    for (uint64_t i = 0; i < r->ribbon_n; i++) {
+        uint64_t s = slot_of(r->ribbon_keys[i], f->rmask);
+        while (f->rval[s] != 2 && f->rkey[s] != r->ribbon_keys[i]) s = (s + 1) & f->rmask;
+        f->rkey[s] = r->ribbon_keys[i];
+        f->rval[s] = r->ribbon_bits[i] & 1;
+    }
+    *out = f;
+    return SHG_OK;
+}
+
+void shg_flat_destroy(shg_flat *f) { delete f; }
+
+shg_status shg_flat_query_hash(const shg_flat *f, const uint64_t *mhc, uint64_t n, uint64_t *out) {
+    if (!f || (n && (!mhc || !out))) return SHG_ERR_ARG;
+    for (uint64_t i = 0; i < n; i++) out[i] = flat_query(f, mhc[i]);
+    return SHG_OK;
+}
+
+shg_status shg_flat_query_strings(const shg_flat *f, const char *bytes, const uint64_t *offsets, uint64_t n, uint64_t *out) {
+    if (!f || !offsets || (n && (!bytes || !out))) return SHG_ERR_ARG;
+    for (uint64_t i = 0; i < n; i++)
+        out[i] = flat_query(f, murmur64a((const uint8_t *)bytes + offsets[i], offsets[i + 1] - offsets[i], kMurmurSeed));
+    return SHG_OK;
+}
+
+// getBits() (ShockHash2Flat.h:236-244) with the oracle's size formulas for the stand-in members:
+// object (8 x 336 bytes), fallback PHF, free-position bit vector and its rank/select samples,
+// retrieval bits, packed thresholds-and-seeds, 64 bits per seed-fallback entry.
+uint64_t shg_flat_bits(const shg_flat *f) {
+    if (!f) return 0;
+    const uint64_t nfree = f->free_positions.size();
+    const uint64_t bv = nfree ? nfree + f->free_positions.back() + 1 : 0;
+    const uint64_t rank_select = nfree ? (bv / 512 + 1) * 8 + (nfree / 8192 + 1) * 4 : 0;
+    const uint64_t w = f->fc.threshold_bits + f->fc.seed_bits;
+    const uint64_t tas_bytes = ((f->nbuckets * w + 63) / 64) * 8;
+    return 8 * 336 + shg_mphf_bits(f->fallback) + bv + 8 * rank_select + 8 * ((f->ribbon_n + 7) / 8) + 8 * tas_bytes +
+           64 * f->seed_fallback.size();
+}
 
 } // extern "C"

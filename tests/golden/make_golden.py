@@ -37,6 +37,8 @@ BUILDS = [
     ("sh2_l64_tiny", 2, 64, 3, 2000, 207),
     ("sh1_l30_tiny", 1, 30, 2, 2000, 208),
 ]
+# (k, n, seed) for ShockHash2Flat<k>
+FLATS = [(16, 30000, 401), (32, 20000, 402), (64, 20003, 403), (100, 4100, 404), (8, 5000, 405)]
 LEAVES_SH2 = [(m, 40 if m <= 64 else 4) for m in list(range(2, 65)) + [80, 100, 128]]
 LEAVES_SH1 = [(m, 20) for m in range(2, 41)] + [(48, 3), (60, 2)]
 
@@ -100,6 +102,16 @@ def main():
                         codes=np.array(codes, np.uint64), keys_by_cell=np.concatenate(kc),
                         bits=np.concatenate(bits), levels=np.array(levels, np.int32))
     manifest["sh1_leaves.npz"] = sha(path)
+    # ShockHash2Flat<k> over string keys (MurmurHash64 path)
+    for k, n, seed in FLATS:
+        rng = np.random.default_rng(seed)
+        keys = [bytes(rng.integers(0, 256, size=int(rng.integers(8, 40)), dtype=np.uint8)) for _ in range(n)]
+        keys = list(dict.fromkeys(keys))
+        d = R.flat_build_strings(k, keys)
+        path = os.path.join(HERE, f"flat_k{k}.npz")
+        np.savez_compressed(path, k=k, data=np.frombuffer(b"".join(keys), np.uint8),
+                            lengths=np.array([len(x) for x in keys], np.uint64), **d)
+        manifest[f"flat_k{k}.npz"] = sha(path)
     # string hashing (short and long SpookyHash paths) and the README example
     rng = np.random.default_rng(303)
     strs = [bytes(rng.integers(0, 256, size=L, dtype=np.uint8)) for L in list(range(0, 260)) + [300, 511, 1000]]
