@@ -106,6 +106,14 @@ shg_status shg_build_hash128_device(shg_engine *e, const shg_params *p, const ui
 shg_status shg_build_u64_device(shg_engine *e, const shg_params *p, const uint64_t *d_keys,
                                 uint64_t n, shg_result *out);
 
+/* Batched construction of nreq independent key sets (uint64 keys in HOST memory, hashed as 8-byte
+ * strings): request r's keys[r][0..n[r]) give outs[r], exactly what shg_build_u64 gives for that
+ * request alone. All requests' split nodes and leaves go through the same kernel launches (one
+ * persistent leaf launch for the whole batch); encoding and copy-out are per request. This is the
+ * unit of the continuous-batching build loop (shockhash_b200/serve.py). */
+shg_status shg_build_batch_u64(shg_engine *e, const shg_params *p, const uint64_t *const *keys, const uint64_t *n,
+                               uint64_t nreq, shg_result *outs);
+
 void shg_result_free(shg_result *r);
 
 /* Hash n string keys (bytes + offsets[n+1], host memory) to 128-bit fingerprints on the device:
@@ -206,6 +214,9 @@ void shg_keys_mt19937_64(uint64_t seed, uint64_t n, uint64_t *out);
 /* Integer-pipe peak of the split-search arithmetic (remix + 16-bit part thresholds, operands in
  * registers) on `device`, in evaluations per second: the roofline denominator of the searches. */
 int shg_int_peak(int device, uint64_t iters, double *evals_per_s, double *ms);
+
+/* Free and total device memory (cudaMemGetInfo), for admission control. */
+shg_status shg_device_memory(int device, uint64_t *free_bytes, uint64_t *total_bytes);
 
 /* Message of the last failure on this thread ("" if none). */
 const char *shg_last_error(void);

@@ -90,6 +90,7 @@ def lib():
         "shg_build_u64_device": ([_vp, P, _vp, _u64, R], ctypes.c_int),
         "shg_build_strings": ([_vp, P, ctypes.c_char_p, _vp, _u64, R], ctypes.c_int),
         "shg_result_free": ([R], None),
+        "shg_build_batch_u64": ([_vp, P, _vp, _vp, _u64, _vp], ctypes.c_int),
         "shg_hash_strings": ([_vp, ctypes.c_char_p, _vp, _u64, _vp, _vp], ctypes.c_int),
         "shg_sh2_construct_leaves": ([_vp, _vp, _vp, _u64, _vp, _vp], ctypes.c_int),
         "shg_sh1_construct_leaves": ([_vp, _vp, _vp, _u64, ctypes.c_int, _vp, _vp, _vp], ctypes.c_int),
@@ -110,6 +111,7 @@ def lib():
         "shg_flat_query_strings": ([_vp, ctypes.c_char_p, _vp, _u64, _vp], ctypes.c_int),
         "shg_flat_query_hash": ([_vp, _vp, _u64, _vp], ctypes.c_int),
         "shg_flat_bits": ([_vp], _u64),
+        "shg_device_memory": ([ctypes.c_int, ctypes.POINTER(_u64), ctypes.POINTER(_u64)], ctypes.c_int),
         "shg_keys_mt19937_64": ([_u64, _u64, _vp], None),
         "shg_int_peak": ([ctypes.c_int, _u64, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)],
                          ctypes.c_int),
@@ -146,6 +148,13 @@ def keys_mt19937_64(seed, n):
     out = np.zeros(n, dtype=np.uint64)
     lib().shg_keys_mt19937_64(seed, n, _ptr(out))
     return out
+
+
+def device_memory(device=0):
+    """(free, total) device memory in bytes."""
+    f, t = _u64(), _u64()
+    _check(lib().shg_device_memory(device, ctypes.byref(f), ctypes.byref(t)))
+    return f.value, t.value
 
 
 def int_peak(device=0, iters=1 << 16):
@@ -250,6 +259,24 @@ class Engine:
         p, res = self.params(variant, leaf_size, bucket_size, mode, max_trials), _Result()
         st = lib().shg_build_u64(self._h, ctypes.byref(p), _ptr(keys), len(keys), ctypes.byref(res))
         return self._finish(p, st, res, query)
+
+    def build_batch_u64(self, variant, leaf_size, key_arrays, bucket_size=2000, mode=MODE_DEFAULT):
+        """One batched construction of several independent uint64 key sets; returns one
+        BuildResult per key set (each identical to building that set alone)."""
+        arrays = [np.ascontiguousarray(k, dtype=np.uint64) for k in key_arrays]
+        R = len(arrays)
+        ptrs = (ctypes.c_void_p * R)(*[a.ctypes.data for a in arrays])
+        ns = np.array([len(a) for a in arrays], dtype=np.uint64)
+        outs = (_Result * R)()
+        p = self.params(variant, leaf_size, bucket_size, mode, 0)
+        st = lib().shg_build_batch_u64(self._h, ctypes.byref(p), ptrs, _ptr(ns), R, outs)
+        _check(st)
+        results = []
+        for r in range(R):
+            res = _Result()
+            ctypes.memmove(ctypes.byref(res), ctypes.byref(outs[r]), ctypes.sizeof(_Result))
+            results.append(BuildResult(p, res, self))
+        return results
 
     def build_u64_device(self, variant, leaf_size, d_keys_ptr, n, bucket_size=2000, mode=MODE_DEFAULT):
         p, res = self.params(variant, leaf_size, bucket_size, mode, 0), _Result()

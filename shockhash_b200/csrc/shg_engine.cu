@@ -180,14 +180,26 @@ shg_status check_params(const shg_params *p, uint64_t n) {
 }
 
 // The core build from 128-bit fingerprints already in device memory (e->first / e->second).
-shg_status build_core(shg_engine *e, const shg_params *p, const uint64_t *d_first, const uint64_t *d_second, uint64_t n,
-                      shg_result *out, float hash_ms) {
+// The build of a batch of R independent key sets (requests) whose 128-bit fingerprints lie back to
+// back in d_first / d_second (request r holds nr[r] keys). Every request gets its own bucket range
+// and its own products (as if built alone); the partition, the split levels and the leaf search of
+// all requests share the same launches.
+shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_first, const uint64_t *d_second,
+                       const std::vector<uint64_t> &nr, shg_result *outs, float hash_ms) {
     const Config &cfg = config_of(p->variant, p->leaf_size);
     cudaStream_t s = e->stream;
-    const uint64_t nb = std::max<uint64_t>(1, (n + p->bucket_size - 1) / p->bucket_size);  // ShockHash.h:616
-    memset(out, 0, sizeof(*out));
-    out->n = n;
-    out->nbuckets = nb;
+    const size_t R = nr.size();
+    std::vector<uint64_t> off(R + 1, 0), nbr(R), boff(R + 1, 0);
+    for (size_t r = 0; r < R; r++) {
+        off[r + 1] = off[r] + nr[r];
+        nbr[r] = std::max<uint64_t>(1, (nr[r] + p->bucket_size - 1) / p->bucket_size);  // ShockHash.h:616
+        boff[r + 1] = boff[r] + nbr[r];
+        memset(&outs[r], 0, sizeof(shg_result));
+        outs[r].n = nr[r];
+        outs[r].nbuckets = nbr[r];
+    }
+    const uint64_t n = off[R], nb = boff[R];
+    if (n >= (1ull << 32)) return fail(SHG_ERR_ARG, "at most 2^32 - 1 keys per batch");
 
     CU(e->misc.ensure(sizeof(Misc)));
     Misc *misc = e->misc.as<Misc>();
@@ -199,9 +211,10 @@ shg_status build_core(shg_engine *e, const shg_params *p, const uint64_t *d_firs
     CU(e->sidx.ensure(std::max<uint64_t>(n, 1) * 4));
     CU(e->keys.ensure(std::max<uint64_t>(n, 1) * 8));
 
-    // ---- partition
+    // ---- partition: each request's keys into its own bucket range, then one sort pass
     CU(cudaEventRecord(e->ev[0], s));
-    launch_bucket_count(d_first, n, nb, e->counts.as<uint32_t>(), s);
+    for (size_t r = 0; r < R; r++)
+        launch_bucket_count(d_first + off[r], nr[r], nbr[r], e->counts.as<uint32_t>() + boff[r], s);
     launch_scan_counts(e->counts.as<uint32_t>(), nb, e->acc.as<uint64_t>(), e->cursor.as<uint32_t>(), &misc->maxsz, s);
     std::vector<uint64_t> acc(nb + 1);
     uint32_t maxsz = 0;
@@ -210,7 +223,9 @@ shg_status build_core(shg_engine *e, const shg_params *p, const uint64_t *d_firs
     CU(cudaStreamSynchronize(s));
     if (maxsz >= (uint32_t)kMaxBucket)
         return fail(SHG_ERR_BUCKET, "a bucket holds " + std::to_string(maxsz) + " keys (MAX_BUCKET_SIZE is 3000)");
-    launch_bucket_scatter(d_first, n, nb, e->cursor.as<uint32_t>(), e->sfirst.as<uint64_t>(), e->sidx.as<uint32_t>(), s);
+    for (size_t r = 0; r < R; r++)
+        launch_bucket_scatter(d_first + off[r], nr[r], nbr[r], e->cursor.as<uint32_t>() + boff[r], e->sfirst.as<uint64_t>(),
+                              e->sidx.as<uint32_t>(), off[r], s);
     launch_bucket_sort(e->acc.as<uint64_t>(), nb, e->sfirst.as<uint64_t>(), e->sidx.as<uint32_t>(), d_second,
                        e->keys.as<uint64_t>(), s);
     CU(cudaEventRecord(e->ev[1], s));
@@ -342,66 +357,91 @@ shg_status build_core(shg_engine *e, const shg_params *p, const uint64_t *d_firs
     CU(cudaGetLastError());
     CU(cudaEventRecord(e->ev[4], s));
 
-    // ---- Golomb-Rice encode
-    launch_gr_bucket_bits(e->nodes.as<Node>(), e->bnb.as<uint32_t>(), nb, e->acc.as<uint64_t>(), e->codes.as<uint64_t>(),
-                          e->skip_bits.as<uint32_t>(), e->bucket_bits.as<uint64_t>(), s);
-    launch_scan_u64(e->bucket_bits.as<uint64_t>(), nb, e->pos_acc.as<uint64_t>(), s);
-    uint64_t total_bits = 0;
-    CU(cudaMemcpyAsync(&total_bits, e->pos_acc.as<uint64_t>() + nb, 8, cudaMemcpyDeviceToHost, s));
+    // ---- Golomb-Rice encode, one stream per request
+    CU(e->pos_acc.ensure((nb + R) * 8));
+    for (size_t r = 0; r < R; r++) {
+        launch_gr_bucket_bits(e->nodes.as<Node>(), e->bnb.as<uint32_t>() + boff[r], nbr[r], e->acc.as<uint64_t>() + boff[r],
+                              e->codes.as<uint64_t>(), e->skip_bits.as<uint32_t>(), e->bucket_bits.as<uint64_t>() + boff[r], s);
+        launch_scan_u64(e->bucket_bits.as<uint64_t>() + boff[r], nbr[r], e->pos_acc.as<uint64_t>() + boff[r] + r, s);
+    }
+    std::vector<uint64_t> pos(nb + R);
+    CU(cudaMemcpyAsync(pos.data(), e->pos_acc.p, (nb + R) * 8, cudaMemcpyDeviceToHost, s));
     uint32_t err = 0;
     CU(cudaMemcpyAsync(&err, &misc->err, 4, cudaMemcpyDeviceToHost, s));
     CU(cudaStreamSynchronize(s));
     if (err & kErrTrialLimit) return fail(SHG_ERR_TRIAL_LIMIT, "a seed search exceeded its trial cap (duplicate keys?)");
     if (err & kErrScratch) return fail(SHG_ERR_TRIAL_LIMIT, "a bipartite leaf exceeded its candidate capacity (duplicate keys?)");
     if (err) return fail(SHG_ERR_CUDA, "internal device error flag " + std::to_string(err));
-    const uint64_t bits = total_bits + 1;  // + sentinel (ShockHash.h:652)
-    const uint64_t words = ((bits + 7) / 8 + 7 + 7) / 8;
-    CU(e->words.ensure(words * 8));
-    CU(cudaMemsetAsync(e->words.p, 0, words * 8, s));
-    launch_gr_write(e->nodes.as<Node>(), e->fixed_off.as<uint16_t>(), e->bnb.as<uint32_t>(), nb, e->acc.as<uint64_t>(),
-                    e->pos_acc.as<uint64_t>(), e->codes.as<uint64_t>(), e->skip_bits.as<uint32_t>(),
-                    e->words.as<unsigned long long>(), s);
-    launch_set_bit(e->words.as<unsigned long long>(), total_bits, s);
-    launches += 4;
+    std::vector<uint64_t> total(R), words(R), wbase(R + 1, 0);
+    for (size_t r = 0; r < R; r++) {
+        total[r] = pos[boff[r] + r + nbr[r]];
+        const uint64_t bits = total[r] + 1;          // + sentinel (ShockHash.h:652)
+        words[r] = ((bits + 7) / 8 + 7 + 7) / 8;     // the builder's final size (RiceBitVector.h:71)
+        wbase[r + 1] = wbase[r] + words[r];
+    }
+    CU(e->words.ensure(wbase[R] * 8));
+    CU(cudaMemsetAsync(e->words.p, 0, wbase[R] * 8, s));
+    for (size_t r = 0; r < R; r++) {
+        unsigned long long *w = e->words.as<unsigned long long>() + wbase[r];
+        launch_gr_write(e->nodes.as<Node>(), e->fixed_off.as<uint16_t>(), e->bnb.as<uint32_t>() + boff[r], nbr[r],
+                        e->acc.as<uint64_t>() + boff[r], e->pos_acc.as<uint64_t>() + boff[r] + r, e->codes.as<uint64_t>(),
+                        e->skip_bits.as<uint32_t>(), w, s);
+        launch_set_bit(w, total[r], s);
+        launches += 4;
+    }
     CU(cudaGetLastError());
     CU(cudaEventRecord(e->ev[5], s));
 
-    // ---- copy-out: compact the retrieval input on the device (drop keys of size-1 children), then
-    // copy every product into one pinned host block owned by the engine.
+    // ---- copy-out: compact each request's retrieval input on the device (drop keys of size-1
+    // children), then copy its products into a pinned host block owned by the engine.
     const uint64_t nsingles = plan.singles.size();
-    const uint64_t rn = n - nsingles;
     CU(e->singles.ensure(std::max<uint64_t>(nsingles, 1) * 8));
-    CU(e->ckeys.ensure(std::max<uint64_t>(rn, 1) * 8));
-    CU(e->cbits.ensure(std::max<uint64_t>(rn, 1)));
-    if (nsingles) CU(cudaMemcpyAsync(e->singles.p, plan.singles.data(), nsingles * 8, cudaMemcpyHostToDevice, s));
-    launch_compact_ribbon(p->variant == SHG_SHOCKHASH ? e->rib_keys.as<uint64_t>() : e->keys.as<uint64_t>(),
-                          e->rib_bits.as<uint8_t>(), n, e->singles.as<uint64_t>(), nsingles, e->ckeys.as<uint64_t>(),
-                          e->cbits.as<uint8_t>(), s);
-    const size_t acc_bytes = (nb + 1) * 8;
-    const size_t block_bytes = 2 * acc_bytes + words * 8 + rn * 8 + rn + 64;
-    PinnedBlock *blk = acquire_pinned(e, block_bytes);
-    if (!blk) return fail(SHG_ERR_OOM, "pinned host allocation failed");
-    uint8_t *hp = (uint8_t *)blk->p;
-    out->owner = blk;
-    out->bucket_size_acc = (uint64_t *)hp;
-    out->bucket_pos_acc = (uint64_t *)(hp + acc_bytes);
-    out->descriptors = (uint64_t *)(hp + 2 * acc_bytes);
-    out->ribbon_keys = (uint64_t *)(hp + 2 * acc_bytes + words * 8);
-    out->ribbon_bits = hp + 2 * acc_bytes + words * 8 + rn * 8;
-    memcpy(out->bucket_size_acc, acc.data(), acc_bytes);
-    CU(cudaMemcpyAsync(out->bucket_pos_acc, e->pos_acc.p, acc_bytes, cudaMemcpyDeviceToHost, s));
-    CU(cudaMemcpyAsync(out->descriptors, e->words.p, words * 8, cudaMemcpyDeviceToHost, s));
-    if (rn) {
-        CU(cudaMemcpyAsync(out->ribbon_keys, e->ckeys.p, rn * 8, cudaMemcpyDeviceToHost, s));
-        CU(cudaMemcpyAsync(out->ribbon_bits, e->cbits.p, rn, cudaMemcpyDeviceToHost, s));
+    CU(e->ckeys.ensure(std::max<uint64_t>(n, 1) * 8));
+    CU(e->cbits.ensure(std::max<uint64_t>(n, 1)));
+    std::vector<uint64_t> rel_singles(nsingles), soff(R + 1, 0);
+    for (size_t r = 0, j = 0; r < R; r++) {
+        while (j < nsingles && plan.singles[j] < off[r + 1]) {
+            rel_singles[j] = plan.singles[j] - off[r];
+            j++;
+        }
+        soff[r + 1] = j;
+    }
+    if (nsingles) CU(cudaMemcpyAsync(e->singles.p, rel_singles.data(), nsingles * 8, cudaMemcpyHostToDevice, s));
+    const uint64_t *src_keys = p->variant == SHG_SHOCKHASH ? e->rib_keys.as<uint64_t>() : e->keys.as<uint64_t>();
+    std::vector<PinnedBlock *> blocks(R, nullptr);
+    for (size_t r = 0; r < R; r++) {
+        shg_result *out = &outs[r];
+        const uint64_t ns = soff[r + 1] - soff[r], rn = nr[r] - ns;
+        launch_compact_ribbon(src_keys + off[r], e->rib_bits.as<uint8_t>() + off[r], nr[r], e->singles.as<uint64_t>() + soff[r], ns,
+                              e->ckeys.as<uint64_t>() + off[r], e->cbits.as<uint8_t>() + off[r], s);
+        const size_t acc_bytes = (nbr[r] + 1) * 8;
+        PinnedBlock *blk = acquire_pinned(e, 2 * acc_bytes + words[r] * 8 + rn * 8 + rn + 64);
+        if (!blk) {
+            for (size_t q = 0; q < r; q++) shg_result_free(&outs[q]);
+            return fail(SHG_ERR_OOM, "pinned host allocation failed");
+        }
+        uint8_t *hp = (uint8_t *)blk->p;
+        out->owner = blk;
+        out->bucket_size_acc = (uint64_t *)hp;
+        out->bucket_pos_acc = (uint64_t *)(hp + acc_bytes);
+        out->descriptors = (uint64_t *)(hp + 2 * acc_bytes);
+        out->ribbon_keys = (uint64_t *)(hp + 2 * acc_bytes + words[r] * 8);
+        out->ribbon_bits = hp + 2 * acc_bytes + words[r] * 8 + rn * 8;
+        for (uint64_t b = 0; b <= nbr[r]; b++) out->bucket_size_acc[b] = acc[boff[r] + b] - acc[boff[r]];
+        CU(cudaMemcpyAsync(out->bucket_pos_acc, e->pos_acc.as<uint64_t>() + boff[r] + r, acc_bytes, cudaMemcpyDeviceToHost, s));
+        CU(cudaMemcpyAsync(out->descriptors, e->words.as<uint64_t>() + wbase[r], words[r] * 8, cudaMemcpyDeviceToHost, s));
+        if (rn) {
+            CU(cudaMemcpyAsync(out->ribbon_keys, e->ckeys.as<uint64_t>() + off[r], rn * 8, cudaMemcpyDeviceToHost, s));
+            CU(cudaMemcpyAsync(out->ribbon_bits, e->cbits.as<uint8_t>() + off[r], rn, cudaMemcpyDeviceToHost, s));
+        }
+        out->desc_words = words[r];
+        out->desc_bits = total[r] + 1;
+        out->ribbon_n = rn;
     }
     unsigned long long work[8];
     CU(cudaMemcpyAsync(work, misc->work, sizeof(work), cudaMemcpyDeviceToHost, s));
     CU(cudaEventRecord(e->ev[6], s));
     CU(cudaStreamSynchronize(s));
-    out->desc_words = words;
-    out->desc_bits = bits;
-    out->ribbon_n = rn;
     float ms[6] = {};
     cudaEventElapsedTime(&ms[0], e->ev[0], e->ev[1]);
     cudaEventElapsedTime(&ms[1], e->ev[1], e->ev[2]);
@@ -409,25 +449,24 @@ shg_status build_core(shg_engine *e, const shg_params *p, const uint64_t *d_firs
     cudaEventElapsedTime(&ms[3], e->ev[3], e->ev[4]);
     cudaEventElapsedTime(&ms[4], e->ev[4], e->ev[5]);
     cudaEventElapsedTime(&ms[5], e->ev[5], e->ev[6]);
-    out->stage_ms[0] = hash_ms;
-    out->stage_ms[1] = ms[0];
-    out->stage_ms[2] = ms[1];
-    out->stage_ms[3] = ms[2];
-    out->stage_ms[4] = ms[3];
-    out->stage_ms[5] = ms[4];
-    out->stage_ms[6] = ms[5];
-    out->stage_ms[7] = hash_ms + ms[0] + ms[1] + ms[2] + ms[3] + ms[4] + ms[5];
-    for (int i = 0; i < 7; i++) out->work[i] = work[i];
-    out->work[5] = nleaves;
-    out->work[6] = nn - nleaves;
-    out->work[7] = launches + 5;
+    for (size_t r = 0; r < R; r++) {
+        shg_result *out = &outs[r];
+        out->stage_ms[0] = hash_ms;
+        for (int i = 0; i < 6; i++) out->stage_ms[1 + i] = ms[i];
+        out->stage_ms[7] = hash_ms + ms[0] + ms[1] + ms[2] + ms[3] + ms[4] + ms[5];
+        for (int i = 0; i < 7; i++) out->work[i] = work[i];
+        out->work[5] = nleaves;
+        out->work[6] = nn - nleaves;
+        out->work[7] = launches + 1 + 4 * R;
+    }
     return SHG_OK;
 }
 
-extern "C" shg_status shg_mphf_create(const shg_params *p, shg_result *r, shg_mphf **out);
-extern "C" void shg_mphf_destroy(shg_mphf *f);
-extern "C" shg_status shg_mphf_query_strings(const shg_mphf *f, const char *bytes, const uint64_t *offsets, uint64_t n,
-                                             uint64_t *out);
+shg_status build_core(shg_engine *e, const shg_params *p, const uint64_t *d_first, const uint64_t *d_second, uint64_t n,
+                      shg_result *out, float hash_ms) {
+    return build_batch(e, p, d_first, d_second, std::vector<uint64_t>{n}, out, hash_ms);
+}
+
 
 // ------------------------------------------------------------------ ShockHash2Flat<k>
 double ms_since(std::chrono::steady_clock::time_point t) {
@@ -809,6 +848,29 @@ shg_status shg_build_u64(shg_engine *e, const shg_params *p, const uint64_t *key
     return build_core(e, p, e->first.as<uint64_t>(), e->second.as<uint64_t>(), n, out, ms);
 }
 
+shg_status shg_build_batch_u64(shg_engine *e, const shg_params *p, const uint64_t *const *keys, const uint64_t *n,
+                               uint64_t nreq, shg_result *outs) {
+    if (!e || !outs || !keys || !n || nreq == 0) return fail(SHG_ERR_ARG, "null argument or empty batch");
+    uint64_t total = 0;
+    for (uint64_t r = 0; r < nreq; r++) {
+        if (n[r] && !keys[r]) return fail(SHG_ERR_ARG, "null key array");
+        total += n[r];
+    }
+    shg_status st = check_params(p, total);
+    if (st) return st;
+    CU(cudaSetDevice(e->device));
+    CU(e->in_keys.ensure(std::max<uint64_t>(total, 1) * 8));
+    uint64_t off = 0;
+    for (uint64_t r = 0; r < nreq; r++) {
+        if (n[r]) CU(cudaMemcpyAsync(e->in_keys.as<uint64_t>() + off, keys[r], n[r] * 8, cudaMemcpyHostToDevice, e->stream));
+        off += n[r];
+    }
+    float ms = 0;
+    st = timed_hash_u64(e, e->in_keys.as<uint64_t>(), total, ms);
+    if (st) return st;
+    return build_batch(e, p, e->first.as<uint64_t>(), e->second.as<uint64_t>(), std::vector<uint64_t>(n, n + nreq), outs, ms);
+}
+
 static shg_status hash_strings_dev(shg_engine *e, const char *bytes, const uint64_t *offsets, uint64_t n, float &ms) {
     return hash_strings_into(e, bytes, offsets, n, ms);
 }
@@ -1016,6 +1078,16 @@ shg_status shg_memo_table(int variant, int leaf_size, uint64_t *out) {
     if (leaf_size < 2 || leaf_size > maxleaf) return fail(SHG_ERR_ARG, "leaf size out of range");
     const Config &c = config_of(variant, leaf_size);
     memcpy(out, c.memo.data(), kMaxBucket * 8);
+    return SHG_OK;
+}
+
+shg_status shg_device_memory(int device, uint64_t *free_bytes, uint64_t *total_bytes) {
+    if (!free_bytes || !total_bytes) return fail(SHG_ERR_ARG, "null output");
+    CU(cudaSetDevice(device));
+    size_t f = 0, t = 0;
+    CU(cudaMemGetInfo(&f, &t));
+    *free_bytes = f;
+    *total_bytes = t;
     return SHG_OK;
 }
 

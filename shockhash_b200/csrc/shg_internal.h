@@ -104,7 +104,7 @@ void launch_bucket_count(const uint64_t *first, uint64_t n, uint64_t nb, uint32_
 void launch_scan_counts(const uint32_t *counts, uint64_t nb, uint64_t *acc, uint32_t *cursor, uint32_t *maxsz,
                         cudaStream_t s);
 void launch_bucket_scatter(const uint64_t *first, uint64_t n, uint64_t nb, uint32_t *cursor, uint64_t *sfirst,
-                           uint32_t *sidx, cudaStream_t s);
+                           uint32_t *sidx, uint64_t idx_base, cudaStream_t s);
 void launch_bucket_sort(const uint64_t *acc, uint64_t nb, const uint64_t *sfirst, const uint32_t *sidx,
                         const uint64_t *second, uint64_t *keys, cudaStream_t s);
 void launch_split_level(const Node *nodes, const uint32_t *ids, uint32_t count, uint64_t *keys,

@@ -100,13 +100,13 @@ __global__ void k_scan_counts(const uint32_t *__restrict__ counts, uint64_t nb, 
 
 __global__ void k_bucket_scatter(const uint64_t *__restrict__ first, uint64_t n, uint64_t nb,
                                  uint32_t *__restrict__ cursor, uint64_t *__restrict__ sfirst,
-                                 uint32_t *__restrict__ sidx) {
+                                 uint32_t *__restrict__ sidx, uint64_t idx_base) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t f = first[i];
         const uint64_t b = remap128(f, nb);
         const uint32_t pos = atomicAdd(&cursor[b], 1u);
         sfirst[pos] = f;
-        sidx[pos] = (uint32_t)i;
+        sidx[pos] = (uint32_t)(idx_base + i);
     }
 }
 
@@ -190,8 +190,8 @@ void launch_scan_counts(const uint32_t *counts, uint64_t nb, uint64_t *acc, uint
     k_scan_counts<<<1, 1024, 0, s>>>(counts, nb, acc, cursor, maxsz);
 }
 void launch_bucket_scatter(const uint64_t *first, uint64_t n, uint64_t nb, uint32_t *cursor, uint64_t *sfirst,
-                           uint32_t *sidx, cudaStream_t s) {
-    if (n) k_bucket_scatter<<<grid_for(n, 256), 256, 0, s>>>(first, n, nb, cursor, sfirst, sidx);
+                           uint32_t *sidx, uint64_t idx_base, cudaStream_t s) {
+    if (n) k_bucket_scatter<<<grid_for(n, 256), 256, 0, s>>>(first, n, nb, cursor, sfirst, sidx, idx_base);
 }
 void launch_bucket_sort(const uint64_t *acc, uint64_t nb, const uint64_t *sfirst, const uint32_t *sidx,
                         const uint64_t *second, uint64_t *keys, cudaStream_t s) {

@@ -28,6 +28,11 @@ def test_library_exports_declared_symbols():
     assert len(declared_symbols()) >= 20
 
 
+def test_library_has_no_unresolved_own_symbols():
+    out = subprocess.check_output(["nm", "-D", "--undefined-only", shg.LIB_PATH]).decode()
+    assert not re.findall(r"\bshg_\w+", out)
+
+
 def test_no_device_is_an_error_not_a_fallback():
     import torch
     if torch.cuda.is_available():
