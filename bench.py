@@ -264,6 +264,23 @@ def main():
             forms["per_leaf_launch_ns_per_key_at_%d" % pl_n] = round(rp.stage_ms["total"] * 1e6 / pl_n, 3)
             forms["batched_ns_per_key_at_%d" % pl_n] = round(rl.stage_ms["total"] * 1e6 / pl_n, 3)
             forms["per_leaf_bit_exact_vs_batched"] = bool(np.array_equal(rp.descriptors, rl.descriptors))
+        if ws == 1 and not args.no_forms:
+            # operator() for every key of the build on the device (keys resident, SpookyV2 fused)
+            dq = shg.DeviceMphf(r, local)
+            d_out = torch.empty(n, dtype=torch.int64, device=dev)
+            for _ in range(3):
+                dq.query_u64_device(d_keys.data_ptr(), n, d_out.data_ptr())
+            q_ms = []
+            for _ in range(5):
+                flush.zero_()
+                torch.cuda.synchronize()
+                dq.query_u64_device(d_keys.data_ptr(), n, d_out.data_ptr())
+                q_ms.append(dq.last_kernel_ms())
+            forms["device_query_ns_per_key"] = round(statistics.mean(q_ms) * 1e6 / n, 4)
+            forms["device_query_is_permutation"] = bool(
+                torch.equal(torch.sort(d_out).values, torch.arange(n, device=dev, dtype=torch.int64)))
+            dq.close()
+            del d_out
         d2h = (r.bucket_size_acc.nbytes + r.bucket_pos_acc.nbytes + r.descriptors.nbytes + r.ribbon_keys.nbytes
                + r.ribbon_bits.nbytes)
         line = {

@@ -171,6 +171,31 @@ uint64_t shg_mphf_bits(const shg_mphf *f);
 /* size(): number of keys. */
 uint64_t shg_mphf_size(const shg_mphf *f);
 
+/* Device query object: the same operator() evaluated on the GPU for many keys per call, one thread
+ * per key (bucket lookup, Golomb-Rice walk RiceBitVector.h:149-213, leaf hash, retrieval bit from
+ * a device hash table built from the result's retrieval input). No counterpart in the reference,
+ * which queries one key per call on the host; the outputs equal shg_mphf_query_* key for key.
+ * Calls are synchronous on the object's own stream; one object is not thread-safe. */
+typedef struct shg_dmphf shg_dmphf;
+shg_status shg_dmphf_create(int device, const shg_params *p, const shg_result *r, shg_dmphf **out);
+void shg_dmphf_destroy(shg_dmphf *f);
+/* Fingerprints (first, second) or results in host memory. */
+shg_status shg_dmphf_query_hash128(shg_dmphf *f, const uint64_t *first, const uint64_t *second, uint64_t n,
+                                   uint64_t *out);
+/* uint64 keys, each hashed as its 8-byte little-endian string (SpookyV2-128 fused in the kernel). */
+shg_status shg_dmphf_query_u64(shg_dmphf *f, const uint64_t *keys, uint64_t n, uint64_t *out);
+/* String keys (bytes + offsets[n+1]), hashed in the kernel. */
+shg_status shg_dmphf_query_strings(shg_dmphf *f, const char *bytes, const uint64_t *offsets, uint64_t n,
+                                   uint64_t *out);
+/* Device-memory forms of the two above (all pointers on the object's device). */
+shg_status shg_dmphf_query_hash128_device(shg_dmphf *f, const uint64_t *d_first, const uint64_t *d_second,
+                                          uint64_t n, uint64_t *d_out);
+shg_status shg_dmphf_query_u64_device(shg_dmphf *f, const uint64_t *d_keys, uint64_t n, uint64_t *d_out);
+uint64_t shg_dmphf_bits(const shg_dmphf *f);
+uint64_t shg_dmphf_size(const shg_dmphf *f);
+/* Device time of the last query kernel, in milliseconds (CUDA events on the object's stream). */
+float shg_dmphf_last_kernel_ms(const shg_dmphf *f);
+
 /* ------------------------------------------------------------------ ShockHash2Flat<k>
  * k-perfect "flat" variant (include/ShockHash2Flat.h:37-302): MurmurHash64 keys, two threshold
  * layers of k-key buckets, a fallback ShockHash2<k> for bumped keys, one bipartite leaf search per
@@ -203,6 +228,18 @@ void shg_flat_destroy(shg_flat *f);
 shg_status shg_flat_query_strings(const shg_flat *f, const char *bytes, const uint64_t *offsets, uint64_t n, uint64_t *out);
 shg_status shg_flat_query_hash(const shg_flat *f, const uint64_t *mhc, uint64_t n, uint64_t *out);
 uint64_t shg_flat_bits(const shg_flat *f);
+/* Device query object for ShockHash2Flat<k>: operator()(const string&) / operator()(uint64_t)
+ * (ShockHash2Flat.h:258-301) for many keys per call, one GPU thread per key (MurmurHash64, the
+ * threshold layers, the fallback ShockHash2<k> over the decimal string of the hash, seed fallback,
+ * retrieval bit). No counterpart in the reference, which queries one key per call on the host;
+ * outputs equal shg_flat_query_* key for key. Synchronous; one object is not thread-safe. */
+typedef struct shg_dflat shg_dflat;
+shg_status shg_dflat_create(int device, const shg_flat_result *r, shg_dflat **out);
+void shg_dflat_destroy(shg_dflat *f);
+shg_status shg_dflat_query_strings(shg_dflat *f, const char *bytes, const uint64_t *offsets, uint64_t n,
+                                   uint64_t *out);
+shg_status shg_dflat_query_hash(shg_dflat *f, const uint64_t *mhc, uint64_t n, uint64_t *out);
+float shg_dflat_last_kernel_ms(const shg_dflat *f);
 
 /* Golomb-Rice memo table of a configuration (ShockHash.h:121-127 / ShockHash2.h:106-115):
  * out[m] for m < 3000 packs golomb parameter << 27 | subtree nodes << 16 | subtree fixed bits. */

@@ -103,6 +103,21 @@ def lib():
         "shg_mphf_query_strings": ([_vp, ctypes.c_char_p, _vp, _u64, _vp], ctypes.c_int),
         "shg_mphf_bits": ([_vp], _u64),
         "shg_mphf_size": ([_vp], _u64),
+        "shg_dmphf_create": ([ctypes.c_int, P, R, ctypes.POINTER(_vp)], ctypes.c_int),
+        "shg_dmphf_destroy": ([_vp], None),
+        "shg_dmphf_query_hash128": ([_vp, _vp, _vp, _u64, _vp], ctypes.c_int),
+        "shg_dmphf_query_u64": ([_vp, _vp, _u64, _vp], ctypes.c_int),
+        "shg_dmphf_query_strings": ([_vp, ctypes.c_char_p, _vp, _u64, _vp], ctypes.c_int),
+        "shg_dmphf_query_hash128_device": ([_vp, _vp, _vp, _u64, _vp], ctypes.c_int),
+        "shg_dmphf_query_u64_device": ([_vp, _vp, _u64, _vp], ctypes.c_int),
+        "shg_dmphf_bits": ([_vp], _u64),
+        "shg_dmphf_size": ([_vp], _u64),
+        "shg_dmphf_last_kernel_ms": ([_vp], ctypes.c_float),
+        "shg_dflat_create": ([ctypes.c_int, ctypes.POINTER(_FlatResult), ctypes.POINTER(_vp)], ctypes.c_int),
+        "shg_dflat_destroy": ([_vp], None),
+        "shg_dflat_query_strings": ([_vp, ctypes.c_char_p, _vp, _u64, _vp], ctypes.c_int),
+        "shg_dflat_query_hash": ([_vp, _vp, _u64, _vp], ctypes.c_int),
+        "shg_dflat_last_kernel_ms": ([_vp], ctypes.c_float),
         "shg_sh2_construct_leaves_noalloc": ([_vp, _vp, _u64, _vp, _vp, _vp], ctypes.c_int),
         "shg_build_flat_strings": ([_vp, _u64, ctypes.c_char_p, _vp, _u64, ctypes.POINTER(_FlatResult)], ctypes.c_int),
         "shg_flat_result_free": ([ctypes.POINTER(_FlatResult)], None),
@@ -365,6 +380,10 @@ class FlatBuild:
     def bits(self):
         return int(lib().shg_flat_bits(self._q))
 
+    def device_query(self, device=0):
+        """A DeviceFlat over this build (operator() on the GPU for many keys per call)."""
+        return DeviceFlat(self, device)
+
     def free(self):
         if getattr(self, "_q", None):
             lib().shg_flat_destroy(self._q)
@@ -376,6 +395,43 @@ class FlatBuild:
     def __del__(self):
         try:
             self.free()
+        except Exception:
+            pass
+
+
+class DeviceFlat:
+    """ShockHash2Flat<k> operator() on the GPU (``shg_dflat_*``); outputs equal the host query."""
+
+    def __init__(self, flat_build, device=0):
+        if flat_build._res is None:
+            raise ShgError(1, "flat build already freed")
+        h = _vp()
+        _check(lib().shg_dflat_create(device, ctypes.byref(flat_build._res), ctypes.byref(h)))
+        self._h = h
+
+    def query_strings(self, keys):
+        data, offs = pack_strings(keys)
+        out = np.zeros(len(offs) - 1, np.uint64)
+        _check(lib().shg_dflat_query_strings(self._h, data, _ptr(offs), len(offs) - 1, _ptr(out)))
+        return out
+
+    def query_hash(self, mhc):
+        mhc = np.ascontiguousarray(mhc, dtype=np.uint64)
+        out = np.zeros(len(mhc), np.uint64)
+        _check(lib().shg_dflat_query_hash(self._h, _ptr(mhc), len(mhc), _ptr(out)))
+        return out
+
+    def last_kernel_ms(self):
+        return float(lib().shg_dflat_last_kernel_ms(self._h))
+
+    def close(self):
+        if self._h:
+            lib().shg_dflat_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
         except Exception:
             pass
 
@@ -406,6 +462,61 @@ class _Mphf:
         try:
             if self._h:
                 lib().shg_mphf_destroy(self._h)
+        except Exception:
+            pass
+
+
+class DeviceMphf:
+    """operator() evaluated on the GPU for many keys per call (``shg_dmphf_*``), over a build result.
+    Outputs equal the host query key for key. The result may be freed afterwards."""
+
+    def __init__(self, result, device=0):
+        if result._res is None:
+            raise ShgError(1, "build result already freed")
+        h = _vp()
+        _check(lib().shg_dmphf_create(device, ctypes.byref(result.params), ctypes.byref(result._res), ctypes.byref(h)))
+        self._h = h
+
+    def query_hash(self, first, second):
+        first = np.ascontiguousarray(first, dtype=np.uint64)
+        second = np.ascontiguousarray(second, dtype=np.uint64)
+        out = np.zeros(len(first), np.uint64)
+        _check(lib().shg_dmphf_query_hash128(self._h, _ptr(first), _ptr(second), len(first), _ptr(out)))
+        return out
+
+    def query_u64(self, keys):
+        keys = np.ascontiguousarray(keys, dtype=np.uint64)
+        out = np.zeros(len(keys), np.uint64)
+        _check(lib().shg_dmphf_query_u64(self._h, _ptr(keys), len(keys), _ptr(out)))
+        return out
+
+    def query_strings(self, keys):
+        data, offs = pack_strings(keys)
+        out = np.zeros(len(offs) - 1, np.uint64)
+        _check(lib().shg_dmphf_query_strings(self._h, data, _ptr(offs), len(offs) - 1, _ptr(out)))
+        return out
+
+    def query_u64_device(self, d_keys, n, d_out):
+        """Device pointers (ints); synchronous."""
+        _check(lib().shg_dmphf_query_u64_device(self._h, _vp(d_keys), n, _vp(d_out)))
+
+    def last_kernel_ms(self):
+        return float(lib().shg_dmphf_last_kernel_ms(self._h))
+
+    def bits(self):
+        return int(lib().shg_dmphf_bits(self._h))
+
+    def size(self):
+        return int(lib().shg_dmphf_size(self._h))
+
+    def close(self):
+        if self._h:
+            lib().shg_dmphf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
         except Exception:
             pass
 

@@ -98,22 +98,31 @@ SHG_HD void sh1_cells(uint64_t key, uint64_t seed, uint32_t m, uint32_t &c1, uin
 }
 // Bipartite half-table cell (ShockHash2-internal.h:100-102, 473-477).
 SHG_HD uint32_t half_hash(uint64_t key, uint64_t s, uint32_t half) { return (uint32_t)fastrange64(remix(key + s), half); }
-// Cell of `key` under a bipartite candidate seed: Basic finder for m < 10, QuadSplit (elegant
-// pair; even keys use seedA, odd keys seedB) for m >= 10 (ShockHash2-precompiled.cpp:11-13).
-SHG_HD uint32_t sh2_cand_hash(uint64_t key, uint64_t seed, uint32_t m) {
+// Cell of `key` under a bipartite candidate seed: the Basic finder's hash
+// (ShockHash2-internal.h:100-102), or QuadSplit's (elegant pair; even keys use seedA, odd keys
+// seedB, :473-477). The RecSplit leaves use QuadSplit from m = 10 on
+// (ShockHash2-precompiled.cpp:11-13); ShockHash2Flat uses it for every k (ShockHash2Flat.h:39).
+constexpr uint32_t kQuadMinRecSplit = 10, kQuadMinFlat = 0;
+SHG_HD uint32_t sh2_cand_hash(uint64_t key, uint64_t seed, uint32_t m, bool quad) {
     const uint32_t half = (m + 1) / 2;
-    if (m < 10) return half_hash(key, seed, half);
+    if (!quad) return half_hash(key, seed, half);
     uint64_t a, b;
     unpair_elegant(seed, a, b);
     return half_hash(key, (key & 1) == 0 ? a : b, half);
 }
+SHG_HD uint32_t sh2_cand_hash(uint64_t key, uint64_t seed, uint32_t m) {
+    return sh2_cand_hash(key, seed, m, m >= kQuadMinRecSplit);
+}
 // Leaf query (ShockHash2-internal.h:574-584); leaves of size <= 1 map to 0
 // (ShockHash2-precompiled.cpp:6-9).
-SHG_HD uint64_t sh2_leaf_query(uint32_t m, uint64_t seed, uint64_t key, uint64_t retrieved) {
+SHG_HD uint64_t sh2_leaf_query(uint32_t m, uint64_t seed, uint64_t key, uint64_t retrieved, bool quad) {
     if (m <= 1) return 0;
     uint64_t s1, s2;
     unpair_triangular(seed, s1, s2);
-    return retrieved == 0 ? (uint64_t)sh2_cand_hash(key, s1, m) + m / 2 : (uint64_t)sh2_cand_hash(key, s2, m);
+    return retrieved == 0 ? (uint64_t)sh2_cand_hash(key, s1, m, quad) + m / 2 : (uint64_t)sh2_cand_hash(key, s2, m, quad);
+}
+SHG_HD uint64_t sh2_leaf_query(uint32_t m, uint64_t seed, uint64_t key, uint64_t retrieved) {
+    return sh2_leaf_query(m, seed, key, retrieved, m >= kQuadMinRecSplit);
 }
 
 // ------------------------------------------------------------------ SpookyHash V2 (Jenkins)

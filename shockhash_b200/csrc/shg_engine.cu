@@ -29,7 +29,7 @@ void launch_leaves_sh1_ctr(const Node *nodes, const uint32_t *ids, uint32_t coun
 void launch_leaves_sh2_ctr(const Node *nodes, const uint32_t *ids, uint32_t count, const uint64_t *keys, uint64_t *codes,
                            uint8_t *rib_bits, uint8_t *scratch, uint64_t scratch_per_warp, uint32_t smax, uint32_t cmax,
                            uint32_t *err, unsigned long long *work, unsigned int *ctr, int grid, cudaStream_t s,
-                           int max_leaf);
+                           int max_leaf, uint32_t quad_min = kQuadMinRecSplit);
 int sh2_smem_per_warp(int max_leaf);
 int leaves_sh1_warps_per_block();
 } // namespace shg
@@ -682,7 +682,7 @@ shg_status build_flat(shg_engine *e, uint64_t k, const char *bytes, const uint64
         CU(e->scratch.ensure(per_warp * (uint64_t)grid * 4));
         launch_leaves_sh2_ctr(e->f_nodes.as<Node>(), e->f_ids.as<uint32_t>(), (uint32_t)nbuckets, e->f_leaf_keys.as<uint64_t>(),
                               e->f_codes.as<uint64_t>(), e->f_bits.as<uint8_t>(), e->scratch.as<uint8_t>(), per_warp, smax, cmax,
-                              &misc->err, misc->work, &misc->leaf_ctr, grid, s, (int)k);
+                              &misc->err, misc->work, &misc->leaf_ctr, grid, s, (int)k, kQuadMinFlat);
         CU(cudaGetLastError());
     }
     uint32_t err = 0;

@@ -5,7 +5,8 @@
 // (cells = vertices, keys = edges) is a pseudoforest. The pseudoforest test is a per-lane
 // union-find with a cycle flag per root; the reference inserts into a cuckoo table instead, and
 // ordered cuckoo insertion succeeds exactly when the graph is a pseudoforest, so both accept the
-// same seeds. The smallest accepted seed is kept (ballot + find-first-set), then lane 0 replays
+// same seeds. The coverage mask is kept as two 32-bit halves (first-half and second-half cells).
+// The smallest accepted seed is kept (ballot + find-first-set), then lane 0 replays
 // the reference's ordered cuckoo insertion to obtain the cell of every key (the retrieval bits).
 //
 // The bipartite leaf search is in shg_leaves_sh2.cu.
@@ -109,7 +110,11 @@ __global__ void __launch_bounds__(kLeafWarps * 32) k_leaves_sh1(const Node *__re
         for (uint32_t k = lane; k < m; k += 32) sm.keys[k] = keys[nd.start + k];
         __syncwarp();
         const uint64_t seed0 = start_seed(nd.level);
-        const uint64_t all = (1ull << m) - 1;
+        // Coverage in two 32-bit halves: c1 < m/2 and c2 - m/2 < (m+1)/2, both <= 30 for m <= 60.
+        const uint32_t h1 = m / 2, h2 = (m + 1) / 2;
+        // (m = 1: fastrange32(., 0) = 0 always sets bit 0 of the empty first half; that cell is the
+        // second half's cell 0, which c2 = 0 covers, so bit 0 counts as covered.)
+        const uint32_t all1 = h1 ? (1u << h1) - 1 : 1u, all2 = (1u << h2) - 1;
         // ~2^(g+1) trials are expected; 2^(g+10) is only reached by duplicate keys.
         uint64_t cap = 1ull << min(nd.g + 10, 40);
         if (max_trials && max_trials < cap) cap = max_trials;
@@ -117,13 +122,13 @@ __global__ void __launch_bounds__(kLeafWarps * 32) k_leaves_sh1(const Node *__re
         uint64_t found = ~0ull;
         for (uint64_t base = 0; base < cap; base += 32) {
             const uint64_t x = seed0 + base + lane;
-            uint64_t mask = 0;
+            uint32_t mask1 = 0, mask2 = 0;
             for (uint32_t k = 0; k < m; k++) {
-                uint32_t c1, c2;
-                sh1_cells(sm.keys[k], x, m, c1, c2);
-                mask |= (1ull << c1) | (1ull << c2);
+                const uint64_t r = remix(sm.keys[k] + x);
+                mask1 |= 1u << fastrange32((uint32_t)r, h1);
+                mask2 |= 1u << fastrange32((uint32_t)(r >> 32), h2);
             }
-            bool ok = mask == all;
+            bool ok = mask1 == all1 && mask2 == all2;
             if (__any_sync(0xffffffffu, ok)) {
                 if (ok) {
                     uf.init(m);

@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(128) k_leaves_sh2_v2(Src src, uint32_t count, 
                                                        uint8_t *__restrict__ scratch, uint64_t scratch_per_warp,
                                                        uint32_t smax, uint32_t cmax, uint32_t *__restrict__ err,
                                                        unsigned long long *__restrict__ work,
-                                                       unsigned int *__restrict__ next_leaf) {
+                                                       unsigned int *__restrict__ next_leaf, uint32_t quad_min) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     constexpr int WPB = 4;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(128) k_leaves_sh2_v2(Src src, uint32_t count, 
         cx.m = m_leaf;
         cx.half = (cx.m + 1) / 2;
         cx.full = cx.half >= 64 ? ~0ull : (1ull << cx.half) - 1;
-        cx.quad = cx.m >= 10;
+        cx.quad = cx.m >= quad_min;
         cx.smax = smax;
         cx.cmax = cmax;
         const uint32_t m = cx.m, half = cx.half;
@@ -432,8 +432,8 @@ __global__ void __launch_bounds__(128) k_leaves_sh2_v2(Src src, uint32_t count, 
         uint64_t s1, s2;
         unpair_triangular(answer, s1, s2);
         for (uint32_t k = lane; k < m; k += 32) {
-            sm.c1[k] = (uint8_t)(sh2_cand_hash(sm.orig[k], s1, m) + m / 2);
-            sm.c2[k] = (uint8_t)sh2_cand_hash(sm.orig[k], s2, m);
+            sm.c1[k] = (uint8_t)(sh2_cand_hash(sm.orig[k], s1, m, cx.quad) + m / 2);
+            sm.c2[k] = (uint8_t)sh2_cand_hash(sm.orig[k], s2, m, cx.quad);
             sm.cell[k] = -1;
         }
         __syncwarp();
@@ -464,7 +464,7 @@ __global__ void __launch_bounds__(128) k_leaves_sh2_v2(Src src, uint32_t count, 
 template <int MAXM>
 void launch_v2(const Node *nodes, const uint32_t *ids, uint32_t count, const uint64_t *keys, uint64_t *codes,
                uint8_t *rib_bits, uint8_t *scratch, uint64_t scratch_per_warp, uint32_t smax, uint32_t cmax,
-               uint32_t *err, unsigned long long *work, unsigned int *ctr, int grid, cudaStream_t s) {
+               uint32_t *err, unsigned long long *work, unsigned int *ctr, int grid, cudaStream_t s, uint32_t quad_min) {
     const size_t smem = sizeof(Sh2Smem<MAXM>) * 4;
     static bool attr = false;
     if (!attr) {
@@ -472,7 +472,7 @@ void launch_v2(const Node *nodes, const uint32_t *ids, uint32_t count, const uin
         attr = true;
     }
     k_leaves_sh2_v2<MAXM, NodeLeaves><<<grid, 128, smem, s>>>(NodeLeaves{nodes, ids, codes}, count, keys, rib_bits, scratch,
-                                                              scratch_per_warp, smax, cmax, err, work, ctr);
+                                                              scratch_per_warp, smax, cmax, err, work, ctr, quad_min);
 }
 
 } // namespace
@@ -483,13 +483,15 @@ uint64_t sh2_scratch_bytes(uint32_t smax, uint32_t cmax) { return 16ull * smax +
 void launch_leaves_sh2_ctr(const Node *nodes, const uint32_t *ids, uint32_t count, const uint64_t *keys, uint64_t *codes,
                            uint8_t *rib_bits, uint8_t *scratch, uint64_t scratch_per_warp, uint32_t smax, uint32_t cmax,
                            uint32_t *err, unsigned long long *work, unsigned int *ctr, int grid, cudaStream_t s,
-                           int max_leaf) {
+                           int max_leaf, uint32_t quad_min) {
     if (!count) return;
     cudaMemsetAsync(ctr, 0, sizeof(unsigned int), s);
     if (max_leaf <= 64)
-        launch_v2<64>(nodes, ids, count, keys, codes, rib_bits, scratch, scratch_per_warp, smax, cmax, err, work, ctr, grid, s);
+        launch_v2<64>(nodes, ids, count, keys, codes, rib_bits, scratch, scratch_per_warp, smax, cmax, err, work, ctr, grid, s,
+                      quad_min);
     else
-        launch_v2<128>(nodes, ids, count, keys, codes, rib_bits, scratch, scratch_per_warp, smax, cmax, err, work, ctr, grid, s);
+        launch_v2<128>(nodes, ids, count, keys, codes, rib_bits, scratch, scratch_per_warp, smax, cmax, err, work, ctr, grid, s,
+                       quad_min);
 }
 
 int sh2_smem_per_warp(int max_leaf) { return max_leaf <= 64 ? (int)sizeof(Sh2Smem<64>) : (int)sizeof(Sh2Smem<128>); }
@@ -557,7 +559,7 @@ extern "C" shg_status shg_sh2_construct_leaves_noalloc(const uint64_t *d_keys, c
     const size_t smem = sizeof(Sh2Smem<64>) * 4;
     k_leaves_sh2_v2<64, OffsetLeaves<64>><<<(int)blocks, 128, smem, s>>>(
         OffsetLeaves<64>{d_leaf_offsets, d_seeds}, (uint32_t)nleaves, d_keys, d_bits, base + 256, per_warp,
-        kNoAllocSmax, kNoAllocCmax, &ctr->err, ctr->work, &ctr->leaf_ctr);
+        kNoAllocSmax, kNoAllocCmax, &ctr->err, ctr->work, &ctr->leaf_ctr, kQuadMinRecSplit);
     if ((st = cudaGetLastError()) != cudaSuccess)
         return shg_set_error(SHG_ERR_CUDA, std::string("leaf kernel launch: ") + cudaGetErrorString(st));
     uint32_t err = 0;

@@ -289,7 +289,7 @@ uint64_t flat_query(const shg_flat *f, uint64_t hash) {
         seed = (it != f->seed_fallback.end() && it->first == bucket) ? it->second : 0;
     }
     const uint64_t retrieved = flat_retrieve(f, hash);
-    return bucket * f->k + sh2_leaf_query((uint32_t)f->k, seed, hash, retrieved);
+    return bucket * f->k + sh2_leaf_query((uint32_t)f->k, seed, hash, retrieved, true);  // QuadSplit for every k
 }
 
 } // namespace

@@ -40,6 +40,12 @@ def test_no_device_is_an_error_not_a_fallback():
     with pytest.raises(shg.ShgError) as ei:
         shg.Engine(0)
     assert ei.value.status == 6
+    import ctypes
+    p, r, h = shg._Params(2, 64, 2000, 0, 0), shg._Result(), ctypes.c_void_p()
+    acc = np.zeros(2, np.uint64)
+    r.nbuckets = 1
+    r.bucket_size_acc = r.bucket_pos_acc = acc.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+    assert shg.lib().shg_dmphf_create(0, ctypes.byref(p), ctypes.byref(r), ctypes.byref(h)) == 6
 
 
 @pytest.mark.parametrize("variant,leaves", [(1, [2, 5, 8, 24, 30, 40, 60]), (2, [2, 9, 10, 33, 64, 100, 128])])
