@@ -254,9 +254,15 @@ def main():
         forms = {"default_ns_per_key": round(ms * 1e6 / n, 3)}
         if ws == 1 and not args.no_forms:
             for name, mode in (("levels", shg.MODE_LEVELS), ("pipelined", shg.MODE_PIPELINED)):
-                rm = eng.build_u64_device(VARIANT, LEAF, d_keys.data_ptr(), n, BUCKET, mode)
-                forms[f"{name}_device_ns_per_key"] = round(rm.stage_ms["total"] * 1e6 / n, 3)
-                rm.free()
+                t = []
+                for it in range(4):  # one warm-up, then the mean of three
+                    flush.zero_()
+                    torch.cuda.synchronize()
+                    rm = eng.build_u64_device(VARIANT, LEAF, d_keys.data_ptr(), n, BUCKET, mode)
+                    if it:
+                        t.append(rm.stage_ms["total"])
+                    rm.free()
+                forms[f"{name}_device_ns_per_key"] = round(statistics.mean(t) * 1e6 / n, 3)
         if ws == 1 and not args.no_forms:
             pl_n = int(os.environ.get("SHG_PER_LEAF_SAMPLE", "100000"))
             rp = eng.build_u64_device(VARIANT, LEAF, d_keys.data_ptr(), pl_n, BUCKET, shg.MODE_PER_LEAF)

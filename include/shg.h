@@ -251,6 +251,9 @@ void shg_keys_mt19937_64(uint64_t seed, uint64_t n, uint64_t *out);
 /* Integer-pipe peak of the split-search arithmetic (remix + 16-bit part thresholds, operands in
  * registers) on `device`, in evaluations per second: the roofline denominator of the searches. */
 int shg_int_peak(int device, uint64_t iters, double *evals_per_s, double *ms);
+/* Same for the inner loop of one search: 0 = split (as shg_int_peak), 1 = original leaf coverage
+ * (remix, two fastrange32 cells, half masks), 2 = bipartite raw seeds (remix, fastrange64, mask). */
+int shg_int_peak_kind(int device, int kind, uint64_t iters, double *evals_per_s, double *ms);
 
 /* Free and total device memory (cudaMemGetInfo), for admission control. */
 shg_status shg_device_memory(int device, uint64_t *free_bytes, uint64_t *total_bytes);

@@ -130,6 +130,8 @@ def lib():
         "shg_keys_mt19937_64": ([_u64, _u64, _vp], None),
         "shg_int_peak": ([ctypes.c_int, _u64, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)],
                          ctypes.c_int),
+        "shg_int_peak_kind": ([ctypes.c_int, ctypes.c_int, _u64, ctypes.POINTER(ctypes.c_double),
+                               ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -172,10 +174,11 @@ def device_memory(device=0):
     return f.value, t.value
 
 
-def int_peak(device=0, iters=1 << 16):
-    """Measured evaluations/s of the split-search arithmetic with no memory traffic."""
+def int_peak(device=0, iters=1 << 16, kind=0):
+    """Measured evaluations/s of a search's inner-loop arithmetic with no memory traffic
+    (kind 0 = split, 1 = original leaf coverage, 2 = bipartite raw seeds)."""
     e, ms = ctypes.c_double(), ctypes.c_double()
-    _check(lib().shg_int_peak(device, iters, ctypes.byref(e), ctypes.byref(ms)))
+    _check(lib().shg_int_peak_kind(device, kind, iters, ctypes.byref(e), ctypes.byref(ms)))
     return e.value, ms.value
 
 

@@ -1,10 +1,11 @@
 // Measurement utilities (not part of the reference's interface):
 //  * the seeded key generators the benchmark configurations name (std::mt19937_64), shared by the
 //    CPU and GPU runs so both build from the same keys;
-//  * the integer-pipe peak of the split search: the arithmetic of the split kernel's dominant inner
-//    loop (remix to 16 bits, quarter-split part, moment sums; two seeds per lane) on
-//    register-resident operands with no memory traffic. Its evaluations per second are the
-//    denominator of the search kernels' roofline fraction.
+//  * the integer-pipe peaks of the searches: the arithmetic of each search kernel's dominant inner
+//    loop (split: remix to 16 bits, quarter-split part, moment sums; original leaf: remix, two
+//    fastrange32 cells, half masks; bipartite leaf: remix, fastrange64, mask), two seeds per lane,
+//    on register-resident operands with no memory traffic. Their evaluations per second are the
+//    denominators of the search kernels' roofline fractions.
 #include <algorithm>
 #include <cstdint>
 #include <random>
@@ -33,6 +34,38 @@ __global__ void __launch_bounds__(kPeakThreads) k_int_peak(uint64_t iters, uint3
         d0 += p1; d1 += q1; d2 += q1 * p1;
     }
     if ((c0 ^ c1 ^ c2 ^ d0 ^ d1 ^ d2 ^ T0 ^ T1 ^ T2) == 0xFFFFFFFFu) atomicAdd(sink, 1ull);
+}
+
+// The arithmetic of the original leaf search's coverage loop: full 64-bit remix, both cells by
+// fastrange32 on its halves, one bit each into two 32-bit half masks; two seeds per lane.
+__global__ void __launch_bounds__(kPeakThreads) k_int_peak_sh1(uint64_t iters, uint32_t h1, uint32_t h2,
+                                                               unsigned long long *sink) {
+    const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    uint64_t k0 = shg::remix(tid * 0x9E3779B97F4A7C15ULL), k1 = shg::remix(k0);
+    const uint64_t x0 = 0x643e521ddbd2be98ULL + tid;
+    uint32_t a0 = 0, a1 = 0, b0 = 0, b1 = 0;
+    for (uint64_t i = 0; i < iters; i++) {
+        const uint64_t r0 = shg::remix(k0 + x0 + i), r1 = shg::remix(k1 + x0 + i);
+        a0 |= 1u << shg::fastrange32((uint32_t)r0, h1);
+        b0 |= 1u << shg::fastrange32((uint32_t)(r0 >> 32), h2);
+        a1 |= 1u << shg::fastrange32((uint32_t)r1, h1);
+        b1 |= 1u << shg::fastrange32((uint32_t)(r1 >> 32), h2);
+    }
+    if ((a0 ^ a1 ^ b0 ^ b1) == 0x12345678u) atomicAdd(sink, 1ull);
+}
+
+// The arithmetic of the bipartite leaf search's raw-seed loop: remix, fastrange64 to the half
+// table, one bit into a 64-bit mask; two seeds per lane.
+__global__ void __launch_bounds__(kPeakThreads) k_int_peak_sh2(uint64_t iters, uint64_t half, unsigned long long *sink) {
+    const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    uint64_t k0 = shg::remix(tid * 0x9E3779B97F4A7C15ULL), k1 = shg::remix(k0);
+    const uint64_t x0 = 0x643e521ddbd2be98ULL + tid;
+    uint64_t a0 = 0, a1 = 0;
+    for (uint64_t i = 0; i < iters; i++) {
+        a0 |= 1ull << shg::fastrange64(shg::remix(k0 + x0 + i), half);
+        a1 |= 1ull << shg::fastrange64(shg::remix(k1 + x0 + i), half);
+    }
+    if ((a0 ^ a1) == 0x123456789ull) atomicAdd(sink, 1ull);
 }
 
 } // namespace
@@ -91,6 +124,41 @@ int shg_int_peak(int device, uint64_t iters, double *evals_per_s, double *ms_out
     cudaEventRecord(a);
     k_int_peak<<<blocks, kPeakThreads>>>(iters, T0, T1, T2, sink);
     cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(sink);
+    if (cudaGetLastError() != cudaSuccess) return SHG_ERR_CUDA;
+    *evals_per_s = 2.0 * (double)iters * blocks * kPeakThreads / (ms * 1e-3);
+    if (ms_out) *ms_out = ms;
+    return SHG_OK;
+}
+
+// Integer-pipe peak of one search's inner loop (0 = split, 1 = original leaf, 2 = bipartite leaf).
+int shg_int_peak_kind(int device, int kind, uint64_t iters, double *evals_per_s, double *ms_out) {
+    if (kind == 0) return shg_int_peak(device, iters, evals_per_s, ms_out);
+    if (kind != 1 && kind != 2) return SHG_ERR_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return SHG_ERR_CUDA;
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, device);
+    const int blocks = prop.multiProcessorCount * 8;
+    unsigned long long *sink;
+    if (cudaMalloc(&sink, 8) != cudaSuccess) return SHG_ERR_OOM;
+    cudaMemset(sink, 0, 8);
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    for (int rep = 0; rep < 2; rep++) {  // warm-up, then the timed run
+        const uint64_t it = rep ? iters : iters / 16 + 1;
+        if (rep) cudaEventRecord(a);
+        if (kind == 1)
+            k_int_peak_sh1<<<blocks, kPeakThreads>>>(it, 20, 20, sink);
+        else
+            k_int_peak_sh2<<<blocks, kPeakThreads>>>(it, 32, sink);
+        if (rep) cudaEventRecord(b);
+    }
     cudaEventSynchronize(b);
     float ms = 0;
     cudaEventElapsedTime(&ms, a, b);

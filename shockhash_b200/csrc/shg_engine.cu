@@ -78,16 +78,29 @@ struct DevBuf {
 
 } // namespace
 
-// Pinned host block that a result's arrays live in; reused across builds once released.
+// Pinned host block that a result's arrays live in; reused across builds once released. One
+// process-wide mutex guards every engine's pool, so a result can be released from any thread and
+// after its engine is gone: the engine's destructor frees the idle blocks and orphans the ones
+// still held by results (eng = nullptr), which are freed when those results are released.
 struct PinnedBlock {
     void *p = nullptr;
     size_t cap = 0;
     bool in_use = false;
     shg_engine *eng = nullptr;
 };
+static std::mutex g_pool_mu;
+
+static void release_pinned(PinnedBlock *b) {
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    if (b->eng) {
+        b->in_use = false;
+        return;
+    }
+    if (b->p) cudaFreeHost(b->p);
+    delete b;
+}
 
 struct shg_engine {
-    std::mutex pool_mu;
     std::vector<PinnedBlock *> pool;
     int device = 0;
     int sms = 148;
@@ -112,9 +125,17 @@ struct shg_engine {
                          &f_bump_cnt, &f_first, &f_free_off, &f_bump_off, &f_free_out, &f_bucket, &f_last, &f_list,
                          &f_slot, &f_leaf_keys, &f_nodes, &f_ids, &f_codes, &f_bits, &f_mapping, &f_lb, &f_tmp, &f_tmp2};
         for (DevBuf *b : all) b->release();
-        for (PinnedBlock *b : pool) {
-            if (b->p) cudaFreeHost(b->p);
-            delete b;
+        {
+            std::lock_guard<std::mutex> lock(g_pool_mu);
+            for (PinnedBlock *b : pool) {
+                if (b->in_use) {
+                    b->eng = nullptr;  // freed by release_pinned when its result is released
+                    continue;
+                }
+                if (b->p) cudaFreeHost(b->p);
+                delete b;
+            }
+            pool.clear();
         }
         for (auto &e : ev)
             if (e) cudaEventDestroy(e);
@@ -131,7 +152,7 @@ shg_status hash_strings_into(shg_engine *e, const char *bytes, const uint64_t *o
 namespace {
 
 PinnedBlock *acquire_pinned(shg_engine *e, size_t bytes) {
-    std::lock_guard<std::mutex> lock(e->pool_mu);
+    std::lock_guard<std::mutex> lock(g_pool_mu);
     PinnedBlock *best = nullptr;
     for (PinnedBlock *b : e->pool)
         if (!b->in_use && b->cap >= bytes && (!best || b->cap < best->cap)) best = b;
@@ -928,11 +949,7 @@ shg_status shg_hash_strings(shg_engine *e, const char *bytes, const uint64_t *of
 
 void shg_result_free(shg_result *r) {
     if (!r) return;
-    if (r->owner) {
-        PinnedBlock *b = (PinnedBlock *)r->owner;
-        std::lock_guard<std::mutex> lock(b->eng->pool_mu);
-        b->in_use = false;
-    }
+    if (r->owner) release_pinned((PinnedBlock *)r->owner);
     r->owner = nullptr;
     r->bucket_size_acc = r->bucket_pos_acc = r->descriptors = r->ribbon_keys = nullptr;
     r->ribbon_bits = nullptr;
@@ -1057,11 +1074,7 @@ shg_status shg_build_flat_strings(shg_engine *e, uint64_t k, const char *bytes, 
 void shg_flat_result_free(shg_flat_result *r) {
     if (!r) return;
     shg_result_free(&r->fallback);
-    if (r->owner) {
-        PinnedBlock *b = (PinnedBlock *)r->owner;
-        std::lock_guard<std::mutex> lock(b->eng->pool_mu);
-        b->in_use = false;
-    }
+    if (r->owner) release_pinned((PinnedBlock *)r->owner);
     r->owner = nullptr;
     r->thresholds_and_seeds = r->fallback_seed_buckets = r->fallback_seeds = r->free_positions = r->ribbon_keys = nullptr;
     r->ribbon_bits = nullptr;

@@ -1,6 +1,7 @@
 // ShockHash leaf searches, one warp per leaf, leaves pulled from a device counter.
 //
-// Original ShockHash (ShockHash.h:404-434): lanes take consecutive seeds x; a lane's seed passes
+// Original ShockHash (ShockHash.h:404-434): lanes take consecutive seeds x (two per lane, x and
+// x + 32, per round of 64); a lane's seed passes
 // when the two candidate cells of all m keys cover all m cells (64-bit OR) and the cuckoo graph
 // (cells = vertices, keys = edges) is a pseudoforest. The pseudoforest test is a per-lane
 // union-find with a cycle flag per root; the reference inserts into a cuckoo table instead, and
@@ -120,27 +121,41 @@ __global__ void __launch_bounds__(kLeafWarps * 32) k_leaves_sh1(const Node *__re
         if (max_trials && max_trials < cap) cap = max_trials;
         LaneUF uf{sm.uf, lane};
         uint64_t found = ~0ull;
-        for (uint64_t base = 0; base < cap; base += 32) {
-            const uint64_t x = seed0 + base + lane;
-            uint32_t mask1 = 0, mask2 = 0;
-            for (uint32_t k = 0; k < m; k++) {
-                const uint64_t r = remix(sm.keys[k] + x);
-                mask1 |= 1u << fastrange32((uint32_t)r, h1);
-                mask2 |= 1u << fastrange32((uint32_t)(r >> 32), h2);
+        // Pseudoforest test of one lane's seed (union-find with a cycle flag per root).
+        auto pseudoforest = [&](uint64_t x) {
+            uf.init(m);
+            bool ok = true;
+            for (uint32_t k = 0; k < m && ok; k++) {
+                uint32_t c1, c2;
+                sh1_cells(sm.keys[k], x, m, c1, c2);
+                ok = uf.add(c1, c2);
             }
-            bool ok = mask1 == all1 && mask2 == all2;
-            if (__any_sync(0xffffffffu, ok)) {
-                if (ok) {
-                    uf.init(m);
-                    for (uint32_t k = 0; k < m && ok; k++) {
-                        uint32_t c1, c2;
-                        sh1_cells(sm.keys[k], x, m, c1, c2);
-                        ok = uf.add(c1, c2);
-                    }
-                }
-                const unsigned bal = __ballot_sync(0xffffffffu, ok);
+            return ok;
+        };
+        // Two seeds per lane (x and x + 32): one shared-memory key read feeds two evaluations.
+        for (uint64_t base = 0; base < cap; base += 64) {
+            const uint64_t xa = seed0 + base + lane, xb = xa + 32;
+            uint32_t a1 = 0, a2 = 0, b1 = 0, b2 = 0;
+            for (uint32_t k = 0; k < m; k++) {
+                const uint64_t key = sm.keys[k];
+                const uint64_t ra = remix(key + xa), rb = remix(key + xb);
+                a1 |= 1u << fastrange32((uint32_t)ra, h1);
+                a2 |= 1u << fastrange32((uint32_t)(ra >> 32), h2);
+                b1 |= 1u << fastrange32((uint32_t)rb, h1);
+                b2 |= 1u << fastrange32((uint32_t)(rb >> 32), h2);
+            }
+            bool oka = a1 == all1 && a2 == all2, okb = b1 == all1 && b2 == all2;
+            if (__any_sync(0xffffffffu, oka || okb)) {
+                if (oka) oka = pseudoforest(xa);
+                unsigned bal = __ballot_sync(0xffffffffu, oka);
                 if (bal) {
                     found = base + (__ffs(bal) - 1);
+                    break;
+                }
+                if (okb) okb = pseudoforest(xb);
+                bal = __ballot_sync(0xffffffffu, okb);
+                if (bal) {
+                    found = base + 32 + (__ffs(bal) - 1);
                     break;
                 }
             }

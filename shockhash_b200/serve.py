@@ -40,7 +40,8 @@ class Request:
         self._event = threading.Event()
 
     def wait(self, timeout=None):
-        self._event.wait(timeout)
+        if not self._event.wait(timeout):
+            raise TimeoutError(f"request {self.rid} not built within {timeout} s")
         if self.error:
             raise self.error
         return self.result
@@ -108,14 +109,19 @@ class BuildServer:
                 self.busy_s += t1 - t0
                 self.batches.append((t0, t1, len(batch), sum(len(r.keys) for r in batch)))
             for r, res in zip(batch, results):
-                r.t_done = t1
-                r.error = err
-                if self.keep_results:
-                    r.result = res
-                elif res is not None:
-                    res.free()
-                r.keys = None if not self.keep_results else r.keys
-                r._event.set()
+                try:
+                    r.t_done = t1
+                    r.error = err
+                    if self.keep_results:
+                        r.result = res
+                    else:
+                        if res is not None:
+                            res.free()
+                        r.keys = None
+                except Exception as ex:  # never leave a waiter without an answer
+                    r.error = ex
+                finally:
+                    r._event.set()
 
     def close(self):
         with self._cv:
@@ -138,12 +144,15 @@ def poisson_stream(n_requests, rate=200.0, seed=31, lo_exp=3.0, hi_exp=7.0):
 
 
 def run_stream(stream, workers=2, leaf=64, bucket=2000, mem_fraction=0.5, max_batch_keys=None):
+    # every request's keys exist before the clock starts, as a client's would when it submits
+    all_keys = [keys_mt19937_64(kseed, size) for _, size, kseed in stream]
     srv = BuildServer(leaf=leaf, bucket=bucket, workers=workers, mem_fraction=mem_fraction,
                       max_batch_keys=max_batch_keys, keep_results=False)
     reqs = []
     t0 = time.perf_counter()
     for i, (at, size, kseed) in enumerate(stream):
-        keys = keys_mt19937_64(kseed, size)
+        keys = all_keys[i]
+        all_keys[i] = None
         delay = t0 + at - time.perf_counter()
         if delay > 0:
             time.sleep(delay)

@@ -25,19 +25,24 @@ def test_batch_equals_alone(engine):
         assert same(got, engine.build_u64(1, 30, keys, 2000))
 
 
-def test_server_results_equal_alone_builds():
+def test_server_results_equal_alone_builds(engine):
     stream = serve.poisson_stream(40, rate=2000.0, seed=7, lo_exp=3.0, hi_exp=5.3)
     srv = serve.BuildServer(workers=2, max_batch_keys=300_000)
-    reqs = [srv.submit(i, shg.keys_mt19937_64(kseed, size)) for i, (_, size, kseed) in enumerate(stream)]
-    for r in reqs:
-        r.wait(timeout=120)
-    ref = shg.Engine(0)
-    batched = sum(1 for r in reqs if r.batch_size > 1)
-    for (_, size, kseed), r in zip(stream, reqs):
-        alone = ref.build_u64(2, 64, shg.keys_mt19937_64(kseed, size), 2000)
-        assert same(r.result, alone), r.rid
-    srv.close()
+    try:
+        reqs = [srv.submit(i, shg.keys_mt19937_64(kseed, size)) for i, (_, size, kseed) in enumerate(stream)]
+        for r in reqs:
+            r.wait(timeout=120)
+        batched = sum(1 for r in reqs if r.batch_size > 1)
+        for (_, size, kseed), r in zip(stream, reqs):
+            alone = engine.build_u64(2, 64, shg.keys_mt19937_64(kseed, size), 2000)
+            assert same(r.result, alone), r.rid
+            alone.free()
+    finally:
+        srv.close()
     assert batched > 0  # the stream is fast enough that some requests were built in a mix
+    # results outlive their server's engines: releasing them afterwards is safe
+    for r in reqs:
+        r.result.free()
 
 
 def test_serving_stream_reports_latency():
