@@ -22,7 +22,7 @@
 #include "shg_internal.h"
 
 namespace shg {
-uint64_t sh2_scratch_bytes(uint32_t smax, uint32_t cmax);
+uint64_t sh2_scratch_bytes(uint32_t smax, uint32_t cmax, int max_leaf);
 void launch_leaves_sh1_ctr(const Node *nodes, const uint32_t *ids, uint32_t count, const uint64_t *keys, uint64_t *codes,
                            uint64_t *rib_keys, uint8_t *rib_bits, uint64_t max_trials, uint32_t *err,
                            unsigned long long *work, unsigned int *ctr, int grid, cudaStream_t s);
@@ -293,7 +293,7 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
     if (p->variant == SHG_SHOCKHASH2) {
         // bipartite leaf scratch for the widest leaf grid any schedule uses (grown once, then reused)
         const uint32_t sm_ = p->leaf_size > 64 ? 16384 : 4096, cm_ = p->leaf_size > 64 ? 16384 : 2048;
-        const uint64_t pw = (sh2_scratch_bytes(sm_, cm_) + 255) & ~255ull;
+        const uint64_t pw = (sh2_scratch_bytes(sm_, cm_, p->leaf_size) + 255) & ~255ull;
         const int bps = std::max(1, std::min(8, (228 * 1024) / (4 * sh2_smem_per_warp(p->leaf_size) + 1024)));
         CU(e->scratch.ensure(pw * (uint64_t)e->sms * bps * 4));
     }
@@ -308,7 +308,7 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
     // leaf kernel launch shape and scratch
     const int maxm = p->leaf_size;
     const uint32_t smax = maxm > 64 ? 16384 : 4096, cmax = maxm > 64 ? 16384 : 2048;
-    const uint64_t per_warp = (sh2_scratch_bytes(smax, cmax) + 255) & ~255ull;
+    const uint64_t per_warp = (sh2_scratch_bytes(smax, cmax, maxm) + 255) & ~255ull;
     int leaf_grid;
     if (sh2) {
         const int per_block_smem = 4 * sh2_smem_per_warp(maxm);
@@ -697,7 +697,7 @@ shg_status build_flat(shg_engine *e, uint64_t k, const char *bytes, const uint64
         CU(cudaMemcpyAsync(e->f_nodes.p, nodes.data(), nbuckets * sizeof(Node), cudaMemcpyHostToDevice, s));
         CU(cudaMemcpyAsync(e->f_ids.p, ids.data(), nbuckets * 4, cudaMemcpyHostToDevice, s));
         const uint32_t smax = k > 64 ? 16384 : 4096, cmax = k > 64 ? 16384 : 2048;
-        const uint64_t per_warp = (sh2_scratch_bytes(smax, cmax) + 255) & ~255ull;
+        const uint64_t per_warp = (sh2_scratch_bytes(smax, cmax, (int)k) + 255) & ~255ull;
         const int bps = std::max(1, std::min(8, (228 * 1024) / (4 * sh2_smem_per_warp((int)k) + 1024)));
         const int grid = std::max(1, std::min<int>(e->sms * bps, (int)((nbuckets + 3) / 4)));
         CU(e->scratch.ensure(per_warp * (uint64_t)grid * 4));
@@ -1001,7 +1001,7 @@ shg_status shg_sh2_construct_leaves(shg_engine *e, const uint64_t *keys, const u
     uint64_t maxm = 0;
     for (auto &nd : nodes) maxm = std::max<uint64_t>(maxm, nd.m);
     const uint32_t smax = maxm > 64 ? 16384 : 4096, cmax = maxm > 64 ? 16384 : 2048;
-    const uint64_t per_warp = (sh2_scratch_bytes(smax, cmax) + 255) & ~255ull;
+    const uint64_t per_warp = (sh2_scratch_bytes(smax, cmax, (int)maxm) + 255) & ~255ull;
     const int per_block_smem = 4 * sh2_smem_per_warp((int)maxm);
     const int blocks_per_sm = std::max(1, std::min(8, (228 * 1024) / (per_block_smem + 1024)));
     const int grid = std::max(1, std::min<int>(e->sms * blocks_per_sm, (int)((nleaves + 3) / 4)));

@@ -29,22 +29,32 @@ namespace shg {
 namespace {
 
 template <int MAXM> struct Sh2Cfg;
+// A raw seed's two half-table coverage masks (keys of set A, keys of set B), adjacent so that one
+// shared-memory load brings both.
+template <class M> struct alignas(2 * sizeof(M)) MaskPair {
+    M a, b;
+};
+
 template <> struct Sh2Cfg<64> {
-    static constexpr int SMS = 256;  // raw seeds whose masks stay in shared memory
-    static constexpr int CMS = 256;  // candidates held in shared memory
+    using Mask = uint32_t;            // half-table coverage: (m + 1) / 2 <= 32 cells
+    static constexpr int SMS = 256;   // raw seeds whose masks stay in shared memory
+    static constexpr int CMS = 256;   // candidates held in shared memory
     static constexpr int ISO_WORDS = 1;
+    static constexpr uint32_t ROWS = 2048;  // candidates whose cell rows are cached in global scratch
 };
 template <> struct Sh2Cfg<128> {
+    using Mask = uint64_t;
     static constexpr int SMS = 512;
     static constexpr int CMS = 384;
     static constexpr int ISO_WORDS = 2;
+    static constexpr uint32_t ROWS = 4096;
 };
 
 template <int MAXM> struct Sh2Smem {
     using C = Sh2Cfg<MAXM>;
     uint64_t keys[MAXM];  // finder order (QuadSplit: even keys in order, odd keys from the back)
     uint64_t orig[MAXM];  // leaf order
-    uint64_t maskA[C::SMS], maskB[C::SMS];
+    MaskPair<typename C::Mask> mask[C::SMS];
     uint32_t csa[C::CMS], csb[C::CMS];           // raw seeds (seedA, seedB) of each candidate
     uint64_t iso[C::CMS][C::ISO_WORDS];          // isolated-key masks
     uint8_t uf[MAXM * 32];                       // per-lane union-find parents / per-lane hash rows
@@ -55,10 +65,23 @@ template <int MAXM> struct Sh2Smem {
     uint8_t xr[MAXM];
 };
 
-struct Sh2Global {
-    uint64_t *maskA, *maskB;  // [smax]
-    uint32_t *csa, *csb;      // [cmax]
-    uint64_t *iso;            // [cmax][2]
+// Per-warp global scratch (L2-resident in practice): what does not fit shared memory, and the
+// candidates' cell rows (one byte per key, MAXM / 8 words per candidate) for the pair tests.
+template <int MAXM> struct Sh2Global {
+    using Mask = typename Sh2Cfg<MAXM>::Mask;
+    MaskPair<Mask> *mask;  // [smax]
+    uint32_t *csa, *csb;  // [cmax]
+    uint64_t *iso;        // [cmax][2]
+    uint64_t *rows;       // [rcap][MAXM / 8]
+    uint32_t rcap;
+    __device__ void carve(uint8_t *base, uint32_t smax, uint32_t cmax) {
+        mask = (MaskPair<Mask> *)base;
+        iso = (uint64_t *)(base + ((2ull * smax * sizeof(Mask) + 255) & ~255ull));
+        csa = (uint32_t *)(iso + 2 * (uint64_t)cmax);
+        csb = csa + cmax;
+        rows = (uint64_t *)(csb + cmax);  // 8-byte aligned: cmax is even
+        rcap = cmax < Sh2Cfg<MAXM>::ROWS ? cmax : Sh2Cfg<MAXM>::ROWS;
+    }
 };
 
 // Per-lane union-find over at most MAXM vertices: parents in shared memory (byte per vertex,
@@ -124,13 +147,15 @@ __device__ bool cuckoo_insert2(int16_t *cell, uint8_t *xr, int e, uint32_t c1, u
 }
 
 template <int MAXM> struct LeafCtx {
+    using Mask = typename Sh2Cfg<MAXM>::Mask;
     Sh2Smem<MAXM> &sm;
-    Sh2Global g;
+    Sh2Global<MAXM> g;
     uint32_t m, half, sizeA, smax, cmax;
-    uint64_t full;
+    Mask full;
     bool quad;
-    __device__ __forceinline__ uint64_t &maskA(uint64_t s) { return s < Sh2Cfg<MAXM>::SMS ? sm.maskA[s] : g.maskA[s]; }
-    __device__ __forceinline__ uint64_t &maskB(uint64_t s) { return s < Sh2Cfg<MAXM>::SMS ? sm.maskB[s] : g.maskB[s]; }
+    __device__ __forceinline__ MaskPair<Mask> &mp(uint64_t s) { return s < Sh2Cfg<MAXM>::SMS ? sm.mask[s] : g.mask[s]; }
+    __device__ __forceinline__ Mask maskA(uint64_t s) { return mp(s).a; }
+    __device__ __forceinline__ Mask maskB(uint64_t s) { return mp(s).b; }
     __device__ __forceinline__ uint32_t &csa(uint32_t j) { return j < Sh2Cfg<MAXM>::CMS ? sm.csa[j] : g.csa[j]; }
     __device__ __forceinline__ uint32_t &csb(uint32_t j) { return j < Sh2Cfg<MAXM>::CMS ? sm.csb[j] : g.csb[j]; }
     __device__ __forceinline__ uint64_t &iso(uint32_t j, int w) {
@@ -140,11 +165,25 @@ template <int MAXM> struct LeafCtx {
         const uint32_t a = csa(j), b = csb(j);
         return quad ? pair_elegant(a, b) : a;
     }
-    // candidate pair test on the edges (h_j + m/2, h_i), recomputing the cells
+    // candidate pair test on the edges (h_j + m/2, h_i): cells from the cached rows, or
+    // recomputed for candidates beyond the row cache
     __device__ __forceinline__ bool pair_ok(LaneUF2<MAXM> &uf, uint32_t j, uint32_t i, unsigned long long &edges) {
-        const uint64_t ja = csa(j), jb = csb(j), ia = csa(i), ib = csb(i);
         uf.init(m);
         const uint32_t off = m / 2;
+        if (j < g.rcap) {  // i < j
+            constexpr uint32_t W = MAXM / 8;
+            const uint64_t *rj = g.rows + (uint64_t)j * W, *ri = g.rows + (uint64_t)i * W;
+            for (uint32_t w = 0; w * 8 < m; w++) {
+                const uint64_t a = rj[w], b = ri[w];
+                const uint32_t kend = min(8u, m - w * 8);
+                for (uint32_t t = 0; t < kend; t++) {
+                    edges++;
+                    if (!uf.add((uint32_t)((a >> (8 * t)) & 0xFF) + off, (uint32_t)((b >> (8 * t)) & 0xFF))) return false;
+                }
+            }
+            return true;
+        }
+        const uint64_t ja = csa(j), jb = csb(j), ia = csa(i), ib = csb(i);
         for (uint32_t k = 0; k < m; k++) {
             const uint64_t key = sm.keys[k];
             const bool inA = k < sizeA;
@@ -198,12 +237,8 @@ __global__ void __launch_bounds__(128) k_leaves_sh2_v2(Src src, uint32_t count, 
     Sh2Smem<MAXM> &sm = reinterpret_cast<Sh2Smem<MAXM> *>(smem_raw)[warp];
     const uint64_t gw = (uint64_t)blockIdx.x * WPB + warp;
     uint8_t *gbase = scratch + gw * scratch_per_warp;
-    Sh2Global g;
-    g.maskA = (uint64_t *)gbase;
-    g.maskB = g.maskA + smax;
-    g.iso = g.maskB + smax;
-    g.csa = (uint32_t *)(g.iso + 2 * (uint64_t)cmax);
-    g.csb = g.csa + cmax;
+    Sh2Global<MAXM> g;
+    g.carve(gbase, smax, cmax);
     LaneUF2<MAXM> uf{sm.uf, lane, 0, 0};
     unsigned long long w_evals = 0, w_pairs = 0, w_filtered = 0, w_edges = 0;
     const unsigned below = (1u << lane) - 1;
@@ -222,7 +257,8 @@ __global__ void __launch_bounds__(128) k_leaves_sh2_v2(Src src, uint32_t count, 
         LeafCtx<MAXM> cx{sm, g};
         cx.m = m_leaf;
         cx.half = (cx.m + 1) / 2;
-        cx.full = cx.half >= 64 ? ~0ull : (1ull << cx.half) - 1;
+        cx.full = cx.half >= 8 * sizeof(typename LeafCtx<MAXM>::Mask) ? ~(typename LeafCtx<MAXM>::Mask)0
+                                                                     : (((typename LeafCtx<MAXM>::Mask)1 << cx.half) - 1);
         cx.quad = cx.m >= quad_min;
         cx.smax = smax;
         cx.cmax = cmax;
@@ -299,13 +335,12 @@ __global__ void __launch_bounds__(128) k_leaves_sh2_v2(Src src, uint32_t count, 
                     break;
                 }
                 const uint64_t s = S + lane;
-                uint64_t tA = 0, tB = 0;
+                typename LeafCtx<MAXM>::Mask tA = 0, tB = 0;
                 for (uint32_t k = 0; k < m; k++) {
-                    const uint64_t bit = 1ull << half_hash(sm.keys[k], s, half);
+                    const auto bit = (typename LeafCtx<MAXM>::Mask)1 << half_hash(sm.keys[k], s, half);
                     if (k < cx.sizeA) tA |= bit; else tB |= bit;
                 }
-                cx.maskA(s) = tA;
-                cx.maskB(s) = tB;
+                cx.mp(s) = MaskPair<typename LeafCtx<MAXM>::Mask>{tA, tB};
                 w_evals += m;
                 S += 32;
                 __syncwarp();
@@ -313,14 +348,30 @@ __global__ void __launch_bounds__(128) k_leaves_sh2_v2(Src src, uint32_t count, 
             // 2. candidates whose larger raw seed is s (lane L: s = S_proc + L), in the reference's order
             const uint64_t s = S_proc + lane;
             const bool live = s < S;
-            uint32_t mine = 0;
+            uint32_t mine = 0, mineA = 0, mineB = 0;
+            uint32_t ha0 = 0, ha1 = 0, hb0 = 0, hb1 = 0;  // first two partners on each side
             if (live) {
                 if (cx.quad) {
-                    const uint64_t tA = cx.maskA(s), tB = cx.maskB(s);
-                    for (uint64_t a = 0; a < s; a++)
-                        mine += (cx.maskA(a) | tB) == cx.full && float_accurate_elegant(a, s);
-                    for (uint64_t b = 0; b <= s; b++)
-                        mine += (cx.maskB(b) | tA) == cx.full && float_accurate_elegant(s, b);
+                    // one pass over the earlier raw seeds p <= s: A-side pairs (p, s) for p < s and
+                    // B-side pairs (s, p) for p <= s (candidatesA/B.filter, ShockHash2-internal.h:446-465)
+                    const auto ts = cx.mp(s);
+                    const auto tA = ts.a, tB = ts.b;
+                    auto visit = [&](uint64_t p, MaskPair<typename LeafCtx<MAXM>::Mask> w) {
+                        if (p < s && (w.a | tB) == cx.full && float_accurate_elegant(p, s)) {
+                            ha0 = mineA == 0 ? (uint32_t)p : ha0;
+                            ha1 = mineA == 1 ? (uint32_t)p : ha1;
+                            mineA++;
+                        }
+                        if ((w.b | tA) == cx.full && float_accurate_elegant(s, p)) {
+                            hb0 = mineB == 0 ? (uint32_t)p : hb0;
+                            hb1 = mineB == 1 ? (uint32_t)p : hb1;
+                            mineB++;
+                        }
+                    };
+                    const uint64_t in_sm = min(s + 1, (uint64_t)Sh2Cfg<MAXM>::SMS);
+                    for (uint64_t p = 0; p < in_sm; p++) visit(p, sm.mask[p]);
+                    for (uint64_t p = in_sm; p <= s; p++) visit(p, g.mask[p]);
+                    mine = mineA + mineB;
                 } else {
                     mine = cx.maskA(s) == cx.full;
                 }
@@ -342,8 +393,17 @@ __global__ void __launch_bounds__(128) k_leaves_sh2_v2(Src src, uint32_t count, 
             const uint32_t T = __shfl_sync(0xffffffffu, incl, take - 1);
             if (lane < take) {
                 uint32_t pos = J + incl - mine;
-                if (cx.quad) {
-                    const uint64_t tA = cx.maskA(s), tB = cx.maskB(s);
+                if (cx.quad && mineA <= 2 && mineB <= 2) {
+                    for (uint32_t t = 0; t < mineA; t++, pos++) {  // A side first: (a, s), a ascending
+                        cx.csa(pos) = t == 0 ? ha0 : ha1;
+                        cx.csb(pos) = (uint32_t)s;
+                    }
+                    for (uint32_t t = 0; t < mineB; t++, pos++) {  // then B side: (s, b), b ascending
+                        cx.csa(pos) = (uint32_t)s;
+                        cx.csb(pos) = t == 0 ? hb0 : hb1;
+                    }
+                } else if (cx.quad) {  // more than two partners on a side (rare): scan again
+                    const auto tA = cx.maskA(s), tB = cx.maskB(s);
                     for (uint64_t a = 0; a < s && mine; a++)
                         if ((cx.maskA(a) | tB) == cx.full && float_accurate_elegant(a, s)) {
                             cx.csa(pos) = (uint32_t)a;
@@ -369,10 +429,16 @@ __global__ void __launch_bounds__(128) k_leaves_sh2_v2(Src src, uint32_t count, 
                 const uint32_t c = c0 + lane;
                 if (c < J + T) {
                     const uint64_t sa = cx.csa(c), sb = cx.csb(c);
-                    uint64_t seen1 = 0, seen2 = 0;
+                    uint64_t seen1 = 0, seen2 = 0, word = 0;
+                    uint64_t *row = c < g.rcap ? g.rows + (uint64_t)c * (MAXM / 8) : nullptr;
                     for (uint32_t k = 0; k < m; k++) {
                         const uint32_t h = half_hash(sm.keys[k], k < cx.sizeA ? sa : sb, half);
                         sm.uf[k * 32 + lane] = (uint8_t)h;
+                        word |= (uint64_t)h << (8 * (k & 7));
+                        if ((k & 7) == 7 || k + 1 == m) {
+                            if (row) row[k >> 3] = word;
+                            word = 0;
+                        }
                         const uint64_t bit = 1ull << h;
                         seen2 |= seen1 & bit;
                         seen1 |= bit;
@@ -478,7 +544,10 @@ void launch_v2(const Node *nodes, const uint32_t *ids, uint32_t count, const uin
 } // namespace
 
 // Bytes of global scratch per warp for the given capacities (raw seeds, candidates).
-uint64_t sh2_scratch_bytes(uint32_t smax, uint32_t cmax) { return 16ull * smax + 16ull * cmax + 8ull * cmax; }
+uint64_t sh2_scratch_bytes(uint32_t smax, uint32_t cmax, int max_leaf) {
+    const uint64_t rows = std::min<uint64_t>(cmax, max_leaf > 64 ? Sh2Cfg<128>::ROWS : Sh2Cfg<64>::ROWS);
+    return 16ull * smax + 256 + 24ull * cmax + rows * (max_leaf > 64 ? 128 : 64);
+}
 
 void launch_leaves_sh2_ctr(const Node *nodes, const uint32_t *ids, uint32_t count, const uint64_t *keys, uint64_t *codes,
                            uint8_t *rib_bits, uint8_t *scratch, uint64_t scratch_per_warp, uint32_t smax, uint32_t cmax,
@@ -553,7 +622,7 @@ extern "C" shg_status shg_sh2_construct_leaves_noalloc(const uint64_t *d_keys, c
     // counters start at zero on every call; the spill slices need no clearing (written before read)
     if ((st = cudaMemsetAsync(ctr, 0, sizeof(NoAllocCounters), s)) != cudaSuccess)
         return shg_set_error(SHG_ERR_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(st));
-    const uint64_t per_warp = (sh2_scratch_bytes(kNoAllocSmax, kNoAllocCmax) + 255) & ~255ull;
+    const uint64_t per_warp = (sh2_scratch_bytes(kNoAllocSmax, kNoAllocCmax, 64) + 255) & ~255ull;
     const uint64_t warps = (kNoAllocScratchBytes - 256) / per_warp;
     const uint64_t blocks = std::min<uint64_t>(warps / 4, (nleaves + 3) / 4);
     const size_t smem = sizeof(Sh2Smem<64>) * 4;
