@@ -35,6 +35,16 @@ METRIC = "build ns/key on 1 B200, batched vs per-leaf GPU vs CPU, bit-exact; p99
 CONFIG_NAME = "ShockHash2<64> b=2000, 10M uint64 keys (mt19937_64 seed 7) hashed to 128-bit"
 
 
+def _workload(args):
+    """--variant / --leaf / --seed / --n pick another configuration of the same path (e.g. the
+    original ShockHash<40> with seed 11 for profiling); the defaults are the configuration above."""
+    global VARIANT, LEAF, SEED, CONFIG_NAME
+    VARIANT, LEAF, SEED = args.variant, args.leaf, args.seed
+    name = "ShockHash2" if VARIANT == 2 else "ShockHash"
+    CONFIG_NAME = (f"{name}<{LEAF}> b={BUCKET}, {args.n / 1e6:g}M uint64 keys (mt19937_64 seed {SEED}) "
+                   "hashed to 128-bit")
+
+
 class _Summary:
     """What the report needs from one build, kept after its result block is released."""
 
@@ -156,9 +166,13 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_KEYS)
     ap.add_argument("--mode", type=int, default=0)
+    ap.add_argument("--variant", type=int, default=VARIANT, choices=[1, 2])
+    ap.add_argument("--leaf", type=int, default=LEAF)
+    ap.add_argument("--seed", type=int, default=SEED)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-forms", action="store_true", help="skip the per-leaf-launch comparison form")
     args = ap.parse_args()
+    _workload(args)
     if args.impl == "reference":
         return run_reference_arm(args)
 
@@ -179,6 +193,7 @@ def main():
     h_keys = torch.from_numpy(keys.view(np.int64)).pin_memory()
     eng = shg.Engine(local)
     peak_evals, _ = shg.int_peak(local, 1 << 15)
+    leaf_peak, _ = shg.int_peak(local, 1 << 15, 1 if VARIANT == 1 else 2)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
 
     def barrier():
@@ -294,7 +309,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
             "config": {"workload": CONFIG_NAME, "keys_per_gpu": n, "leaf_size": LEAF, "bucket_size": BUCKET,
-                       "variant": "ShockHash2", "mode": ["default (levels)", "levels", "per_leaf", "pipelined"][args.mode],
+                       "variant": "ShockHash2" if VARIANT == 2 else "ShockHash", "mode": ["default (levels)", "levels", "per_leaf", "pipelined"][args.mode],
                        "l2": "flushed (256 MB write) before every timed step, outside the timing",
                        "parallelism": f"{ws} independent bucket shards, no data-path collective"},
             "device_ms_per_step": round(ms_dev, 3),
@@ -308,6 +323,12 @@ def main():
                                  "the split stage; peak = measured integer microbenchmark of the same "
                                  "arithmetic (no memory traffic)"},
             "leaf_stage": {"ms": round(leaf_ms, 3), "leaf_evals": last.work["leaf_evals"],
+                           "evals_per_s_g": round(last.work["leaf_evals"] / (leaf_ms * 1e-3) / 1e9, 3),
+                           "peak_g": round(leaf_peak / 1e9, 3),
+                           "frac": round(last.work["leaf_evals"] / (leaf_ms * 1e-3) / leaf_peak, 4),
+                           "note": "hash evaluations of the leaf search per second vs the measured peak of its "
+                                   "inner loop (original leaves: coverage loop; bipartite leaves: raw-seed loop, "
+                                   "which leaves out the candidate scans and pseudoforest tests)",
                            "pairs": last.work["pairs"], "uf_edges": last.work["uf_edges"]},
             "work": last.work, "bits_per_key_trees": round(bits_per_key, 4),
             "gpu_launches": int(last.work["launches"] * args.steps),

@@ -116,6 +116,22 @@ shg_status shg_build_batch_u64(shg_engine *e, const shg_params *p, const uint64_
 
 void shg_result_free(shg_result *r);
 
+/* Shards of one structure (no counterpart in the reference, whose compute_thread splits the same
+ * bucket ranges over threads, ShockHash.h:566-570). Bucket b = remap128(first, nb_global) is
+ * monotone in `first`, so a key set can be split by bucket range over GPUs or processes:
+ * shg_build_shard_hash128 builds the buckets [b0, b1) of a structure with nb_global buckets from
+ * exactly the keys that fall in them (any other key is SHG_ERR_ARG); its result holds those
+ * buckets only (accumulators from 0, no other shard's bits). shg_merge_shards joins the shard
+ * results, given in bucket order, into the result a single build of all keys produces, bit for
+ * bit: accumulators offset, Golomb-Rice codes concatenated at bit granularity
+ * (appendRiceBitVector, RiceBitVector.h:102-120), one sentinel, retrieval input concatenated.
+ * nb_global must be max(1, ceil(N / bucket_size)) for the total key count N. The merged result
+ * lives in plain host memory and is released with shg_result_free like any other. */
+shg_status shg_build_shard_hash128(shg_engine *e, const shg_params *p, const uint64_t *first,
+                                   const uint64_t *second, uint64_t n, uint64_t nb_global, uint64_t b0,
+                                   uint64_t b1, shg_result *out);
+shg_status shg_merge_shards(const shg_params *p, const shg_result *shards, uint64_t nshards, shg_result *out);
+
 /* Hash n string keys (bytes + offsets[n+1], host memory) to 128-bit fingerprints on the device:
  * sux spooky(key, len, 0) as used by ShockHash.h:129. */
 shg_status shg_hash_strings(shg_engine *e, const char *bytes, const uint64_t *offsets, uint64_t n,

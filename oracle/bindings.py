@@ -203,6 +203,9 @@ class PortLib(_Lib):
         L = self.lib
         L.port_build.restype = _vp
         L.port_build.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_uint64, ctypes.c_uint64]
+        L.port_build_shard.restype = _vp
+        L.port_build_shard.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_uint64, ctypes.c_uint64,
+                                       ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64]
         L.port_node_count.restype = ctypes.c_uint64
         L.port_node_count.argtypes = [_vp]
         L.port_sh2_leaf.restype = ctypes.c_uint64
@@ -227,6 +230,18 @@ class PortLib(_Lib):
         self.lib.port_get_sorted_keys(_vp(h), _ptr(b.sorted_keys))
         b.work = np.zeros(7, np.uint64)
         self.lib.port_get_work(_vp(h), _ptr(b.work))
+        return b
+
+    def build_shard(self, variant, leaf, first, second, nb_global, b0, b1, bucket_size=2000):
+        """Buckets [b0, b1) of a structure with nb_global buckets, from exactly the keys in them."""
+        first = np.ascontiguousarray(first, dtype=np.uint64)
+        second = np.ascontiguousarray(second, dtype=np.uint64)
+        h = self.lib.port_build_shard(variant, leaf, _ptr(first), _ptr(second), len(first), bucket_size, nb_global, b0,
+                                      b1)
+        if not h:
+            raise ValueError("port shard build failed")
+        b = Built(self.lib, "port_", h)
+        b.n = len(first)
         return b
 
     def memo(self, variant, leaf):

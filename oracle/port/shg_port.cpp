@@ -483,10 +483,15 @@ struct PortResult {
 
 // hash_gen (ShockHash.h:602-654 / ShockHash2.h:441-494) with parallelPartition (Sorter.hpp:15-36):
 // sort by `first` (ties by input position), bucket = remap128(first, nbuckets).
-PortResult *build(int variant, int leaf, const uint64_t *first, const uint64_t *second, uint64_t n, uint64_t bucket_size) {
+// A shard (nb_map != 0) holds the buckets [b0, b0 + nb_local) of a structure with nb_map buckets,
+// built from exactly the keys that fall in them; bucket = remap128(first, nb_map) - b0.
+PortResult *build(int variant, int leaf, const uint64_t *first, const uint64_t *second, uint64_t n, uint64_t bucket_size,
+                  uint64_t nb_map = 0, uint64_t b0 = 0, uint64_t nb_local = 0) {
     auto *r = new PortResult(variant, leaf);
     r->n = n;
     r->nbuckets = std::max<uint64_t>(1, (n + bucket_size - 1) / bucket_size);
+    if (nb_map) r->nbuckets = nb_local;
+    else nb_map = r->nbuckets;
     std::vector<uint64_t> idx(n);
     for (uint64_t i = 0; i < n; i++) idx[i] = i;
     std::stable_sort(idx.begin(), idx.end(), [&](uint64_t a, uint64_t b) { return first[a] < first[b]; });
@@ -496,8 +501,9 @@ PortResult *build(int variant, int leaf, const uint64_t *first, const uint64_t *
         uint64_t i = 0;
         for (uint64_t bk = 0; bk < r->nbuckets; bk++) {
             r->size_acc[bk] = i;
-            while (i < n && remap128(first[idx[i]], r->nbuckets) == bk) { r->sorted_keys[i] = second[idx[i]]; i++; }
+            while (i < n && remap128(first[idx[i]], nb_map) - b0 == bk) { r->sorted_keys[i] = second[idx[i]]; i++; }
         }
+        if (i != n) throw std::runtime_error("a key lies outside the shard's buckets");
         r->size_acc[r->nbuckets] = n;
     }
     std::vector<uint64_t> keys = r->sorted_keys;
@@ -647,6 +653,15 @@ void port_memo(int variant, int leaf, uint64_t *out) {
 void *port_build(int variant, int leaf, const uint64_t *first, const uint64_t *second, uint64_t n, uint64_t bucket_size) {
     try {
         return build(variant, leaf, first, second, n, bucket_size);
+    } catch (...) {
+        return nullptr;
+    }
+}
+void *port_build_shard(int variant, int leaf, const uint64_t *first, const uint64_t *second, uint64_t n,
+                       uint64_t bucket_size, uint64_t nb_global, uint64_t b0, uint64_t b1) {
+    try {
+        if (b0 >= b1 || b1 > nb_global) return nullptr;
+        return build(variant, leaf, first, second, n, bucket_size, nb_global, b0, b1 - b0);
     } catch (...) {
         return nullptr;
     }

@@ -91,6 +91,8 @@ def lib():
         "shg_build_strings": ([_vp, P, ctypes.c_char_p, _vp, _u64, R], ctypes.c_int),
         "shg_result_free": ([R], None),
         "shg_build_batch_u64": ([_vp, P, _vp, _vp, _u64, _vp], ctypes.c_int),
+        "shg_build_shard_hash128": ([_vp, P, _vp, _vp, _u64, _u64, _u64, _u64, R], ctypes.c_int),
+        "shg_merge_shards": ([P, _vp, _u64, R], ctypes.c_int),
         "shg_hash_strings": ([_vp, ctypes.c_char_p, _vp, _u64, _vp, _vp], ctypes.c_int),
         "shg_sh2_construct_leaves": ([_vp, _vp, _vp, _u64, _vp, _vp], ctypes.c_int),
         "shg_sh1_construct_leaves": ([_vp, _vp, _vp, _u64, ctypes.c_int, _vp, _vp, _vp], ctypes.c_int),
@@ -296,6 +298,16 @@ class Engine:
             results.append(BuildResult(p, res, self))
         return results
 
+    def build_shard_hash128(self, variant, leaf_size, first, second, nb_global, b0, b1, bucket_size=2000,
+                            mode=MODE_DEFAULT):
+        """Buckets [b0, b1) of a structure with nb_global buckets, from exactly the keys in them."""
+        first = np.ascontiguousarray(first, dtype=np.uint64)
+        second = np.ascontiguousarray(second, dtype=np.uint64)
+        p, res = self.params(variant, leaf_size, bucket_size, mode, 0), _Result()
+        st = lib().shg_build_shard_hash128(self._h, ctypes.byref(p), _ptr(first), _ptr(second), len(first), nb_global,
+                                           b0, b1, ctypes.byref(res))
+        return self._finish(p, st, res)
+
     def build_u64_device(self, variant, leaf_size, d_keys_ptr, n, bucket_size=2000, mode=MODE_DEFAULT):
         p, res = self.params(variant, leaf_size, bucket_size, mode, 0), _Result()
         st = lib().shg_build_u64_device(self._h, ctypes.byref(p), _vp(d_keys_ptr), n, ctypes.byref(res))
@@ -467,6 +479,38 @@ class _Mphf:
                 lib().shg_mphf_destroy(self._h)
         except Exception:
             pass
+
+
+def merge_shards(variant, leaf_size, shards, bucket_size=2000):
+    """Join shard results (bucket order) into the result of one build over all their keys.
+    ``shards`` are BuildResults or objects with the same array attributes (numpy uint64/uint8)."""
+    R = len(shards)
+    arr = (_Result * R)()
+    keep = []
+    for g, sh in enumerate(shards):
+        cols = {}
+        for name, dt in (("bucket_size_acc", np.uint64), ("bucket_pos_acc", np.uint64), ("descriptors", np.uint64),
+                         ("ribbon_keys", np.uint64), ("ribbon_bits", np.uint8)):
+            a = np.ascontiguousarray(getattr(sh, name), dtype=dt)
+            if a.size == 0:
+                a = np.zeros(1, dt)
+            keep.append(a)
+            cols[name] = a
+        r = arr[g]
+        r.n = int(sh.n)
+        r.nbuckets = int(sh.nbuckets)
+        r.bucket_size_acc = cols["bucket_size_acc"].ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+        r.bucket_pos_acc = cols["bucket_pos_acc"].ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+        r.descriptors = cols["descriptors"].ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+        r.desc_words = len(sh.descriptors)
+        r.desc_bits = int(cols["bucket_pos_acc"][-1]) + 1  # code bits + the sentinel
+        r.ribbon_keys = cols["ribbon_keys"].ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+        r.ribbon_bits = cols["ribbon_bits"].ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
+        r.ribbon_n = len(sh.ribbon_keys)
+    p = Engine.params(variant, leaf_size, bucket_size)
+    out = _Result()
+    _check(lib().shg_merge_shards(ctypes.byref(p), arr, R, ctypes.byref(out)))
+    return BuildResult(p, out, None)
 
 
 class DeviceMphf:

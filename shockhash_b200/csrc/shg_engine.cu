@@ -86,6 +86,7 @@ struct PinnedBlock {
     void *p = nullptr;
     size_t cap = 0;
     bool in_use = false;
+    bool host = false;  // plain malloc (merged shards), freed on release
     shg_engine *eng = nullptr;
 };
 static std::mutex g_pool_mu;
@@ -96,7 +97,10 @@ static void release_pinned(PinnedBlock *b) {
         b->in_use = false;
         return;
     }
-    if (b->p) cudaFreeHost(b->p);
+    if (b->host)
+        free(b->p);
+    else if (b->p)
+        cudaFreeHost(b->p);
     delete b;
 }
 
@@ -205,15 +209,28 @@ shg_status check_params(const shg_params *p, uint64_t n) {
 // back in d_first / d_second (request r holds nr[r] keys). Every request gets its own bucket range
 // and its own products (as if built alone); the partition, the split levels and the leaf search of
 // all requests share the same launches.
+// A request that is one shard of a larger structure: it owns buckets [b0, b1) of nb_global.
+struct ShardSpec {
+    uint64_t nb_global, b0, b1;
+};
+
 shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_first, const uint64_t *d_second,
-                       const std::vector<uint64_t> &nr, shg_result *outs, float hash_ms) {
+                       const std::vector<uint64_t> &nr, shg_result *outs, float hash_ms,
+                       const ShardSpec *shard = nullptr) {
     const Config &cfg = config_of(p->variant, p->leaf_size);
     cudaStream_t s = e->stream;
     const size_t R = nr.size();
-    std::vector<uint64_t> off(R + 1, 0), nbr(R), boff(R + 1, 0);
+    if (shard && R != 1) return fail(SHG_ERR_ARG, "a shard build holds one request");
+    std::vector<uint64_t> off(R + 1, 0), nbr(R), boff(R + 1, 0), nb_map(R), b0(R, 0);
     for (size_t r = 0; r < R; r++) {
         off[r + 1] = off[r] + nr[r];
         nbr[r] = std::max<uint64_t>(1, (nr[r] + p->bucket_size - 1) / p->bucket_size);  // ShockHash.h:616
+        nb_map[r] = nbr[r];
+        if (shard) {
+            nbr[r] = shard->b1 - shard->b0;
+            nb_map[r] = shard->nb_global;
+            b0[r] = shard->b0;
+        }
         boff[r + 1] = boff[r] + nbr[r];
         memset(&outs[r], 0, sizeof(shg_result));
         outs[r].n = nr[r];
@@ -235,17 +252,22 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
     // ---- partition: each request's keys into its own bucket range, then one sort pass
     CU(cudaEventRecord(e->ev[0], s));
     for (size_t r = 0; r < R; r++)
-        launch_bucket_count(d_first + off[r], nr[r], nbr[r], e->counts.as<uint32_t>() + boff[r], s);
+        launch_bucket_count(d_first + off[r], nr[r], nbr[r], nb_map[r], b0[r], e->counts.as<uint32_t>() + boff[r], &misc->err,
+                            s);
     launch_scan_counts(e->counts.as<uint32_t>(), nb, e->acc.as<uint64_t>(), e->cursor.as<uint32_t>(), &misc->maxsz, s);
     std::vector<uint64_t> acc(nb + 1);
     uint32_t maxsz = 0;
     CU(cudaMemcpyAsync(acc.data(), e->acc.p, (nb + 1) * 8, cudaMemcpyDeviceToHost, s));
     CU(cudaMemcpyAsync(&maxsz, &misc->maxsz, 4, cudaMemcpyDeviceToHost, s));
+    uint32_t perr = 0;
+    CU(cudaMemcpyAsync(&perr, &misc->err, 4, cudaMemcpyDeviceToHost, s));
     CU(cudaStreamSynchronize(s));
+    if (perr & kErrArg) return fail(SHG_ERR_ARG, "a key lies outside the shard's bucket range");
     if (maxsz >= (uint32_t)kMaxBucket)
         return fail(SHG_ERR_BUCKET, "a bucket holds " + std::to_string(maxsz) + " keys (MAX_BUCKET_SIZE is 3000)");
     for (size_t r = 0; r < R; r++)
-        launch_bucket_scatter(d_first + off[r], nr[r], nbr[r], e->cursor.as<uint32_t>() + boff[r], e->sfirst.as<uint64_t>(),
+        launch_bucket_scatter(d_first + off[r], nr[r], nbr[r], nb_map[r], b0[r], e->cursor.as<uint32_t>() + boff[r],
+                              e->sfirst.as<uint64_t>(),
                               e->sidx.as<uint32_t>(), off[r], s);
     launch_bucket_sort(e->acc.as<uint64_t>(), nb, e->sfirst.as<uint64_t>(), e->sidx.as<uint32_t>(), d_second,
                        e->keys.as<uint64_t>(), s);
@@ -843,6 +865,98 @@ shg_status shg_build_hash128(shg_engine *e, const shg_params *p, const uint64_t 
         CU(cudaMemcpyAsync(e->second.p, second, n * 8, cudaMemcpyHostToDevice, e->stream));
     }
     return build_core(e, p, e->first.as<uint64_t>(), e->second.as<uint64_t>(), n, out, 0.f);
+}
+
+shg_status shg_build_shard_hash128(shg_engine *e, const shg_params *p, const uint64_t *first, const uint64_t *second,
+                                   uint64_t n, uint64_t nb_global, uint64_t b0, uint64_t b1, shg_result *out) {
+    if (!e || !out || (n && (!first || !second))) return fail(SHG_ERR_ARG, "null argument");
+    if (b0 >= b1 || b1 > nb_global) return fail(SHG_ERR_ARG, "bucket range must satisfy b0 < b1 <= nb_global");
+    shg_status st = check_params(p, n);
+    if (st) return st;
+    CU(cudaSetDevice(e->device));
+    CU(e->first.ensure(std::max<uint64_t>(n, 1) * 8));
+    CU(e->second.ensure(std::max<uint64_t>(n, 1) * 8));
+    if (n) {
+        CU(cudaMemcpyAsync(e->first.p, first, n * 8, cudaMemcpyHostToDevice, e->stream));
+        CU(cudaMemcpyAsync(e->second.p, second, n * 8, cudaMemcpyHostToDevice, e->stream));
+    }
+    const ShardSpec shard{nb_global, b0, b1};
+    return build_batch(e, p, e->first.as<uint64_t>(), e->second.as<uint64_t>(), std::vector<uint64_t>{n}, out, 0.f, &shard);
+}
+
+shg_status shg_merge_shards(const shg_params *p, const shg_result *shards, uint64_t nshards, shg_result *out) {
+    if (!p || !shards || !out || nshards == 0) return fail(SHG_ERR_ARG, "null argument or no shards");
+    memset(out, 0, sizeof(shg_result));
+    uint64_t n = 0, nb = 0, code_bits = 0, rn = 0;
+    for (uint64_t g = 0; g < nshards; g++) {
+        const shg_result &r = shards[g];
+        if (r.nbuckets == 0 || !r.bucket_size_acc || !r.bucket_pos_acc || r.desc_bits < 1 ||
+            (r.desc_words && !r.descriptors) || (r.ribbon_n && (!r.ribbon_keys || !r.ribbon_bits)))
+            return fail(SHG_ERR_ARG, "shard " + std::to_string(g) + " is not a build result");
+        if (r.bucket_size_acc[r.nbuckets] != r.n) return fail(SHG_ERR_ARG, "shard key count mismatch");
+        n += r.n;
+        nb += r.nbuckets;
+        code_bits += r.desc_bits - 1;  // without the shard's sentinel
+        rn += r.ribbon_n;
+    }
+    if (nb != std::max<uint64_t>(1, (n + p->bucket_size - 1) / p->bucket_size))
+        return fail(SHG_ERR_ARG, "shards do not cover the buckets of one structure of " + std::to_string(n) + " keys");
+    // RiceBitVector::Builder: the sentinel appendFixed(1, 1), then the word count of its final resize
+    const uint64_t bits = code_bits + 1;
+    const uint64_t words = ((bits + 7) / 8 + 14) / 8;
+    const size_t acc_bytes = (nb + 1) * 8;
+    const size_t bytes = 2 * acc_bytes + words * 8 + rn * 8 + rn + 64;
+    auto *blk = new PinnedBlock();
+    blk->host = true;
+    blk->in_use = true;
+    blk->p = calloc(1, bytes);
+    blk->cap = bytes;
+    if (!blk->p) {
+        delete blk;
+        return fail(SHG_ERR_OOM, "host allocation failed");
+    }
+    uint8_t *hp = (uint8_t *)blk->p;
+    out->owner = blk;
+    out->n = n;
+    out->nbuckets = nb;
+    out->bucket_size_acc = (uint64_t *)hp;
+    out->bucket_pos_acc = (uint64_t *)(hp + acc_bytes);
+    out->descriptors = (uint64_t *)(hp + 2 * acc_bytes);
+    out->ribbon_keys = (uint64_t *)(hp + 2 * acc_bytes + words * 8);
+    out->ribbon_bits = hp + 2 * acc_bytes + words * 8 + rn * 8;
+    out->desc_words = words;
+    out->desc_bits = bits;
+    out->ribbon_n = rn;
+    uint64_t kb = 0, bb = 0, bitpos = 0, ro = 0;
+    for (uint64_t g = 0; g < nshards; g++) {
+        const shg_result &r = shards[g];
+        for (uint64_t b = 0; b < r.nbuckets; b++) {
+            out->bucket_size_acc[bb + b] = kb + r.bucket_size_acc[b];
+            out->bucket_pos_acc[bb + b] = bitpos + r.bucket_pos_acc[b];
+        }
+        // appendRiceBitVector (RiceBitVector.h:102-120): the shard's code bits at the current bit position
+        const uint64_t nbits = r.desc_bits - 1;
+        for (uint64_t w = 0; w * 64 < nbits; w++) {
+            uint64_t v = r.descriptors[w];
+            const uint64_t left = nbits - w * 64;
+            if (left < 64) v &= (1ull << left) - 1;
+            const uint64_t at = bitpos + w * 64;
+            out->descriptors[at / 64] |= v << (at % 64);
+            if (at % 64) out->descriptors[at / 64 + 1] |= v >> (64 - at % 64);
+        }
+        if (r.ribbon_n) {
+            memcpy(out->ribbon_keys + ro, r.ribbon_keys, r.ribbon_n * 8);
+            memcpy(out->ribbon_bits + ro, r.ribbon_bits, r.ribbon_n);
+        }
+        kb += r.n;
+        bb += r.nbuckets;
+        bitpos += nbits;
+        ro += r.ribbon_n;
+    }
+    out->bucket_size_acc[nb] = kb;
+    out->bucket_pos_acc[nb] = bitpos;
+    out->descriptors[bitpos / 64] |= 1ull << (bitpos % 64);  // sentinel
+    return SHG_OK;
 }
 
 shg_status shg_build_u64_device(shg_engine *e, const shg_params *p, const uint64_t *d_keys, uint64_t n, shg_result *out) {

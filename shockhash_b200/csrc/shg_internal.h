@@ -100,11 +100,12 @@ enum : uint32_t { kErrTrialLimit = 1, kErrScratch = 2, kErrBucket = 4, kErrInter
 void launch_spooky_u64(const uint64_t *keys, uint64_t n, uint64_t *first, uint64_t *second, cudaStream_t s);
 void launch_spooky_strings(const uint8_t *bytes, const uint64_t *offsets, uint64_t n, uint64_t *first,
                            uint64_t *second, cudaStream_t s);
-void launch_bucket_count(const uint64_t *first, uint64_t n, uint64_t nb, uint32_t *counts, cudaStream_t s);
+void launch_bucket_count(const uint64_t *first, uint64_t n, uint64_t nb, uint64_t nb_map, uint64_t b0, uint32_t *counts,
+                         uint32_t *err, cudaStream_t s);
 void launch_scan_counts(const uint32_t *counts, uint64_t nb, uint64_t *acc, uint32_t *cursor, uint32_t *maxsz,
                         cudaStream_t s);
-void launch_bucket_scatter(const uint64_t *first, uint64_t n, uint64_t nb, uint32_t *cursor, uint64_t *sfirst,
-                           uint32_t *sidx, uint64_t idx_base, cudaStream_t s);
+void launch_bucket_scatter(const uint64_t *first, uint64_t n, uint64_t nb, uint64_t nb_map, uint64_t b0, uint32_t *cursor,
+                           uint64_t *sfirst, uint32_t *sidx, uint64_t idx_base, cudaStream_t s);
 void launch_bucket_sort(const uint64_t *acc, uint64_t nb, const uint64_t *sfirst, const uint32_t *sidx,
                         const uint64_t *second, uint64_t *keys, cudaStream_t s);
 void launch_split_level(const Node *nodes, const uint32_t *ids, uint32_t count, uint64_t *keys,

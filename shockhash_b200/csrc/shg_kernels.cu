@@ -47,9 +47,16 @@ void launch_spooky_strings(const uint8_t *bytes, const uint64_t *offsets, uint64
 // ------------------------------------------------------------------------------ partition
 // Bucket of a key: remap128(first, nbuckets) (ShockHash.h:297, Sorter.hpp:248); monotone in
 // `first`, so sorting by `first` globally equals bucketing followed by a sort inside each bucket.
-__global__ void k_bucket_count(const uint64_t *__restrict__ first, uint64_t n, uint64_t nb, uint32_t *__restrict__ counts) {
+// bucket = remap128(first, nb_map) - b0 must fall in [0, nb): a shard of a larger structure owns
+// the buckets [b0, b0 + nb) of nb_map; a key outside them sets kErrArg and is skipped.
+__global__ void k_bucket_count(const uint64_t *__restrict__ first, uint64_t n, uint64_t nb, uint64_t nb_map, uint64_t b0,
+                               uint32_t *__restrict__ counts, uint32_t *__restrict__ err) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t b = remap128(first[i], nb);
+        const uint64_t b = remap128(first[i], nb_map) - b0;
+        if (b >= nb) {
+            atomicOr(err, kErrArg);
+            continue;
+        }
         atomicAdd(&counts[b], 1u);
     }
 }
@@ -98,12 +105,13 @@ __global__ void k_scan_counts(const uint32_t *__restrict__ counts, uint64_t nb, 
     atomicMax(maxsz, local_max);
 }
 
-__global__ void k_bucket_scatter(const uint64_t *__restrict__ first, uint64_t n, uint64_t nb,
-                                 uint32_t *__restrict__ cursor, uint64_t *__restrict__ sfirst,
+__global__ void k_bucket_scatter(const uint64_t *__restrict__ first, uint64_t n, uint64_t nb, uint64_t nb_map,
+                                 uint64_t b0, uint32_t *__restrict__ cursor, uint64_t *__restrict__ sfirst,
                                  uint32_t *__restrict__ sidx, uint64_t idx_base) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t f = first[i];
-        const uint64_t b = remap128(f, nb);
+        const uint64_t b = remap128(f, nb_map) - b0;
+        if (b >= nb) continue;  // reported by k_bucket_count
         const uint32_t pos = atomicAdd(&cursor[b], 1u);
         sfirst[pos] = f;
         sidx[pos] = (uint32_t)(idx_base + i);
@@ -180,18 +188,19 @@ void launch_compact_ribbon(const uint64_t *keys, const uint8_t *bits, uint64_t n
     if (n) k_compact_ribbon<<<grid_for(n, 256), 256, 0, s>>>(keys, bits, n, singles, nsingles, out_keys, out_bits);
 }
 
-void launch_bucket_count(const uint64_t *first, uint64_t n, uint64_t nb, uint32_t *counts, cudaStream_t s) {
+void launch_bucket_count(const uint64_t *first, uint64_t n, uint64_t nb, uint64_t nb_map, uint64_t b0, uint32_t *counts,
+                         uint32_t *err, cudaStream_t s) {
     cudaMemsetAsync(counts, 0, nb * sizeof(uint32_t), s);
-    if (n) k_bucket_count<<<grid_for(n, 256), 256, 0, s>>>(first, n, nb, counts);
+    if (n) k_bucket_count<<<grid_for(n, 256), 256, 0, s>>>(first, n, nb, nb_map, b0, counts, err);
 }
 void launch_scan_counts(const uint32_t *counts, uint64_t nb, uint64_t *acc, uint32_t *cursor, uint32_t *maxsz,
                         cudaStream_t s) {
     cudaMemsetAsync(maxsz, 0, sizeof(uint32_t), s);
     k_scan_counts<<<1, 1024, 0, s>>>(counts, nb, acc, cursor, maxsz);
 }
-void launch_bucket_scatter(const uint64_t *first, uint64_t n, uint64_t nb, uint32_t *cursor, uint64_t *sfirst,
-                           uint32_t *sidx, uint64_t idx_base, cudaStream_t s) {
-    if (n) k_bucket_scatter<<<grid_for(n, 256), 256, 0, s>>>(first, n, nb, cursor, sfirst, sidx, idx_base);
+void launch_bucket_scatter(const uint64_t *first, uint64_t n, uint64_t nb, uint64_t nb_map, uint64_t b0, uint32_t *cursor,
+                           uint64_t *sfirst, uint32_t *sidx, uint64_t idx_base, cudaStream_t s) {
+    if (n) k_bucket_scatter<<<grid_for(n, 256), 256, 0, s>>>(first, n, nb, nb_map, b0, cursor, sfirst, sidx, idx_base);
 }
 void launch_bucket_sort(const uint64_t *acc, uint64_t nb, const uint64_t *sfirst, const uint32_t *sidx,
                         const uint64_t *second, uint64_t *keys, cudaStream_t s) {
