@@ -44,8 +44,8 @@ template <> struct Sh2Cfg<64> {
 };
 template <> struct Sh2Cfg<128> {
     using Mask = uint64_t;
-    static constexpr int SMS = 512;
-    static constexpr int CMS = 384;
+    static constexpr int SMS = 256;   // 17 KB of shared memory per warp: three 4-warp blocks per SM
+    static constexpr int CMS = 256;
     static constexpr int ISO_WORDS = 2;
     static constexpr uint32_t ROWS = 4096;
 };
@@ -370,6 +370,7 @@ __global__ void __launch_bounds__(128) k_leaves_sh2_v2(Src src, uint32_t count, 
                     };
                     const uint64_t in_sm = min(s + 1, (uint64_t)Sh2Cfg<MAXM>::SMS);
                     for (uint64_t p = 0; p < in_sm; p++) visit(p, sm.mask[p]);
+#pragma unroll 4
                     for (uint64_t p = in_sm; p <= s; p++) visit(p, g.mask[p]);
                     mine = mineA + mineB;
                 } else {
