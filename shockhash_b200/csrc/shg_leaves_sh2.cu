@@ -41,6 +41,7 @@ template <> struct Sh2Cfg<64> {
     static constexpr int CMS = 256;   // candidates held in shared memory
     static constexpr int ISO_WORDS = 1;
     static constexpr uint32_t ROWS = 2048;  // candidates whose cell rows are cached in global scratch
+    static constexpr uint32_t RAW_ROWS = 2048;  // raw seeds whose cell rows are cached
 };
 template <> struct Sh2Cfg<128> {
     using Mask = uint64_t;
@@ -48,6 +49,7 @@ template <> struct Sh2Cfg<128> {
     static constexpr int CMS = 256;
     static constexpr int ISO_WORDS = 2;
     static constexpr uint32_t ROWS = 4096;
+    static constexpr uint32_t RAW_ROWS = 1024;
 };
 
 template <int MAXM> struct Sh2Smem {
@@ -73,7 +75,8 @@ template <int MAXM> struct Sh2Global {
     uint32_t *csa, *csb;  // [cmax]
     uint64_t *iso;        // [cmax][2]
     uint64_t *rows;       // [rcap][MAXM / 8]
-    uint32_t rcap;
+    uint64_t *raw;        // [rawcap][MAXM / 8]: cells of every key (finder order) under raw seed s
+    uint32_t rcap, rawcap;
     __device__ void carve(uint8_t *base, uint32_t smax, uint32_t cmax) {
         mask = (MaskPair<Mask> *)base;
         iso = (uint64_t *)(base + ((2ull * smax * sizeof(Mask) + 255) & ~255ull));
@@ -81,6 +84,8 @@ template <int MAXM> struct Sh2Global {
         csb = csa + cmax;
         rows = (uint64_t *)(csb + cmax);  // 8-byte aligned: cmax is even
         rcap = cmax < Sh2Cfg<MAXM>::ROWS ? cmax : Sh2Cfg<MAXM>::ROWS;
+        raw = rows + (uint64_t)rcap * (MAXM / 8);
+        rawcap = smax < Sh2Cfg<MAXM>::RAW_ROWS ? smax : Sh2Cfg<MAXM>::RAW_ROWS;
     }
 };
 
@@ -336,9 +341,17 @@ __global__ void __launch_bounds__(128) k_leaves_sh2_v2(Src src, uint32_t count, 
                 }
                 const uint64_t s = S + lane;
                 typename LeafCtx<MAXM>::Mask tA = 0, tB = 0;
+                uint64_t *rrow = s < g.rawcap ? g.raw + s * (MAXM / 8) : nullptr;
+                uint64_t word = 0;
                 for (uint32_t k = 0; k < m; k++) {
-                    const auto bit = (typename LeafCtx<MAXM>::Mask)1 << half_hash(sm.keys[k], s, half);
+                    const uint32_t h = half_hash(sm.keys[k], s, half);
+                    const auto bit = (typename LeafCtx<MAXM>::Mask)1 << h;
                     if (k < cx.sizeA) tA |= bit; else tB |= bit;
+                    word |= (uint64_t)h << (8 * (k & 7));
+                    if ((k & 7) == 7 || k + 1 == m) {
+                        if (rrow) rrow[k >> 3] = word;
+                        word = 0;
+                    }
                 }
                 cx.mp(s) = MaskPair<typename LeafCtx<MAXM>::Mask>{tA, tB};
                 w_evals += m;
@@ -428,7 +441,56 @@ __global__ void __launch_bounds__(128) k_leaves_sh2_v2(Src src, uint32_t count, 
             // 3. isolated-key masks of the new candidates (calculateIsolatedVertices), one per lane
             for (uint32_t c0 = J; c0 < J + T; c0 += 32) {
                 const uint32_t c = c0 + lane;
-                if (c < J + T) {
+                if (c < J + T && cx.csa(c) < g.rawcap && cx.csb(c) < g.rawcap) {
+                    // cells from the two raw seeds' rows: set-A keys under seedA, set-B keys under seedB
+                    const uint64_t *ra = g.raw + (uint64_t)cx.csa(c) * (MAXM / 8);
+                    const uint64_t *rb = g.raw + (uint64_t)cx.csb(c) * (MAXM / 8);
+                    uint64_t *row = c < g.rcap ? g.rows + (uint64_t)c * (MAXM / 8) : nullptr;
+                    const uint32_t sizeA = cx.sizeA;
+                    auto word_of = [&](uint32_t w) {  // cells of keys 8w..8w+7, one byte each
+                        const uint32_t k0 = 8 * w;
+                        uint64_t v;
+                        if (k0 + 8 <= sizeA) v = ra[w];
+                        else if (k0 >= sizeA) v = rb[w];
+                        else {
+                            const uint64_t keep = (1ull << (8 * (sizeA - k0))) - 1;
+                            v = (ra[w] & keep) | (rb[w] & ~keep);
+                        }
+                        if (k0 + 8 > m) v &= (1ull << (8 * (m - k0))) - 1;
+                        return v;
+                    };
+                    uint64_t seen1 = 0, seen2 = 0;
+#pragma unroll 1
+                    for (uint32_t w = 0; 8 * w < m; w++) {
+                        const uint64_t v = word_of(w);
+                        if (row) row[w] = v;
+                        const uint32_t kn = min(8u, m - 8 * w);
+#pragma unroll
+                        for (uint32_t t = 0; t < 8; t++) {
+                            if (t < kn) {
+                                const uint64_t bit = 1ull << ((v >> (8 * t)) & 0xFF);
+                                seen2 |= seen1 & bit;
+                                seen1 |= bit;
+                            }
+                        }
+                    }
+                    const uint64_t single = seen1 & ~seen2;
+                    uint64_t iso0 = 0, iso1 = 0;
+#pragma unroll 1
+                    for (uint32_t w = 0; 8 * w < m; w++) {
+                        const uint64_t v = word_of(w);
+                        const uint32_t kn = min(8u, m - 8 * w);
+                        uint64_t b8 = 0;
+#pragma unroll
+                        for (uint32_t t = 0; t < 8; t++)
+                            if (t < kn) b8 |= ((single >> ((v >> (8 * t)) & 0xFF)) & 1) << t;
+                        const uint32_t k0 = 8 * w;
+                        if (k0 < 64) iso0 |= b8 << k0; else iso1 |= b8 << (k0 - 64);
+                    }
+                    cx.iso(c, 0) = iso0;
+                    if (Sh2Cfg<MAXM>::ISO_WORDS > 1) cx.iso(c, 1) = iso1;
+                    w_evals += m;  // the reference hashes the candidate's keys here (makeCache)
+                } else if (c < J + T) {
                     const uint64_t sa = cx.csa(c), sb = cx.csb(c);
                     uint64_t seen1 = 0, seen2 = 0, word = 0;
                     uint64_t *row = c < g.rcap ? g.rows + (uint64_t)c * (MAXM / 8) : nullptr;
@@ -547,7 +609,8 @@ void launch_v2(const Node *nodes, const uint32_t *ids, uint32_t count, const uin
 // Bytes of global scratch per warp for the given capacities (raw seeds, candidates).
 uint64_t sh2_scratch_bytes(uint32_t smax, uint32_t cmax, int max_leaf) {
     const uint64_t rows = std::min<uint64_t>(cmax, max_leaf > 64 ? Sh2Cfg<128>::ROWS : Sh2Cfg<64>::ROWS);
-    return 16ull * smax + 256 + 24ull * cmax + rows * (max_leaf > 64 ? 128 : 64);
+    const uint64_t raw = std::min<uint64_t>(smax, max_leaf > 64 ? Sh2Cfg<128>::RAW_ROWS : Sh2Cfg<64>::RAW_ROWS);
+    return 16ull * smax + 256 + 24ull * cmax + (rows + raw) * (max_leaf > 64 ? 128 : 64);
 }
 
 void launch_leaves_sh2_ctr(const Node *nodes, const uint32_t *ids, uint32_t count, const uint64_t *keys, uint64_t *codes,
