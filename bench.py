@@ -280,8 +280,9 @@ def main():
                 forms[f"{name}_device_ns_per_key"] = round(statistics.mean(t) * 1e6 / n, 3)
         if ws == 1 and not args.no_forms:
             pl_n = int(os.environ.get("SHG_PER_LEAF_SAMPLE", "100000"))
-            rp = eng.build_u64_device(VARIANT, LEAF, d_keys.data_ptr(), pl_n, BUCKET, shg.MODE_PER_LEAF)
-            rl = eng.build_u64_device(VARIANT, LEAF, d_keys.data_ptr(), pl_n, BUCKET, shg.MODE_LEVELS)
+            for _ in range(2):  # the second of each is reported (the first grows buffers for the size)
+                rp = eng.build_u64_device(VARIANT, LEAF, d_keys.data_ptr(), pl_n, BUCKET, shg.MODE_PER_LEAF)
+                rl = eng.build_u64_device(VARIANT, LEAF, d_keys.data_ptr(), pl_n, BUCKET, shg.MODE_LEVELS)
             forms["per_leaf_launch_ns_per_key_at_%d" % pl_n] = round(rp.stage_ms["total"] * 1e6 / pl_n, 3)
             forms["batched_ns_per_key_at_%d" % pl_n] = round(rl.stage_ms["total"] * 1e6 / pl_n, 3)
             forms["per_leaf_bit_exact_vs_batched"] = bool(np.array_equal(rp.descriptors, rl.descriptors))

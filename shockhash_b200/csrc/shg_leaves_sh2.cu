@@ -5,17 +5,20 @@
 // candidate i), that passes the isolated-key filter and the pseudoforest test, where candidates
 // arrive in ascending candidate-seed order. This kernel computes the same pair with the work laid
 // out for a warp:
-//   1. raw seeds are hashed 32 at a time (one seed per lane): coverage masks of set A / set B;
+//   1. raw seeds are hashed 32 at a time (one seed per lane): coverage masks of set A / set B
+//      (32-bit masks for leaves of up to 64 keys) and the seed's cell row (one byte per key);
 //   2. the candidates whose larger raw seed lies in that block of 32 are listed in the reference's
 //      order (lane L owns raw seed s0+L; its candidates (a<s, s) by a, then (s, b<=s) by b; lanes in
-//      order) with a count pass, a warp prefix sum and a write pass;
-//   3. every new candidate's isolated-key mask is computed (one candidate per lane);
+//      order): one scan over the earlier seeds' paired masks, the first partners kept in
+//      registers, a warp prefix sum for the positions;
+//   3. every new candidate's cell row and isolated-key mask are assembled from its two raw seeds'
+//      rows (one candidate per lane);
 //   4. all pairs (j, i) of the new batch are filtered lane-parallel in lexicographic order; the
 //      survivors go through a queue, 32 pseudoforest tests at a time (one per lane, union-find with
-//      a cycle flag per root; the cells are recomputed, nothing per key is stored); the first
-//      passing survivor in queue order is the answer (all pairs of earlier batches failed).
+//      a cycle flag per root over the cached cell rows); fewer than 32 wait for the next batch,
+//      and the first passing survivor in queue order is the answer.
 // Candidate and raw-seed state live in shared memory; indices past its capacity spill to a
-// per-warp slice of global scratch.
+// per-warp slice of global scratch, which also holds the cell rows.
 #include <algorithm>
 #include <cstdint>
 #include <mutex>
@@ -520,19 +523,28 @@ __global__ void __launch_bounds__(128) k_leaves_sh2_v2(Src src, uint32_t count, 
             }
             __syncwarp();
             // 4. all pairs (j, i), J <= j < J+T, i < j, in lexicographic order
+            // pair q = j(j-1)/2 + i; lanes take 32 consecutive q, decoded by stepping from the
+            // batch's first pair (jb, ib), which advances by 32 per batch
             const uint64_t q0 = (uint64_t)J * (J - 1) / 2, q1 = (uint64_t)(J + T) * (J + T - 1) / 2;
             bool done = false;
+            uint32_t jb = J > 0 ? J : 1, ib = 0;
             for (uint64_t qb = q0; qb < q1 && !done; qb += 32) {
                 const uint64_t q = qb + lane;
                 bool filt = false;
-                uint32_t j = 0, i = 0;
+                uint32_t j = jb, i = ib + lane;
+                while (i >= j) {
+                    i -= j;
+                    j++;
+                }
+                for (uint32_t adv = ib + 32; ; ) {  // next batch's first pair
+                    if (adv < jb) {
+                        ib = adv;
+                        break;
+                    }
+                    adv -= jb;
+                    jb++;
+                }
                 if (q < q1) {
-                    // j = largest with j(j-1)/2 <= q
-                    uint64_t jj = (uint64_t)((1.0 + sqrt(1.0 + 8.0 * (double)q)) * 0.5);
-                    while (jj * (jj - 1) / 2 > q) jj--;
-                    while ((jj + 1) * jj / 2 <= q) jj++;
-                    j = (uint32_t)jj;
-                    i = (uint32_t)(q - jj * (jj - 1) / 2);
                     uint64_t x = cx.iso(j, 0) & cx.iso(i, 0);
                     if (Sh2Cfg<MAXM>::ISO_WORDS > 1) x |= cx.iso(j, 1) & cx.iso(i, 1);
                     filt = x == 0;
@@ -548,8 +560,15 @@ __global__ void __launch_bounds__(128) k_leaves_sh2_v2(Src src, uint32_t count, 
                 __syncwarp();
                 if (sm.nsurv >= 32) done = drain(32);
             }
-            while (!done && sm.nsurv > 0) done = drain(32);
+            // Fewer than 32 survivors wait for the next round's pairs, so that pseudoforest tests
+            // run with full warps; the queue stays in (j, i) order, so the first passing entry is
+            // still the reference's answer.
+            while (!done && sm.nsurv >= 32) done = drain(32);
             J += T;
+        }
+        if (answer == ~0ull) {  // the survivors still queued come before anything not yet listed
+            while (answer == ~0ull && sm.nsurv > 0) drain(32);
+            if (answer != ~0ull) overflow = false;
         }
         if (overflow || answer == ~0ull) {
             if (lane == 0) atomicOr(err, kErrScratch);
