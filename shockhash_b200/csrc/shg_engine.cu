@@ -87,12 +87,14 @@ struct PinnedBlock {
     size_t cap = 0;
     bool in_use = false;
     bool host = false;  // plain malloc (merged shards), freed on release
+    int refs = 0;       // results that point into the block (a batch's results share one)
     shg_engine *eng = nullptr;
 };
 static std::mutex g_pool_mu;
 
 static void release_pinned(PinnedBlock *b) {
     std::lock_guard<std::mutex> lock(g_pool_mu);
+    if (--b->refs > 0) return;
     if (b->eng) {
         b->in_use = false;
         return;
@@ -155,7 +157,7 @@ shg_status hash_strings_into(shg_engine *e, const char *bytes, const uint64_t *o
 
 namespace {
 
-PinnedBlock *acquire_pinned(shg_engine *e, size_t bytes) {
+PinnedBlock *acquire_pinned(shg_engine *e, size_t bytes, int refs = 1) {
     std::lock_guard<std::mutex> lock(g_pool_mu);
     PinnedBlock *best = nullptr;
     for (PinnedBlock *b : e->pool)
@@ -171,6 +173,7 @@ PinnedBlock *acquire_pinned(shg_engine *e, size_t bytes) {
         e->pool.push_back(best);
     }
     best->in_use = true;
+    best->refs = refs;
     return best;
 }
 
@@ -451,19 +454,22 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
     }
     if (nsingles) CU(cudaMemcpyAsync(e->singles.p, rel_singles.data(), nsingles * 8, cudaMemcpyHostToDevice, s));
     const uint64_t *src_keys = p->variant == SHG_SHOCKHASH ? e->rib_keys.as<uint64_t>() : e->keys.as<uint64_t>();
-    std::vector<PinnedBlock *> blocks(R, nullptr);
+    // one pinned block for all of the batch's results (each result holds a reference)
+    std::vector<size_t> roff(R + 1, 0);
+    for (size_t r = 0; r < R; r++) {
+        const uint64_t rn = nr[r] - (soff[r + 1] - soff[r]);
+        const size_t acc_bytes = (nbr[r] + 1) * 8;
+        roff[r + 1] = roff[r] + ((2 * acc_bytes + words[r] * 8 + rn * 8 + rn + 64 + 63) & ~(size_t)63);
+    }
+    PinnedBlock *blk = acquire_pinned(e, roff[R], (int)R);
+    if (!blk) return fail(SHG_ERR_OOM, "pinned host allocation failed");
     for (size_t r = 0; r < R; r++) {
         shg_result *out = &outs[r];
         const uint64_t ns = soff[r + 1] - soff[r], rn = nr[r] - ns;
         launch_compact_ribbon(src_keys + off[r], e->rib_bits.as<uint8_t>() + off[r], nr[r], e->singles.as<uint64_t>() + soff[r], ns,
                               e->ckeys.as<uint64_t>() + off[r], e->cbits.as<uint8_t>() + off[r], s);
         const size_t acc_bytes = (nbr[r] + 1) * 8;
-        PinnedBlock *blk = acquire_pinned(e, 2 * acc_bytes + words[r] * 8 + rn * 8 + rn + 64);
-        if (!blk) {
-            for (size_t q = 0; q < r; q++) shg_result_free(&outs[q]);
-            return fail(SHG_ERR_OOM, "pinned host allocation failed");
-        }
-        uint8_t *hp = (uint8_t *)blk->p;
+        uint8_t *hp = (uint8_t *)blk->p + roff[r];
         out->owner = blk;
         out->bucket_size_acc = (uint64_t *)hp;
         out->bucket_pos_acc = (uint64_t *)(hp + acc_bytes);
@@ -909,6 +915,7 @@ shg_status shg_merge_shards(const shg_params *p, const shg_result *shards, uint6
     auto *blk = new PinnedBlock();
     blk->host = true;
     blk->in_use = true;
+    blk->refs = 1;
     blk->p = calloc(1, bytes);
     blk->cap = bytes;
     if (!blk->p) {
