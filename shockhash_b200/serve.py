@@ -11,7 +11,11 @@ batches of different workers overlap on the device.
 
 Admission is by free device memory: at start the server reads the free HBM, keeps `mem_fraction`
 of it, and gives every worker an equal share, which caps its batch at share / bytes_per_key keys
-(a larger request is built alone). Each result is bit-identical to building that request alone.
+and at `max_batch_keys` (a larger request is built alone). Each worker then builds one batch of
+that size before serving, so that its device buffers and its pinned result block exist before the
+first request arrives: growing them later would allocate and free device and pinned memory, which
+synchronises the whole device and stalls the other workers. Each result is bit-identical to
+building that request alone.
 
     python -m shockhash_b200.serve --requests 400
 prints one JSON line with p50/p99 build latency, aggregate keys/s and device utilisation for a
@@ -53,7 +57,7 @@ class Request:
 
 class BuildServer:
     def __init__(self, variant=SHOCKHASH2, leaf=64, bucket=2000, workers=2, device=0, mem_fraction=0.5,
-                 bytes_per_key=96, max_batch_keys=None, keep_results=True):
+                 bytes_per_key=96, max_batch_keys=32_000_000, keep_results=True, warm=True):
         self.variant, self.leaf, self.bucket = variant, leaf, bucket
         self.keep_results = keep_results
         free, _ = device_memory(device)
@@ -65,6 +69,12 @@ class BuildServer:
         self.busy_s = 0.0
         self.batches = []
         self._engines = [Engine(device) for _ in range(workers)]
+        if warm:  # size every worker's buffers for a full batch before serving
+            sample = keys_mt19937_64(0x5EED, self.batch_keys)
+            for e in self._engines:
+                for r in e.build_batch_u64(variant, leaf, [sample], bucket):
+                    r.free()
+            del sample
         self._threads = [threading.Thread(target=self._worker, args=(e,), daemon=True) for e in self._engines]
         for t in self._threads:
             t.start()
@@ -143,7 +153,7 @@ def poisson_stream(n_requests, rate=200.0, seed=31, lo_exp=3.0, hi_exp=7.0):
     return [(float(arrivals[i]), int(sizes[i]), seed * 1000003 + i) for i in range(n_requests)]
 
 
-def run_stream(stream, workers=2, leaf=64, bucket=2000, mem_fraction=0.5, max_batch_keys=None):
+def run_stream(stream, workers=2, leaf=64, bucket=2000, mem_fraction=0.5, max_batch_keys=32_000_000):
     # every request's keys exist before the clock starts, as a client's would when it submits
     all_keys = [keys_mt19937_64(kseed, size) for _, size, kseed in stream]
     srv = BuildServer(leaf=leaf, bucket=bucket, workers=workers, mem_fraction=mem_fraction,
@@ -184,9 +194,11 @@ def main():
     ap.add_argument("--seed", type=int, default=31)
     ap.add_argument("--leaf", type=int, default=64)
     ap.add_argument("--bucket", type=int, default=2000)
+    ap.add_argument("--max-batch-keys", type=int, default=32_000_000)
     args = ap.parse_args()
     stream = poisson_stream(args.requests, args.rate, args.seed)
-    out = run_stream(stream, workers=args.workers, leaf=args.leaf, bucket=args.bucket)
+    out = run_stream(stream, workers=args.workers, leaf=args.leaf, bucket=args.bucket,
+                     max_batch_keys=args.max_batch_keys)
     out.update({"metric": "ShockHash2 build service: p50/p99 build latency and aggregate keys/s",
                 "config": {"variant": "ShockHash2", "leaf_size": args.leaf, "bucket_size": args.bucket,
                            "arrivals": f"Poisson, mean {args.rate}/s, seed {args.seed}",
