@@ -38,7 +38,9 @@ typedef enum shg_status {
 /* Which reference class the build reproduces. */
 typedef enum shg_variant {
     SHG_SHOCKHASH = 1,   /* shockhash::ShockHash<leaf_size, false>            (include/ShockHash.h:134) */
-    SHG_SHOCKHASH2 = 2   /* shockhash::ShockHash2<leaf_size>                  (include/ShockHash2.h:117) */
+    SHG_SHOCKHASH2 = 2,  /* shockhash::ShockHash2<leaf_size>                  (include/ShockHash2.h:117) */
+    SHG_SHOCKHASH_ROTATION = 3  /* shockhash::ShockHash<leaf_size, true>: leaves of exactly leaf_size keys
+                                   use rotation fitting (ShockHash.h:316-399); leaf_size 2..60 */
 } shg_variant;
 
 /* How the search stages are scheduled on the device. All modes give identical results. */

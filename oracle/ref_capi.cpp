@@ -114,6 +114,7 @@ std::vector<std::string> make_strings(const char *bytes, const uint64_t *offsets
 }
 
 #define SHG_SH1_LEAVES(X) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(10) X(12) X(13) X(16) X(20) X(24) X(25) X(30) X(32) X(33) X(40) X(48) X(60)
+#define SHG_ROT_LEAVES(X) X(8) X(16) X(24) X(30) X(32) X(33) X(40) X(48)
 #define SHG_SH2_LEAVES(X) X(2) X(3) X(4) X(5) X(6) X(8) X(9) X(10) X(11) X(12) X(16) X(20) X(24) X(32) X(33) X(40) X(48) X(64) X(100) X(128)
 
 #define X(L) SHG_ROB_CLASS(shockhash::ShockHash<L COMMA false>, L) template struct Rob<RecSplitTag<shockhash::ShockHash<L COMMA false>>, &shockhash::ShockHash<L COMMA false>::recSplit>;
@@ -122,6 +123,9 @@ SHG_SH1_LEAVES(X)
 #undef X
 #define X(L) SHG_ROB_CLASS(shockhash::ShockHash2<L>, L)
 SHG_SH2_LEAVES(X)
+#undef X
+#define X(L) SHG_ROB_CLASS(shockhash::ShockHash<L COMMA true>, L)
+SHG_ROT_LEAVES(X)
 #undef X
 #undef COMMA
 
@@ -137,6 +141,23 @@ RefBase *make_sh1_str(int leaf, const std::vector<std::string> &keys, size_t b, 
     switch (leaf) {
 #define X(L) case L: return new RefRS<shockhash::ShockHash<L, false>, L>(keys, b, threads);
         SHG_SH1_LEAVES(X)
+#undef X
+        default: return nullptr;
+    }
+}
+// ShockHash<leaf, true>: rotation fitting for leaves of exactly `leaf` keys (ShockHash.h:316-399).
+RefBase *make_rot(int leaf, std::vector<hash128_t> &keys, size_t b, size_t threads) {
+    switch (leaf) {
+#define X(L) case L: return new RefRS<shockhash::ShockHash<L, true>, L>(keys, b, threads);
+        SHG_ROT_LEAVES(X)
+#undef X
+        default: return nullptr;
+    }
+}
+RefBase *make_rot_str(int leaf, const std::vector<std::string> &keys, size_t b, size_t threads) {
+    switch (leaf) {
+#define X(L) case L: return new RefRS<shockhash::ShockHash<L, true>, L>(keys, b, threads);
+        SHG_ROT_LEAVES(X)
 #undef X
         default: return nullptr;
     }
@@ -271,6 +292,7 @@ uint64_t ref_flat_sizeof(int k) {
 }
 uint64_t ref_sizeof(int variant, int leaf) {
     if (variant == 1) return sizeof(shockhash::ShockHash<30, false>);
+    if (variant == 3) return sizeof(shockhash::ShockHash<30, true>);
     return sizeof(shockhash::ShockHash2<64>);
 }
 uint64_t ref_flat_bits(void *h) { return ((FlatBase *)h)->bits(); }
@@ -335,6 +357,7 @@ void *ref_build_hash(int variant, int leaf, const uint64_t *first, const uint64_
     for (size_t i = 0; i < n; i++) keys[i] = hash128_t(first[i], second[i]);
     if (variant == 1) return make_sh1(leaf, keys, bucket_size, threads);
     if (variant == 2) return make_sh2(leaf, keys, bucket_size, threads);
+    if (variant == 3) return make_rot(leaf, keys, bucket_size, threads);
     return nullptr;
 }
 
@@ -344,6 +367,7 @@ void *ref_build_strings(int variant, int leaf, const char *bytes, const uint64_t
     auto keys = make_strings(bytes, offsets, n);
     if (variant == 1) return make_sh1_str(leaf, keys, bucket_size, threads);
     if (variant == 2) return make_sh2_str(leaf, keys, bucket_size, threads);
+    if (variant == 3) return make_rot_str(leaf, keys, bucket_size, threads);
     return nullptr;
 }
 

@@ -3,7 +3,7 @@
 Mirrors the reference's public classes (paths relative to the ShockHash reference project):
 
 * ``ShockHash[l](keys, bucket_size, num_threads=1)``  — ``shockhash::ShockHash<l, false>``
-  (include/ShockHash.h:134-191)
+  (include/ShockHash.h:134-191); ``ShockHash[l, True]`` — ``ShockHash<l, true>`` (rotation fitting)
 * ``ShockHash2[l](keys, bucket_size, num_threads=1)`` — ``shockhash::ShockHash2<l>``
   (include/ShockHash2.h:117-170)
 
@@ -21,12 +21,12 @@ import os
 import numpy as np
 
 __all__ = ["ShgError", "Engine", "BuildResult", "ShockHash", "ShockHash2", "ShockHash2Flat", "lib", "LIB_PATH",
-           "SHOCKHASH", "SHOCKHASH2", "MODE_DEFAULT", "MODE_LEVELS", "MODE_PER_LEAF",
+           "SHOCKHASH", "SHOCKHASH2", "SHOCKHASH_ROTATION", "MODE_DEFAULT", "MODE_LEVELS", "MODE_PER_LEAF",
            "MODE_PIPELINED"]
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libshg.so")
 
-SHOCKHASH, SHOCKHASH2 = 1, 2
+SHOCKHASH, SHOCKHASH2, SHOCKHASH_ROTATION = 1, 2, 3
 MODE_DEFAULT, MODE_LEVELS, MODE_PER_LEAF, MODE_PIPELINED = 0, 1, 2, 3
 _STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_OOM", 3: "ERR_TRIAL_LIMIT", 4: "ERR_CUDA", 5: "ERR_BUCKET",
            6: "ERR_NO_DEVICE"}
@@ -621,15 +621,23 @@ class _RecSplitBase:
 class _Templated(type):
     _cache = {}
 
-    def __getitem__(cls, leaf):
-        key = (cls.__name__, int(leaf))
+    def __getitem__(cls, params):
+        """cls[leaf], or ShockHash[leaf, rotation_fitting] like the reference's template arguments."""
+        leaf, rot = (params if isinstance(params, tuple) else (params, False))
+        key = (cls.__name__, int(leaf), bool(rot))
         if key not in _Templated._cache:
-            _Templated._cache[key] = type(f"{cls.__name__}[{leaf}]", (cls,), {"LEAF": int(leaf)})
+            attrs = {"LEAF": int(leaf)}
+            if rot:
+                if cls.VARIANT != SHOCKHASH:
+                    raise TypeError("rotation fitting exists for ShockHash<l, true> only")
+                attrs["VARIANT"] = SHOCKHASH_ROTATION
+            _Templated._cache[key] = type(f"{cls.__name__}[{leaf}{', True' if rot else ''}]", (cls,), attrs)
         return _Templated._cache[key]
 
 
 class ShockHash(_RecSplitBase, metaclass=_Templated):
-    """shockhash::ShockHash<LEAF_SIZE, false> (include/ShockHash.h:134); use ShockHash[l](keys, b)."""
+    """shockhash::ShockHash<LEAF_SIZE, ROTATION_FITTING> (include/ShockHash.h:134); use ShockHash[l](keys, b)
+    or ShockHash[l, True](keys, b) for rotation fitting."""
     VARIANT = SHOCKHASH
 
 

@@ -165,7 +165,18 @@ __device__ uint64_t dquery_one(const DView &v, uint64_t first, uint64_t second, 
     const uint64_t b = rd.next(v, golomb(v, m));
     bad = bad || rd.bad;
     const uint64_t ret = dretrieve(v, second);
-    if (v.variant == SHG_SHOCKHASH) {
+    if (v.variant == SHG_SHOCKHASH_ROTATION && m == v.leaf) {  // rotation fitting (ShockHash.h:251-265)
+        const uint32_t r = (uint32_t)(b % m);
+        const uint64_t x = b / m + start_seed(level);
+        uint32_t c1, c2;
+        if ((second & 1) == 0) {
+            sh1_cells(second, x & ~(uint64_t)(m > 32 ? 7 : 0), m, c1, c2);
+            return cum + (ret == 0 ? c1 : c2);
+        }
+        sh1_cells(second, x, m, c1, c2);
+        return cum + ((ret == 0 ? c1 : c2) + r) % m;
+    }
+    if (is_sh1(v.variant)) {
         uint32_t c1, c2;
         sh1_cells(second, b + start_seed(level), m, c1, c2);  // TinyBinaryCuckooHashTable.h:116-123
         return cum + (ret == 0 ? c1 : c2);
@@ -455,8 +466,8 @@ extern "C" {
 shg_status shg_dmphf_create(int device, const shg_params *p, const shg_result *r, shg_dmphf **out) {
     if (!p || !r || !out) return shg_set_error(SHG_ERR_ARG, "null argument");
     *out = nullptr;
-    if (p->variant != SHG_SHOCKHASH && p->variant != SHG_SHOCKHASH2) return shg_set_error(SHG_ERR_ARG, "unknown variant");
-    const int maxleaf = p->variant == SHG_SHOCKHASH ? kMaxLeaf1 : kMaxLeaf2;
+    if (!is_sh1(p->variant) && p->variant != SHG_SHOCKHASH2) return shg_set_error(SHG_ERR_ARG, "unknown variant");
+    const int maxleaf = is_sh1(p->variant) ? kMaxLeaf1 : kMaxLeaf2;
     if (p->leaf_size < 2 || p->leaf_size > maxleaf) return shg_set_error(SHG_ERR_ARG, "leaf size out of range");
     if (r->nbuckets == 0 || !r->bucket_size_acc || !r->bucket_pos_acc)
         return shg_set_error(SHG_ERR_ARG, "result has no buckets");
@@ -509,7 +520,7 @@ shg_status shg_dmphf_create(int device, const shg_params *p, const shg_result *r
     v.leaf = (uint32_t)p->leaf_size;
     v.variant = p->variant;
     f->n = r->n;
-    const uint64_t obj = p->variant == SHG_SHOCKHASH ? 144 : 136;
+    const uint64_t obj = is_sh1(p->variant) ? 144 : 136;
     f->bits = ef_bits(r->bucket_size_acc, nb + 1) + ef_bits(r->bucket_pos_acc, nb + 1) + nw * 64 + 8 * ((rn + 7) / 8) +
               8 * obj;
     *out = f;

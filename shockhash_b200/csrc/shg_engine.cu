@@ -25,7 +25,7 @@ namespace shg {
 uint64_t sh2_scratch_bytes(uint32_t smax, uint32_t cmax, int max_leaf);
 void launch_leaves_sh1_ctr(const Node *nodes, const uint32_t *ids, uint32_t count, const uint64_t *keys, uint64_t *codes,
                            uint64_t *rib_keys, uint8_t *rib_bits, uint64_t max_trials, uint32_t *err,
-                           unsigned long long *work, unsigned int *ctr, int grid, cudaStream_t s);
+                           unsigned long long *work, unsigned int *ctr, int grid, cudaStream_t s, uint32_t rot_leaf = 0);
 void launch_leaves_sh2_ctr(const Node *nodes, const uint32_t *ids, uint32_t count, const uint64_t *keys, uint64_t *codes,
                            uint8_t *rib_bits, uint8_t *scratch, uint64_t scratch_per_warp, uint32_t smax, uint32_t cmax,
                            uint32_t *err, unsigned long long *work, unsigned int *ctr, int grid, cudaStream_t s,
@@ -198,8 +198,8 @@ const Config &config_of(int variant, int leaf) {
 
 shg_status check_params(const shg_params *p, uint64_t n) {
     if (!p) return fail(SHG_ERR_ARG, "null params");
-    if (p->variant != SHG_SHOCKHASH && p->variant != SHG_SHOCKHASH2) return fail(SHG_ERR_ARG, "unknown variant");
-    const int maxleaf = p->variant == SHG_SHOCKHASH ? kMaxLeaf1 : kMaxLeaf2;
+    if (!is_sh1(p->variant) && p->variant != SHG_SHOCKHASH2) return fail(SHG_ERR_ARG, "unknown variant");
+    const int maxleaf = is_sh1(p->variant) ? kMaxLeaf1 : kMaxLeaf2;
     if (p->leaf_size < 2 || p->leaf_size > maxleaf) return fail(SHG_ERR_ARG, "leaf size out of range");
     if (p->bucket_size < 1) return fail(SHG_ERR_ARG, "bucket size must be >= 1");
     if (n >= (1ull << 32)) return fail(SHG_ERR_ARG, "at most 2^32 - 1 keys per build");
@@ -307,7 +307,7 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
     CU(e->bucket_bits.ensure(nb * 8));
     CU(e->pos_acc.ensure((nb + 1) * 8));
     CU(e->rib_bits.ensure(std::max<uint64_t>(n, 1)));
-    if (p->variant == SHG_SHOCKHASH) CU(e->rib_keys.ensure(std::max<uint64_t>(n, 1) * 8));
+    if (is_sh1(p->variant)) CU(e->rib_keys.ensure(std::max<uint64_t>(n, 1) * 8));
     if (nn) {
         CU(cudaMemcpyAsync(e->nodes.p, plan.nodes.data(), nn * sizeof(Node), cudaMemcpyHostToDevice, s));
         CU(cudaMemcpyAsync(e->fixed_off.p, plan.fixed_off.data(), nn * 2, cudaMemcpyHostToDevice, s));
@@ -361,7 +361,8 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
         else
             launch_leaves_sh1_ctr(e->nodes.as<Node>(), d_ids + leaf_off + a, (uint32_t)(b - a), e->keys.as<uint64_t>(),
                                   e->codes.as<uint64_t>(), e->rib_keys.as<uint64_t>(), e->rib_bits.as<uint8_t>(), p->max_trials,
-                                  &misc->err, misc->work, &misc->leaf_ctr, grid, st);
+                                  &misc->err, misc->work, &misc->leaf_ctr, grid, st,
+                                  p->variant == SHG_SHOCKHASH_ROTATION ? (uint32_t)p->leaf_size : 0);
         launches++;
     };
     if (pipelined) {
@@ -453,7 +454,7 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
         soff[r + 1] = j;
     }
     if (nsingles) CU(cudaMemcpyAsync(e->singles.p, rel_singles.data(), nsingles * 8, cudaMemcpyHostToDevice, s));
-    const uint64_t *src_keys = p->variant == SHG_SHOCKHASH ? e->rib_keys.as<uint64_t>() : e->keys.as<uint64_t>();
+    const uint64_t *src_keys = is_sh1(p->variant) ? e->rib_keys.as<uint64_t>() : e->keys.as<uint64_t>();
     // one pinned block for all of the batch's results (each result holds a reference)
     std::vector<size_t> roff(R + 1, 0);
     for (size_t r = 0; r < R; r++) {
@@ -1207,8 +1208,8 @@ uint64_t shg_sh2_query(uint64_t leaf_size, uint64_t seed, uint64_t key, uint64_t
 
 shg_status shg_memo_table(int variant, int leaf_size, uint64_t *out) {
     if (!out) return fail(SHG_ERR_ARG, "null output");
-    if (variant != SHG_SHOCKHASH && variant != SHG_SHOCKHASH2) return fail(SHG_ERR_ARG, "unknown variant");
-    const int maxleaf = variant == SHG_SHOCKHASH ? kMaxLeaf1 : kMaxLeaf2;
+    if (!is_sh1(variant) && variant != SHG_SHOCKHASH2) return fail(SHG_ERR_ARG, "unknown variant");
+    const int maxleaf = is_sh1(variant) ? kMaxLeaf1 : kMaxLeaf2;
     if (leaf_size < 2 || leaf_size > maxleaf) return fail(SHG_ERR_ARG, "leaf size out of range");
     const Config &c = config_of(variant, leaf_size);
     memcpy(out, c.memo.data(), kMaxBucket * 8);

@@ -28,6 +28,9 @@ static_assert(sizeof(Node) == 16, "Node must stay 16 bytes");
 // Splitting thresholds and the Golomb-Rice memo of one configuration.
 // ShockHash<l>: lower = l*(l>24?4:2), upper = lower*(l>24?3:2) (ShockHash.h:63-72);
 // ShockHash2<l>: lower = 4l, upper = 12l (ShockHash2.h:49-56).
+// ShockHash<l, true> shares the tree, memo tables and retrieval layout of ShockHash<l, false>.
+SHG_HD bool is_sh1(int variant) { return variant == SHG_SHOCKHASH || variant == SHG_SHOCKHASH_ROTATION; }
+
 struct Config {
     int variant = 0, leaf = 0;
     uint32_t lower = 0, upper = 0;

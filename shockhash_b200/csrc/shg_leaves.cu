@@ -85,17 +85,109 @@ __device__ bool cuckoo_insert(int16_t *cell, uint8_t *xr, int e, uint32_t c1, ui
 // ------------------------------------------------------------------ original ShockHash leaves
 struct Sh1WarpSmem {
     uint64_t keys[64];
+    uint64_t fkeys[64];  // rotation fitting: even keys in order, odd keys from the back
     uint8_t uf[64 * 32];
     int16_t cell[64];
     uint8_t xr[64];
 };
+
+// Rotation of the low l bits of v by r (ShockHash.h:299-301).
+__device__ __forceinline__ uint64_t rot_bits(uint64_t v, uint32_t r, uint32_t l) {
+    return r ? ((v << r) | (v >> (l - r))) & ((1ull << l) - 1) : v;
+}
+
+// ShockHash<L, true>: a leaf of exactly L keys with rotation fitting (ShockHash.h:316-399). Keys
+// are split into set A (even keys, in order) and set B (odd keys, from the back); for seed x, set A
+// hashes with x & ~mask (mask 7 when L > 32, so eight seeds share set A's cells) and set B with x.
+// For r = 0..L-1 the candidate is set B's cells rotated by r: it passes when A's cells and B's
+// rotated cells cover all L cells and the cuckoo graph is a pseudoforest. The answer is the
+// smallest x, then the smallest r (lanes take consecutive x, each lane tries its r in order);
+// the stored code is (x - start_seed) * L + r.
+__device__ bool rotation_leaf(Sh1WarpSmem &sm, LaneUF &uf, int lane, uint32_t m, uint64_t seed0, uint64_t cap_x,
+                              uint64_t &code) {
+    const unsigned below = (1u << lane) - 1;
+    uint32_t nA = 0, nB = 0;
+    for (uint32_t k0 = 0; k0 < m; k0 += 32) {
+        const uint32_t k = k0 + lane;
+        const uint64_t key = k < m ? sm.keys[k] : 0;
+        const bool even = (key & 1) == 0;
+        const unsigned be = __ballot_sync(0xffffffffu, k < m && even), bo = __ballot_sync(0xffffffffu, k < m && !even);
+        if (k < m) sm.fkeys[even ? nA + __popc(be & below) : m - 1 - (nB + __popc(bo & below))] = key;
+        nA += __popc(be);
+        nB += __popc(bo);
+    }
+    __syncwarp();
+    const uint64_t gmask = m > 32 ? 7 : 0;
+    const uint64_t all = (1ull << m) - 1;
+    auto pseudoforest = [&](uint64_t x, uint32_t r) {
+        uf.init(m);
+        bool ok = true;
+        for (uint32_t k = 0; k < m && ok; k++) {
+            uint32_t c1, c2;
+            if (k < nA) {
+                sh1_cells(sm.fkeys[k], x & ~gmask, m, c1, c2);
+            } else {
+                sh1_cells(sm.fkeys[k], x, m, c1, c2);
+                c1 = (c1 + r) % m;
+                c2 = (c2 + r) % m;
+            }
+            ok = uf.add(c1, c2);
+        }
+        return ok;
+    };
+    for (uint64_t base = 0; base < cap_x; base += 32) {
+        const uint64_t x = seed0 + base + lane, xa = x & ~gmask;
+        uint64_t a = 0, b = 0;
+        for (uint32_t k = 0; k < m; k++) {
+            uint32_t c1, c2;
+            sh1_cells(sm.fkeys[k], k < nA ? xa : x, m, c1, c2);
+            const uint64_t bits = (1ull << c1) | (1ull << c2);
+            if (k < nA) a |= bits; else b |= bits;
+        }
+        int rr = -1;
+        for (uint32_t r = 0; r < m; r++)
+            if ((a | rot_bits(b, r, m)) == all && pseudoforest(x, r)) {
+                rr = (int)r;
+                break;
+            }
+        const unsigned bal = __ballot_sync(0xffffffffu, rr >= 0);
+        if (bal) {
+            const int src = __ffs(bal) - 1;
+            const uint64_t fx = base + src;
+            const int fr = __shfl_sync(0xffffffffu, rr, src);
+            if (fx >= cap_x) return false;
+            code = fx * m + (uint64_t)fr;
+            // orientation: the reference's ordered insertion in set order, then cell order
+            if (lane == 0) {
+                const uint64_t xf = seed0 + fx;
+                for (uint32_t c = 0; c < m; c++) sm.cell[c] = -1;
+                bool okc = true;
+                for (uint32_t k = 0; k < m && okc; k++) {
+                    uint32_t c1, c2;
+                    if (k < nA) {
+                        sh1_cells(sm.fkeys[k], xf & ~gmask, m, c1, c2);
+                    } else {
+                        sh1_cells(sm.fkeys[k], xf, m, c1, c2);
+                        c1 = (c1 + fr) % m;
+                        c2 = (c2 + fr) % m;
+                    }
+                    okc = cuckoo_insert(sm.cell, sm.xr, (int)k, c1, c2, 8 * (int)m + 16);
+                }
+                if (!okc) code = ~0ull;
+            }
+            code = __shfl_sync(0xffffffffu, code, 0);
+            return code != ~0ull;
+        }
+    }
+    return false;
+}
 
 __global__ void __launch_bounds__(kLeafWarps * 32) k_leaves_sh1(const Node *__restrict__ nodes, const uint32_t *__restrict__ ids,
                                                                 uint32_t count, const uint64_t *__restrict__ keys,
                                                                 uint64_t *__restrict__ codes, uint64_t *__restrict__ rib_keys,
                                                                 uint8_t *__restrict__ rib_bits, uint64_t max_trials,
                                                                 uint32_t *__restrict__ err, unsigned long long *__restrict__ work,
-                                                                unsigned int *__restrict__ next_leaf) {
+                                                                unsigned int *__restrict__ next_leaf, uint32_t rot_leaf) {
     __shared__ Sh1WarpSmem wsm[kLeafWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     Sh1WarpSmem &sm = wsm[warp];
@@ -120,6 +212,33 @@ __global__ void __launch_bounds__(kLeafWarps * 32) k_leaves_sh1(const Node *__re
         uint64_t cap = 1ull << min(nd.g + 10, 40);
         if (max_trials && max_trials < cap) cap = max_trials;
         LaneUF uf{sm.uf, lane};
+        if (rot_leaf && m == rot_leaf) {
+            // ~2^(g+1) codes x * L + r are expected; the cap counts seeds x
+            uint64_t cap_x = (1ull << min(nd.g + 10, 40)) / m + 1;
+            if (max_trials && max_trials < cap_x) cap_x = max_trials;
+            uint64_t code = 0;
+            const bool ok = rotation_leaf(sm, uf, lane, m, seed0, cap_x, code);
+            if (!ok) {
+                if (lane == 0) atomicOr(err, code == ~0ull ? kErrInternal : kErrTrialLimit);
+                continue;
+            }
+            if (lane == 0) {
+                codes[id] = code;
+                evals += (code / m + 1) * m;
+            }
+            __syncwarp();
+            // retrieval input in cell order; the bit is the unrotated cell's half (ShockHash.h:384-391)
+            for (uint32_t c = lane; c < m; c += 32) {
+                const int e = sm.cell[c];
+                const uint64_t key = e >= 0 ? sm.fkeys[e] : 0;
+                const uint32_t r = (uint32_t)(code % m);
+                const uint32_t cell = (key & 1) ? (c + m - r) % m : c;
+                rib_keys[nd.start + c] = key;
+                rib_bits[nd.start + c] = cell < m / 2 ? 0 : 1;
+            }
+            __syncwarp();
+            continue;
+        }
         uint64_t found = ~0ull;
         // Pseudoforest test of one lane's seed (union-find with a cycle flag per root).
         auto pseudoforest = [&](uint64_t x) {
@@ -194,11 +313,11 @@ int leaves_sh1_warps_per_block() { return kLeafWarps; }
 
 void launch_leaves_sh1_ctr(const Node *nodes, const uint32_t *ids, uint32_t count, const uint64_t *keys, uint64_t *codes,
                            uint64_t *rib_keys, uint8_t *rib_bits, uint64_t max_trials, uint32_t *err,
-                           unsigned long long *work, unsigned int *ctr, int grid, cudaStream_t s) {
+                           unsigned long long *work, unsigned int *ctr, int grid, cudaStream_t s, uint32_t rot_leaf) {
     if (!count) return;
     cudaMemsetAsync(ctr, 0, sizeof(unsigned int), s);
     k_leaves_sh1<<<grid, kLeafWarps * 32, 0, s>>>(nodes, ids, count, keys, codes, rib_keys, rib_bits, max_trials, err,
-                                                  work, ctr);
+                                                  work, ctr, rot_leaf);
 }
 
 } // namespace shg

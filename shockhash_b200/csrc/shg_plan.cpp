@@ -24,7 +24,7 @@ static const uint8_t kBijMemo2[129] = {
     43, 45, 44, 45, 45, 47, 46, 47, 46, 48, 47, 49, 48, 50, 49, 51, 50, 52, 51, 53, 52, 54, 53, 54, 54};
 
 Config::Config(int variant_, int leaf_) : variant(variant_), leaf(leaf_) {
-    if (variant == SHG_SHOCKHASH) {
+    if (is_sh1(variant)) {
         lower = leaf * (leaf > 24 ? 4 : 2);
         upper = lower * (leaf > 24 ? 3 : 2);
     } else {
@@ -35,7 +35,7 @@ Config::Config(int variant_, int leaf_) : variant(variant_), leaf(leaf_) {
     uint32_t s = 0;
     // fill_golomb_rice (ShockHash.h:121-127) / fill_golomb_rice2 (ShockHash2.h:106-115)
     for (; s <= (uint32_t)leaf; ++s) {
-        const uint64_t b = variant == SHG_SHOCKHASH ? kBijMemo[s] : kBijMemo2[s];
+        const uint64_t b = is_sh1(variant) ? kBijMemo[s] : kBijMemo2[s];
         memo[s] = b << 27 | (uint64_t)(s > 1) << 16 | b;
     }
     // _fill_golomb_rice (ShockHash.h:79-119) / _fill_golomb_rice2 (ShockHash2.h:63-104): the Rice

@@ -144,7 +144,20 @@ uint64_t query_one(const shg_mphf *f, uint64_t first, uint64_t second) {
     }
     const uint64_t b = rd.next(c.golomb(m));
     const uint64_t ret = retrieve(f, second);
-    if (f->variant == SHG_SHOCKHASH) {
+    if (f->variant == SHG_SHOCKHASH_ROTATION && m == (uint32_t)f->leaf) {
+        // rotation fitting (ShockHash.h:251-265): code = x * L + r; set B's cells rotate by r
+        const uint32_t r = (uint32_t)(b % m);
+        const uint64_t x = b / m + start_seed(level);
+        const uint64_t gmask = m > 32 ? 7 : 0;
+        uint32_t c1, c2;
+        if ((second & 1) == 0) {
+            sh1_cells(second, x & ~gmask, m, c1, c2);
+            return cum + (ret == 0 ? c1 : c2);
+        }
+        sh1_cells(second, x, m, c1, c2);
+        return cum + ((ret == 0 ? c1 : c2) + r) % m;
+    }
+    if (is_sh1(f->variant)) {
         // hashToCell (TinyBinaryCuckooHashTable.h:116-123)
         uint32_t c1, c2;
         sh1_cells(second, b + start_seed(level), m, c1, c2);
@@ -224,7 +237,7 @@ shg_status shg_mphf_query_strings(const shg_mphf *f, const char *bytes, const ui
 // ShockHash, which also stores bucket_size, and 136 for ShockHash2).
 uint64_t shg_mphf_bits(const shg_mphf *f) {
     if (!f) return 0;
-    const uint64_t obj = f->variant == SHG_SHOCKHASH ? 144 : 136;
+    const uint64_t obj = is_sh1(f->variant) ? 144 : 136;
     return ef_bits(f->size_acc) + ef_bits(f->pos_acc) + f->desc.size() * 64 + 8 * ((f->ribbon_n + 7) / 8) + 8 * obj;
 }
 

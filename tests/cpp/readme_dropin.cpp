@@ -50,5 +50,7 @@ int main() {
         if (v < hashes.size()) seen[v] = 1;
     }
     std::cout << (ok ? "ShockHash hash128 ok" : "ShockHash hash128 FAIL") << std::endl;
+    shockhash::ShockHash<30, true> hr(many, 2000);  // rotation fitting
+    std::cout << (is_mphf(hr, many) ? "ShockHash rotation ok" : "ShockHash rotation FAIL") << std::endl;
     return 0;
 }

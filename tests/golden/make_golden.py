@@ -36,6 +36,13 @@ BUILDS = [
     ("sh2_l100_b1000", 2, 100, 2000, 1000, 206),
     ("sh2_l64_tiny", 2, 64, 3, 2000, 207),
     ("sh1_l30_tiny", 1, 30, 2, 2000, 208),
+    # ShockHash<l, true> (rotation fitting); l > 32 shares set A's cells over eight seeds
+    ("rot_l30_b2000", 3, 30, 20000, 2000, 111),
+    ("rot_l40_b2000", 3, 40, 8000, 2000, 112),
+    ("rot_l16_b100", 3, 16, 5000, 100, 113),
+    ("rot_l8_b50", 3, 8, 3000, 50, 114),
+    ("rot_l33_b500", 3, 33, 5000, 500, 115),
+    ("rot_l48_b2000", 3, 48, 6000, 2000, 116),
 ]
 # (k, n, seed) for ShockHash2Flat<k>
 FLATS = [(16, 30000, 401), (32, 20000, 402), (64, 20003, 403), (100, 4100, 404), (8, 5000, 405)]

@@ -68,4 +68,6 @@ def test_invalid_arguments_rejected():
     with pytest.raises(shg.ShgError):
         shg.memo_table(1, 61)
     with pytest.raises(shg.ShgError):
-        shg.memo_table(3, 10)
+        shg.memo_table(4, 10)
+    # ShockHash<l, true> keeps the memo table of ShockHash<l, false> (ShockHash.h:145)
+    assert np.array_equal(shg.memo_table(3, 30), shg.memo_table(1, 30))

@@ -36,3 +36,4 @@ def test_dropin_readme_example(tmp_path):
     assert float(out[1].split()[2]) < 2.0
     assert out[2] == "ShockHash2Flat ok"
     assert out[3] == "ShockHash hash128 ok"
+    assert out[4] == "ShockHash rotation ok"

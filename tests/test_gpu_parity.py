@@ -167,3 +167,54 @@ def test_duplicate_keys_match_oracle(engine, port):
         p = port.build_hash(variant, leaf, f, s, 100)
         r = engine.build_hash128(variant, leaf, f, s, 100)
         assert np.array_equal(r.descriptors, p.desc) and np.array_equal(r.ribbon_bits, p.ribbon_bits)
+
+
+@pytest.mark.parametrize("variant,leaf", [(1, 30), (2, 64)])
+def test_empty_key_set_matches_oracle(engine, port, variant, leaf):
+    # no keys: one empty bucket, a descriptor stream holding only the sentinel (ShockHash.h:616-654)
+    f = np.zeros(0, np.uint64)
+    p = port.build_hash(variant, leaf, f, f, 2000)
+    r = engine.build_hash128(variant, leaf, f, f, 2000)
+    assert r.n == 0 and r.nbuckets == 1
+    assert np.array_equal(r.bucket_size_acc, p.size_acc) and np.array_equal(r.bucket_pos_acc, p.pos_acc)
+    assert np.array_equal(r.descriptors, p.desc) and len(r.ribbon_keys) == 0
+
+
+def test_oversized_bucket_is_an_error(engine):
+    # a bucket of >= 3000 keys exceeds MAX_BUCKET_SIZE (ShockHash.h:33); the reference's memo tables
+    # stop there, so the engine refuses instead of reading past them, and stays usable
+    rng = np.random.default_rng(8)
+    n = 6000
+    f = np.full(n, 12345, np.uint64)  # every key in the same bucket
+    s = unique_u64(rng, n)
+    with pytest.raises(shg.ShgError) as ei:
+        engine.build_hash128(2, 64, f, s, 6000)
+    assert ei.value.status == 5
+    g = load("sh2_l10_b100")
+    assert_same(engine.build_hash128(2, 10, g["first"], g["second"], 100), g)
+
+
+ROT_FIXTURES = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "rot_*.npz")))
+
+
+@pytest.mark.parametrize("name", ROT_FIXTURES)
+def test_rotation_fitting_matches_golden(engine, name):
+    # ShockHash<l, true>: leaves of exactly l keys use rotation fitting (ShockHash.h:316-399)
+    g = load(name)
+    assert int(g["variant"]) == shg.SHOCKHASH_ROTATION
+    r = engine.build_hash128(int(g["variant"]), int(g["leaf"]), g["first"], g["second"], int(g["bucket_size"]),
+                             query=True)
+    assert_same(r, g)
+    assert np.array_equal(r._mphf.query_hash(g["first"], g["second"]), g["query"])
+    assert np.array_equal(shg.DeviceMphf(r).query_hash(g["first"], g["second"]), g["query"])
+    assert r._mphf.bits() == int(g["bits"])
+
+
+@pytest.mark.parametrize("leaf", [30, 40])
+def test_rotation_fitting_at_scale_is_mphf(engine, leaf):
+    keys = unique_u64(np.random.default_rng(leaf + 900), 1_000_000)
+    r = engine.build_u64(shg.SHOCKHASH_ROTATION, leaf, keys, 2000, query=True)
+    out = shg.DeviceMphf(r).query_u64(keys)
+    assert np.array_equal(np.sort(out), np.arange(len(keys), dtype=np.uint64))
+    idx = np.random.default_rng(2).choice(len(keys), 5000, replace=False)
+    assert np.array_equal(r._mphf.query_strings([int(k).to_bytes(8, "little") for k in keys[idx]]), out[idx])

@@ -72,7 +72,7 @@ def test_port_spooky_matches_golden(port):
 
 
 def test_ref_matches_golden(ref):
-    for name in ("sh2_l64_b2000", "sh1_l30_b2000", "sh2_l9_b50"):
+    for name in ("sh2_l64_b2000", "sh1_l30_b2000", "sh2_l9_b50", "rot_l30_b2000", "rot_l40_b2000"):
         g = load(name)
         r = ref.build_hash(int(g["variant"]), int(g["leaf"]), g["first"], g["second"], int(g["bucket_size"]), 1)
         assert np.array_equal(r.desc, g["desc"])
@@ -121,3 +121,12 @@ def test_mphf_property_port(port):
         r = port.build_hash(variant, leaf, f, s, 1000)
         q = r.query_hash(f, s)
         assert np.array_equal(np.sort(q), np.arange(n, dtype=np.uint64))
+
+
+def test_ref_rotation_fitting_is_mphf_and_differs_from_plain(ref):
+    # ShockHash<l, true> stores x * l + r for full leaves; its structure is a different one
+    rng = np.random.default_rng(44)
+    f, s = rand_u64(rng, 6000), unique_u64(rng, 6000)
+    r = ref.build_hash(3, 24, f, s, 500, 1)
+    assert np.array_equal(np.sort(r.query_hash(f, s)), np.arange(6000, dtype=np.uint64))
+    assert not np.array_equal(r.desc, ref.build_hash(1, 24, f, s, 500, 1).desc)
