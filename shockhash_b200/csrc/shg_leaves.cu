@@ -103,8 +103,8 @@ __device__ __forceinline__ uint64_t rot_bits(uint64_t v, uint32_t r, uint32_t l)
 // rotated cells cover all L cells and the cuckoo graph is a pseudoforest. The answer is the
 // smallest x, then the smallest r (lanes take consecutive x, each lane tries its r in order);
 // the stored code is (x - start_seed) * L + r.
-__device__ bool rotation_leaf(Sh1WarpSmem &sm, LaneUF &uf, int lane, uint32_t m, uint64_t seed0, uint64_t cap_x,
-                              uint64_t &code) {
+__device__ bool rotation_leaf(Sh1WarpSmem &sm, uint16_t *cells, LaneUF &uf, int lane, uint32_t m, uint64_t seed0,
+                              uint64_t cap_x, uint64_t &code) {
     const unsigned below = (1u << lane) - 1;
     uint32_t nA = 0, nB = 0;
     for (uint32_t k0 = 0; k0 < m; k0 += 32) {
@@ -119,41 +119,70 @@ __device__ bool rotation_leaf(Sh1WarpSmem &sm, LaneUF &uf, int lane, uint32_t m,
     __syncwarp();
     const uint64_t gmask = m > 32 ? 7 : 0;
     const uint64_t all = (1ull << m) - 1;
-    auto pseudoforest = [&](uint64_t x, uint32_t r) {
+    // cells[k * 32 + lane] = c1 | c2 << 8 of key k under the lane's seed, written by the coverage
+    // pass; with gmask a set-A key's cells sit in the slot of the group lane that hashed it
+    auto pseudoforest = [&](uint32_t r) {
         uf.init(m);
         bool ok = true;
         for (uint32_t k = 0; k < m && ok; k++) {
             uint32_t c1, c2;
             if (k < nA) {
-                sh1_cells(sm.fkeys[k], x & ~gmask, m, c1, c2);
+                const uint32_t w = cells[k * 32 + (gmask ? ((lane & ~7) | (k & 7)) : lane)];
+                c1 = w & 0xFF;
+                c2 = w >> 8;
             } else {
-                sh1_cells(sm.fkeys[k], x, m, c1, c2);
-                c1 = (c1 + r) % m;
-                c2 = (c2 + r) % m;
+                const uint32_t w = cells[k * 32 + lane];
+                c1 = ((w & 0xFF) + r) % m;
+                c2 = ((w >> 8) + r) % m;
             }
             ok = uf.add(c1, c2);
         }
         return ok;
     };
-    for (uint64_t base = 0; base < cap_x; base += 32) {
-        const uint64_t x = seed0 + base + lane, xa = x & ~gmask;
+    // Rounds of 32 seeds start at a multiple of 8 (seeds below seed0 in the first round take no
+    // part), so with gmask = 7 each aligned group of 8 lanes shares set A's seed: its lanes hash
+    // every eighth set-A key and OR their masks together.
+    const uint64_t x_lo = seed0 & ~7ull;
+    for (uint64_t off = 0; off < cap_x + (seed0 - x_lo); off += 32) {
+        const uint64_t x = x_lo + off + lane, xa = x & ~gmask;
+        const bool live = x >= seed0 && x - seed0 < cap_x;
         uint64_t a = 0, b = 0;
-        for (uint32_t k = 0; k < m; k++) {
-            uint32_t c1, c2;
-            sh1_cells(sm.fkeys[k], k < nA ? xa : x, m, c1, c2);
-            const uint64_t bits = (1ull << c1) | (1ull << c2);
-            if (k < nA) a |= bits; else b |= bits;
-        }
-        int rr = -1;
-        for (uint32_t r = 0; r < m; r++)
-            if ((a | rot_bits(b, r, m)) == all && pseudoforest(x, r)) {
-                rr = (int)r;
-                break;
+        if (gmask) {
+            for (uint32_t k = lane & 7; k < nA; k += 8) {
+                uint32_t c1, c2;
+                sh1_cells(sm.fkeys[k], xa, m, c1, c2);
+                a |= (1ull << c1) | (1ull << c2);
+                cells[k * 32 + lane] = (uint16_t)(c1 | c2 << 8);
             }
-        const unsigned bal = __ballot_sync(0xffffffffu, rr >= 0);
+            a |= __shfl_xor_sync(0xffffffffu, a, 1);
+            a |= __shfl_xor_sync(0xffffffffu, a, 2);
+            a |= __shfl_xor_sync(0xffffffffu, a, 4);
+        } else {
+            for (uint32_t k = 0; k < nA; k++) {
+                uint32_t c1, c2;
+                sh1_cells(sm.fkeys[k], xa, m, c1, c2);
+                a |= (1ull << c1) | (1ull << c2);
+                cells[k * 32 + lane] = (uint16_t)(c1 | c2 << 8);
+            }
+        }
+        for (uint32_t k = nA; k < m; k++) {
+            uint32_t c1, c2;
+            sh1_cells(sm.fkeys[k], x, m, c1, c2);
+            b |= (1ull << c1) | (1ull << c2);
+            cells[k * 32 + lane] = (uint16_t)(c1 | c2 << 8);
+        }
+        __syncwarp();
+        int rr = -1;
+        if (live)
+            for (uint32_t r = 0; r < m; r++)
+                if ((a | rot_bits(b, r, m)) == all && pseudoforest(r)) {
+                    rr = (int)r;
+                    break;
+                }
+        const unsigned bal = __ballot_sync(0xffffffffu, rr >= 0);  // also orders the cell reads before the next round's writes
         if (bal) {
             const int src = __ffs(bal) - 1;
-            const uint64_t fx = base + src;
+            const uint64_t fx = x_lo + off + src - seed0;
             const int fr = __shfl_sync(0xffffffffu, rr, src);
             if (fx >= cap_x) return false;
             code = fx * m + (uint64_t)fr;
@@ -189,6 +218,7 @@ __global__ void __launch_bounds__(kLeafWarps * 32) k_leaves_sh1(const Node *__re
                                                                 uint32_t *__restrict__ err, unsigned long long *__restrict__ work,
                                                                 unsigned int *__restrict__ next_leaf, uint32_t rot_leaf) {
     __shared__ Sh1WarpSmem wsm[kLeafWarps];
+    extern __shared__ uint16_t rot_cells[];  // rotation fitting only: [warp][64 keys][32 lanes]
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     Sh1WarpSmem &sm = wsm[warp];
     unsigned long long evals = 0;
@@ -217,7 +247,7 @@ __global__ void __launch_bounds__(kLeafWarps * 32) k_leaves_sh1(const Node *__re
             uint64_t cap_x = (1ull << min(nd.g + 10, 40)) / m + 1;
             if (max_trials && max_trials < cap_x) cap_x = max_trials;
             uint64_t code = 0;
-            const bool ok = rotation_leaf(sm, uf, lane, m, seed0, cap_x, code);
+            const bool ok = rotation_leaf(sm, rot_cells + warp * 64 * 32, uf, lane, m, seed0, cap_x, code);
             if (!ok) {
                 if (lane == 0) atomicOr(err, code == ~0ull ? kErrInternal : kErrTrialLimit);
                 continue;
@@ -316,8 +346,9 @@ void launch_leaves_sh1_ctr(const Node *nodes, const uint32_t *ids, uint32_t coun
                            unsigned long long *work, unsigned int *ctr, int grid, cudaStream_t s, uint32_t rot_leaf) {
     if (!count) return;
     cudaMemsetAsync(ctr, 0, sizeof(unsigned int), s);
-    k_leaves_sh1<<<grid, kLeafWarps * 32, 0, s>>>(nodes, ids, count, keys, codes, rib_keys, rib_bits, max_trials, err,
-                                                  work, ctr, rot_leaf);
+    const size_t dyn = rot_leaf ? (size_t)kLeafWarps * 64 * 32 * sizeof(uint16_t) : 0;  // 16 KB per block
+    k_leaves_sh1<<<grid, kLeafWarps * 32, dyn, s>>>(nodes, ids, count, keys, codes, rib_keys, rib_bits, max_trials, err,
+                                                    work, ctr, rot_leaf);
 }
 
 } // namespace shg
