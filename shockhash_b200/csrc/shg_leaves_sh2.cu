@@ -41,7 +41,7 @@ template <class M> struct alignas(2 * sizeof(M)) MaskPair {
 template <> struct Sh2Cfg<64> {
     using Mask = uint32_t;            // half-table coverage: (m + 1) / 2 <= 32 cells
     static constexpr int SMS = 256;   // raw seeds whose masks stay in shared memory
-    static constexpr int CMS = 256;   // candidates held in shared memory
+    static constexpr int CMS = 128;   // candidates held in shared memory
     static constexpr int ISO_WORDS = 1;
     static constexpr uint32_t ROWS = 2048;  // candidates whose cell rows are cached in global scratch
     static constexpr uint32_t RAW_ROWS = 2048;  // raw seeds whose cell rows are cached
@@ -233,7 +233,7 @@ template <int MAXM> struct OffsetLeaves {
 };
 
 template <int MAXM, class Src>
-__global__ void __launch_bounds__(128) k_leaves_sh2_v2(Src src, uint32_t count, const uint64_t *__restrict__ keys,
+__global__ void __launch_bounds__(128, MAXM <= 64 ? 6 : 1) k_leaves_sh2_v2(Src src, uint32_t count, const uint64_t *__restrict__ keys,
                                                        uint8_t *__restrict__ rib_bits,
                                                        uint8_t *__restrict__ scratch, uint64_t scratch_per_warp,
                                                        uint32_t smax, uint32_t cmax, uint32_t *__restrict__ err,
