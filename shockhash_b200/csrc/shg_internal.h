@@ -2,6 +2,7 @@
 #pragma once
 #include <cstdint>
 #include <string>
+#include <memory>
 #include <vector>
 #include <cuda_runtime.h>
 #include "shg.h"
@@ -31,10 +32,12 @@ static_assert(sizeof(Node) == 16, "Node must stay 16 bytes");
 // ShockHash<l, true> shares the tree, memo tables and retrieval layout of ShockHash<l, false>.
 SHG_HD bool is_sh1(int variant) { return variant == SHG_SHOCKHASH || variant == SHG_SHOCKHASH_ROTATION; }
 
+struct ShapeCache;  // tree shapes by bucket size, built on first use (shg_plan.cpp)
 struct Config {
     int variant = 0, leaf = 0;
     uint32_t lower = 0, upper = 0;
     std::vector<uint64_t> memo;  // kMaxBucket entries, fill_golomb_rice(2) layout
+    std::shared_ptr<ShapeCache> shapes;  // shared by copies; kept across builds
     Config() {}
     Config(int variant, int leaf);
     int golomb(uint32_t m) const { return (int)(memo[m] >> 27); }

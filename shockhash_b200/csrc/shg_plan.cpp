@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdint>
 #include <stdexcept>
+#include <mutex>
 #include <vector>
 #include "shg_common.cuh"
 #include "shg_internal.h"
@@ -23,7 +24,13 @@ static const uint8_t kBijMemo2[129] = {
     32, 33, 33, 34, 33, 35, 34, 36, 35, 37, 36, 38, 37, 39, 38, 40, 38, 40, 40, 41, 40, 42, 41, 43, 42, 44,
     43, 45, 44, 45, 45, 47, 46, 47, 46, 48, 47, 49, 48, 50, 49, 51, 50, 52, 51, 53, 52, 54, 53, 54, 54};
 
-Config::Config(int variant_, int leaf_) : variant(variant_), leaf(leaf_) {
+struct ShapeCache {
+    std::mutex mu;
+    std::vector<Shape> cache = std::vector<Shape>(kMaxBucket);
+    std::vector<char> have = std::vector<char>(kMaxBucket, 0);
+};
+
+Config::Config(int variant_, int leaf_) : variant(variant_), leaf(leaf_), shapes(std::make_shared<ShapeCache>()) {
     if (is_sh1(variant)) {
         lower = leaf * (leaf > 24 ? 4 : 2);
         upper = lower * (leaf > 24 ? 3 : 2);
@@ -130,8 +137,11 @@ const Shape &shape_of(const Config &c, uint32_t m, std::vector<Shape> &cache, st
 
 void make_plan(const Config &c, const std::vector<uint64_t> &acc, Plan &plan) {
     const uint64_t nb = acc.size() - 1;
-    std::vector<Shape> cache(kMaxBucket);
-    std::vector<char> have(kMaxBucket, 0);
+    // shapes depend only on the configuration and the bucket size: reuse them across builds
+    std::shared_ptr<ShapeCache> sc = c.shapes ? c.shapes : std::make_shared<ShapeCache>();
+    std::lock_guard<std::mutex> lock(sc->mu);
+    std::vector<Shape> &cache = sc->cache;
+    std::vector<char> &have = sc->have;
     uint64_t total = 0;
     for (uint64_t b = 0; b < nb; b++) {
         const uint64_t m = acc[b + 1] - acc[b];
