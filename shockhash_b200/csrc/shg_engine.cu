@@ -322,6 +322,52 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
         const int bps = std::max(1, std::min(8, (228 * 1024) / (4 * sh2_smem_per_warp(p->leaf_size) + 1024)));
         CU(e->scratch.ensure(pw * (uint64_t)e->sms * bps * 4));
     }
+    // retrieval input per request: its keys minus those of size-1 children (no retrieval bit)
+    const uint64_t nsingles = plan.singles.size();
+    CU(e->singles.ensure(std::max<uint64_t>(nsingles, 1) * 8));
+    CU(e->ckeys.ensure(std::max<uint64_t>(n, 1) * 8));
+    CU(e->cbits.ensure(std::max<uint64_t>(n, 1)));
+    std::vector<uint64_t> rel_singles(nsingles), soff(R + 1, 0), rnv(R);
+    for (size_t r = 0, j = 0; r < R; r++) {
+        while (j < nsingles && plan.singles[j] < off[r + 1]) {
+            rel_singles[j] = plan.singles[j] - off[r];
+            j++;
+        }
+        soff[r + 1] = j;
+        rnv[r] = nr[r] - (soff[r + 1] - soff[r]);
+    }
+    if (nsingles) CU(cudaMemcpyAsync(e->singles.p, rel_singles.data(), nsingles * 8, cudaMemcpyHostToDevice, s));
+    // Bipartite retrieval keys are final once the splits are done (the leaves only add the bits),
+    // so in the level schedule they go to the host on the second stream while the leaf kernel
+    // runs. The pinned block is then taken before the splits, with room for descriptor words
+    // bounded by the fixed bits plus 8 unary bits per node; a longer stream (not seen in
+    // practice) takes a new block after encoding.
+    const bool early_keys = p->variant == SHG_SHOCKHASH2 && p->mode != SHG_MODE_PIPELINED;
+    std::vector<uint64_t> wcap(R, 0);
+    std::vector<size_t> roff(R + 1, 0);
+    auto layout = [&]() {
+        for (size_t r = 0; r < R; r++) {
+            const size_t acc_bytes = (nbr[r] + 1) * 8;
+            roff[r + 1] = roff[r] + ((2 * acc_bytes + rnv[r] * 9 + wcap[r] * 8 + 64 + 63) & ~(size_t)63);
+        }
+    };
+    PinnedBlock *blk = nullptr;
+    if (early_keys) {
+        for (size_t r = 0; r < R; r++) {
+            uint64_t fixed = 0;
+            for (uint64_t b = boff[r]; b < boff[r + 1]; b++) fixed += cfg.skip_bits((uint32_t)(acc[b + 1] - acc[b]));
+            const uint64_t nodes_r = plan.bucket_node_begin[boff[r + 1]] - plan.bucket_node_begin[boff[r]];
+            const uint64_t bits = fixed + 8 * nodes_r + 1;
+            wcap[r] = ((bits + 7) / 8 + 14) / 8;
+        }
+        layout();
+        blk = acquire_pinned(e, roff[R], (int)R);
+        if (!blk) return fail(SHG_ERR_OOM, "pinned host allocation failed");
+    }
+    auto keys_host = [&](PinnedBlock *b, size_t r) { return (uint64_t *)((uint8_t *)b->p + roff[r] + 2 * (nbr[r] + 1) * 8); };
+    auto release_all = [&](PinnedBlock *b) {  // drop every reference a failed build still holds
+        for (size_t r = 0; r < R; r++) release_pinned(b);
+    };
     CU(cudaEventRecord(e->ev[2], s));
 
     // ---- splits and leaves
@@ -396,6 +442,21 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
     } else {
         for (size_t lv = 0; lv < plan.split_levels.size(); lv++) split_range(lv, 0, plan.split_levels[lv].size(), s);
         CU(cudaEventRecord(e->ev[3], s));
+        if (early_keys) {
+            // compaction on the engine stream before the leaf kernel takes every SM; only the
+            // copies run on the second stream, next to the leaves
+            for (size_t r = 0; r < R; r++)
+                if (rnv[r])
+                    launch_compact_ribbon(e->keys.as<uint64_t>() + off[r], nullptr, nr[r], e->singles.as<uint64_t>() + soff[r],
+                                          soff[r + 1] - soff[r], e->ckeys.as<uint64_t>() + off[r], nullptr, s);
+            CU(cudaEventRecord(e->chunk_ev[0], s));
+            CU(cudaStreamWaitEvent(e->stream2, e->chunk_ev[0], 0));
+            for (size_t r = 0; r < R; r++)
+                if (rnv[r])
+                    CU(cudaMemcpyAsync(keys_host(blk, r), e->ckeys.as<uint64_t>() + off[r], rnv[r] * 8, cudaMemcpyDeviceToHost,
+                                       e->stream2));
+            CU(cudaEventRecord(e->join_ev, e->stream2));
+        }
         if (p->mode == SHG_MODE_PER_LEAF)
             for (uint32_t l = 0; l < nleaves; l++) leaf_range(l, l + 1, s, 1);
         else
@@ -416,6 +477,10 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
     uint32_t err = 0;
     CU(cudaMemcpyAsync(&err, &misc->err, 4, cudaMemcpyDeviceToHost, s));
     CU(cudaStreamSynchronize(s));
+    if (err && blk) {
+        cudaStreamSynchronize(e->stream2);
+        release_all(blk);
+    }
     if (err & kErrTrialLimit) return fail(SHG_ERR_TRIAL_LIMIT, "a seed search exceeded its trial cap (duplicate keys?)");
     if (err & kErrScratch) return fail(SHG_ERR_TRIAL_LIMIT, "a bipartite leaf exceeded its candidate capacity (duplicate keys?)");
     if (err) return fail(SHG_ERR_CUDA, "internal device error flag " + std::to_string(err));
@@ -439,55 +504,52 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
     CU(cudaGetLastError());
     CU(cudaEventRecord(e->ev[5], s));
 
-    // ---- copy-out: compact each request's retrieval input on the device (drop keys of size-1
-    // children), then copy its products into a pinned host block owned by the engine.
-    const uint64_t nsingles = plan.singles.size();
-    CU(e->singles.ensure(std::max<uint64_t>(nsingles, 1) * 8));
-    CU(e->ckeys.ensure(std::max<uint64_t>(n, 1) * 8));
-    CU(e->cbits.ensure(std::max<uint64_t>(n, 1)));
-    std::vector<uint64_t> rel_singles(nsingles), soff(R + 1, 0);
-    for (size_t r = 0, j = 0; r < R; r++) {
-        while (j < nsingles && plan.singles[j] < off[r + 1]) {
-            rel_singles[j] = plan.singles[j] - off[r];
-            j++;
+    // ---- copy-out: the products of each request into the pinned block (one block per batch,
+    // each result holding a reference); the retrieval input is compacted on the device first.
+    bool keys_done = early_keys;
+    if (early_keys) {
+        bool fits = true;
+        for (size_t r = 0; r < R; r++) fits = fits && words[r] <= wcap[r];
+        if (!fits) {  // descriptor stream longer than the bound: a new block, keys copied again
+            CU(cudaStreamSynchronize(e->stream2));
+            release_all(blk);
+            blk = nullptr;
+            keys_done = false;
         }
-        soff[r + 1] = j;
     }
-    if (nsingles) CU(cudaMemcpyAsync(e->singles.p, rel_singles.data(), nsingles * 8, cudaMemcpyHostToDevice, s));
+    if (!blk) {
+        for (size_t r = 0; r < R; r++) wcap[r] = words[r];
+        layout();
+        blk = acquire_pinned(e, roff[R], (int)R);
+        if (!blk) return fail(SHG_ERR_OOM, "pinned host allocation failed");
+    }
     const uint64_t *src_keys = is_sh1(p->variant) ? e->rib_keys.as<uint64_t>() : e->keys.as<uint64_t>();
-    // one pinned block for all of the batch's results (each result holds a reference)
-    std::vector<size_t> roff(R + 1, 0);
-    for (size_t r = 0; r < R; r++) {
-        const uint64_t rn = nr[r] - (soff[r + 1] - soff[r]);
-        const size_t acc_bytes = (nbr[r] + 1) * 8;
-        roff[r + 1] = roff[r] + ((2 * acc_bytes + words[r] * 8 + rn * 8 + rn + 64 + 63) & ~(size_t)63);
-    }
-    PinnedBlock *blk = acquire_pinned(e, roff[R], (int)R);
-    if (!blk) return fail(SHG_ERR_OOM, "pinned host allocation failed");
     for (size_t r = 0; r < R; r++) {
         shg_result *out = &outs[r];
-        const uint64_t ns = soff[r + 1] - soff[r], rn = nr[r] - ns;
+        const uint64_t ns = soff[r + 1] - soff[r], rn = rnv[r];
         launch_compact_ribbon(src_keys + off[r], e->rib_bits.as<uint8_t>() + off[r], nr[r], e->singles.as<uint64_t>() + soff[r], ns,
-                              e->ckeys.as<uint64_t>() + off[r], e->cbits.as<uint8_t>() + off[r], s);
+                              keys_done ? nullptr : e->ckeys.as<uint64_t>() + off[r], e->cbits.as<uint8_t>() + off[r], s);
         const size_t acc_bytes = (nbr[r] + 1) * 8;
         uint8_t *hp = (uint8_t *)blk->p + roff[r];
         out->owner = blk;
         out->bucket_size_acc = (uint64_t *)hp;
         out->bucket_pos_acc = (uint64_t *)(hp + acc_bytes);
-        out->descriptors = (uint64_t *)(hp + 2 * acc_bytes);
-        out->ribbon_keys = (uint64_t *)(hp + 2 * acc_bytes + words[r] * 8);
-        out->ribbon_bits = hp + 2 * acc_bytes + words[r] * 8 + rn * 8;
+        out->ribbon_keys = (uint64_t *)(hp + 2 * acc_bytes);
+        out->ribbon_bits = hp + 2 * acc_bytes + rn * 8;
+        out->descriptors = (uint64_t *)(hp + ((2 * acc_bytes + rn * 9 + 7) & ~(size_t)7));
         for (uint64_t b = 0; b <= nbr[r]; b++) out->bucket_size_acc[b] = acc[boff[r] + b] - acc[boff[r]];
         CU(cudaMemcpyAsync(out->bucket_pos_acc, e->pos_acc.as<uint64_t>() + boff[r] + r, acc_bytes, cudaMemcpyDeviceToHost, s));
         CU(cudaMemcpyAsync(out->descriptors, e->words.as<uint64_t>() + wbase[r], words[r] * 8, cudaMemcpyDeviceToHost, s));
         if (rn) {
-            CU(cudaMemcpyAsync(out->ribbon_keys, e->ckeys.as<uint64_t>() + off[r], rn * 8, cudaMemcpyDeviceToHost, s));
+            if (!keys_done)
+                CU(cudaMemcpyAsync(out->ribbon_keys, e->ckeys.as<uint64_t>() + off[r], rn * 8, cudaMemcpyDeviceToHost, s));
             CU(cudaMemcpyAsync(out->ribbon_bits, e->cbits.as<uint8_t>() + off[r], rn, cudaMemcpyDeviceToHost, s));
         }
         out->desc_words = words[r];
         out->desc_bits = total[r] + 1;
         out->ribbon_n = rn;
     }
+    if (keys_done) CU(cudaStreamWaitEvent(s, e->join_ev, 0));  // the keys copied during the leaves
     unsigned long long work[8];
     CU(cudaMemcpyAsync(work, misc->work, sizeof(work), cudaMemcpyDeviceToHost, s));
     CU(cudaEventRecord(e->ev[6], s));

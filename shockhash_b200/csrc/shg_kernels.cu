@@ -178,8 +178,8 @@ __global__ void k_compact_ribbon(const uint64_t *__restrict__ keys, const uint8_
             if (singles[mid] < i) lo = mid + 1; else hi = mid;
         }
         if (lo < nsingles && singles[lo] == i) continue;
-        out_keys[i - lo] = keys[i];
-        out_bits[i - lo] = bits[i];
+        if (out_keys) out_keys[i - lo] = keys[i];  // either part may be compacted on its own
+        if (out_bits) out_bits[i - lo] = bits[i];
     }
 }
 
