@@ -6,6 +6,7 @@
 #include <vector>
 #include <cuda_runtime.h>
 #include "shg.h"
+#include "shg_common.cuh"
 
 namespace shg {
 
