@@ -55,7 +55,7 @@ template <> struct Sh2Cfg<128> {
     static constexpr uint32_t RAW_ROWS = 1024;
 };
 
-template <int MAXM> struct Sh2Smem {
+template <int MAXM> struct alignas(16) Sh2Smem {  // 16-byte aligned per warp: the masks are read 16 bytes at a time
     using C = Sh2Cfg<MAXM>;
     uint64_t keys[MAXM];  // finder order (QuadSplit: even keys in order, odd keys from the back)
     uint64_t orig[MAXM];  // leaf order
@@ -384,8 +384,24 @@ __global__ void __launch_bounds__(128, MAXM <= 64 ? 6 : 1) k_leaves_sh2_v2(Src s
                             mineB++;
                         }
                     };
-                    const uint64_t in_sm = min(s + 1, (uint64_t)Sh2Cfg<MAXM>::SMS);
-                    for (uint64_t p = 0; p < in_sm; p++) visit(p, sm.mask[p]);
+                    const uint32_t in_sm = (uint32_t)min(s + 1, (uint64_t)Sh2Cfg<MAXM>::SMS);
+                    uint32_t p = 0;
+                    if constexpr (sizeof(typename LeafCtx<MAXM>::Mask) == 4) {
+                        // two raw seeds per 16-byte load; one combined test rejects the common case
+                        // that neither side of either seed covers the half table
+                        const uint4 *m2 = reinterpret_cast<const uint4 *>(sm.mask);
+                        const uint32_t full = cx.full;
+                        for (; p + 2 <= in_sm; p += 2) {
+                            const uint4 w = m2[p >> 1];
+                            const uint32_t z = min(min((w.x | tB) ^ full, (w.y | tA) ^ full),
+                                                   min((w.z | tB) ^ full, (w.w | tA) ^ full));
+                            if (z == 0) {
+                                visit(p, MaskPair<uint32_t>{w.x, w.y});
+                                visit(p + 1, MaskPair<uint32_t>{w.z, w.w});
+                            }
+                        }
+                    }
+                    for (; p < in_sm; p++) visit(p, sm.mask[p]);
 #pragma unroll 4
                     for (uint64_t p = in_sm; p <= s; p++) visit(p, g.mask[p]);
                     mine = mineA + mineB;
