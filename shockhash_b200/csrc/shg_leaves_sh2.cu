@@ -401,9 +401,41 @@ __global__ void __launch_bounds__(128, MAXM <= 64 ? 6 : 1) k_leaves_sh2_v2(Src s
                             }
                         }
                     }
+                    if constexpr (sizeof(typename LeafCtx<MAXM>::Mask) == 8) {
+                        // one raw seed per 16-byte load, two per round; a tight scan finds the next
+                        // pair in which some side covers the half table, and only then records it
+                        const uint64_t full = cx.full;
+                        for (;;) {
+                            MaskPair<uint64_t> w{0, 0}, v{0, 0};
+                            for (; p + 2 <= in_sm; p += 2) {
+                                w = sm.mask[p];
+                                v = sm.mask[p + 1];
+                                if ((((w.a | tB) ^ full) == 0) | (((w.b | tA) ^ full) == 0) | (((v.a | tB) ^ full) == 0) |
+                                    (((v.b | tA) ^ full) == 0))
+                                    break;
+                            }
+                            if (p + 2 > in_sm) break;
+                            visit(p, w);
+                            visit(p + 1, v);
+                            p += 2;
+                        }
+                    }
                     for (; p < in_sm; p++) visit(p, sm.mask[p]);
+                    uint64_t q = in_sm;
+                    if constexpr (sizeof(typename LeafCtx<MAXM>::Mask) == 8) {  // spilled masks: same paired test
+                        const uint64_t full = cx.full;
+                        for (; q + 2 <= s + 1; q += 2) {
+                            const MaskPair<uint64_t> w = g.mask[q], v = g.mask[q + 1];
+                            const bool any = (((w.a | tB) ^ full) == 0) | (((w.b | tA) ^ full) == 0) |
+                                             (((v.a | tB) ^ full) == 0) | (((v.b | tA) ^ full) == 0);
+                            if (any) {
+                                visit(q, w);
+                                visit(q + 1, v);
+                            }
+                        }
+                    }
 #pragma unroll 4
-                    for (uint64_t p = in_sm; p <= s; p++) visit(p, g.mask[p]);
+                    for (; q <= s; q++) visit(q, g.mask[q]);
                     mine = mineA + mineB;
                 } else {
                     mine = cx.maskA(s) == cx.full;
