@@ -569,7 +569,11 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
         for (int i = 0; i < 7; i++) out->work[i] = work[i];
         out->work[5] = nleaves;
         out->work[6] = nn - nleaves;
-        out->work[7] = launches + 1 + 4 * R;
+        // kernels of this build: hashing (when the keys were hashed on the device), partition
+        // (count and scatter per request, one scan, one sort), split levels and leaves, Golomb-Rice
+        // encoding (4 per request, counted above), retrieval compaction (keys and bits together,
+        // or keys before the leaves and bits after them)
+        out->work[7] = (hash_ms > 0.f ? 1 : 0) + 2 * R + 2 + launches + R * (early_keys ? 2 : 1);
     }
     return SHG_OK;
 }
