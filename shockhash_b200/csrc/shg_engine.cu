@@ -2,7 +2,7 @@
 //
 // Pipeline of one build (all on the engine's stream):
 //   hash (optional) -> bucket count/scan -> scatter + per-bucket sort  [partition, Sorter.hpp:15-36]
-//   -> host plan of the RecSplit trees from bucket_size_acc            [shapes, ShockHash.h:303-555]
+//   -> plan of the RecSplit trees: per-size shapes stamped out per bucket [ShockHash.h:303-555]
 //   -> split-seed search per tree level                                 [ShockHash.h:451-547]
 //   -> leaf searches                                                    [ShockHash.h:404-434 / ShockHash2.h:267-285]
 //   -> Golomb-Rice encode                                               [RiceBitVector.h:67-127]
@@ -112,11 +112,19 @@ struct shg_engine {
     int sms = 148;
     cudaStream_t stream = nullptr;
     DevBuf in_keys, in_bytes, in_offsets, first, second, sfirst, sidx, counts, cursor, acc, keys, nodes, ids, codes,
-        fixed_off, bnb, bucket_bits, pos_acc, words, rib_keys, rib_bits, skip_bits, scratch, misc, singles, ckeys, cbits;
+        fixed_off, bucket_bits, pos_acc, words, rib_keys, rib_bits, scratch, misc, singles, ckeys, cbits;
     // ShockHash2Flat state kept across its nested fallback build
     DevBuf f_bytes, f_offs, f_mhc0, f_cur, f_sorted, f_next, f_thr, f_counts, f_cursor, f_acc, f_free_cnt, f_bump_cnt,
         f_first, f_free_off, f_bump_off, f_free_out, f_bucket, f_last, f_list, f_slot, f_leaf_keys, f_nodes, f_ids, f_codes,
         f_bits, f_mapping, f_lb, f_tmp, f_tmp2;
+    // device shape tables of the configurations this engine has built, grown to the largest bucket
+    struct Shapes {
+        int variant = 0, leaf = 0;
+        ShapeTables host;
+        DevBuf cnt, nodes, node_off, singles, single_off, skip_bits;
+    };
+    std::vector<Shapes *> shapes;
+    DevBuf plan_offs;
     cudaEvent_t ev[8] = {};
     cudaStream_t stream2 = nullptr;  // leaves of the pipelined mode
     static constexpr int kMaxChunks = 64;
@@ -125,12 +133,18 @@ struct shg_engine {
     int pipe_chunks = 8;
     ~shg_engine() {
         DevBuf *all[] = {&in_keys, &in_bytes, &in_offsets, &first, &second, &sfirst, &sidx, &counts, &cursor,
-                         &acc, &keys, &nodes, &ids, &codes, &fixed_off, &bnb, &bucket_bits, &pos_acc, &words,
-                         &rib_keys, &rib_bits, &skip_bits, &scratch, &misc, &singles, &ckeys, &cbits, &f_bytes, &f_offs,
+                         &acc, &keys, &nodes, &ids, &codes, &fixed_off, &bucket_bits, &pos_acc, &words,
+                         &rib_keys, &rib_bits, &scratch, &misc, &singles, &ckeys, &cbits, &f_bytes, &f_offs,
                          &f_mhc0, &f_cur, &f_sorted, &f_next, &f_thr, &f_counts, &f_cursor, &f_acc, &f_free_cnt,
                          &f_bump_cnt, &f_first, &f_free_off, &f_bump_off, &f_free_out, &f_bucket, &f_last, &f_list,
                          &f_slot, &f_leaf_keys, &f_nodes, &f_ids, &f_codes, &f_bits, &f_mapping, &f_lb, &f_tmp, &f_tmp2};
         for (DevBuf *b : all) b->release();
+        plan_offs.release();
+        for (Shapes *sh : shapes) {
+            DevBuf *sb[] = {&sh->cnt, &sh->nodes, &sh->node_off, &sh->singles, &sh->single_off, &sh->skip_bits};
+            for (DevBuf *b : sb) b->release();
+            delete sh;
+        }
         {
             std::lock_guard<std::mutex> lock(g_pool_mu);
             for (PinnedBlock *b : pool) {
@@ -196,6 +210,49 @@ const Config &config_of(int variant, int leaf) {
     return *cache.back();
 }
 
+// The device shape tables of a configuration covering bucket sizes below `rows` (grown in steps of
+// a quarter, then uploaded once; later builds of the configuration reuse them).
+shg_status ensure_shapes(shg_engine *e, const Config &cfg, uint32_t rows, shg_engine::Shapes *&out) {
+    shg_engine::Shapes *sh = nullptr;
+    for (shg_engine::Shapes *x : e->shapes)
+        if (x->variant == cfg.variant && x->leaf == cfg.leaf) sh = x;
+    if (!sh) {
+        sh = new shg_engine::Shapes();
+        sh->variant = cfg.variant;
+        sh->leaf = cfg.leaf;
+        e->shapes.push_back(sh);
+    }
+    out = sh;
+    if (rows <= sh->host.rows) return SHG_OK;
+    rows = std::min<uint32_t>(kMaxBucket, ((rows + rows / 4 + 255) / 256) * 256);
+    try {
+        make_shape_tables(cfg, rows, sh->host);
+    } catch (const std::exception &ex) {
+        sh->host = ShapeTables();
+        return fail(SHG_ERR_ARG, ex.what());
+    }
+    const ShapeTables &t = sh->host;
+    std::vector<uint32_t> skip(rows);
+    for (uint32_t m = 0; m < rows; m++) skip[m] = cfg.skip_bits(m);
+    auto up = [&](DevBuf &b, const void *src, size_t bytes) -> cudaError_t {
+        cudaError_t err = b.ensure(std::max<size_t>(bytes, 16));
+        if (err == cudaSuccess && bytes) err = cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, e->stream);
+        return err;
+    };
+    cudaError_t err = up(sh->cnt, t.cnt.data(), t.cnt.size() * 4);
+    if (err == cudaSuccess) err = up(sh->nodes, t.nodes.data(), t.nodes.size() * sizeof(ShapeNode));
+    if (err == cudaSuccess) err = up(sh->node_off, t.node_off.data(), t.node_off.size() * 4);
+    if (err == cudaSuccess) err = up(sh->singles, t.singles.data(), t.singles.size() * 2);
+    if (err == cudaSuccess) err = up(sh->single_off, t.single_off.data(), t.single_off.size() * 4);
+    if (err == cudaSuccess) err = up(sh->skip_bits, skip.data(), skip.size() * 4);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);  // the host vectors may change later
+    if (err != cudaSuccess) {
+        sh->host = ShapeTables();
+        return fail(SHG_ERR_CUDA, std::string("shape tables: ") + cudaGetErrorString(err));
+    }
+    return SHG_OK;
+}
+
 shg_status check_params(const shg_params *p, uint64_t n) {
     if (!p) return fail(SHG_ERR_ARG, "null params");
     if (!is_sh1(p->variant) && p->variant != SHG_SHOCKHASH2) return fail(SHG_ERR_ARG, "unknown variant");
@@ -252,22 +309,51 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
     CU(e->sidx.ensure(std::max<uint64_t>(n, 1) * 4));
     CU(e->keys.ensure(std::max<uint64_t>(n, 1) * 8));
 
-    // ---- partition: each request's keys into its own bucket range, then one sort pass
+    // ---- partition: each request's keys into its own bucket range, then one sort pass; the
+    // plan's per-bucket offsets are scanned from the bucket sizes before the host looks at them
+    shg_engine::Shapes *shp = nullptr;
+    {
+        const shg_status st = ensure_shapes(e, cfg, std::min<uint64_t>(kMaxBucket, 2 * p->bucket_size + 64), shp);
+        if (st != SHG_OK) return st;
+    }
+    const uint64_t offs_stride = nb + 1;
+    uint64_t plan_launches = 0;
+    auto plan_scan = [&]() -> cudaError_t {
+        plan_launches++;
+        cudaError_t err = e->plan_offs.ensure(((uint64_t)shp->host.ncol * offs_stride + kMaxPlanCols) * 4);
+        if (err == cudaSuccess)
+            launch_plan_scan(e->acc.as<uint64_t>(), nb, shp->cnt.as<uint32_t>(), shp->host.rows, shp->host.ncol,
+                             e->plan_offs.as<uint32_t>(), s);
+        return err;
+    };
     CU(cudaEventRecord(e->ev[0], s));
     for (size_t r = 0; r < R; r++)
         launch_bucket_count(d_first + off[r], nr[r], nbr[r], nb_map[r], b0[r], e->counts.as<uint32_t>() + boff[r], &misc->err,
                             s);
     launch_scan_counts(e->counts.as<uint32_t>(), nb, e->acc.as<uint64_t>(), e->cursor.as<uint32_t>(), &misc->maxsz, s);
+    CU(plan_scan());
     std::vector<uint64_t> acc(nb + 1);
+    uint32_t totals[kMaxPlanCols] = {};
     uint32_t maxsz = 0;
     CU(cudaMemcpyAsync(acc.data(), e->acc.p, (nb + 1) * 8, cudaMemcpyDeviceToHost, s));
     CU(cudaMemcpyAsync(&maxsz, &misc->maxsz, 4, cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(totals, e->plan_offs.as<uint32_t>() + shp->host.ncol * offs_stride, shp->host.ncol * 4,
+                       cudaMemcpyDeviceToHost, s));
     uint32_t perr = 0;
     CU(cudaMemcpyAsync(&perr, &misc->err, 4, cudaMemcpyDeviceToHost, s));
     CU(cudaStreamSynchronize(s));
     if (perr & kErrArg) return fail(SHG_ERR_ARG, "a key lies outside the shard's bucket range");
     if (maxsz >= (uint32_t)kMaxBucket)
         return fail(SHG_ERR_BUCKET, "a bucket holds " + std::to_string(maxsz) + " keys (MAX_BUCKET_SIZE is 3000)");
+    if (maxsz >= shp->host.rows) {  // a bucket larger than the shape tables cover: grow them, scan again
+        const shg_status st = ensure_shapes(e, cfg, maxsz + 1, shp);
+        if (st != SHG_OK) return st;
+        CU(plan_scan());
+        CU(cudaMemcpyAsync(totals, e->plan_offs.as<uint32_t>() + shp->host.ncol * offs_stride, shp->host.ncol * 4,
+                           cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+    }
+    const ShapeTables &tab = shp->host;
     for (size_t r = 0; r < R; r++)
         launch_bucket_scatter(d_first + off[r], nr[r], nbr[r], nb_map[r], b0[r], e->cursor.as<uint32_t>() + boff[r],
                               e->sfirst.as<uint64_t>(),
@@ -276,45 +362,36 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
                        e->keys.as<uint64_t>(), s);
     CU(cudaEventRecord(e->ev[1], s));
 
-    // ---- plan (host)
-    Plan plan;
-    try {
-        make_plan(cfg, acc, plan);
-    } catch (const std::exception &ex) {
-        return fail(SHG_ERR_ARG, ex.what());
+    // ---- plan: launch lists are the split levels in order, then the leaves
+    const uint64_t nn = totals[kColNodes];
+    const uint64_t nsingles = totals[kColSingles];
+    const uint32_t nleaves = totals[kColLeaves];
+    const int nlevels = tab.ncol - kColLevel0;
+    ListOffsets lists{};
+    std::vector<uint64_t> level_count(nlevels), level_off(nlevels);
+    uint64_t nids = 0;
+    for (int lv = 0; lv < nlevels; lv++) {
+        level_off[lv] = lists.level[lv] = (uint32_t)nids;
+        level_count[lv] = totals[kColLevel0 + lv];
+        nids += level_count[lv];
     }
-    const uint64_t nn = plan.nodes.size();
-    uint64_t nids = plan.leaves.size();
-    for (auto &l : plan.split_levels) nids += l.size();
-    std::vector<uint32_t> ids;
-    ids.reserve(nids);
-    std::vector<uint64_t> level_off;
-    for (auto &l : plan.split_levels) {
-        level_off.push_back(ids.size());
-        ids.insert(ids.end(), l.begin(), l.end());
-    }
-    const uint64_t leaf_off = ids.size();
-    ids.insert(ids.end(), plan.leaves.begin(), plan.leaves.end());
-    std::vector<uint32_t> skip(kMaxBucket);
-    for (int m = 0; m < kMaxBucket; m++) skip[m] = cfg.skip_bits(m);
-
+    const uint64_t leaf_off = lists.leaf = (uint32_t)nids;
+    nids += nleaves;
     CU(e->nodes.ensure(std::max<uint64_t>(nn, 1) * sizeof(Node)));
     CU(e->fixed_off.ensure(std::max<uint64_t>(nn, 1) * 2));
     CU(e->codes.ensure(std::max<uint64_t>(nn, 1) * 8));
     CU(e->ids.ensure(std::max<uint64_t>(nids, 1) * 4));
-    CU(e->bnb.ensure((nb + 1) * 4));
-    CU(e->skip_bits.ensure(kMaxBucket * 4));
     CU(e->bucket_bits.ensure(nb * 8));
     CU(e->pos_acc.ensure((nb + 1) * 8));
     CU(e->rib_bits.ensure(std::max<uint64_t>(n, 1)));
     if (is_sh1(p->variant)) CU(e->rib_keys.ensure(std::max<uint64_t>(n, 1) * 8));
-    if (nn) {
-        CU(cudaMemcpyAsync(e->nodes.p, plan.nodes.data(), nn * sizeof(Node), cudaMemcpyHostToDevice, s));
-        CU(cudaMemcpyAsync(e->fixed_off.p, plan.fixed_off.data(), nn * 2, cudaMemcpyHostToDevice, s));
-    }
-    if (nids) CU(cudaMemcpyAsync(e->ids.p, ids.data(), nids * 4, cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(e->bnb.p, plan.bucket_node_begin.data(), (nb + 1) * 4, cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(e->skip_bits.p, skip.data(), kMaxBucket * 4, cudaMemcpyHostToDevice, s));
+    CU(e->singles.ensure(std::max<uint64_t>(nsingles, 1) * 8));
+    plan_launches += nb ? 1 : 0;
+    launch_plan_expand(e->acc.as<uint64_t>(), nb, tab.rows, e->plan_offs.as<uint32_t>(), shp->nodes.as<ShapeNode>(),
+                       shp->node_off.as<uint32_t>(), shp->singles.as<uint16_t>(), shp->single_off.as<uint32_t>(), lists,
+                       e->nodes.as<Node>(), e->fixed_off.as<uint16_t>(), e->ids.as<uint32_t>(), e->singles.as<uint64_t>(), s);
+    const uint32_t *d_bnb = e->plan_offs.as<uint32_t>() + kColNodes * offs_stride;  // first node of each bucket
+    const uint32_t *d_skip = shp->skip_bits.as<uint32_t>();
     if (p->variant == SHG_SHOCKHASH2) {
         // bipartite leaf scratch for the widest leaf grid any schedule uses (grown once, then reused)
         const uint32_t sm_ = p->leaf_size > 64 ? 16384 : 4096, cm_ = p->leaf_size > 64 ? 16384 : 2048;
@@ -322,21 +399,23 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
         const int bps = std::max(1, std::min(8, (228 * 1024) / (4 * sh2_smem_per_warp(p->leaf_size) + 1024)));
         CU(e->scratch.ensure(pw * (uint64_t)e->sms * bps * 4));
     }
-    // retrieval input per request: its keys minus those of size-1 children (no retrieval bit)
-    const uint64_t nsingles = plan.singles.size();
-    CU(e->singles.ensure(std::max<uint64_t>(nsingles, 1) * 8));
+    // per request: its nodes, its size-1 positions (no retrieval bit) and its fixed code bits,
+    // from the host copy of the shape table
+    std::vector<uint64_t> soff(R + 1, 0), rnv(R), rnodes(R, 0), rfixed(R, 0);
+    for (size_t r = 0; r < R; r++) {
+        uint64_t singles_r = 0;
+        for (uint64_t b = boff[r]; b < boff[r + 1]; b++) {
+            const uint32_t m = (uint32_t)(acc[b + 1] - acc[b]);
+            const uint32_t *row = &tab.cnt[(size_t)m * tab.ncol];
+            rnodes[r] += row[kColNodes];
+            singles_r += row[kColSingles];
+            rfixed[r] += cfg.skip_bits(m);
+        }
+        soff[r + 1] = soff[r] + singles_r;
+        rnv[r] = nr[r] - singles_r;
+    }
     CU(e->ckeys.ensure(std::max<uint64_t>(n, 1) * 8));
     CU(e->cbits.ensure(std::max<uint64_t>(n, 1)));
-    std::vector<uint64_t> rel_singles(nsingles), soff(R + 1, 0), rnv(R);
-    for (size_t r = 0, j = 0; r < R; r++) {
-        while (j < nsingles && plan.singles[j] < off[r + 1]) {
-            rel_singles[j] = plan.singles[j] - off[r];
-            j++;
-        }
-        soff[r + 1] = j;
-        rnv[r] = nr[r] - (soff[r + 1] - soff[r]);
-    }
-    if (nsingles) CU(cudaMemcpyAsync(e->singles.p, rel_singles.data(), nsingles * 8, cudaMemcpyHostToDevice, s));
     // Bipartite retrieval keys are final once the splits are done (the leaves only add the bits),
     // so in the level schedule they go to the host on the second stream while the leaf kernel
     // runs. The pinned block is then taken before the splits, with room for descriptor words
@@ -354,10 +433,7 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
     PinnedBlock *blk = nullptr;
     if (early_keys) {
         for (size_t r = 0; r < R; r++) {
-            uint64_t fixed = 0;
-            for (uint64_t b = boff[r]; b < boff[r + 1]; b++) fixed += cfg.skip_bits((uint32_t)(acc[b + 1] - acc[b]));
-            const uint64_t nodes_r = plan.bucket_node_begin[boff[r + 1]] - plan.bucket_node_begin[boff[r]];
-            const uint64_t bits = fixed + 8 * nodes_r + 1;
+            const uint64_t bits = rfixed[r] + 8 * rnodes[r] + 1;
             wcap[r] = ((bits + 7) / 8 + 14) / 8;
         }
         layout();
@@ -373,7 +449,6 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
     // ---- splits and leaves
     uint64_t launches = 0;
     const uint32_t *d_ids = e->ids.as<uint32_t>();
-    const uint32_t nleaves = (uint32_t)plan.leaves.size();
     const bool sh2 = p->variant == SHG_SHOCKHASH2;
     const bool pipelined = p->mode == SHG_MODE_PIPELINED;
     // leaf kernel launch shape and scratch
@@ -416,22 +491,20 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
         // second stream as soon as those splits are done, overlapping the next chunk's splits.
         // Node and leaf lists are in bucket order, so a chunk is a contiguous range of each list.
         const int C = (int)std::max<uint64_t>(1, std::min<uint64_t>(nb, (uint64_t)e->pipe_chunks));
-        auto chunk_bounds = [&](const std::vector<uint32_t> &list, std::vector<uint64_t> &bounds) {
-            bounds.assign(C + 1, list.size());
-            bounds[0] = 0;
-            uint64_t j = 0;
-            for (int c = 1; c < C; c++) {
-                const uint64_t bucket_lo = nb * (uint64_t)c / C;
-                while (j < list.size() && plan.nodes[list[j]].bucket < bucket_lo) j++;
-                bounds[c] = j;
-            }
+        // bounds of each launch list at the chunk borders: the per-bucket list offsets of the plan
+        std::vector<uint32_t> offs_h((uint64_t)tab.ncol * offs_stride);
+        CU(cudaMemcpyAsync(offs_h.data(), e->plan_offs.p, offs_h.size() * 4, cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        auto chunk_bounds = [&](int col, std::vector<uint64_t> &bounds) {
+            bounds.assign(C + 1, 0);
+            for (int c = 0; c <= C; c++) bounds[c] = offs_h[(uint64_t)col * offs_stride + nb * (uint64_t)c / C];
         };
-        std::vector<std::vector<uint64_t>> lvb(plan.split_levels.size());
-        for (size_t lv = 0; lv < plan.split_levels.size(); lv++) chunk_bounds(plan.split_levels[lv], lvb[lv]);
+        std::vector<std::vector<uint64_t>> lvb(nlevels);
+        for (int lv = 0; lv < nlevels; lv++) chunk_bounds(kColLevel0 + lv, lvb[lv]);
         std::vector<uint64_t> lb;
-        chunk_bounds(plan.leaves, lb);
+        chunk_bounds(kColLeaves, lb);
         for (int c = 0; c < C; c++) {
-            for (size_t lv = 0; lv < plan.split_levels.size(); lv++) split_range(lv, lvb[lv][c], lvb[lv][c + 1], s);
+            for (int lv = 0; lv < nlevels; lv++) split_range(lv, lvb[lv][c], lvb[lv][c + 1], s);
             CU(cudaEventRecord(e->chunk_ev[c], s));
             CU(cudaStreamWaitEvent(e->stream2, e->chunk_ev[c], 0));
             leaf_range(lb[c], lb[c + 1], e->stream2, leaf_grid);
@@ -440,7 +513,7 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
         CU(cudaEventRecord(e->join_ev, e->stream2));
         CU(cudaStreamWaitEvent(s, e->join_ev, 0));
     } else {
-        for (size_t lv = 0; lv < plan.split_levels.size(); lv++) split_range(lv, 0, plan.split_levels[lv].size(), s);
+        for (int lv = 0; lv < nlevels; lv++) split_range(lv, 0, level_count[lv], s);
         CU(cudaEventRecord(e->ev[3], s));
         if (early_keys) {
             // compaction on the engine stream before the leaf kernel takes every SM; only the
@@ -448,7 +521,7 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
             for (size_t r = 0; r < R; r++)
                 if (rnv[r])
                     launch_compact_ribbon(e->keys.as<uint64_t>() + off[r], nullptr, nr[r], e->singles.as<uint64_t>() + soff[r],
-                                          soff[r + 1] - soff[r], e->ckeys.as<uint64_t>() + off[r], nullptr, s);
+                                          soff[r + 1] - soff[r], off[r], e->ckeys.as<uint64_t>() + off[r], nullptr, s);
             CU(cudaEventRecord(e->chunk_ev[0], s));
             CU(cudaStreamWaitEvent(e->stream2, e->chunk_ev[0], 0));
             for (size_t r = 0; r < R; r++)
@@ -468,8 +541,8 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
     // ---- Golomb-Rice encode, one stream per request
     CU(e->pos_acc.ensure((nb + R) * 8));
     for (size_t r = 0; r < R; r++) {
-        launch_gr_bucket_bits(e->nodes.as<Node>(), e->bnb.as<uint32_t>() + boff[r], nbr[r], e->acc.as<uint64_t>() + boff[r],
-                              e->codes.as<uint64_t>(), e->skip_bits.as<uint32_t>(), e->bucket_bits.as<uint64_t>() + boff[r], s);
+        launch_gr_bucket_bits(e->nodes.as<Node>(), d_bnb + boff[r], nbr[r], e->acc.as<uint64_t>() + boff[r],
+                              e->codes.as<uint64_t>(), d_skip, e->bucket_bits.as<uint64_t>() + boff[r], s);
         launch_scan_u64(e->bucket_bits.as<uint64_t>() + boff[r], nbr[r], e->pos_acc.as<uint64_t>() + boff[r] + r, s);
     }
     std::vector<uint64_t> pos(nb + R);
@@ -495,9 +568,9 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
     CU(cudaMemsetAsync(e->words.p, 0, wbase[R] * 8, s));
     for (size_t r = 0; r < R; r++) {
         unsigned long long *w = e->words.as<unsigned long long>() + wbase[r];
-        launch_gr_write(e->nodes.as<Node>(), e->fixed_off.as<uint16_t>(), e->bnb.as<uint32_t>() + boff[r], nbr[r],
+        launch_gr_write(e->nodes.as<Node>(), e->fixed_off.as<uint16_t>(), d_bnb + boff[r], nbr[r],
                         e->acc.as<uint64_t>() + boff[r], e->pos_acc.as<uint64_t>() + boff[r] + r, e->codes.as<uint64_t>(),
-                        e->skip_bits.as<uint32_t>(), w, s);
+                        d_skip, w, s);
         launch_set_bit(w, total[r], s);
         launches += 4;
     }
@@ -528,7 +601,7 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
         shg_result *out = &outs[r];
         const uint64_t ns = soff[r + 1] - soff[r], rn = rnv[r];
         launch_compact_ribbon(src_keys + off[r], e->rib_bits.as<uint8_t>() + off[r], nr[r], e->singles.as<uint64_t>() + soff[r], ns,
-                              keys_done ? nullptr : e->ckeys.as<uint64_t>() + off[r], e->cbits.as<uint8_t>() + off[r], s);
+                              off[r], keys_done ? nullptr : e->ckeys.as<uint64_t>() + off[r], e->cbits.as<uint8_t>() + off[r], s);
         const size_t acc_bytes = (nbr[r] + 1) * 8;
         uint8_t *hp = (uint8_t *)blk->p + roff[r];
         out->owner = blk;
@@ -570,10 +643,10 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
         out->work[5] = nleaves;
         out->work[6] = nn - nleaves;
         // kernels of this build: hashing (when the keys were hashed on the device), partition
-        // (count and scatter per request, one scan, one sort), split levels and leaves, Golomb-Rice
-        // encoding (4 per request, counted above), retrieval compaction (keys and bits together,
-        // or keys before the leaves and bits after them)
-        out->work[7] = (hash_ms > 0.f ? 1 : 0) + 2 * R + 2 + launches + R * (early_keys ? 2 : 1);
+        // (count and scatter per request, one scan, one sort), plan (offset scan and expansion),
+        // split levels and leaves, Golomb-Rice encoding (4 per request, counted above), retrieval
+        // compaction (keys and bits together, or keys before the leaves and bits after them)
+        out->work[7] = (hash_ms > 0.f ? 1 : 0) + 2 * R + 2 + plan_launches + launches + R * (early_keys ? 2 : 1);
     }
     return SHG_OK;
 }

@@ -61,18 +61,37 @@ struct Shape {
 };
 const Shape &shape_of(const Config &c, uint32_t m, std::vector<Shape> &cache, std::vector<char> &have);
 
-// Expanded plan of a whole build.
-struct Plan {
-    std::vector<Node> nodes;                      // all nodes, buckets in order, preorder within a bucket
-    std::vector<uint16_t> fixed_off;              // per node
-    std::vector<uint32_t> bucket_node_begin;      // [nbuckets + 1]
-    std::vector<std::vector<uint32_t>> split_levels;  // split node ids per level
-    std::vector<uint32_t> leaves;                 // leaf node ids
-    std::vector<uint32_t> leaf_sizes_hist;        // count of leaves per size
-    std::vector<uint64_t> singles;                // global positions of keys in size-1 children or buckets
-    uint64_t leaf_keys = 0;
+// Every tree shape of one configuration for bucket sizes 0 .. rows-1, laid out for the device,
+// which expands the plan of a build from it (k_plan_scan, k_plan_expand). Per size m, row m of
+// `cnt` holds its node count, its size-1 children, its leaves and its split nodes per level
+// (columns kColNodes, kColSingles, kColLeaves, kColLevel0 + level); its nodes sit in preorder at
+// nodes[node_off[m] .. node_off[m + 1]), each with its rank in its launch list (the leaves, or the
+// split nodes of its level) within the shape; its size-1 children in ascending order at
+// singles[single_off[m] .. single_off[m + 1]).
+enum : int { kColNodes = 0, kColSingles = 1, kColLeaves = 2, kColLevel0 = 3 };
+constexpr int kMaxPlanCols = kColLevel0 + kMaxLevels;
+struct __align__(16) ShapeNode {
+    uint16_t rel, m;
+    uint8_t level, kind, fanout, g;
+    uint16_t unit, fixed_off, rank, pad;
 };
-void make_plan(const Config &c, const std::vector<uint64_t> &bucket_size_acc, Plan &plan);
+static_assert(sizeof(ShapeNode) == 16, "ShapeNode must stay 16 bytes");
+struct ShapeTables {
+    uint32_t rows = 0;
+    int ncol = kColLevel0;
+    std::vector<uint32_t> cnt;  // [rows][ncol]
+    std::vector<ShapeNode> nodes;
+    std::vector<uint32_t> node_off;  // [rows + 1]
+    std::vector<uint16_t> singles;
+    std::vector<uint32_t> single_off;  // [rows + 1]
+};
+void make_shape_tables(const Config &c, uint32_t rows, ShapeTables &t);
+
+// Start of each launch list in the id array of a build: split levels in order, then the leaves.
+struct ListOffsets {
+    uint32_t level[kMaxLevels];
+    uint32_t leaf;
+};
 
 // ShockHash2Flat<k> constants (ShockHash2Flat.h:16-46).
 struct FlatConsts {
@@ -128,6 +147,13 @@ void launch_gr_write(const Node *nodes, const uint16_t *fixed_off, const uint32_
                      const uint32_t *memo_skip_bits, unsigned long long *words, cudaStream_t s);
 void launch_set_bit(unsigned long long *words, uint64_t bit, cudaStream_t s);
 void launch_compact_ribbon(const uint64_t *keys, const uint8_t *bits, uint64_t n, const uint64_t *singles,
-                           uint64_t nsingles, uint64_t *out_keys, uint8_t *out_bits, cudaStream_t s);
+                           uint64_t nsingles, uint64_t single_base, uint64_t *out_keys, uint8_t *out_bits,
+                           cudaStream_t s);
+void launch_plan_scan(const uint64_t *acc, uint64_t nb, const uint32_t *cnt, uint32_t rows, int ncol, uint32_t *offs,
+                      cudaStream_t s);
+void launch_plan_expand(const uint64_t *acc, uint64_t nb, uint32_t rows, const uint32_t *offs, const ShapeNode *shape_nodes,
+                        const uint32_t *node_off, const uint16_t *shape_singles, const uint32_t *single_off,
+                        const ListOffsets &lists, Node *nodes, uint16_t *fixed_off, uint32_t *ids, uint64_t *singles,
+                        cudaStream_t s);
 
 } // namespace shg

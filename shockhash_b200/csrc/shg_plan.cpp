@@ -1,7 +1,8 @@
-// Host-side planning of a build: the Golomb-Rice memo of a configuration and the RecSplit tree
-// of every bucket, laid out in preorder. The tree's shape depends only on the bucket size, so one
-// shape per distinct size is derived (mirroring the recursion of ShockHash.h:303-555 /
-// ShockHash2.h:259-394) and then stamped out for every bucket of that size.
+// Planning of a build: the Golomb-Rice memo of a configuration and the RecSplit tree of every
+// bucket size, in preorder. The tree's shape depends only on the bucket size, so one shape per
+// size is derived here (mirroring the recursion of ShockHash.h:303-555 / ShockHash2.h:259-394) and
+// the device stamps it out for every bucket of that size (k_plan_expand).
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <stdexcept>
@@ -135,56 +136,45 @@ const Shape &shape_of(const Config &c, uint32_t m, std::vector<Shape> &cache, st
     return cache[m];
 }
 
-void make_plan(const Config &c, const std::vector<uint64_t> &acc, Plan &plan) {
-    const uint64_t nb = acc.size() - 1;
+void make_shape_tables(const Config &c, uint32_t rows, ShapeTables &t) {
+    if (rows > (uint32_t)kMaxBucket) throw std::runtime_error("bucket size beyond MAX_BUCKET_SIZE");
     // shapes depend only on the configuration and the bucket size: reuse them across builds
     std::shared_ptr<ShapeCache> sc = c.shapes ? c.shapes : std::make_shared<ShapeCache>();
     std::lock_guard<std::mutex> lock(sc->mu);
-    std::vector<Shape> &cache = sc->cache;
-    std::vector<char> &have = sc->have;
-    uint64_t total = 0;
-    for (uint64_t b = 0; b < nb; b++) {
-        const uint64_t m = acc[b + 1] - acc[b];
-        if (m >= (uint64_t)kMaxBucket) throw std::runtime_error("bucket too large");
-        total += shape_of(c, (uint32_t)m, cache, have).nodes.size();
-    }
-    plan.nodes.resize(total);
-    plan.fixed_off.resize(total);
-    plan.bucket_node_begin.assign(nb + 1, 0);
-    plan.split_levels.clear();
-    plan.leaves.clear();
-    plan.singles.clear();
-    plan.leaf_sizes_hist.assign(kMaxLeaf2 + 1, 0);
-    plan.leaf_keys = 0;
-    uint64_t id = 0;
-    for (uint64_t b = 0; b < nb; b++) {
-        plan.bucket_node_begin[b] = (uint32_t)id;
-        const uint32_t m = (uint32_t)(acc[b + 1] - acc[b]);
-        const Shape &sh = shape_of(c, m, cache, have);
-        for (uint16_t s : sh.singles) plan.singles.push_back(acc[b] + s);
-        for (const TNode &t : sh.nodes) {
-            Node &n = plan.nodes[id];
-            n.start = (uint32_t)(acc[b] + t.rel);
-            n.m = t.m;
-            n.level = t.level;
-            n.kind = t.kind;
-            n.bucket = (uint32_t)b;
-            n.unit = t.unit;
-            n.fanout = t.fanout;
-            n.g = t.g;
-            plan.fixed_off[id] = t.fixed_off;
-            if (t.kind == kLeaf) {
-                plan.leaves.push_back((uint32_t)id);
-                plan.leaf_sizes_hist[t.m]++;
-                plan.leaf_keys += t.m;
-            } else {
-                if (plan.split_levels.size() <= t.level) plan.split_levels.resize(t.level + 1);
-                plan.split_levels[t.level].push_back((uint32_t)id);
-            }
-            id++;
+    int depth = 0;
+    for (uint32_t m = 0; m < rows; m++) depth = std::max(depth, shape_of(c, m, sc->cache, sc->have).depth);
+    t.rows = rows;
+    t.ncol = kColLevel0 + depth;
+    t.cnt.assign((size_t)rows * t.ncol, 0);
+    t.nodes.clear();
+    t.singles.clear();
+    t.node_off.assign(rows + 1, 0);
+    t.single_off.assign(rows + 1, 0);
+    for (uint32_t m = 0; m < rows; m++) {
+        const Shape &sh = shape_of(c, m, sc->cache, sc->have);
+        uint32_t *row = &t.cnt[(size_t)m * t.ncol];
+        t.node_off[m] = (uint32_t)t.nodes.size();
+        t.single_off[m] = (uint32_t)t.singles.size();
+        for (const TNode &tn : sh.nodes) {
+            ShapeNode n{};
+            n.rel = tn.rel;
+            n.m = tn.m;
+            n.level = tn.level;
+            n.kind = tn.kind;
+            n.fanout = tn.fanout;
+            n.g = tn.g;
+            n.unit = tn.unit;
+            n.fixed_off = tn.fixed_off;
+            const int col = tn.kind == kLeaf ? kColLeaves : kColLevel0 + tn.level;
+            n.rank = (uint16_t)row[col]++;
+            t.nodes.push_back(n);
         }
+        row[kColNodes] = (uint32_t)sh.nodes.size();
+        row[kColSingles] = (uint32_t)sh.singles.size();
+        t.singles.insert(t.singles.end(), sh.singles.begin(), sh.singles.end());
     }
-    plan.bucket_node_begin[nb] = (uint32_t)id;
+    t.node_off[rows] = (uint32_t)t.nodes.size();
+    t.single_off[rows] = (uint32_t)t.singles.size();
 }
 
 } // namespace shg
