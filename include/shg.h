@@ -7,7 +7,9 @@
  *   - bucket_size_acc / bucket_pos_acc   (hash_gen, include/ShockHash.h:616-654; ShockHash2.h:455-494)
  *   - the retrieval input (key, bit)      (ShockHash.h:425-428; ShockHash2-internal.h:548-572),
  *     in the reference's push order.
- * The elias-fano and retrieval structures built from those arrays stay on the host.
+ * The Elias-Fano structure built from those arrays stays on the host; the retrieval input can go
+ * to the reference's SimpleRibbon or to the compact retrieval structure built on the device
+ * (shg_retrieval_*).
  *
  * Errors: every entry point returns an shg_status; no C++ exception crosses this boundary. The
  * message of the last failure on the calling thread is available from shg_last_error().
@@ -213,6 +215,44 @@ uint64_t shg_dmphf_bits(const shg_dmphf *f);
 uint64_t shg_dmphf_size(const shg_dmphf *f);
 /* Device time of the last query kernel, in milliseconds (CUDA events on the object's stream). */
 float shg_dmphf_last_kernel_ms(const shg_dmphf *f);
+/* The same object with the compact retrieval structure (shg_retrieval_*, below) built on the device
+ * in place of the exact table: outputs equal shg_mphf_query_* for every key of the build (other
+ * keys may differ, as they may between any two retrieval structures). Size in bits of the
+ * object's retrieval part, compact structure or table. */
+shg_status shg_dmphf_create_compact(int device, const shg_params *p, const shg_result *r, shg_dmphf **out);
+uint64_t shg_dmphf_retrieval_bits(const shg_dmphf *f);
+
+/* ------------------------------------------------------------------ retrieval structure
+ * Compact 1-bit retrieval built on the GPU from a retrieval input (key, bit): the role of
+ * SimpleRibbon<1, w> in the reference (built at ShockHash.h:657 and ShockHash2.h:497 from
+ * ribbonInput, read by retrieve() at ShockHash.h:267-270 and ShockHash2.h:226-229). SimpleRibbon's
+ * source is absent from the reference tree, so the format is this library's own: levels of buckets
+ * of ~240 keys, each bucket a 256-bit GF(2) solution and an 8-bit priority threshold (keys at or
+ * above it go to the next level), about 1.1 bits per key. query(key) returns the stored bit of
+ * every input key (any bit for other keys). Duplicate keys with different bits fail with
+ * SHG_ERR_ARG. */
+typedef struct shg_retrieval shg_retrieval;
+/* Build from host arrays (copied to the engine's device) or from device arrays; synchronous. */
+shg_status shg_retrieval_build(shg_engine *e, const uint64_t *keys, const uint8_t *bits, uint64_t n,
+                               shg_retrieval **out);
+shg_status shg_retrieval_build_device(shg_engine *e, const uint64_t *d_keys, const uint8_t *d_bits, uint64_t n,
+                                      shg_retrieval **out);
+/* A structure from its arrays (as read back with the accessors below): host queries only. */
+shg_status shg_retrieval_load(const uint64_t *level_buckets, uint32_t levels, const uint64_t *solutions,
+                              const uint8_t *thresholds, uint64_t n, shg_retrieval **out);
+void shg_retrieval_destroy(shg_retrieval *r);
+/* Host query, and device query over device arrays (synchronous, on the building engine's device). */
+shg_status shg_retrieval_query(const shg_retrieval *r, const uint64_t *keys, uint64_t n, uint8_t *out);
+shg_status shg_retrieval_query_device(shg_retrieval *r, const uint64_t *d_keys, uint64_t n, uint8_t *d_out);
+/* Format accessors: levels, buckets of a level, 4 solution words per bucket and one threshold per
+ * bucket (levels back to back), size in bits, device times of the build and of the last query. */
+uint32_t shg_retrieval_levels(const shg_retrieval *r);
+uint64_t shg_retrieval_buckets(const shg_retrieval *r, uint32_t level);
+const uint64_t *shg_retrieval_solutions(const shg_retrieval *r);
+const uint8_t *shg_retrieval_thresholds(const shg_retrieval *r);
+uint64_t shg_retrieval_bits(const shg_retrieval *r);
+float shg_retrieval_build_ms(const shg_retrieval *r);
+float shg_retrieval_query_ms(const shg_retrieval *r);
 
 /* ------------------------------------------------------------------ ShockHash2Flat<k>
  * k-perfect "flat" variant (include/ShockHash2Flat.h:37-302): MurmurHash64 keys, two threshold

@@ -115,6 +115,8 @@ def lib():
         "shg_dmphf_bits": ([_vp], _u64),
         "shg_dmphf_size": ([_vp], _u64),
         "shg_dmphf_last_kernel_ms": ([_vp], ctypes.c_float),
+        "shg_dmphf_create_compact": ([ctypes.c_int, P, R, ctypes.POINTER(_vp)], ctypes.c_int),
+        "shg_dmphf_retrieval_bits": ([_vp], _u64),
         "shg_dflat_create": ([ctypes.c_int, ctypes.POINTER(_FlatResult), ctypes.POINTER(_vp)], ctypes.c_int),
         "shg_dflat_destroy": ([_vp], None),
         "shg_dflat_query_strings": ([_vp, ctypes.c_char_p, _vp, _u64, _vp], ctypes.c_int),
@@ -128,6 +130,19 @@ def lib():
         "shg_flat_query_strings": ([_vp, ctypes.c_char_p, _vp, _u64, _vp], ctypes.c_int),
         "shg_flat_query_hash": ([_vp, _vp, _u64, _vp], ctypes.c_int),
         "shg_flat_bits": ([_vp], _u64),
+        "shg_retrieval_build": ([_vp, _vp, _vp, _u64, ctypes.POINTER(_vp)], ctypes.c_int),
+        "shg_retrieval_build_device": ([_vp, _vp, _vp, _u64, ctypes.POINTER(_vp)], ctypes.c_int),
+        "shg_retrieval_load": ([_vp, ctypes.c_uint32, _vp, _vp, _u64, ctypes.POINTER(_vp)], ctypes.c_int),
+        "shg_retrieval_destroy": ([_vp], None),
+        "shg_retrieval_query": ([_vp, _vp, _u64, _vp], ctypes.c_int),
+        "shg_retrieval_query_device": ([_vp, _vp, _u64, _vp], ctypes.c_int),
+        "shg_retrieval_levels": ([_vp], ctypes.c_uint32),
+        "shg_retrieval_buckets": ([_vp, ctypes.c_uint32], _u64),
+        "shg_retrieval_solutions": ([_vp], _vp),
+        "shg_retrieval_thresholds": ([_vp], _vp),
+        "shg_retrieval_bits": ([_vp], _u64),
+        "shg_retrieval_build_ms": ([_vp], ctypes.c_float),
+        "shg_retrieval_query_ms": ([_vp], ctypes.c_float),
         "shg_device_memory": ([ctypes.c_int, ctypes.POINTER(_u64), ctypes.POINTER(_u64)], ctypes.c_int),
         "shg_keys_mt19937_64": ([_u64, _u64, _vp], None),
         "shg_int_peak": ([ctypes.c_int, _u64, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)],
@@ -515,13 +530,16 @@ def merge_shards(variant, leaf_size, shards, bucket_size=2000):
 
 class DeviceMphf:
     """operator() evaluated on the GPU for many keys per call (``shg_dmphf_*``), over a build result.
-    Outputs equal the host query key for key. The result may be freed afterwards."""
+    Outputs equal the host query key for key. The result may be freed afterwards. ``compact=True``
+    reads the retrieval bit from the compact structure built on the device (``Retrieval``) instead of
+    an exact table; outputs then equal the host query for the keys of the build."""
 
-    def __init__(self, result, device=0):
+    def __init__(self, result, device=0, compact=False):
         if result._res is None:
             raise ShgError(1, "build result already freed")
         h = _vp()
-        _check(lib().shg_dmphf_create(device, ctypes.byref(result.params), ctypes.byref(result._res), ctypes.byref(h)))
+        create = lib().shg_dmphf_create_compact if compact else lib().shg_dmphf_create
+        _check(create(device, ctypes.byref(result.params), ctypes.byref(result._res), ctypes.byref(h)))
         self._h = h
 
     def query_hash(self, first, second):
@@ -553,12 +571,103 @@ class DeviceMphf:
     def bits(self):
         return int(lib().shg_dmphf_bits(self._h))
 
+    def retrieval_bits(self):
+        """Size of the retrieval part actually held on the device (compact structure or table)."""
+        return int(lib().shg_dmphf_retrieval_bits(self._h))
+
     def size(self):
         return int(lib().shg_dmphf_size(self._h))
 
     def close(self):
         if self._h:
             lib().shg_dmphf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Retrieval:
+    """Compact 1-bit retrieval structure built on the GPU from a retrieval input (``shg_retrieval_*``):
+    the role of SimpleRibbon<1, w> in the reference (ShockHash.h:657, ShockHash2.h:497), in this
+    library's own format (levels of ~240-key buckets, a 256-bit GF(2) solution and an 8-bit priority
+    threshold per bucket). ``query`` returns the stored bit of every input key."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def build(cls, engine, keys, bits):
+        keys = np.ascontiguousarray(keys, dtype=np.uint64)
+        bits = np.ascontiguousarray(bits, dtype=np.uint8)
+        if len(keys) != len(bits):
+            raise ShgError(1, "keys and bits differ in length")
+        h = _vp()
+        _check(lib().shg_retrieval_build(engine._h, _ptr(keys), _ptr(bits), len(keys), ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def build_device(cls, engine, d_keys, d_bits, n):
+        """Device pointers (ints) to n uint64 keys and n uint8 bits."""
+        h = _vp()
+        _check(lib().shg_retrieval_build_device(engine._h, _vp(d_keys), _vp(d_bits), n, ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def load(cls, level_buckets, solutions, thresholds, n=0):
+        """A structure from its arrays (host queries only)."""
+        lb = np.ascontiguousarray(level_buckets, dtype=np.uint64)
+        sol = np.ascontiguousarray(solutions, dtype=np.uint64)
+        thr = np.ascontiguousarray(thresholds, dtype=np.uint8)
+        if len(sol) != 4 * len(thr) or int(lb.sum()) != len(thr):
+            raise ShgError(1, "solution, threshold and bucket counts disagree")
+        h = _vp()
+        _check(lib().shg_retrieval_load(_ptr(lb), len(lb), _ptr(sol), _ptr(thr), n, ctypes.byref(h)))
+        return cls(h)
+
+    def query(self, keys):
+        keys = np.ascontiguousarray(keys, dtype=np.uint64)
+        out = np.zeros(len(keys), np.uint8)
+        _check(lib().shg_retrieval_query(self._h, _ptr(keys), len(keys), _ptr(out)))
+        return out
+
+    def query_device(self, d_keys, n, d_out):
+        """Device pointers (ints); synchronous."""
+        _check(lib().shg_retrieval_query_device(self._h, _vp(d_keys), n, _vp(d_out)))
+
+    def levels(self):
+        return int(lib().shg_retrieval_levels(self._h))
+
+    def level_buckets(self):
+        return np.array([lib().shg_retrieval_buckets(self._h, l) for l in range(self.levels())], dtype=np.uint64)
+
+    def arrays(self):
+        """(level buckets, solutions [4 words per bucket], thresholds) copied out."""
+        lb = self.level_buckets()
+        nb = int(lb.sum())
+        if nb == 0:
+            return lb, np.zeros(0, np.uint64), np.zeros(0, np.uint8)
+        sol = np.ctypeslib.as_array(ctypes.cast(lib().shg_retrieval_solutions(self._h), ctypes.POINTER(ctypes.c_uint64)),
+                                    (4 * nb,)).copy()
+        thr = np.ctypeslib.as_array(ctypes.cast(lib().shg_retrieval_thresholds(self._h), ctypes.POINTER(ctypes.c_uint8)),
+                                    (nb,)).copy()
+        return lb, sol, thr
+
+    def bits(self):
+        return int(lib().shg_retrieval_bits(self._h))
+
+    def build_ms(self):
+        return float(lib().shg_retrieval_build_ms(self._h))
+
+    def query_ms(self):
+        return float(lib().shg_retrieval_query_ms(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().shg_retrieval_destroy(self._h)
             self._h = None
 
     def __del__(self):

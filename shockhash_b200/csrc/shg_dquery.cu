@@ -18,6 +18,7 @@
 #include "shg.h"
 #include "shg_common.cuh"
 #include "shg_internal.h"
+#include "shg_retrieval.cuh"
 
 using namespace shg;
 
@@ -31,6 +32,9 @@ struct DView {
     const uint64_t *tkey;
     const uint32_t *tbits;
     const uint32_t *special;  // bit 1: key kEmpty present; bit 0: its retrieval bit
+    const RetLevels *rlv;     // compact retrieval structure instead of the table (or null)
+    const uint64_t *rsol;
+    const uint8_t *rthr;
     uint64_t nb, nw, tmask;
     uint32_t lower, upper, leaf;
     int variant;
@@ -102,6 +106,7 @@ struct DReader {
 };
 
 __device__ __forceinline__ uint64_t dretrieve(const DView &v, uint64_t key) {
+    if (v.rlv) return ret_lookup(*v.rlv, v.rsol, v.rthr, key);
     if (key == kEmpty) return __ldg(v.special) & 1u;
     uint64_t s = remix(key) & v.tmask;
     for (uint64_t probe = 0; probe <= v.tmask; probe++) {
@@ -412,6 +417,7 @@ struct shg_dmphf {
     uint64_t n = 0, bits = 0;
     QBuf size_acc, pos_acc, desc, memo, err;
     RTable table;
+    shg_retrieval *compact = nullptr;  // owned; replaces the table when set
     QBuf in_a, in_b, in_bytes, out;  // staging for host-buffer queries
     float last_ms = 0.f;
 };
@@ -461,9 +467,13 @@ struct DeviceGuard {
 
 } // namespace
 
-extern "C" {
+namespace shg {
+shg_status retrieval_build_on(int device, cudaStream_t s, const uint64_t *d_keys, const uint8_t *d_bits, uint64_t n,
+                              shg_retrieval **out);
+const RetLevels *retrieval_device_view(const shg_retrieval *r, const uint64_t **sol, const uint8_t **thr);
+} // namespace shg
 
-shg_status shg_dmphf_create(int device, const shg_params *p, const shg_result *r, shg_dmphf **out) {
+static shg_status dmphf_create(int device, const shg_params *p, const shg_result *r, bool compact, shg_dmphf **out) {
     if (!p || !r || !out) return shg_set_error(SHG_ERR_ARG, "null argument");
     *out = nullptr;
     if (!is_sh1(p->variant) && p->variant != SHG_SHOCKHASH2) return shg_set_error(SHG_ERR_ARG, "unknown variant");
@@ -501,10 +511,20 @@ shg_status shg_dmphf_create(int device, const shg_params *p, const shg_result *r
         cudaMemsetAsync(f->desc.p, 0, (nw + 2) * 8, s) || up(f->desc.p, r->descriptors, nw * 8) ||
         up(f->memo.p, cfg.memo.data(), kMaxBucket * 8))
         return bail(shg_set_error(SHG_ERR_CUDA, "device query: upload failed"));
-    if (cudaError_t e = f->table.build(r->ribbon_keys, r->ribbon_bits, rn, s, f->in_a, f->in_bytes))
+    DView &v = f->v;
+    if (compact) {
+        if (f->in_a.ensure(rn * 8 + 8) || f->in_bytes.ensure(rn + 1))
+            return bail(shg_set_error(SHG_ERR_OOM, "device query: cudaMalloc failed"));
+        if (up(f->in_a.p, r->ribbon_keys, rn * 8) || up(f->in_bytes.p, r->ribbon_bits, rn))
+            return bail(shg_set_error(SHG_ERR_CUDA, "device query: upload failed"));
+        const shg_status st = retrieval_build_on(device, s, (const uint64_t *)f->in_a.p, (const uint8_t *)f->in_bytes.p,
+                                                 rn, &f->compact);
+        if (st != SHG_OK) return bail(st);
+        v.rlv = retrieval_device_view(f->compact, &v.rsol, &v.rthr);
+    } else if (cudaError_t e = f->table.build(r->ribbon_keys, r->ribbon_bits, rn, s, f->in_a, f->in_bytes)) {
         return bail(shg_set_error(e == cudaErrorMemoryAllocation ? SHG_ERR_OOM : SHG_ERR_CUDA,
                                   std::string("device query: retrieval table: ") + cudaGetErrorString(e)));
-    DView &v = f->v;
+    }
     v.size_acc = (const uint64_t *)f->size_acc.p;
     v.pos_acc = (const uint64_t *)f->pos_acc.p;
     v.desc = (const uint64_t *)f->desc.p;
@@ -527,6 +547,22 @@ shg_status shg_dmphf_create(int device, const shg_params *p, const shg_result *r
     return SHG_OK;
 }
 
+extern "C" {
+
+shg_status shg_dmphf_create(int device, const shg_params *p, const shg_result *r, shg_dmphf **out) {
+    return dmphf_create(device, p, r, false, out);
+}
+
+shg_status shg_dmphf_create_compact(int device, const shg_params *p, const shg_result *r, shg_dmphf **out) {
+    return dmphf_create(device, p, r, true, out);
+}
+
+uint64_t shg_dmphf_retrieval_bits(const shg_dmphf *f) {
+    if (!f) return 0;
+    if (f->compact) return shg_retrieval_bits(f->compact);
+    return (f->table.mask + 1) * 65 + 32;  // table keys and bits, and the special slot
+}
+
 void shg_dmphf_destroy(shg_dmphf *f) {
     if (!f) return;
     DeviceGuard guard(f->device);
@@ -534,6 +570,7 @@ void shg_dmphf_destroy(shg_dmphf *f) {
     for (QBuf *b : {&f->size_acc, &f->pos_acc, &f->desc, &f->memo, &f->err, &f->in_a, &f->in_b, &f->in_bytes, &f->out})
         b->release();
     f->table.release();
+    shg_retrieval_destroy(f->compact);
     if (f->ev0) cudaEventDestroy(f->ev0);
     if (f->ev1) cudaEventDestroy(f->ev1);
     if (f->stream) cudaStreamDestroy(f->stream);

@@ -935,6 +935,14 @@ shg_status build_flat(shg_engine *e, uint64_t k, const char *bytes, const uint64
 
 } // namespace
 
+namespace shg {
+// The engine's stream and device, for the other translation units' entry points.
+cudaStream_t engine_stream(shg_engine *e, int *device) {
+    *device = e->device;
+    return e->stream;
+}
+} // namespace shg
+
 extern "C" {
 
 shg_status shg_engine_create(int device, shg_engine **out) {
