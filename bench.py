@@ -303,6 +303,23 @@ def main():
                 torch.equal(torch.sort(d_out).values, torch.arange(n, device=dev, dtype=torch.int64)))
             dq.close()
             del d_out
+            # compact retrieval structure from the build's retrieval input (device-resident input)
+            d_rk = torch.from_numpy(r.ribbon_keys.view(np.int64)).to(dev)
+            d_rb = torch.from_numpy(r.ribbon_bits).to(dev)
+            rt_ms = []
+            for it in range(3):  # one warm-up, then the mean of two
+                rt = shg.Retrieval.build_device(eng, d_rk.data_ptr(), d_rb.data_ptr(), len(r.ribbon_keys))
+                if it:
+                    rt_ms.append(rt.build_ms())
+                if it < 2:
+                    rt.close()
+            d_rout = torch.empty(len(r.ribbon_keys), dtype=torch.uint8, device=dev)
+            rt.query_device(d_rk.data_ptr(), len(r.ribbon_keys), d_rout.data_ptr())
+            forms["retrieval"] = {"keys": len(r.ribbon_keys), "build_ms": round(statistics.mean(rt_ms), 3),
+                                  "bits_per_key": round(rt.bits() / max(1, len(r.ribbon_keys)), 4),
+                                  "levels": rt.levels(), "all_bits_retrieved": bool(torch.equal(d_rout, d_rb))}
+            rt.close()
+            del d_rk, d_rb, d_rout
         d2h = (r.bucket_size_acc.nbytes + r.bucket_pos_acc.nbytes + r.descriptors.nbytes + r.ribbon_keys.nbytes
                + r.ribbon_bits.nbytes)
         line = {

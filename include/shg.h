@@ -120,6 +120,13 @@ shg_status shg_build_batch_u64(shg_engine *e, const shg_params *p, const uint64_
 
 void shg_result_free(shg_result *r);
 
+/* A build result on disk and back (no counterpart in the reference classes, which persist only
+ * the RiceBitVector, RiceBitVector.h:133-141; the descriptors section of the file is in that
+ * stream layout: u64 word count, then the words). A loaded result is freed with shg_result_free
+ * and feeds shg_mphf_create / shg_dmphf_create like a fresh one; `p` receives the configuration. */
+shg_status shg_result_save(const shg_params *p, const shg_result *r, const char *path);
+shg_status shg_result_load(const char *path, shg_params *p, shg_result *out);
+
 /* Shards of one structure (no counterpart in the reference, whose compute_thread splits the same
  * bucket ranges over threads, ShockHash.h:566-570). Bucket b = remap128(first, nb_global) is
  * monotone in `first`, so a key set can be split by bucket range over GPUs or processes:

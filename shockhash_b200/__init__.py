@@ -90,6 +90,8 @@ def lib():
         "shg_build_u64_device": ([_vp, P, _vp, _u64, R], ctypes.c_int),
         "shg_build_strings": ([_vp, P, ctypes.c_char_p, _vp, _u64, R], ctypes.c_int),
         "shg_result_free": ([R], None),
+        "shg_result_save": ([P, R, ctypes.c_char_p], ctypes.c_int),
+        "shg_result_load": ([ctypes.c_char_p, P, R], ctypes.c_int),
         "shg_build_batch_u64": ([_vp, P, _vp, _vp, _u64, _vp], ctypes.c_int),
         "shg_build_shard_hash128": ([_vp, P, _vp, _vp, _u64, _u64, _u64, _u64, R], ctypes.c_int),
         "shg_merge_shards": ([P, _vp, _u64, R], ctypes.c_int),
@@ -208,6 +210,13 @@ def sh2_construct_leaves_noalloc(d_keys, d_leaf_offsets, nleaves, d_seeds, d_bit
                                                    _vp(d_bits), _vp(stream)))
 
 
+def load_result(path):
+    """A build result saved with ``BuildResult.save`` (its configuration in ``.params``)."""
+    p, res = _Params(), _Result()
+    _check(lib().shg_result_load(os.fsencode(path), ctypes.byref(p), ctypes.byref(res)))
+    return BuildResult(p, res, None)
+
+
 def memo_table(variant, leaf_size):
     out = np.zeros(3000, dtype=np.uint64)
     _check(lib().shg_memo_table(variant, leaf_size, _ptr(out)))
@@ -242,6 +251,16 @@ class BuildResult:
         if self._res is not None:
             lib().shg_result_free(ctypes.byref(self._res))
             self._res = None
+
+    def save(self, path):
+        """Write the result to a file (``shg_result_save``); ``load_result`` reads it back."""
+        if self._res is None:
+            raise ShgError(1, "build result already freed")
+        _check(lib().shg_result_save(ctypes.byref(self.params), ctypes.byref(self._res), os.fsencode(path)))
+
+    def mphf(self):
+        """Host query object (``operator()``, ``getBits()``) over this result."""
+        return _Mphf(self.params, self._res)
 
     def __del__(self):
         try:

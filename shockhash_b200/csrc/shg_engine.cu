@@ -1038,6 +1038,98 @@ shg_status shg_build_shard_hash128(shg_engine *e, const shg_params *p, const uin
     return build_batch(e, p, e->first.as<uint64_t>(), e->second.as<uint64_t>(), std::vector<uint64_t>{n}, out, 0.f, &shard);
 }
 
+// On-disk form of a build result (no counterpart in the reference classes, which persist only the
+// RiceBitVector, RiceBitVector.h:133-141). Little-endian: "SHGMPHF1", variant u32, leaf size u32,
+// bucket size u64, n, nbuckets, desc_bits, ribbon_n (u64 each), bucket_size_acc and bucket_pos_acc
+// ([nbuckets + 1] u64 each), the descriptors in RiceBitVector's stream layout (u64 word count, then
+// the words, as sux::util::Vector writes them), ribbon_keys ([ribbon_n] u64), ribbon_bits
+// ([ribbon_n] u8).
+static const char kSaveMagic[8] = {'S', 'H', 'G', 'M', 'P', 'H', 'F', '1'};
+
+shg_status shg_result_save(const shg_params *p, const shg_result *r, const char *path) {
+    if (!p || !r || !path) return fail(SHG_ERR_ARG, "null argument");
+    if (r->nbuckets == 0 || !r->bucket_size_acc || !r->bucket_pos_acc || (r->desc_words && !r->descriptors) ||
+        (r->ribbon_n && (!r->ribbon_keys || !r->ribbon_bits)))
+        return fail(SHG_ERR_ARG, "not a build result");
+    FILE *f = fopen(path, "wb");
+    if (!f) return fail(SHG_ERR_ARG, std::string("cannot open ") + path + " for writing");
+    const uint32_t vl[2] = {(uint32_t)p->variant, (uint32_t)p->leaf_size};
+    const uint64_t head[5] = {p->bucket_size, r->n, r->nbuckets, r->desc_bits, r->ribbon_n};
+    const size_t acc = r->nbuckets + 1;
+    bool ok = fwrite(kSaveMagic, 1, 8, f) == 8 && fwrite(vl, 4, 2, f) == 2 && fwrite(head, 8, 5, f) == 5 &&
+              fwrite(r->bucket_size_acc, 8, acc, f) == acc && fwrite(r->bucket_pos_acc, 8, acc, f) == acc &&
+              fwrite(&r->desc_words, 8, 1, f) == 1 &&
+              fwrite(r->descriptors, 8, r->desc_words, f) == r->desc_words &&
+              fwrite(r->ribbon_keys, 8, r->ribbon_n, f) == r->ribbon_n &&
+              fwrite(r->ribbon_bits, 1, r->ribbon_n, f) == r->ribbon_n;
+    ok = (fclose(f) == 0) && ok;
+    return ok ? SHG_OK : fail(SHG_ERR_ARG, std::string("write to ") + path + " failed");
+}
+
+shg_status shg_result_load(const char *path, shg_params *p, shg_result *out) {
+    if (!path || !p || !out) return fail(SHG_ERR_ARG, "null argument");
+    memset(out, 0, sizeof(shg_result));
+    FILE *f = fopen(path, "rb");
+    if (!f) return fail(SHG_ERR_ARG, std::string("cannot open ") + path);
+    auto bad = [&](const char *why) {
+        fclose(f);
+        return fail(SHG_ERR_ARG, std::string(path) + ": " + why);
+    };
+    char magic[8];
+    uint32_t vl[2];
+    uint64_t head[5], words = 0;
+    if (fread(magic, 1, 8, f) != 8 || memcmp(magic, kSaveMagic, 8) != 0) return bad("not a saved build result");
+    if (fread(vl, 4, 2, f) != 2 || fread(head, 8, 5, f) != 5) return bad("truncated header");
+    const uint64_t n = head[1], nb = head[2], bits = head[3], rn = head[4];
+    if (fseek(f, 0, SEEK_END) != 0) return bad("seek failed");
+    const uint64_t fsize = (uint64_t)ftell(f);
+    const uint64_t fixed = 8 + 8 + 40;
+    if (nb == 0 || nb > fsize / 16 || rn > n || bits < 1) return bad("inconsistent sizes");
+    if (fseek(f, (long)(fixed + 16 * (nb + 1)), SEEK_SET) != 0 || fread(&words, 8, 1, f) != 1) return bad("truncated");
+    if (words != ((bits + 7) / 8 + 14) / 8) return bad("descriptor word count does not match its bit count");
+    if (fsize != fixed + 16 * (nb + 1) + 8 + 8 * words + 9 * rn) return bad("file size does not match its header");
+    const size_t acc_bytes = (nb + 1) * 8;
+    const size_t bytes = 2 * acc_bytes + words * 8 + rn * 9 + 64;
+    auto *blk = new PinnedBlock();
+    blk->host = true;
+    blk->in_use = true;
+    blk->refs = 1;
+    blk->p = calloc(1, bytes);
+    blk->cap = bytes;
+    if (!blk->p) {
+        delete blk;
+        return bad("host allocation failed");
+    }
+    uint8_t *hp = (uint8_t *)blk->p;
+    out->owner = blk;
+    out->n = n;
+    out->nbuckets = nb;
+    out->bucket_size_acc = (uint64_t *)hp;
+    out->bucket_pos_acc = (uint64_t *)(hp + acc_bytes);
+    out->descriptors = (uint64_t *)(hp + 2 * acc_bytes);
+    out->ribbon_keys = (uint64_t *)(hp + 2 * acc_bytes + words * 8);
+    out->ribbon_bits = hp + 2 * acc_bytes + words * 8 + rn * 8;
+    out->desc_words = words;
+    out->desc_bits = bits;
+    out->ribbon_n = rn;
+    fseek(f, (long)fixed, SEEK_SET);
+    const bool ok = fread(out->bucket_size_acc, 8, nb + 1, f) == nb + 1 && fread(out->bucket_pos_acc, 8, nb + 1, f) == nb + 1 &&
+                    fseek(f, 8, SEEK_CUR) == 0 && fread(out->descriptors, 8, words, f) == words &&
+                    fread(out->ribbon_keys, 8, rn, f) == rn && fread(out->ribbon_bits, 1, rn, f) == rn;
+    fclose(f);
+    if (!ok || out->bucket_size_acc[nb] != n) {
+        release_pinned(blk);
+        memset(out, 0, sizeof(shg_result));
+        return fail(SHG_ERR_ARG, std::string(path) + ": truncated or inconsistent arrays");
+    }
+    p->variant = (int)vl[0];
+    p->leaf_size = (int)vl[1];
+    p->bucket_size = head[0];
+    p->mode = SHG_MODE_DEFAULT;
+    p->max_trials = 0;
+    return SHG_OK;
+}
+
 shg_status shg_merge_shards(const shg_params *p, const shg_result *shards, uint64_t nshards, shg_result *out) {
     if (!p || !shards || !out || nshards == 0) return fail(SHG_ERR_ARG, "null argument or no shards");
     memset(out, 0, sizeof(shg_result));

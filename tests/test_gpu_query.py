@@ -88,3 +88,13 @@ def test_device_flat_query_at_scale(engine):
     assert np.array_equal(np.sort(q), np.arange(n, dtype=np.uint64))
     idx = rng.choice(n, 5000, replace=False)
     assert np.array_equal(r.query_strings([keys[i] for i in idx]), q[idx])
+
+
+def test_saved_result_queries_on_device(engine, tmp_path):
+    keys = unique_u64(np.random.default_rng(90), 200_000)
+    r = engine.build_u64(2, 64, keys, 2000)
+    path = str(tmp_path / "build.shg")
+    r.save(path)
+    back = shg.load_result(path)
+    assert np.array_equal(shg.DeviceMphf(back).query_u64(keys), shg.DeviceMphf(r).query_u64(keys))
+    assert np.array_equal(back.descriptors, r.descriptors)
