@@ -124,7 +124,7 @@ struct shg_engine {
         DevBuf cnt, nodes, node_off, singles, single_off, skip_bits;
     };
     std::vector<Shapes *> shapes;
-    DevBuf plan_offs;
+    DevBuf plan_offs, ret_scratch;
     cudaEvent_t ev[8] = {};
     cudaStream_t stream2 = nullptr;  // leaves of the pipelined mode
     static constexpr int kMaxChunks = 64;
@@ -140,6 +140,7 @@ struct shg_engine {
                          &f_slot, &f_leaf_keys, &f_nodes, &f_ids, &f_codes, &f_bits, &f_mapping, &f_lb, &f_tmp, &f_tmp2};
         for (DevBuf *b : all) b->release();
         plan_offs.release();
+        ret_scratch.release();
         for (Shapes *sh : shapes) {
             DevBuf *sb[] = {&sh->cnt, &sh->nodes, &sh->node_off, &sh->singles, &sh->single_off, &sh->skip_bits};
             for (DevBuf *b : sb) b->release();
@@ -940,6 +941,13 @@ namespace shg {
 cudaStream_t engine_stream(shg_engine *e, int *device) {
     *device = e->device;
     return e->stream;
+}
+// Reusable device buffers of the engine for the retrieval build: slot 0 its scratch region, 1 and 2
+// the staging of host keys and bits (the input buffers of the other builds).
+void *engine_scratch(shg_engine *e, int slot, size_t bytes, cudaError_t &err) {
+    DevBuf &b = slot == 0 ? e->ret_scratch : slot == 1 ? e->in_keys : e->in_bytes;
+    err = b.ensure(bytes);
+    return err == cudaSuccess ? b.p : nullptr;
 }
 } // namespace shg
 

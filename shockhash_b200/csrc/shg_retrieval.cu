@@ -258,6 +258,10 @@ struct shg_retrieval {
     }
 };
 
+namespace shg {
+void *engine_scratch(shg_engine *e, int slot, size_t bytes, cudaError_t &err);
+}
+
 namespace {
 
 #define RCU(call)                                                                                  \
@@ -286,8 +290,10 @@ done:
 }
 
 // The build from keys and bits already in device memory; stream-ordered on `s`, then synchronous.
-shg_status ret_build(int device, cudaStream_t s, const uint64_t *d_keys, const uint8_t *d_bits, uint64_t n,
-                     shg_retrieval **out) {
+// Scratch is one region, carved: the engine's reusable buffer when `e` is given, else a region
+// allocated for this call.
+shg_status ret_build(shg_engine *e, int device, cudaStream_t s, const uint64_t *d_keys, const uint8_t *d_bits,
+                     uint64_t n, shg_retrieval **out) {
     shg_status st = SHG_OK;
     shg_retrieval *r = new shg_retrieval();
     r->device = device;
@@ -297,29 +303,49 @@ shg_status ret_build(int device, cudaStream_t s, const uint64_t *d_keys, const u
     uint32_t *counts = nullptr, *cursor = nullptr, *misc = nullptr;
     unsigned long long *next = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
-    const uint64_t cap_b = n / kRetLoad + 2;
+    void *own = nullptr;  // the region when no engine provides one
+    const uint64_t cap_b = n / kRetLoad + 2, nn = std::max<uint64_t>(n, 1);
+    const uint64_t *in_keys = d_keys;  // level 0 reads the input; later levels the bumped keys
+    const uint8_t *in_bits = d_bits;
     uint64_t cur_n = n;
     int level = 0;
+    {
+        size_t off = 0;
+        auto take = [&](size_t bytes) {
+            const size_t at = off;
+            off += (bytes + 255) & ~(size_t)255;
+            return at;
+        };
+        const size_t o_ka = take(nn * 8), o_kb = take(nn * 8), o_bk = take(nn * 8), o_ba = take(nn), o_bb = take(nn),
+                     o_bbit = take(nn), o_acc = take((cap_b + 1) * 8), o_cnt = take(cap_b * 4),
+                     o_cur = take(cap_b * 4), o_sol = take(cap_b * kRetWords * 8), o_thr = take(cap_b),
+                     o_misc = take(16), o_next = take(8);
+        uint8_t *base = nullptr;
+        if (e) {
+            cudaError_t err = cudaSuccess;
+            base = (uint8_t *)engine_scratch(e, 0, off, err);
+            RCU(err);
+        } else {
+            RCU(cudaMalloc(&own, off));
+            base = (uint8_t *)own;
+        }
+        ka = (uint64_t *)(base + o_ka);
+        kb = (uint64_t *)(base + o_kb);
+        bk = (uint64_t *)(base + o_bk);
+        ba = base + o_ba;
+        bb = base + o_bb;
+        bbit = base + o_bbit;
+        acc = (uint64_t *)(base + o_acc);
+        counts = (uint32_t *)(base + o_cnt);
+        cursor = (uint32_t *)(base + o_cur);
+        dsol = (uint64_t *)(base + o_sol);
+        dthr = base + o_thr;
+        misc = (uint32_t *)(base + o_misc);
+        next = (unsigned long long *)(base + o_next);
+    }
     RCU(cudaEventCreate(&e0));
     RCU(cudaEventCreate(&e1));
-    RCU(cudaMalloc(&ka, std::max<uint64_t>(n, 1) * 8));
-    RCU(cudaMalloc(&kb, std::max<uint64_t>(n, 1) * 8));
-    RCU(cudaMalloc(&bk, std::max<uint64_t>(n, 1) * 8));
-    RCU(cudaMalloc(&ba, std::max<uint64_t>(n, 1)));
-    RCU(cudaMalloc(&bb, std::max<uint64_t>(n, 1)));
-    RCU(cudaMalloc(&bbit, std::max<uint64_t>(n, 1)));
-    RCU(cudaMalloc(&acc, (cap_b + 1) * 8));
-    RCU(cudaMalloc(&counts, cap_b * 4));
-    RCU(cudaMalloc(&cursor, cap_b * 4));
-    RCU(cudaMalloc(&dsol, cap_b * kRetWords * 8));
-    RCU(cudaMalloc(&dthr, cap_b));
-    RCU(cudaMalloc(&misc, 16));
-    RCU(cudaMalloc(&next, 8));
     RCU(cudaMemsetAsync(misc, 0, 16, s));
-    if (n) {
-        RCU(cudaMemcpyAsync(ka, d_keys, n * 8, cudaMemcpyDeviceToDevice, s));
-        RCU(cudaMemcpyAsync(ba, d_bits, n, cudaMemcpyDeviceToDevice, s));
-    }
     RCU(cudaEventRecord(e0, s));
     while (cur_n) {
         if (level == kRetMaxLevels) {
@@ -328,23 +354,23 @@ shg_status ret_build(int device, cudaStream_t s, const uint64_t *d_keys, const u
         }
         const uint64_t nb = std::max<uint64_t>(1, (cur_n + kRetLoad - 1) / kRetLoad);
         RCU(cudaMemsetAsync(counts, 0, nb * 4, s));
-        k_ret_count<<<ret_grid(cur_n, 256), 256, 0, s>>>(ka, cur_n, level, nb, counts);
+        k_ret_count<<<ret_grid(cur_n, 256), 256, 0, s>>>(in_keys, cur_n, level, nb, counts);
         launch_scan_counts(counts, nb, acc, cursor, misc + 1, s);
-        k_ret_scatter<<<ret_grid(cur_n, 256), 256, 0, s>>>(ka, ba, cur_n, level, nb, cursor, bk, bbit);
+        k_ret_scatter<<<ret_grid(cur_n, 256), 256, 0, s>>>(in_keys, in_bits, cur_n, level, nb, cursor, bk, bbit);
         RCU(cudaMemsetAsync(next, 0, 8, s));
         {
             const uint64_t blocks = std::min<uint64_t>((nb + kRetWarps - 1) / kRetWarps, 148ull * 16);
-            k_ret_solve<<<(int)blocks, kRetWarps * 32, 0, s>>>(acc, nb, level, bk, bbit, dsol, dthr, kb, bb, next, misc);
+            k_ret_solve<<<(int)blocks, kRetWarps * 32, 0, s>>>(acc, nb, level, bk, bbit, dsol, dthr, ka, ba, next, misc);
         }
         RCU(cudaGetLastError());
-        unsigned long long nn = 0;
+        unsigned long long bumped = 0;
         uint32_t err = 0;
         const size_t off = r->thr.size();
         r->sol.resize(off * kRetWords + nb * kRetWords);
         r->thr.resize(off + nb);
         RCU(cudaMemcpyAsync(r->sol.data() + off * kRetWords, dsol, nb * kRetWords * 8, cudaMemcpyDeviceToHost, s));
         RCU(cudaMemcpyAsync(r->thr.data() + off, dthr, nb, cudaMemcpyDeviceToHost, s));
-        RCU(cudaMemcpyAsync(&nn, next, 8, cudaMemcpyDeviceToHost, s));
+        RCU(cudaMemcpyAsync(&bumped, next, 8, cudaMemcpyDeviceToHost, s));
         RCU(cudaMemcpyAsync(&err, misc, 4, cudaMemcpyDeviceToHost, s));
         RCU(cudaStreamSynchronize(s));
         if (err) {
@@ -354,28 +380,21 @@ shg_status ret_build(int device, cudaStream_t s, const uint64_t *d_keys, const u
         r->lv.buckets[level] = nb;
         r->lv.first[level] = off;
         r->lv.count = ++level;
+        in_keys = ka;  // the bumped keys are the next level's input; the other pair takes its bumps
+        in_bits = ba;
         std::swap(ka, kb);
         std::swap(ba, bb);
-        cur_n = nn;
+        cur_n = bumped;
     }
     RCU(cudaEventRecord(e1, s));
     RCU(cudaEventSynchronize(e1));
     RCU(cudaEventElapsedTime(&r->build_ms, e0, e1));
     st = ret_upload(r);
 done:
-    cudaFree(ka);
-    cudaFree(kb);
-    cudaFree(bk);
-    cudaFree(ba);
-    cudaFree(bb);
-    cudaFree(bbit);
-    cudaFree(acc);
-    cudaFree(counts);
-    cudaFree(cursor);
-    cudaFree(dsol);
-    cudaFree(dthr);
-    cudaFree(misc);
-    cudaFree(next);
+    if (own) {
+        cudaStreamSynchronize(s);
+        cudaFree(own);
+    }
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     if (st != SHG_OK) {
@@ -394,7 +413,7 @@ cudaStream_t engine_stream(shg_engine *e, int *device);
 // For the device query: a build on another object's stream, and the structure's device arrays.
 shg_status retrieval_build_on(int device, cudaStream_t s, const uint64_t *d_keys, const uint8_t *d_bits, uint64_t n,
                               shg_retrieval **out) {
-    return ret_build(device, s, d_keys, d_bits, n, out);
+    return ret_build(nullptr, device, s, d_keys, d_bits, n, out);
 }
 const RetLevels *retrieval_device_view(const shg_retrieval *r, const uint64_t **sol, const uint8_t **thr) {
     *sol = r->d_sol;
@@ -413,16 +432,17 @@ shg_status shg_retrieval_build(shg_engine *e, const uint64_t *keys, const uint8_
     uint64_t *dk = nullptr;
     uint8_t *db = nullptr;
     shg_status st = SHG_OK;
-    RCU(cudaMalloc(&dk, std::max<uint64_t>(n, 1) * 8));
-    RCU(cudaMalloc(&db, std::max<uint64_t>(n, 1)));
+    cudaError_t err = cudaSuccess;
+    dk = (uint64_t *)engine_scratch(e, 1, std::max<uint64_t>(n, 1) * 8, err);
+    RCU(err);
+    db = (uint8_t *)engine_scratch(e, 2, std::max<uint64_t>(n, 1), err);
+    RCU(err);
     if (n) {
         RCU(cudaMemcpyAsync(dk, keys, n * 8, cudaMemcpyHostToDevice, s));
         RCU(cudaMemcpyAsync(db, bits, n, cudaMemcpyHostToDevice, s));
     }
-    st = ret_build(device, s, dk, db, n, out);
+    st = ret_build(e, device, s, dk, db, n, out);
 done:
-    cudaFree(dk);
-    cudaFree(db);
     return st;
 }
 
@@ -432,7 +452,7 @@ shg_status shg_retrieval_build_device(shg_engine *e, const uint64_t *d_keys, con
     int device = 0;
     cudaStream_t s = engine_stream(e, &device);
     if (cudaSetDevice(device) != cudaSuccess) return shg_set_error(SHG_ERR_CUDA, "cudaSetDevice failed");
-    return ret_build(device, s, d_keys, d_bits, n, out);
+    return ret_build(e, device, s, d_keys, d_bits, n, out);
 }
 
 shg_status shg_retrieval_load(const uint64_t *level_buckets, uint32_t levels, const uint64_t *sol, const uint8_t *thr,
