@@ -1,0 +1,133 @@
+"""The build service's host logic without a GPU (shockhash_b200.serve): fake engines stand in for
+the device, so these tests check admission in arrival order, the batch cap, requests larger than
+a batch, per-request delivery of results and errors, shutdown, and the request stream."""
+import threading
+
+import numpy as np
+import pytest
+
+import shockhash_b200.serve as serve
+
+
+class _FakeResult:
+    def __init__(self, keys):
+        self.n = len(keys)
+        self.freed = False
+
+    def free(self):
+        self.freed = True
+
+
+class _FakeEngine:
+    batches = []
+    lock = threading.Lock()
+    gate = None      # when set, builds wait for it (keeps requests queued)
+    entered = None   # set when a build starts
+    fail_on = None   # a key value that makes the batch raise
+
+    def __init__(self, device=0):
+        self.closed = False
+
+    def build_batch_u64(self, variant, leaf, key_arrays, bucket):
+        _FakeEngine.entered.set()
+        if _FakeEngine.gate is not None:
+            _FakeEngine.gate.wait(5)
+        with _FakeEngine.lock:
+            _FakeEngine.batches.append([len(k) for k in key_arrays])
+        if _FakeEngine.fail_on is not None and any((k == _FakeEngine.fail_on).any() for k in key_arrays):
+            raise RuntimeError("device build failed")
+        return [_FakeResult(k) for k in key_arrays]
+
+    def close(self):
+        self.closed = True
+
+
+@pytest.fixture
+def fake(monkeypatch):
+    _FakeEngine.batches = []
+    _FakeEngine.gate = None
+    _FakeEngine.entered = threading.Event()
+    _FakeEngine.fail_on = None
+    monkeypatch.setattr(serve, "Engine", _FakeEngine)
+    monkeypatch.setattr(serve, "device_memory", lambda device=0: (96 * 1000 * 4, 10 ** 12))
+    return _FakeEngine
+
+
+def _keys(n, base=1):
+    return np.arange(base, base + n, dtype=np.uint64)
+
+
+def test_batch_cap_from_memory_share_and_limit(fake):
+    # free 384000 B, half kept, 2 workers: 96000 B each -> 1000 keys of 96 B
+    srv = serve.BuildServer(workers=2, warm=False)
+    assert srv.batch_keys == 1000
+    srv.close()
+    srv = serve.BuildServer(workers=2, warm=False, max_batch_keys=300)
+    assert srv.batch_keys == 300
+    srv.close()
+
+
+def test_warm_up_builds_a_full_batch_per_worker(fake):
+    srv = serve.BuildServer(workers=3, warm=True, max_batch_keys=500)
+    srv.close()
+    assert fake.batches == [[500]] * 3
+
+
+def test_arrival_order_batches_and_results(fake):
+    fake.gate = threading.Event()
+    srv = serve.BuildServer(workers=1, warm=False, max_batch_keys=1000)
+    first = srv.submit(0, _keys(10))          # taken at once; blocks on the gate
+    assert fake.entered.wait(5)
+    sizes = [400, 500, 300, 2500, 100]
+    reqs = [srv.submit(i + 1, _keys(n, 100 * i + 1)) for i, n in enumerate(sizes)]
+    fake.gate.set()
+    for r in [first] + reqs:
+        res = r.wait(5)
+        assert res.n == len(r.keys)
+        assert r.latency is not None and r.latency >= 0
+    srv.close()
+    # queue prefixes in arrival order, each within 1000 keys unless a single request exceeds it
+    assert fake.batches == [[10], [400, 500], [300], [2500], [100]]
+    assert [r.batch_size for r in reqs] == [2, 2, 1, 1, 1]
+
+
+def test_errors_reach_every_request_of_the_batch(fake):
+    fake.gate = threading.Event()
+    fake.fail_on = 7
+    srv = serve.BuildServer(workers=1, warm=False, max_batch_keys=1000)
+    blocker = srv.submit(0, _keys(5, 1000))
+    assert fake.entered.wait(5)
+    bad = srv.submit(1, _keys(10, 1))         # holds key 7
+    good_same_batch = srv.submit(2, _keys(10, 500))
+    fake.gate.set()
+    assert blocker.wait(5).n == 5
+    for r in (bad, good_same_batch):
+        with pytest.raises(RuntimeError):
+            r.wait(5)
+    after = srv.submit(3, _keys(10, 900))     # the service keeps going
+    assert after.wait(5).n == 10
+    srv.close()
+
+
+def test_results_freed_when_not_kept_and_wait_timeout(fake):
+    fake.gate = threading.Event()
+    srv = serve.BuildServer(workers=1, warm=False, max_batch_keys=1000, keep_results=False)
+    r = srv.submit(0, _keys(10))
+    with pytest.raises(TimeoutError):
+        r.wait(0.05)
+    fake.gate.set()
+    assert r.wait(5) is None and r.keys is None
+    srv.close()
+    assert all(e.closed for e in srv._engines)
+
+
+def test_poisson_stream_is_deterministic_and_in_range():
+    a = serve.poisson_stream(500, rate=200.0, seed=31)
+    b = serve.poisson_stream(500, rate=200.0, seed=31)
+    assert a == b
+    arrivals = [t for t, _, _ in a]
+    sizes = [n for _, n, _ in a]
+    assert all(x < y for x, y in zip(arrivals, arrivals[1:]))
+    assert min(sizes) >= 10 ** 3 and max(sizes) <= 10 ** 7
+    assert 1.0 < arrivals[-1] < 5.0  # 500 arrivals at a mean of 200/s
+    assert len({s for _, _, s in a}) == 500
