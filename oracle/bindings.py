@@ -98,6 +98,8 @@ class RefLib(_Lib):
         L.ref_sh2_leaf.argtypes = [_sz, _vp, _vp, _vp]
         L.ref_sh2_leaf_query.restype = ctypes.c_uint64
         L.ref_sh2_leaf_query.argtypes = [_sz, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64]
+        L.ref_cuckoo_construct.restype = ctypes.c_int
+        L.ref_cuckoo_construct.argtypes = [_vp, _sz, ctypes.c_uint64, _vp, _vp]
         L.ref_sh1_leaf.restype = ctypes.c_uint64
         L.ref_sh1_leaf.argtypes = [ctypes.c_int, _vp, _sz, ctypes.c_int, _vp, _vp]
         L.ref_memo.restype = ctypes.c_int
@@ -178,6 +180,15 @@ class RefLib(_Lib):
         rb = np.zeros(m, np.uint8)
         code = self.lib.ref_sh1_leaf(leaf, _ptr(keys), m, level, _ptr(rk), _ptr(rb))
         return int(code), rk, rb
+
+    def cuckoo_construct(self, keys, seed):
+        """The reference's ordered cuckoo insertion under `seed`: (all placed, cell1[], cell2[])."""
+        keys = np.ascontiguousarray(keys, dtype=np.uint64)
+        m = len(keys)
+        c1 = np.zeros(m, np.uint32)
+        c2 = np.zeros(m, np.uint32)
+        ok = self.lib.ref_cuckoo_construct(_ptr(keys), m, seed, _ptr(c1), _ptr(c2))
+        return bool(ok), c1, c2
 
     def spooky128(self, keys):
         data, offs = pack_strings(keys)

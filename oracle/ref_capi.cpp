@@ -421,4 +421,18 @@ uint64_t ref_sh1_leaf(int leaf, const uint64_t *keys, size_t m, int level, uint6
     }
 }
 
+// The reference's ordered cuckoo insertion of m keys under one seed
+// (TinyBinaryCuckooHashTable::construct / insert, TinyBinaryCuckooHashTable.h:80-106,169-198):
+// 1 when every key finds a cell. Its candidate cells (getCandidateCells, :138-149) go to c1, c2.
+int ref_cuckoo_construct(const uint64_t *keys, size_t m, uint64_t seed, uint32_t *c1, uint32_t *c2) {
+    shockhash::TinyBinaryCuckooHashTable table(m);
+    for (size_t i = 0; i < m; i++) {
+        table.prepare(shockhash::HashedKey(keys[i]));
+        const auto cc = shockhash::TinyBinaryCuckooHashTable::getCandidateCells(shockhash::HashedKey(keys[i]), seed, m);
+        c1[i] = cc.cell1;
+        c2[i] = cc.cell2;
+    }
+    return table.construct(seed) ? 1 : 0;
+}
+
 } // extern "C"

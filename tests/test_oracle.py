@@ -130,3 +130,45 @@ def test_ref_rotation_fitting_is_mphf_and_differs_from_plain(ref):
     r = ref.build_hash(3, 24, f, s, 500, 1)
     assert np.array_equal(np.sort(r.query_hash(f, s)), np.arange(6000, dtype=np.uint64))
     assert not np.array_equal(r.desc, ref.build_hash(1, 24, f, s, 500, 1).desc)
+
+
+def _pseudoforest(m, c1, c2):
+    """Union-find with a cycle flag per root: every component has at most as many keys (edges) as
+    cells (vertices)."""
+    parent = list(range(m))
+    cyc = [False] * m
+
+    def root(x):
+        while parent[x] != x:
+            parent[x] = parent[parent[x]]
+            x = parent[x]
+        return x
+
+    for a, b in zip(c1.tolist(), c2.tolist()):
+        ra, rb = root(a), root(b)
+        if ra == rb:
+            if cyc[ra]:
+                return False
+            cyc[ra] = True
+        else:
+            if cyc[ra] and cyc[rb]:
+                return False
+            parent[ra] = rb
+            cyc[rb] = cyc[ra] or cyc[rb]
+    return True
+
+
+def test_ref_cuckoo_insertion_iff_pseudoforest(ref):
+    """The equivalence the leaf kernels rely on: the reference's ordered cuckoo insertion
+    (TinyBinaryCuckooHashTable.h:80-106,169-198) places every key exactly when the cell graph is a
+    pseudoforest, in both directions, on 10^5 random leaves of 2..60 keys and random seeds."""
+    rng = np.random.default_rng(2024)
+    both = {True: 0, False: 0}
+    for _ in range(100_000):
+        m = int(rng.integers(2, 61))
+        keys = rng.integers(0, 2**64, size=m, dtype=np.uint64)
+        seed = int(rng.integers(0, 2**63))
+        placed, c1, c2 = ref.cuckoo_construct(keys, seed)
+        assert placed == _pseudoforest(m, c1, c2), (m, seed)
+        both[placed] += 1
+    assert both[True] > 5_000 and both[False] > 5_000
