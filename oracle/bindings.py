@@ -98,6 +98,8 @@ class RefLib(_Lib):
         L.ref_sh2_leaf.argtypes = [_sz, _vp, _vp, _vp]
         L.ref_sh2_leaf_query.restype = ctypes.c_uint64
         L.ref_sh2_leaf_query.argtypes = [_sz, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64]
+        L.ref_sh2_pair_check.restype = ctypes.c_int
+        L.ref_sh2_pair_check.argtypes = [_sz, _vp, _vp, _vp, _vp]
         L.ref_cuckoo_construct.restype = ctypes.c_int
         L.ref_cuckoo_construct.argtypes = [_vp, _sz, ctypes.c_uint64, _vp, _vp]
         L.ref_sh1_leaf.restype = ctypes.c_uint64
@@ -180,6 +182,16 @@ class RefLib(_Lib):
         rb = np.zeros(m, np.uint8)
         code = self.lib.ref_sh1_leaf(leaf, _ptr(keys), m, level, _ptr(rk), _ptr(rb))
         return int(code), rk, rb
+
+    def sh2_pair_check(self, a, b):
+        """The reference's isolated-vertex filter and union-find on one candidate pair of hash rows:
+        (skipped by the filter, all edges accepted)."""
+        a = np.ascontiguousarray(a, dtype=np.uint8)
+        b = np.ascontiguousarray(b, dtype=np.uint8)
+        sk, fo = ctypes.c_int(0), ctypes.c_int(0)
+        if not self.lib.ref_sh2_pair_check(len(a), _ptr(a), _ptr(b), ctypes.byref(sk), ctypes.byref(fo)):
+            raise ValueError("leaf size not instantiated")
+        return bool(sk.value), bool(fo.value)
 
     def cuckoo_construct(self, keys, seed):
         """The reference's ordered cuckoo insertion under `seed`: (all placed, cell1[], cell2[])."""

@@ -421,6 +421,35 @@ uint64_t ref_sh1_leaf(int leaf, const uint64_t *keys, size_t m, int level, uint6
     }
 }
 
+// Pieces of the bipartite pair test for an L-key leaf (ShockHash2-internal.h:34-44
+// calculateIsolatedVertices; :510-528 the pair loop; CuckooUnionFind.h:19-42): for the hash rows of
+// a new candidate `a` and an earlier one `b` (values below (L + 1) / 2), whether the isolated-vertex
+// filter skips the pair and whether the union-find accepts all L edges (a[i] + L / 2, b[i]).
+} // extern "C"
+template <size_t L> void sh2_pair_check(const uint8_t *a, const uint8_t *b, int *skipped, int *forest) {
+    shockhash::SeedCache<L, true> na, nb;
+    memcpy(na.hashes, a, L);
+    memcpy(nb.hashes, b, L);
+    shockhash::calculateIsolatedVertices<L>(na);
+    shockhash::calculateIsolatedVertices<L>(nb);
+    *skipped = (na.isolatedVertices & nb.isolatedVertices) != 0;
+    shockhash::CuckooUnionFind uf(L);
+    uf.clear();
+    size_t i = 0;
+    for (; i < L; i++)
+        if (!uf.unionIsStillPseudoforest((uint32_t)(a[i] + L / 2), b[i])) break;
+    *forest = i == L;
+}
+extern "C" {
+int ref_sh2_pair_check(size_t L, const uint8_t *a, const uint8_t *b, int *skipped, int *forest) {
+    switch (L) {
+#define X(N) case N: sh2_pair_check<N>(a, b, skipped, forest); return 1;
+        X(10) X(16) X(33) X(64) X(100) X(128)
+#undef X
+        default: return 0;
+    }
+}
+
 // The reference's ordered cuckoo insertion of m keys under one seed
 // (TinyBinaryCuckooHashTable::construct / insert, TinyBinaryCuckooHashTable.h:80-106,169-198):
 // 1 when every key finds a cell. Its candidate cells (getCandidateCells, :138-149) go to c1, c2.

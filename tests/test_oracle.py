@@ -172,3 +172,38 @@ def test_ref_cuckoo_insertion_iff_pseudoforest(ref):
         assert placed == _pseudoforest(m, c1, c2), (m, seed)
         both[placed] += 1
     assert both[True] > 5_000 and both[False] > 5_000
+
+
+def _covering_rows(rng, L, n):
+    """n hash rows of an L-key leaf, each covering all (L + 1) / 2 values, as candidates do."""
+    c = (L + 1) // 2
+    out = rng.integers(0, c, size=(n, L))
+    for r in out:
+        r[:c] = rng.permutation(c)
+        rng.shuffle(r)
+    return out.astype(np.uint8)
+
+
+@pytest.mark.parametrize("L", [10, 16, 33, 64, 100, 128])
+def test_ref_bipartite_pair_filter_and_union_find(ref, L):
+    """The bipartite pair test of the reference (ShockHash2-internal.h:510-528) on random candidate
+    pairs: its CuckooUnionFind accepts exactly the pseudoforests. The isolated-vertex filter
+    (:34-44, :515-517) never skips a pseudoforest for even L; for odd L the two rows share cell
+    L / 2 (rows hash to (L + 1) / 2 values, the new one shifted by L / 2), a key alone in its cell
+    in each row can still lie on a larger component, and the filter skips some pairs that pass.
+    The filter is therefore part of the result, and the device and the restatement apply it
+    exactly as the reference does rather than treating it as a pure speed-up."""
+    rng = np.random.default_rng(7 + L)
+    A, B = _covering_rows(rng, L, 20000), _covering_rows(rng, L, 20000)
+    skipped_forests = forests = 0
+    for a, b in zip(A, B):
+        skipped, forest = ref.sh2_pair_check(a, b)
+        assert forest == _pseudoforest(L, a.astype(np.int64) + L // 2, b.astype(np.int64))
+        forests += forest
+        skipped_forests += skipped and forest
+    if L % 2 == 0:
+        assert skipped_forests == 0
+    else:
+        assert skipped_forests > 0
+    if L <= 64:
+        assert forests > 0
