@@ -132,6 +132,23 @@ def cpu_reference(keys, threads):
     return dt, "port", 1
 
 
+def ref_phase_split(n):
+    """The reference's own -DSTATS phase times for `n` keys of the same stream on one thread
+    (oracle/ref_stats.py in a subprocess, since the STATS build prints to stdout), or None."""
+    helper = os.path.join(os.path.dirname(os.path.abspath(__file__)), "oracle", "ref_stats.py")
+    if not os.path.exists(os.path.join(os.path.dirname(helper), "_ref", "libshref_stats.so")):
+        return None
+    try:
+        out = subprocess.run([sys.executable, helper, "--n", str(n), "--variant", str(VARIANT), "--leaf", str(LEAF),
+                              "--bucket", str(BUCKET), "--seed", str(SEED)],
+                             capture_output=True, text=True, timeout=180)
+        if out.returncode != 0:
+            return None
+        return json.loads(out.stdout.strip().splitlines()[-1])
+    except Exception:
+        return None
+
+
 def run_reference_arm(args):
     ws, rank, local = dist_env()
     if ws > 1 and rank != 0:
@@ -266,6 +283,8 @@ def main():
             dt, kind, cores = cpu_reference(keys[:sample], os.cpu_count() or 1)
             cpu = {"value": round(dt * 1e9 / sample, 3), "unit": "ns/key", "cores": cores, "kind": kind,
                    "sample": f"first {sample} keys of the same stream, constructor only, all host threads"}
+            if kind == "reference":  # the reference's split and leaf phases (its STATS timers, one thread)
+                cpu["phases_1_thread"] = ref_phase_split(int(os.environ.get("SHG_CPU_PHASE_SAMPLE", "200000")))
         forms = {"default_ns_per_key": round(ms * 1e6 / n, 3)}
         if ws == 1 and not args.no_forms:
             for name, mode in (("levels", shg.MODE_LEVELS), ("pipelined", shg.MODE_PIPELINED)):

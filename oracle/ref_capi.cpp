@@ -450,6 +450,19 @@ int ref_sh2_pair_check(size_t L, const uint8_t *a, const uint8_t *b, int *skippe
     }
 }
 
+#ifdef STATS
+// Phase times of the builds since the last call, from the reference's own STATS counters
+// (ShockHash.h:37-44; ShockHash2.h:268-290, 314-388): the leaf searches and the split levels
+// summed, in nanoseconds. The counters are plain globals, so builds measured this way run on one
+// thread. Resets the counters.
+void ref_stats_times(uint64_t *leaves_ns, uint64_t *splits_ns) {
+    *leaves_ns = shockhash::time_bij;
+    uint64_t s = 0;
+    for (int i = 0; i < MAX_LEVEL_TIME; i++) s += shockhash::time_split[i];
+    *splits_ns = s;
+}
+#endif
+
 // The reference's ordered cuckoo insertion of m keys under one seed
 // (TinyBinaryCuckooHashTable::construct / insert, TinyBinaryCuckooHashTable.h:80-106,169-198):
 // 1 when every key finds a cell. Its candidate cells (getCandidateCells, :138-149) go to c1, c2.

@@ -207,3 +207,19 @@ def test_ref_bipartite_pair_filter_and_union_find(ref, L):
         assert skipped_forests > 0
     if L <= 64:
         assert forests > 0
+
+
+def test_ref_stats_phase_times(ref):
+    """The reference's own STATS timers (oracle/ref_stats.py, one thread, a subprocess because the
+    STATS build prints to stdout): leaf-search and split-level totals within the constructor time."""
+    import subprocess
+    import sys
+    helper = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "ref_stats.py")
+    if not os.path.exists(os.path.join(os.path.dirname(helper), "_ref", "libshref_stats.so")):
+        pytest.skip("STATS build of the reference oracle not available")
+    out = subprocess.run([sys.executable, helper, "--n", "20000"], capture_output=True, text=True, timeout=300,
+                         check=True)
+    res = json.loads(out.stdout.strip().splitlines()[-1])
+    assert res["keys"] == 20000 and res["threads"] == 1
+    assert 0 < res["leaves_ms"] and 0 < res["splits_ms"]
+    assert res["leaves_ms"] + res["splits_ms"] <= res["total_ms"] * 1.02
