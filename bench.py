@@ -11,8 +11,16 @@ so shards need no data-path collective (weak scaling); the barrier and the max-o
 device-timed steps use torch.distributed. Rank 0 prints one JSON line.
 
 --impl reference times the reference's own CPU construction (oracle/_ref: the reference headers
-compiled with the restated third-party stand-ins; the C++ restatement oracle/port when that build
-is absent) on a bounded sample of the same key stream, with all host threads.
+compiled with the restated third-party stand-ins) on the same 10M keys, drawn by the oracle's own
+generator, with all host threads; only the constructor call is timed, as the reference's benchmark
+does. That process loads no library of this package.
+
+Besides the headline line the GPU arm reports, on rank 0 at N=1:
+  * cpu_baseline + parity: the reference CPU build of the same keys, its products compared word
+    for word with the device build (descriptors, accumulators, retrieval input);
+  * forms: the level schedule against the pipelined one and the per-leaf-launch form (1M keys),
+    the north-star size (100M keys), a Poisson serving stream, the device query of every key and
+    the device retrieval structure.
 """
 import argparse
 import json
@@ -33,6 +41,10 @@ LEAF, BUCKET, VARIANT = 64, 2000, 2
 SEED = 7
 METRIC = "build ns/key on 1 B200, batched vs per-leaf GPU vs CPU, bit-exact; p99 latency"
 CONFIG_NAME = "ShockHash2<64> b=2000, 10M uint64 keys (mt19937_64 seed 7) hashed to 128-bit"
+MODES = ["default (levels)", "levels", "per_leaf", "pipelined"]
+# DRAM bytes per key of the split stage (all level launches), from one ncu capture of the 1M-key
+# case scaled by keys (the node keys are read once per level and written back once)
+SPLIT_DRAM_BYTES_PER_KEY = None
 
 
 def _workload(args):
@@ -43,6 +55,16 @@ def _workload(args):
     name = "ShockHash2" if VARIANT == 2 else "ShockHash"
     CONFIG_NAME = (f"{name}<{LEAF}> b={BUCKET}, {args.n / 1e6:g}M uint64 keys (mt19937_64 seed {SEED}) "
                    "hashed to 128-bit")
+
+
+def config_dict(args):
+    """The workload, identical in both arms' JSON lines."""
+    return {"workload": CONFIG_NAME, "keys_per_gpu": args.n, "leaf_size": LEAF, "bucket_size": BUCKET,
+            "variant": "ShockHash2" if VARIANT == 2 else "ShockHash", "mode": MODES[args.mode],
+            "key_encoding": "each uint64 key hashed as its 8-byte little-endian string (SpookyV2-128, seed 0)",
+            "l2": "inputs (10M keys: 80 MB keys, 160 MB fingerprints, 240 MB partition buffers) exceed the 126 MB L2, "
+                  "and a 256 MB buffer is written before every timed step, outside the timing",
+            "parallelism": f"{args.gpus} independent bucket shards, no data-path collective"}
 
 
 class _Summary:
@@ -101,42 +123,43 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-def cpu_reference(keys, threads):
-    """Time the reference CPU construction (oracle/_ref, else oracle/port) on `keys`."""
-    from oracle.bindings import PortLib, RefLib, ref_available
-    import shockhash_b200 as shg
-    eng = None
-    # 128-bit fingerprints as the reference computes them (spooky over the 8-byte strings)
-    from oracle import bindings
-    data = keys.astype("<u8").tobytes()
+def u64_as_strings(keys):
+    """uint64 keys as the reference's string keys: 8 little-endian bytes each, packed with offsets."""
+    data = np.ascontiguousarray(keys, dtype="<u8").tobytes()
     offs = np.arange(0, 8 * (len(keys) + 1), 8, dtype=np.uint64)
-    first = np.zeros(len(keys), np.uint64)
-    second = np.zeros(len(keys), np.uint64)
-    if ref_available():
-        lib = RefLib()
-        import ctypes
-        lib.lib.ref_spooky128.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p,
-                                          ctypes.c_void_p]
-        lib.lib.ref_spooky128(data, bindings._ptr(offs), len(keys), bindings._ptr(first), bindings._ptr(second))
-        t = time.perf_counter()
-        b = lib.build_hash(VARIANT, LEAF, first, second, BUCKET, threads)
-        dt = time.perf_counter() - t
-        b.free()
-        return dt, "reference", threads
-    lib = PortLib()
-    first, second = lib.spooky128([keys[i:i + 1].tobytes() for i in range(len(keys))])
+    return data, offs
+
+
+def cpu_reference(keys, threads, keep=False):
+    """The reference CPU construction of `keys` (uint64, given to the reference's string constructor
+    as 8-byte strings): (constructor seconds, kind, threads used, products or None). Uses
+    oracle/_ref; the C++ restatement oracle/_port (one thread) when that build is absent."""
+    from oracle import bindings
+    if bindings.ref_available():
+        data, offs = u64_as_strings(keys)
+        b, secs = bindings.RefLib().build_strings_packed_timed(VARIANT, LEAF, data, offs, BUCKET, threads)
+        if not keep:
+            b.free()
+            b = None
+        return secs, "reference", threads, b
+    lib = bindings.PortLib()
+    data, offs = u64_as_strings(keys)
+    first, second = lib.spooky128(bindings.split_strings(data, offs))
     t = time.perf_counter()
     b = lib.build_hash(VARIANT, LEAF, first, second, BUCKET)
     dt = time.perf_counter() - t
-    b.free()
-    return dt, "port", 1
+    if not keep:
+        b.free()
+        b = None
+    return dt, "port", 1, b
 
 
 def ref_phase_split(n):
     """The reference's own -DSTATS phase times for `n` keys of the same stream on one thread
     (oracle/ref_stats.py in a subprocess, since the STATS build prints to stdout), or None."""
-    helper = os.path.join(os.path.dirname(os.path.abspath(__file__)), "oracle", "ref_stats.py")
-    if not os.path.exists(os.path.join(os.path.dirname(helper), "_ref", "libshref_stats.so")):
+    from oracle import bindings
+    helper = os.path.join(ROOT, "oracle", "ref_stats.py")
+    if not os.path.exists(bindings.STATS_SO):
         return None
     try:
         out = subprocess.run([sys.executable, helper, "--n", str(n), "--variant", str(VARIANT), "--leaf", str(LEAF),
@@ -150,29 +173,93 @@ def ref_phase_split(n):
 
 
 def run_reference_arm(args):
+    """The reference's CPU construction on the same keys and config as the GPU arm (rank 0 only)."""
     ws, rank, local = dist_env()
     if ws > 1 and rank != 0:
         return
-    import shockhash_b200 as shg
+    from oracle import bindings
     threads = os.cpu_count() or 1
-    sample = int(os.environ.get("SHG_REF_SAMPLE", "1000000"))
-    keys = shg.keys_mt19937_64(SEED, sample)
+    n = args.n
+    if not bindings.ref_available():  # the one-thread restatement: a bounded sample of the stream
+        n = min(n, int(os.environ.get("SHG_PORT_SAMPLE", "200000")))
+    keys = bindings.keys_mt19937_64(SEED, n)
     for _ in range(args.warmup):
         cpu_reference(keys, threads)
-    times, kind = [], None
+    times, kind, used = [], None, threads
     for _ in range(args.steps):
-        dt, kind, used = cpu_reference(keys, threads)
+        dt, kind, used, _ = cpu_reference(keys, threads)
         times.append(dt)
     ms = 1e3 * statistics.mean(times)
-    v = ms * 1e6 / sample
+    v = ms * 1e6 / n
+    sample = (f"all {n} keys of the mt19937_64 seed-{SEED} stream (oracle generator), reference string "
+              "constructor, constructor call only" if n == args.n else
+              f"first {n} keys of the mt19937_64 seed-{SEED} stream (bounded sample for the one-thread port)")
     line = {"impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "ns/key", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": {"workload": CONFIG_NAME, "sample_keys": sample, "threads": used},
-            "cpu_baseline": {"value": round(v, 3), "unit": "ns/key", "cores": used, "kind": kind,
-                             "sample": f"{sample} keys of the same mt19937_64 seed-7 stream, constructor only"},
+            "config": config_dict(args),
+            "cpu_baseline": {"value": round(v, 3), "unit": "ns/key", "cores": used, "kind": kind, "sample": sample,
+                             "build": bindings.ref_build_info()},
             "e2e": {"value": round(v, 3), "unit": "ns/key", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def compare_products(r, b):
+    """Word-for-word comparison of a device build with the reference's products."""
+    checks = {
+        "descriptors": np.array_equal(r.descriptors, b.desc),
+        "bucket_size_acc": np.array_equal(r.bucket_size_acc, b.size_acc),
+        "bucket_pos_acc": np.array_equal(r.bucket_pos_acc, b.pos_acc),
+        "ribbon_keys": np.array_equal(r.ribbon_keys, b.ribbon_keys),
+        "ribbon_bits": np.array_equal(r.ribbon_bits, b.ribbon_bits),
+    }
+    return {"bit_exact": all(checks.values()), "compared": sorted(checks), "mismatch": sorted(k for k, v in checks.items() if not v),
+            "descriptor_words": int(len(b.desc)), "retrieval_keys": int(len(b.ribbon_keys))}
+
+
+def leaf_report(last, leaf_ms, leaf_peak, lpeaks, extra):
+    """The leaf stage against its roofline. Original leaves: hash evaluations at the coverage loop's
+    measured peak. Bipartite leaves: the stage's four operation kinds (hash evaluations, candidate-scan
+    mask pairs, pair filters, pseudoforest edges) at their loops' measured peaks, summed into the
+    time the stage's work takes with every lane busy; frac = that time / the measured stage time."""
+    import shockhash_b200 as shg
+    out = {"ms": round(leaf_ms, 3), "leaf_evals": last.work["leaf_evals"], "pairs": last.work["pairs"],
+           "uf_edges": last.work["uf_edges"]}
+    if lpeaks is None:
+        rate = last.work["leaf_evals"] / (leaf_ms * 1e-3)
+        out.update({"evals_per_s_g": round(rate / 1e9, 3), "peak_g": round(leaf_peak / 1e9, 3),
+                    "frac": round(rate / leaf_peak, 4),
+                    "note": "hash evaluations of the original leaf search per second vs the measured peak of its "
+                            "coverage loop"})
+        return out
+    counts = {"hash_evals": last.work["leaf_evals"], "scan_tests": extra["leaf_scan_tests"],
+              "pair_tests": last.work["pairs"], "uf_edges": last.work["uf_edges"]}
+    ceil_s = shg.leaf_ceiling_s(counts, lpeaks)
+    out.update({"counts": counts, "peaks_g_per_s": {k: round(v / 1e9, 3) for k, v in lpeaks.items()},
+                "ceiling_ms": round(ceil_s * 1e3, 3),
+                "ceiling_ms_by_op": {k: round(counts[k] / lpeaks[k] * 1e3, 3) for k in shg.LEAF_OPS},
+                "frac": round(ceil_s * 1e3 / leaf_ms, 4),
+                "note": "work model of the bipartite leaf search: each operation kind's count (as the sequential "
+                        "reference performs them up to its answer, plus the candidates' cell rows) at the measured "
+                        "peak of that loop run alone with every lane busy; frac = ceiling time / stage time"})
+    return out
+
+
+def timed_device_builds(eng, d_ptr, n, mode, flush, reps, warm=1):
+    """Device-resident builds: `warm` untimed, then `reps` with the L2 flushed before each; returns
+    (mean device ms, stage means, last result summary)."""
+    import torch
+    res = []
+    for it in range(warm + reps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        rm = eng.build_u64_device(VARIANT, LEAF, d_ptr, n, BUCKET, mode)
+        if it >= warm:
+            res.append(_Summary(rm))
+        rm.free()
+    import shockhash_b200 as shg
+    stages = {k: round(statistics.mean(x.stage_ms[k] for x in res), 3) for k in shg.STAGES}
+    return statistics.mean(x.stage_ms["total"] for x in res), stages, res[-1]
 
 
 def main():
@@ -186,8 +273,12 @@ def main():
     ap.add_argument("--variant", type=int, default=VARIANT, choices=[1, 2])
     ap.add_argument("--leaf", type=int, default=LEAF)
     ap.add_argument("--seed", type=int, default=SEED)
-    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--no-forms", action="store_true", help="skip the per-leaf-launch comparison form")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and parity leg")
+    ap.add_argument("--no-forms", action="store_true", help="skip the comparison forms")
+    ap.add_argument("--target-n", type=int, default=int(os.environ.get("SHG_TARGET_N", "100000000")),
+                    help="keys of the north-star size leg (0 skips it)")
+    ap.add_argument("--serve-requests", type=int, default=int(os.environ.get("SHG_SERVE_REQUESTS", "400")),
+                    help="requests of the serving leg (0 skips it)")
     args = ap.parse_args()
     _workload(args)
     if args.impl == "reference":
@@ -209,8 +300,9 @@ def main():
     d_keys = torch.from_numpy(keys.view(np.int64)).to(dev)
     h_keys = torch.from_numpy(keys.view(np.int64)).pin_memory()
     eng = shg.Engine(local)
-    peak_evals, _ = shg.int_peak(local, 1 << 15)
+    peaks = shg.split_peaks(local)
     leaf_peak, _ = shg.int_peak(local, 1 << 15, 1 if VARIANT == 1 else 2)
+    lpeaks = shg.leaf_peaks(local) if VARIANT == 2 else None
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
 
     def barrier():
@@ -222,7 +314,7 @@ def main():
         return eng.build_u64_device(VARIANT, LEAF, d_keys.data_ptr(), n, BUCKET, args.mode)
 
     for _ in range(args.warmup):
-        step_device()
+        step_device().free()
     # ---- device-resident timed steps (value)
     results, step_ms = [], []
     r = None
@@ -238,7 +330,8 @@ def main():
             step_ms.append(1e3 * (time.perf_counter() - t0))
             results.append(_Summary(r))
         barrier()
-    dev_ms = [r.stage_ms["total"] for r in results]
+    split_kinds = eng.last_work()
+    dev_ms = [x.stage_ms["total"] for x in results]
     # ---- end to end through the public API, host (pinned) input, host outputs (e2e)
     e2e_ms = []
     r2 = None
@@ -256,6 +349,7 @@ def main():
         r2 = eng.build_u64(VARIANT, LEAF, h_keys.numpy().view(np.uint64), BUCKET, args.mode)
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
     barrier()
+    r2.free()
 
     def maxed(x):
         if ws == 1:
@@ -273,38 +367,49 @@ def main():
     leaf_ms = statistics.mean(x.stage_ms["leaves"] for x in results)
     last = results[-1]
     achieved = last.work["split_evals"] / (split_ms * 1e-3)
+    # denominator: each node kind's useful evaluations at that kind's measured loop peak
+    peak_eff = shg.weighted_split_peak(split_kinds, peaks)
     bits_per_key = (r.descriptors.size * 64) / n
 
     line = None
     if rank == 0:
-        cpu = None
+        cpu, parity = None, None
         if ws == 1 and not args.no_cpu:
-            sample = int(os.environ.get("SHG_CPU_SAMPLE", "2000000"))
-            dt, kind, cores = cpu_reference(keys[:sample], os.cpu_count() or 1)
-            cpu = {"value": round(dt * 1e9 / sample, 3), "unit": "ns/key", "cores": cores, "kind": kind,
-                   "sample": f"first {sample} keys of the same stream, constructor only, all host threads"}
+            cpu_n = min(n, int(os.environ.get("SHG_CPU_SAMPLE", str(n))))
+            dt, kind, cores, b = cpu_reference(keys[:cpu_n], os.cpu_count() or 1, keep=True)
+            from oracle import bindings
+            cpu = {"value": round(dt * 1e9 / cpu_n, 3), "unit": "ns/key", "cores": cores, "kind": kind,
+                   "sample": (f"all {cpu_n} keys of the step's workload" if cpu_n == n else f"first {cpu_n} keys") +
+                             ", reference string constructor, constructor call only, all host threads",
+                   "build": bindings.ref_build_info()}
             if kind == "reference":  # the reference's split and leaf phases (its STATS timers, one thread)
                 cpu["phases_1_thread"] = ref_phase_split(int(os.environ.get("SHG_CPU_PHASE_SAMPLE", "200000")))
+            if cpu_n == n:
+                parity = {"keys": n, "against": kind, **compare_products(r, b)}
+            else:  # compare a device build of the same sample
+                rs = eng.build_u64_device(VARIANT, LEAF, d_keys.data_ptr(), cpu_n, BUCKET, args.mode)
+                parity = {"keys": cpu_n, "against": kind, **compare_products(rs, b)}
+                rs.free()
+            b.free()
         forms = {"default_ns_per_key": round(ms * 1e6 / n, 3)}
         if ws == 1 and not args.no_forms:
             for name, mode in (("levels", shg.MODE_LEVELS), ("pipelined", shg.MODE_PIPELINED)):
-                t = []
-                for it in range(4):  # one warm-up, then the mean of three
-                    flush.zero_()
-                    torch.cuda.synchronize()
-                    rm = eng.build_u64_device(VARIANT, LEAF, d_keys.data_ptr(), n, BUCKET, mode)
-                    if it:
-                        t.append(rm.stage_ms["total"])
-                    rm.free()
-                forms[f"{name}_device_ns_per_key"] = round(statistics.mean(t) * 1e6 / n, 3)
-        if ws == 1 and not args.no_forms:
-            pl_n = int(os.environ.get("SHG_PER_LEAF_SAMPLE", "100000"))
-            for _ in range(2):  # the second of each is reported (the first grows buffers for the size)
-                rp = eng.build_u64_device(VARIANT, LEAF, d_keys.data_ptr(), pl_n, BUCKET, shg.MODE_PER_LEAF)
-                rl = eng.build_u64_device(VARIANT, LEAF, d_keys.data_ptr(), pl_n, BUCKET, shg.MODE_LEVELS)
-            forms["per_leaf_launch_ns_per_key_at_%d" % pl_n] = round(rp.stage_ms["total"] * 1e6 / pl_n, 3)
-            forms["batched_ns_per_key_at_%d" % pl_n] = round(rl.stage_ms["total"] * 1e6 / pl_n, 3)
-            forms["per_leaf_bit_exact_vs_batched"] = bool(np.array_equal(rp.descriptors, rl.descriptors))
+                t, _, _ = timed_device_builds(eng, d_keys.data_ptr(), n, mode, flush, reps=3)
+                forms[f"{name}_device_ns_per_key"] = round(t * 1e6 / n, 3)
+            # the per-leaf-launch comparison form on the first 1M keys of the same stream
+            pl_n = min(n, int(os.environ.get("SHG_PER_LEAF_SAMPLE", "1000000")))
+            t_pl, st_pl, _ = timed_device_builds(eng, d_keys.data_ptr(), pl_n, shg.MODE_PER_LEAF, flush, reps=1)
+            t_b, st_b, _ = timed_device_builds(eng, d_keys.data_ptr(), pl_n, shg.MODE_LEVELS, flush, reps=3)
+            rp = eng.build_u64_device(VARIANT, LEAF, d_keys.data_ptr(), pl_n, BUCKET, shg.MODE_PER_LEAF)
+            rl = eng.build_u64_device(VARIANT, LEAF, d_keys.data_ptr(), pl_n, BUCKET, shg.MODE_LEVELS)
+            forms["per_leaf"] = {"keys": pl_n, "per_leaf_launch_ns_per_key": round(t_pl * 1e6 / pl_n, 3),
+                                 "batched_ns_per_key": round(t_b * 1e6 / pl_n, 3),
+                                 "batched_speedup": round(t_pl / t_b, 2),
+                                 "per_leaf_leaves_ms": st_pl["leaves"], "batched_leaves_ms": st_b["leaves"],
+                                 "bit_exact_vs_batched": bool(np.array_equal(rp.descriptors, rl.descriptors)
+                                                              and np.array_equal(rp.ribbon_bits, rl.ribbon_bits))}
+            rp.free()
+            rl.free()
         if ws == 1 and not args.no_forms:
             # operator() for every key of the build on the device (keys resident, SpookyV2 fused)
             dq = shg.DeviceMphf(r, local)
@@ -341,37 +446,57 @@ def main():
             del d_rk, d_rb, d_rout
         d2h = (r.bucket_size_acc.nbytes + r.bucket_pos_acc.nbytes + r.descriptors.nbytes + r.ribbon_keys.nbytes
                + r.ribbon_bits.nbytes)
+        if ws == 1 and not args.no_forms and args.target_n:
+            # the north-star size: the first 100M keys of the same stream, device-resident
+            tn = args.target_n
+            t_keys = shg.keys_mt19937_64(SEED, tn)
+            d_t = torch.from_numpy(t_keys.view(np.int64)).to(dev)
+            del t_keys
+            t, st, lw = timed_device_builds(eng, d_t.data_ptr(), tn, args.mode, flush, reps=2)
+            sk = eng.last_work()
+            tgt = {"keys": tn, "device_ns_per_key": round(t * 1e6 / tn, 3), "stage_ms": st,
+                   "split_frac": round(lw.work["split_evals"] / (st["splits"] * 1e-3) / shg.weighted_split_peak(sk, peaks), 4)}
+            if cpu:
+                tgt["vs_cpu_reference"] = round(cpu["value"] / (t * 1e6 / tn), 1)
+            if "per_leaf" in forms:
+                tgt["vs_per_leaf_launch_form"] = round(forms["per_leaf"]["per_leaf_launch_ns_per_key"] / (t * 1e6 / tn), 1)
+            forms["target"] = tgt
+            del d_t
+            torch.cuda.empty_cache()
+        if ws == 1 and not args.no_forms and args.serve_requests:
+            from shockhash_b200 import serve
+            eng.close()  # the serving leg's workers hold their own engines
+            eng = None
+            torch.cuda.empty_cache()
+            forms["serving"] = serve.run_stream(serve.poisson_stream(args.serve_requests, 200.0, 31), workers=2)
         line = {
             "metric": METRIC, "value": round(ms * 1e6 / total_keys, 3), "unit": "ns/key", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": {"workload": CONFIG_NAME, "keys_per_gpu": n, "leaf_size": LEAF, "bucket_size": BUCKET,
-                       "variant": "ShockHash2" if VARIANT == 2 else "ShockHash", "mode": ["default (levels)", "levels", "per_leaf", "pipelined"][args.mode],
-                       "l2": "flushed (256 MB write) before every timed step, outside the timing",
-                       "parallelism": f"{ws} independent bucket shards, no data-path collective"},
+            "config": config_dict(args),
             "device_ms_per_step": round(ms_dev, 3),
             "stage_ms": {k: round(statistics.mean(x.stage_ms[k] for x in results), 3) for k in shg.STAGES},
             "e2e": {"value": round(ms_e2e * 1e6 / total_keys, 3), "unit": "ns/key", "p99_ms": round(p99, 3),
                     "h2d_bytes_per_step": int(n * 8), "d2h_bytes_per_step": int(d2h)},
             "roofline": {"kernel": "k_split (RecSplit split-seed search)", "bound": "int",
-                         "achieved": round(achieved / 1e9, 3), "peak": round(peak_evals / 1e9, 3),
-                         "unit": "Gevals/s", "frac": round(achieved / peak_evals, 4), "traffic": None,
-                         "note": "useful split evaluations (the reference's sequential count) / device time of "
-                                 "the split stage; peak = measured integer microbenchmark of the same "
-                                 "arithmetic (no memory traffic)"},
-            "leaf_stage": {"ms": round(leaf_ms, 3), "leaf_evals": last.work["leaf_evals"],
-                           "evals_per_s_g": round(last.work["leaf_evals"] / (leaf_ms * 1e-3) / 1e9, 3),
-                           "peak_g": round(leaf_peak / 1e9, 3),
-                           "frac": round(last.work["leaf_evals"] / (leaf_ms * 1e-3) / leaf_peak, 4),
-                           "note": "hash evaluations of the leaf search per second vs the measured peak of its "
-                                   "inner loop (original leaves: coverage loop; bipartite leaves: raw-seed loop, "
-                                   "which leaves out the candidate scans and pseudoforest tests)",
-                           "pairs": last.work["pairs"], "uf_edges": last.work["uf_edges"]},
+                         "achieved": round(achieved / 1e9, 3), "peak": round(peak_eff / 1e9, 3),
+                         "unit": "Gevals/s", "frac": round(achieved / peak_eff, 4),
+                         "traffic": (None if SPLIT_DRAM_BYTES_PER_KEY is None else
+                                     round(SPLIT_DRAM_BYTES_PER_KEY * n / max(1, split_kinds["split_launches"]))),
+                         "peaks_by_kind_gevals": {k: round(v / 1e9, 3) for k, v in peaks.items()},
+                         "evals_by_kind": {k: split_kinds[k] for k in shg.SPLIT_KINDS},
+                         "launches": split_kinds["split_launches"],
+                         "note": "useful split evaluations (the reference's sequential count) / device time of the "
+                                 "split stage; peak = each node kind's useful evaluations at the measured rate of "
+                                 "that kind's inner loop run with no memory traffic (compare-and-count for 1..3 "
+                                 "thresholds, moment sums for quarter splits)"},
+            "leaf_stage": leaf_report(last, leaf_ms, leaf_peak, lpeaks, split_kinds),
             "work": last.work, "bits_per_key_trees": round(bits_per_key, 4),
             "gpu_launches": int(last.work["launches"] * args.steps),
             "clocks": clocks.summary(),
-            "cpu_baseline": cpu, "forms": forms,
+            "cpu_baseline": cpu, "parity": parity, "forms": forms,
         }
+    r.free()
     if ws > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()

@@ -313,12 +313,26 @@ shg_status shg_memo_table(int variant, int leaf_size, uint64_t *out);
 /* Benchmark utilities (no counterpart in the reference interface). n keys drawn from
  * std::mt19937_64(seed) with duplicates redrawn, as the benchmark configurations specify. */
 void shg_keys_mt19937_64(uint64_t seed, uint64_t n, uint64_t *out);
+/* n distinct uint64 keys out[j] = remix(seed ^ (j * 0x9E3779B97F4A7C15)) (Stafford Mix13, a bijection),
+ * filled by up to `threads` host threads: the per-request key sets of the serving stream. */
+void shg_keys_mix(uint64_t seed, uint64_t n, uint64_t *out, int threads);
 /* Integer-pipe peak of the split-search arithmetic (remix + 16-bit part thresholds, operands in
  * registers) on `device`, in evaluations per second: the roofline denominator of the searches. */
 int shg_int_peak(int device, uint64_t iters, double *evals_per_s, double *ms);
-/* Same for the inner loop of one search: 0 = split (as shg_int_peak), 1 = original leaf coverage
- * (remix, two fastrange32 cells, half masks), 2 = bipartite raw seeds (remix, fastrange64, mask). */
+/* Same for the inner loop of one search: 0 = split quarter-split moments (as shg_int_peak),
+ * 1 = original leaf coverage (remix, two fastrange32 cells, half masks), 2 = bipartite raw seeds
+ * (remix, fastrange64, mask), 3 / 4 / 5 = split compare-and-count against 1 / 2 / 3 part
+ * thresholds (fanout-2 and uneven split nodes), 6 = bipartite candidate-scan mask pairs,
+ * 7 = bipartite isolated-key pair filter, 8 = bipartite pseudoforest edges (union-find). */
 int shg_int_peak_kind(int device, int kind, uint64_t iters, double *evals_per_s, double *ms);
+
+/* Work counts of the engine's last RecSplit build beyond shg_result.work (measurement utility, no
+ * counterpart in the reference; the weights of the search stages' roofline denominators). Writes
+ * min(n, 8) values: [0..2] useful split evaluations of nodes comparing 1, 2 or 3 part thresholds
+ * (fanout-2 and uneven nodes), [3] of quarter splits (moment sums), [4] split level launches,
+ * [5] bipartite leaves' candidate-scan mask-pair tests (for each raw seed, the earlier raw seeds
+ * it is paired with), [6..7] zero. */
+shg_status shg_engine_last_work(const shg_engine *e, uint64_t *out, int n);
 
 /* Free and total device memory (cudaMemGetInfo), for admission control. */
 shg_status shg_device_memory(int device, uint64_t *free_bytes, uint64_t *total_bytes);

@@ -14,8 +14,36 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_SO = os.path.join(HERE, "_ref", "libshref.so")
+
+
+def host_has_avx512():
+    """Whether this host runs x86-64-v4 code (AVX-512 F, BW, CD, DQ, VL)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            flags = next((ln for ln in f if ln.startswith("flags")), "").split()
+    except OSError:
+        return False
+    return all(x in flags for x in ("avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl"))
+
+
+# The reference build whose SIMD width matches this host's -march=native (oracle/Makefile).
+_V4_DIR = os.path.join(HERE, "_ref", "v4")
+REF_DIR = _V4_DIR if host_has_avx512() and os.path.exists(os.path.join(_V4_DIR, "libshref.so")) else os.path.join(HERE, "_ref")
+REF_SO = os.path.join(REF_DIR, "libshref.so")
+STATS_SO = os.path.join(REF_DIR, "libshref_stats.so")
 PORT_SO = os.path.join(HERE, "_port", "libshgport.so")
+
+
+def ref_build_info():
+    """Which compiled reference this process uses: its directory, target ISA and the host's."""
+    arch = None
+    try:
+        with open(os.path.join(REF_DIR, "build_arch.txt")) as f:
+            arch = f.read().strip()
+    except OSError:
+        pass
+    return {"dir": os.path.relpath(REF_DIR, os.path.dirname(HERE)), "march": arch, "host_avx512": host_has_avx512(),
+            "flags": "-std=c++20 -O3 -DNDEBUG"}
 
 _u64p = ctypes.c_void_p
 _vp = ctypes.c_void_p
@@ -127,6 +155,30 @@ class RefLib(_Lib):
         b.bits = int(self.lib.ref_get_bits(_vp(h)))
         b._strings = (data, offs)
         return b
+
+    def build_strings_packed_timed(self, variant, leaf, data, offs, bucket_size=2000, threads=1):
+        """The reference constructor from string keys given packed; returns (products, seconds of the
+        constructor call alone)."""
+        L = self.lib
+        L.ref_build_strings_timed.restype = _vp
+        L.ref_build_strings_timed.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_char_p, _vp, _sz, _sz, _sz,
+                                              ctypes.POINTER(ctypes.c_double)]
+        secs = ctypes.c_double(0)
+        offs = np.ascontiguousarray(offs, dtype=np.uint64)
+        h = L.ref_build_strings_timed(variant, leaf, data, _ptr(offs), len(offs) - 1, bucket_size, threads,
+                                      ctypes.byref(secs))
+        if not h:
+            raise ValueError(f"leaf size {leaf} not instantiated in the reference oracle")
+        b = Built(L, "ref_", h)
+        b.bits = int(L.ref_get_bits(_vp(h)))
+        return b, float(secs.value)
+
+    def query_packed(self, built, data, offs):
+        """operator()(const string&) of a reference build for packed string keys."""
+        offs = np.ascontiguousarray(offs, dtype=np.uint64)
+        out = np.zeros(len(offs) - 1, dtype=np.uint64)
+        self.lib.ref_query_strings(_vp(built.h), data, _ptr(offs), len(offs) - 1, _ptr(out))
+        return out
 
     def query_strings(self, built, keys):
         data, offs = pack_strings(keys)
@@ -298,6 +350,47 @@ class PortLib(_Lib):
         rb = np.zeros(m, np.uint8)
         code = self.lib.port_sh1_leaf(m, level, _ptr(keys), _ptr(rk), _ptr(rb))
         return int(code), rk, rb
+
+
+def _keygen_lib():
+    """The compiled reference when present, else the restatement: both export the same generators."""
+    if ref_available():
+        return ctypes.CDLL(REF_SO), "ref_"
+    return ctypes.CDLL(PORT_SO), "port_"
+
+
+def keys_mt19937_64(seed, n):
+    """n uint64 keys from std::mt19937_64(seed), later duplicates redrawn (oracle/keygen.h); the same
+    keys, draw for draw, as the CUDA library's benchmark generator."""
+    lib, p = _keygen_lib()
+    fn = getattr(lib, p + "keys_mt19937_64")
+    fn.argtypes = [ctypes.c_uint64, ctypes.c_uint64, _vp]
+    fn.restype = None
+    out = np.empty(n, dtype=np.uint64)
+    fn(seed, n, _ptr(out))
+    return out
+
+
+STRINGS_PRINTABLE, STRINGS_ZIPF = 0, 1
+
+
+def strings_mt19937_64(kind, seed, n):
+    """n distinct string keys from std::mt19937_64(seed) (oracle/keygen.h): kind 0 = lengths 16..40
+    of bytes 33..126; kind 1 = Zipf(1.1) lengths 8..200 of bytes 0..255. Returns (bytes, offsets[n+1])."""
+    lib, p = _keygen_lib()
+    fn = getattr(lib, p + "strings_mt19937_64")
+    fn.argtypes = [ctypes.c_int, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_char_p, _vp]
+    fn.restype = ctypes.c_uint64
+    total = int(fn(kind, seed, n, None, None))
+    buf = ctypes.create_string_buffer(max(1, total))
+    offs = np.zeros(n + 1, dtype=np.uint64)
+    fn(kind, seed, n, buf, _ptr(offs))
+    return buf.raw[:total], offs
+
+
+def split_strings(data, offs):
+    """(bytes, offsets) -> list of bytes keys."""
+    return [data[int(offs[i]):int(offs[i + 1])] for i in range(len(offs) - 1)]
 
 
 def ref_available():

@@ -21,6 +21,7 @@
 #include <string>
 #include <vector>
 #include "../shims/shg_thirdparty.h"
+#include "../keygen.h"
 
 using namespace shg_tp;
 
@@ -725,3 +726,5 @@ uint64_t port_sh1_leaf(uint32_t m, int level, const uint64_t *keys, uint64_t *rk
 }
 
 } // extern "C"
+
+SHG_ORACLE_KEYGEN_EXPORTS(port_)

@@ -39,6 +39,7 @@
 #include <bytehamster/util/IntVector.h>
 #include <bytehamster/util/EliasFano.h>
 #include <tlx/math/integer_log2.hpp>
+#include "keygen.h"
 
 #define private public
 #include <ShockHash.h>
@@ -371,6 +372,21 @@ void *ref_build_strings(int variant, int leaf, const char *bytes, const uint64_t
     return nullptr;
 }
 
+// ref_build_strings with the wall time of the reference constructor alone in *seconds: the key
+// strings are made before the clock starts, as the reference's own benchmark times only the
+// constructor call (benchmark/benchmark_construction.cpp:53-56).
+void *ref_build_strings_timed(int variant, int leaf, const char *bytes, const uint64_t *offsets, size_t n,
+                              size_t bucket_size, size_t threads, double *seconds) {
+    auto keys = make_strings(bytes, offsets, n);
+    const auto t0 = std::chrono::steady_clock::now();
+    RefBase *r = nullptr;
+    if (variant == 1) r = make_sh1_str(leaf, keys, bucket_size, threads);
+    if (variant == 2) r = make_sh2_str(leaf, keys, bucket_size, threads);
+    if (variant == 3) r = make_rot_str(leaf, keys, bucket_size, threads);
+    *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return r;
+}
+
 void ref_free(void *h) { delete (RefBase *)h; }
 uint64_t ref_nbuckets(void *h) { return ((RefBase *)h)->nbuckets(); }
 uint64_t ref_desc_words(void *h) { return ((RefBase *)h)->desc_words(); }
@@ -454,12 +470,14 @@ int ref_sh2_pair_check(size_t L, const uint8_t *a, const uint8_t *b, int *skippe
 // Phase times of the builds since the last call, from the reference's own STATS counters
 // (ShockHash.h:37-44; ShockHash2.h:268-290, 314-388): the leaf searches and the split levels
 // summed, in nanoseconds. The counters are plain globals, so builds measured this way run on one
-// thread. Resets the counters.
+// thread. Resets the counters to zero after reading them.
 void ref_stats_times(uint64_t *leaves_ns, uint64_t *splits_ns) {
     *leaves_ns = shockhash::time_bij;
     uint64_t s = 0;
     for (int i = 0; i < MAX_LEVEL_TIME; i++) s += shockhash::time_split[i];
     *splits_ns = s;
+    shockhash::time_bij = 0;
+    for (int i = 0; i < MAX_LEVEL_TIME; i++) shockhash::time_split[i] = 0;
 }
 #endif
 
@@ -478,3 +496,5 @@ int ref_cuckoo_construct(const uint64_t *keys, size_t m, uint64_t seed, uint32_t
 }
 
 } // extern "C"
+
+SHG_ORACLE_KEYGEN_EXPORTS(ref_)

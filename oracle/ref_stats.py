@@ -22,9 +22,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(HERE))
 
-from oracle.bindings import RefLib, _ptr  # noqa: E402
-
-STATS_SO = os.path.join(HERE, "_ref", "libshref_stats.so")
+from oracle.bindings import STATS_SO, RefLib, _ptr  # noqa: E402
 
 
 def phase_times(keys, variant, leaf, bucket):
@@ -38,7 +36,7 @@ def phase_times(keys, variant, leaf, bucket):
     second = np.zeros(len(keys), np.uint64)
     L.ref_spooky128(data, _ptr(offs), len(keys), _ptr(first), _ptr(second))
     t = np.zeros(2, np.uint64)
-    L.ref_stats_times(_ptr(t[:1]), _ptr(t[1:]))  # clear what earlier builds left
+    L.ref_stats_times(_ptr(t[:1]), _ptr(t[1:]))  # read and zero what earlier builds left
     t0 = time.perf_counter()
     b = lib.build_hash(variant, leaf, first, second, bucket, 1)
     wall = time.perf_counter() - t0
@@ -57,8 +55,8 @@ def main():
     ap.add_argument("--bucket", type=int, default=2000)
     ap.add_argument("--seed", type=int, default=7)
     a = ap.parse_args()
-    import shockhash_b200 as shg  # the benchmark's key generator (host code, no device needed)
-    keys = shg.keys_mt19937_64(a.seed, a.n)
+    from oracle.bindings import keys_mt19937_64  # the benchmark's key stream, drawn by the oracle
+    keys = keys_mt19937_64(a.seed, a.n)
     res = phase_times(keys, a.variant, a.leaf, a.bucket)
     ctypes.CDLL(None).fflush(None)  # the STATS report (C stdio) goes out before the JSON line
     sys.stdout.flush()

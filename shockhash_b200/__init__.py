@@ -146,7 +146,9 @@ def lib():
         "shg_retrieval_build_ms": ([_vp], ctypes.c_float),
         "shg_retrieval_query_ms": ([_vp], ctypes.c_float),
         "shg_device_memory": ([ctypes.c_int, ctypes.POINTER(_u64), ctypes.POINTER(_u64)], ctypes.c_int),
+        "shg_engine_last_work": ([_vp, _vp, ctypes.c_int], ctypes.c_int),
         "shg_keys_mt19937_64": ([_u64, _u64, _vp], None),
+        "shg_keys_mix": ([_u64, _u64, _vp, ctypes.c_int], None),
         "shg_int_peak": ([ctypes.c_int, _u64, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)],
                          ctypes.c_int),
         "shg_int_peak_kind": ([ctypes.c_int, ctypes.c_int, _u64, ctypes.POINTER(ctypes.c_double),
@@ -170,7 +172,10 @@ def _ptr(a):
 
 
 def pack_strings(keys):
-    """list of str/bytes -> (bytes, offsets[n+1] uint64)."""
+    """list of str/bytes -> (bytes, offsets[n+1] uint64); an already packed (bytes, offsets) pair
+    passes through unchanged."""
+    if isinstance(keys, tuple) and len(keys) == 2 and isinstance(keys[0], (bytes, bytearray)):
+        return bytes(keys[0]), np.ascontiguousarray(keys[1], dtype=np.uint64)
     bs = [k.encode() if isinstance(k, str) else bytes(k) for k in keys]
     data = b"".join(bs)
     offs = np.zeros(len(bs) + 1, dtype=np.uint64)
@@ -186,6 +191,14 @@ def keys_mt19937_64(seed, n):
     return out
 
 
+def keys_mix(seed, n, threads=8):
+    """n distinct uint64 keys remix(seed ^ (j * 0x9E3779B97F4A7C15)), j < n (the serving stream's
+    per-request key sets; fast enough to draw at submit time)."""
+    out = np.empty(n, dtype=np.uint64)
+    lib().shg_keys_mix(seed, n, _ptr(out), threads)
+    return out
+
+
 def device_memory(device=0):
     """(free, total) device memory in bytes."""
     f, t = _u64(), _u64()
@@ -195,10 +208,44 @@ def device_memory(device=0):
 
 def int_peak(device=0, iters=1 << 16, kind=0):
     """Measured evaluations/s of a search's inner-loop arithmetic with no memory traffic
-    (kind 0 = split, 1 = original leaf coverage, 2 = bipartite raw seeds)."""
+    (kind 0 = split quarter moments, 1 = original leaf coverage, 2 = bipartite raw seeds,
+    3 / 4 / 5 = split compare-and-count with 1 / 2 / 3 part thresholds)."""
     e, ms = ctypes.c_double(), ctypes.c_double()
     _check(lib().shg_int_peak_kind(device, kind, iters, ctypes.byref(e), ctypes.byref(ms)))
     return e.value, ms.value
+
+
+SPLIT_KINDS = ("thresholds_1", "thresholds_2", "thresholds_3", "quarter_moments")
+
+
+def split_peaks(device=0, iters=1 << 15):
+    """Measured evaluations/s of each split inner loop, keyed as SPLIT_KINDS."""
+    kinds = (3, 4, 5, 0)
+    return {name: int_peak(device, iters, k)[0] for name, k in zip(SPLIT_KINDS, kinds)}
+
+
+LEAF_OPS = ("hash_evals", "scan_tests", "pair_tests", "uf_edges")
+
+
+def leaf_peaks(device=0, iters=1 << 15):
+    """Measured operations/s of the bipartite leaf search's inner loops, keyed as LEAF_OPS:
+    hashing (remix, fastrange64, mask), candidate-scan mask pairs, isolated-key pair filter,
+    pseudoforest (union-find) edges."""
+    return {name: int_peak(device, iters, k)[0] for name, k in zip(LEAF_OPS, (2, 6, 7, 8))}
+
+
+def leaf_ceiling_s(counts, peaks):
+    """Seconds the bipartite leaf stage's operations take at their loops' measured peaks (the
+    stage's roofline: the sum over the four operation kinds of count / peak)."""
+    return sum(counts[k] / peaks[k] for k in LEAF_OPS if counts.get(k))
+
+
+def weighted_split_peak(kind_evals, peaks):
+    """The split stage's ceiling for a build: its useful evaluations over the time each node kind's
+    evaluations take at that kind's measured peak (a harmonic mean weighted by evaluations)."""
+    total = sum(kind_evals[k] for k in SPLIT_KINDS)
+    t = sum(kind_evals[k] / peaks[k] for k in SPLIT_KINDS if kind_evals[k])
+    return total / t if t > 0 else float("nan")
 
 
 def sh2_construct_leaves_noalloc(d_keys, d_leaf_offsets, nleaves, d_seeds, d_bits, stream=0):
@@ -287,6 +334,16 @@ class Engine:
             self.close()
         except Exception:
             pass
+
+    def last_work(self):
+        """Work counts of this engine's last build beyond BuildResult.work: useful split evaluations
+        by inner loop (SPLIT_KINDS), split level launches, bipartite candidate-scan mask tests."""
+        k = np.zeros(8, np.uint64)
+        _check(lib().shg_engine_last_work(self._h, _ptr(k), 8))
+        out = {name: int(v) for name, v in zip(SPLIT_KINDS, k[:4])}
+        out["split_launches"] = int(k[4])
+        out["leaf_scan_tests"] = int(k[5])
+        return out
 
     @staticmethod
     def params(variant, leaf_size, bucket_size=2000, mode=MODE_DEFAULT, max_trials=0):

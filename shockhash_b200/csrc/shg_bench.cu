@@ -9,10 +9,12 @@
 #include <algorithm>
 #include <cstdint>
 #include <random>
+#include <thread>
 #include <vector>
 #include <cuda_runtime.h>
 #include "shg.h"
 #include "shg_common.cuh"
+#include "shg_internal.h"
 
 namespace {
 
@@ -34,6 +36,28 @@ __global__ void __launch_bounds__(kPeakThreads) k_int_peak(uint64_t iters, uint3
         d0 += p1; d1 += q1; d2 += q1 * p1;
     }
     if ((c0 ^ c1 ^ c2 ^ d0 ^ d1 ^ d2 ^ T0 ^ T1 ^ T2) == 0xFFFFFFFFu) atomicAdd(sink, 1ull);
+}
+
+// The arithmetic of the split kernel's compare-and-count loop (fanout-2 and uneven nodes): remix to
+// 16 bits, one count per part threshold (NT of them); two seeds per key pair, as k_int_peak.
+template <int NT>
+__global__ void __launch_bounds__(kPeakThreads) k_int_peak_cmp(uint64_t iters, uint32_t T0, uint32_t T1, uint32_t T2,
+                                                               unsigned long long *sink) {
+    const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    uint64_t k0 = shg::remix(tid * 0x9E3779B97F4A7C15ULL), k1 = shg::remix(k0);
+    const uint64_t x0 = 0x643e521ddbd2be98ULL + tid;
+    const uint32_t T[3] = {T0, T1, T2};
+    uint32_t c[2][3] = {};
+    for (uint64_t i = 0; i < iters; i++) {
+        const uint32_t r0 = shg::remix_low16(k0 + x0 + i);
+        const uint32_t r1 = shg::remix_low16(k1 + x0 + i);
+#pragma unroll
+        for (int t = 0; t < NT; t++) {
+            c[0][t] += r0 < T[t];
+            c[1][t] += r1 < T[t];
+        }
+    }
+    if ((c[0][0] ^ c[0][1] ^ c[0][2] ^ c[1][0] ^ c[1][1] ^ c[1][2]) == 0xFFFFFFFFu) atomicAdd(sink, 1ull);
 }
 
 // The arithmetic of the original leaf search's coverage loop: full 64-bit remix, both cells by
@@ -107,6 +131,27 @@ void shg_keys_mt19937_64(uint64_t seed, uint64_t n, uint64_t *out) {
     }
 }
 
+// Request keys of the serving stream: out[j] = remix(seed ^ (j * 0x9E3779B97F4A7C15)), j < n. Each
+// step is a bijection of 64-bit words, so the n keys are distinct with no check; host threads each
+// fill a contiguous range.
+void shg_keys_mix(uint64_t seed, uint64_t n, uint64_t *out, int threads) {
+    const uint64_t T = (uint64_t)std::max(1, std::min(threads, 64));
+    const uint64_t chunk = (n + T - 1) / T;
+    auto fill = [&](uint64_t a, uint64_t b) {
+        for (uint64_t j = a; j < b; j++) out[j] = shg::remix(seed ^ (j * 0x9E3779B97F4A7C15ULL));
+    };
+    if (T == 1 || n < (1u << 16)) {
+        fill(0, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (uint64_t t = 0; t < T; t++) {
+        const uint64_t a = std::min(n, t * chunk), b = std::min(n, a + chunk);
+        if (a < b) pool.emplace_back(fill, a, b);
+    }
+    for (auto &th : pool) th.join();
+}
+
 // Integer-pipe peak: evaluations per second of the split search arithmetic on `device`.
 int shg_int_peak(int device, uint64_t iters, double *evals_per_s, double *ms_out) {
     if (cudaSetDevice(device) != cudaSuccess) return SHG_ERR_CUDA;
@@ -136,10 +181,12 @@ int shg_int_peak(int device, uint64_t iters, double *evals_per_s, double *ms_out
     return SHG_OK;
 }
 
-// Integer-pipe peak of one search's inner loop (0 = split, 1 = original leaf, 2 = bipartite leaf).
+// Integer-pipe peak of one search's inner loop (0 = split quarter moments, 1 = original leaf,
+// 2 = bipartite leaf hashing, 3..5 = split compare-and-count with 1..3 thresholds, 6..8 = bipartite
+// candidate scan, pair filter and pseudoforest edges).
 int shg_int_peak_kind(int device, int kind, uint64_t iters, double *evals_per_s, double *ms_out) {
     if (kind == 0) return shg_int_peak(device, iters, evals_per_s, ms_out);
-    if (kind != 1 && kind != 2) return SHG_ERR_ARG;
+    if (kind < 1 || kind > 8) return SHG_ERR_ARG;
     if (cudaSetDevice(device) != cudaSuccess) return SHG_ERR_CUDA;
     cudaDeviceProp prop;
     cudaGetDeviceProperties(&prop, device);
@@ -155,8 +202,16 @@ int shg_int_peak_kind(int device, int kind, uint64_t iters, double *evals_per_s,
         if (rep) cudaEventRecord(a);
         if (kind == 1)
             k_int_peak_sh1<<<blocks, kPeakThreads>>>(it, 20, 20, sink);
-        else
+        else if (kind == 2)
             k_int_peak_sh2<<<blocks, kPeakThreads>>>(it, 32, sink);
+        else if (kind == 3)
+            k_int_peak_cmp<1><<<blocks, kPeakThreads>>>(it, 50331, 65536, 65536, sink);
+        else if (kind == 4)
+            k_int_peak_cmp<2><<<blocks, kPeakThreads>>>(it, 21846, 43691, 65536, sink);
+        else if (kind == 5)
+            k_int_peak_cmp<3><<<blocks, kPeakThreads>>>(it, 16384, 32768, 49152, sink);
+        else  // the bipartite leaf's scan, pair filter and pseudoforest loops (64 edges per iteration)
+            shg::launch_sh2_op_peak(kind - 6, blocks, kind == 8 ? it / 64 + 1 : it, sink);
         if (rep) cudaEventRecord(b);
     }
     cudaEventSynchronize(b);
@@ -166,7 +221,13 @@ int shg_int_peak_kind(int device, int kind, uint64_t iters, double *evals_per_s,
     cudaEventDestroy(b);
     cudaFree(sink);
     if (cudaGetLastError() != cudaSuccess) return SHG_ERR_CUDA;
-    *evals_per_s = 2.0 * (double)iters * blocks * kPeakThreads / (ms * 1e-3);
+    double per_iter = 2.0;
+    uint64_t timed_iters = iters;
+    if (kind >= 6) {
+        per_iter = shg::sh2_op_peak_per_iter(kind - 6);
+        if (kind == 8) timed_iters = iters / 64 + 1;
+    }
+    *evals_per_s = per_iter * (double)timed_iters * blocks * kPeakThreads / (ms * 1e-3);
     if (ms_out) *ms_out = ms;
     return SHG_OK;
 }

@@ -131,6 +131,8 @@ struct shg_engine {
     cudaEvent_t chunk_ev[kMaxChunks] = {};
     cudaEvent_t join_ev = nullptr;
     int pipe_chunks = 8;
+    unsigned long long split_kind[4] = {};  // of the last build (shg_engine_last_work)
+    uint64_t split_launches = 0, leaf_scan = 0;
     ~shg_engine() {
         DevBuf *all[] = {&in_keys, &in_bytes, &in_offsets, &first, &second, &sfirst, &sidx, &counts, &cursor,
                          &acc, &keys, &nodes, &ids, &codes, &fixed_off, &bucket_bits, &pos_acc, &words,
@@ -198,6 +200,7 @@ struct Misc {  // small device-side counters, one allocation
     unsigned int leaf_ctr;
     unsigned int pad;
     unsigned long long work[8];
+    unsigned long long split_kind[4];  // useful split evaluations by inner loop (see launch_split_level)
 };
 
 // Memo tables are cached per configuration (they cost ~3000 transcendental evaluations).
@@ -471,7 +474,7 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
     auto split_range = [&](size_t lv, uint64_t a, uint64_t b, cudaStream_t st) {
         if (b <= a) return;
         launch_split_level(e->nodes.as<Node>(), d_ids + level_off[lv] + a, (uint32_t)(b - a), e->keys.as<uint64_t>(),
-                           e->codes.as<uint64_t>(), p->max_trials, &misc->err, &misc->work[0], st);
+                           e->codes.as<uint64_t>(), p->max_trials, &misc->err, &misc->work[0], misc->split_kind, st);
         launches++;
     };
     auto leaf_range = [&](uint64_t a, uint64_t b, cudaStream_t st, int grid) {
@@ -626,8 +629,12 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
     if (keys_done) CU(cudaStreamWaitEvent(s, e->join_ev, 0));  // the keys copied during the leaves
     unsigned long long work[8];
     CU(cudaMemcpyAsync(work, misc->work, sizeof(work), cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(e->split_kind, misc->split_kind, sizeof(e->split_kind), cudaMemcpyDeviceToHost, s));
     CU(cudaEventRecord(e->ev[6], s));
     CU(cudaStreamSynchronize(s));
+    e->split_launches = 0;
+    for (int lv = 0; lv < nlevels; lv++) e->split_launches += level_count[lv] ? 1 : 0;
+    e->leaf_scan = work[5];  // the leaf kernel's candidate-scan count (the slot is reported as leaves below)
     float ms[6] = {};
     cudaEventElapsedTime(&ms[0], e->ev[0], e->ev[1]);
     cudaEventElapsedTime(&ms[1], e->ev[1], e->ev[2]);
@@ -1460,6 +1467,14 @@ shg_status shg_memo_table(int variant, int leaf_size, uint64_t *out) {
     if (leaf_size < 2 || leaf_size > maxleaf) return fail(SHG_ERR_ARG, "leaf size out of range");
     const Config &c = config_of(variant, leaf_size);
     memcpy(out, c.memo.data(), kMaxBucket * 8);
+    return SHG_OK;
+}
+
+shg_status shg_engine_last_work(const shg_engine *e, uint64_t *out, int n) {
+    if (!e || !out || n < 0) return fail(SHG_ERR_ARG, "null argument");
+    const uint64_t v[8] = {e->split_kind[0], e->split_kind[1], e->split_kind[2], e->split_kind[3], e->split_launches,
+                           e->leaf_scan, 0, 0};
+    for (int k = 0; k < n && k < 8; k++) out[k] = v[k];
     return SHG_OK;
 }
 

@@ -134,10 +134,16 @@ void launch_bucket_scatter(const uint64_t *first, uint64_t n, uint64_t nb, uint6
                            uint64_t *sfirst, uint32_t *sidx, uint64_t idx_base, cudaStream_t s);
 void launch_bucket_sort(const uint64_t *acc, uint64_t nb, const uint64_t *sfirst, const uint32_t *sidx,
                         const uint64_t *second, uint64_t *keys, cudaStream_t s);
+// work[0] += useful evaluations; kind_work[k] += the same per inner loop (k = compared thresholds
+// - 1, or 3 for quarter-split moments)
 void launch_split_level(const Node *nodes, const uint32_t *ids, uint32_t count, uint64_t *keys,
                         uint64_t *codes, uint64_t max_trials, uint32_t *err, unsigned long long *work,
-                        cudaStream_t s);
+                        unsigned long long *kind_work, cudaStream_t s);
 int leaves_sh1_warps_per_block();
+// Inner-loop peaks of the bipartite leaf search (kind 0 scan, 1 pair filter, 2 pseudoforest edges),
+// 256-thread blocks; operations per thread and iteration from sh2_op_peak_per_iter.
+void launch_sh2_op_peak(int kind, int blocks, uint64_t iters, unsigned long long *sink);
+int sh2_op_peak_per_iter(int kind);
 void launch_gr_bucket_bits(const Node *nodes, const uint32_t *bnb, uint64_t nb, const uint64_t *acc,
                            const uint64_t *codes, const uint32_t *memo_skip_bits, uint64_t *bucket_bits,
                            cudaStream_t s);

@@ -248,7 +248,7 @@ __global__ void __launch_bounds__(128, MAXM <= 64 ? 6 : 1) k_leaves_sh2_v2(Src s
     Sh2Global<MAXM> g;
     g.carve(gbase, smax, cmax);
     LaneUF2<MAXM> uf{sm.uf, lane, 0, 0};
-    unsigned long long w_evals = 0, w_pairs = 0, w_filtered = 0, w_edges = 0;
+    unsigned long long w_evals = 0, w_pairs = 0, w_filtered = 0, w_edges = 0, w_scan = 0;
     const unsigned below = (1u << lane) - 1;
 
     for (;;) {
@@ -366,6 +366,7 @@ __global__ void __launch_bounds__(128, MAXM <= 64 ? 6 : 1) k_leaves_sh2_v2(Src s
             const bool live = s < S;
             uint32_t mine = 0, mineA = 0, mineB = 0;
             uint32_t ha0 = 0, ha1 = 0, hb0 = 0, hb1 = 0;  // first two partners on each side
+            if (live) w_scan += cx.quad ? s + 1 : 1;  // mask pairs this raw seed is tested against
             if (live) {
                 if (cx.quad) {
                     // one pass over the earlier raw seeds p <= s: A-side pairs (p, s) for p < s and
@@ -648,12 +649,14 @@ __global__ void __launch_bounds__(128, MAXM <= 64 ? 6 : 1) k_leaves_sh2_v2(Src s
         w_pairs += __shfl_xor_sync(0xffffffffu, w_pairs, o);
         w_filtered += __shfl_xor_sync(0xffffffffu, w_filtered, o);
         w_edges += __shfl_xor_sync(0xffffffffu, w_edges, o);
+        w_scan += __shfl_xor_sync(0xffffffffu, w_scan, o);
     }
     if (lane == 0) {
         atomicAdd(&work[1], w_evals);
         atomicAdd(&work[2], w_pairs);
         atomicAdd(&work[3], w_filtered);
         atomicAdd(&work[4], w_edges);
+        atomicAdd(&work[5], w_scan);
     }
 }
 
@@ -662,11 +665,9 @@ void launch_v2(const Node *nodes, const uint32_t *ids, uint32_t count, const uin
                uint8_t *rib_bits, uint8_t *scratch, uint64_t scratch_per_warp, uint32_t smax, uint32_t cmax,
                uint32_t *err, unsigned long long *work, unsigned int *ctr, int grid, cudaStream_t s, uint32_t quad_min) {
     const size_t smem = sizeof(Sh2Smem<MAXM>) * 4;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_leaves_sh2_v2<MAXM, NodeLeaves>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr = true;
-    }
+    // The shared-memory limit is an attribute of the kernel on the current device: set it on every
+    // launch (a cheap host call), so engines on several devices and threads each get it.
+    cudaFuncSetAttribute(k_leaves_sh2_v2<MAXM, NodeLeaves>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_leaves_sh2_v2<MAXM, NodeLeaves><<<grid, 128, smem, s>>>(NodeLeaves{nodes, ids, codes}, count, keys, rib_bits, scratch,
                                                               scratch_per_warp, smax, cmax, err, work, ctr, quad_min);
 }
@@ -695,6 +696,74 @@ void launch_leaves_sh2_ctr(const Node *nodes, const uint32_t *ids, uint32_t coun
 }
 
 int sh2_smem_per_warp(int max_leaf) { return max_leaf <= 64 ? (int)sizeof(Sh2Smem<64>) : (int)sizeof(Sh2Smem<128>); }
+
+// ------------------------------------------------------------------ inner-loop peaks
+// The leaf search's three non-hashing inner loops run alone on register and shared-memory operands,
+// with every lane busy (no divergence, no early exit): their operations per second are the
+// denominators of the leaf stage's work model (the hashing loop's is k_int_peak_sh2).
+//   kind 0: candidate scan, one (A, B) mask pair of an earlier raw seed against the lane's raw seed
+//           (two pairs per 16-byte broadcast load, as the 64-key scan);
+//   kind 1: isolated-key filter of one candidate pair (two 64-bit masks from shared memory);
+//   kind 2: one pseudoforest edge of a 64-key leaf (LaneUF2::add on shared-memory parents; each
+//           test initialises the parents and adds 64 edges).
+namespace {
+template <int KIND>
+__global__ void __launch_bounds__(256) k_sh2_op_peak(uint64_t iters, unsigned long long *sink) {
+    __shared__ uint4 masks[128];
+    __shared__ uint64_t iso[256];
+    __shared__ uint8_t par[8][64 * 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    for (int i = threadIdx.x; i < 128; i += blockDim.x) {
+        const uint64_t a = remix(0x51ull * i + 7), b = remix(a);
+        masks[i] = make_uint4((uint32_t)a, (uint32_t)(a >> 32), (uint32_t)b, (uint32_t)(b >> 32));
+    }
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) iso[i] = remix(0x93ull * i + 3) & remix(0x77ull * i + 1);
+    __syncthreads();
+    uint64_t acc = 0;
+    if (KIND == 0) {
+        const uint64_t r = remix(tid);
+        const uint32_t tA = (uint32_t)r, tB = (uint32_t)(r >> 32), full = 0xFFFFFFFFu;
+        uint32_t hits = 0;
+        for (uint64_t i = 0; i < iters; i++) {
+            const uint4 w = masks[i & 127];
+            const uint32_t z = min(min((w.x | tB) ^ full, (w.y | tA) ^ full), min((w.z | tB) ^ full, (w.w | tA) ^ full));
+            hits += z == 0;
+        }
+        acc = hits;
+    } else if (KIND == 1) {
+        uint32_t j = 1 + (uint32_t)(tid & 63), i = (uint32_t)(tid >> 6) % j, hits = 0;
+        for (uint64_t q = 0; q < iters; q++) {
+            hits += (iso[j & 255] & iso[i & 255]) == 0;
+            if (++i == j) {  // (j, i) in lexicographic order, as the pair enumeration steps
+                i = 0;
+                j++;
+            }
+        }
+        acc = hits;
+    } else {
+        LaneUF2<64> uf{par[warp], lane, 0, 0};
+        uint64_t x = remix(tid), ok = 0;
+        for (uint64_t t = 0; t < iters; t++) {
+            uf.init(64);
+            for (int k = 0; k < 64; k++) {
+                x = x * 0x9E3779B97F4A7C15ull + 1;
+                ok += uf.add(32 + (uint32_t)((x >> 20) & 31), (uint32_t)((x >> 40) & 31));
+            }
+        }
+        acc = ok;
+    }
+    if (acc == 0x123456789ull) atomicAdd(sink, 1ull);
+}
+}  // namespace
+
+// Operations per launch thread and iteration: 2 (kind 0), 1 (kind 1), 64 (kind 2).
+int sh2_op_peak_per_iter(int kind) { return kind == 0 ? 2 : kind == 1 ? 1 : 64; }
+void launch_sh2_op_peak(int kind, int blocks, uint64_t iters, unsigned long long *sink) {
+    if (kind == 0) k_sh2_op_peak<0><<<blocks, 256>>>(iters, sink);
+    else if (kind == 1) k_sh2_op_peak<1><<<blocks, 256>>>(iters, sink);
+    else k_sh2_op_peak<2><<<blocks, 256>>>(iters, sink);
+}
 
 // ------------------------------------------------------------------ no-allocation variant
 // Some callers cannot allocate device memory at the moment they need leaf seeds: code running

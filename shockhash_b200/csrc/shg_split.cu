@@ -150,7 +150,8 @@ __device__ uint64_t search_seeds(SplitSmem &sm, uint32_t m, uint64_t seed0, cons
 __global__ void __launch_bounds__(kSplitThreads) k_split(const Node *__restrict__ nodes, const uint32_t *__restrict__ ids,
                                                          uint64_t *__restrict__ keys, uint64_t *__restrict__ codes,
                                                          uint64_t max_trials, uint32_t *__restrict__ err,
-                                                         unsigned long long *__restrict__ work) {
+                                                         unsigned long long *__restrict__ work,
+                                                         unsigned long long *__restrict__ kind_work) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
     SplitSmem &sm = *reinterpret_cast<SplitSmem *>(smem_raw);
     const uint32_t id = ids[blockIdx.x];
@@ -249,15 +250,18 @@ __global__ void __launch_bounds__(kSplitThreads) k_split(const Node *__restrict_
     if (threadIdx.x == 0) {
         codes[id] = trial;  // x - start_seed[level]
         atomicAdd(work, (unsigned long long)(trial + 1) * m);
+        // useful evaluations by inner loop: 1, 2 or 3 compared thresholds, or quarter-split moments
+        atomicAdd(&kind_work[quarter ? 3 : NT - 1], (unsigned long long)(trial + 1) * m);
     }
 }
 
 void launch_split_level(const Node *nodes, const uint32_t *ids, uint32_t count, uint64_t *keys, uint64_t *codes,
-                        uint64_t max_trials, uint32_t *err, unsigned long long *work, cudaStream_t s) {
+                        uint64_t max_trials, uint32_t *err, unsigned long long *work, unsigned long long *kind_work,
+                        cudaStream_t s) {
     if (!count) return;
     const size_t smem = sizeof(SplitSmem);
     cudaFuncSetAttribute(k_split, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_split<<<count, kSplitThreads, smem, s>>>(nodes, ids, keys, codes, max_trials, err, work);
+    k_split<<<count, kSplitThreads, smem, s>>>(nodes, ids, keys, codes, max_trials, err, work, kind_work);
 }
 
 } // namespace shg

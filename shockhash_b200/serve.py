@@ -9,17 +9,22 @@ leaves share the same kernel launches, one persistent leaf launch for the whole 
 that arrive while batches run wait for the next free worker; with two or more workers, the
 batches of different workers overlap on the device.
 
-Admission is by free device memory: at start the server reads the free HBM, keeps `mem_fraction`
-of it, and gives every worker an equal share, which caps its batch at share / bytes_per_key keys
-and at `max_batch_keys` (a larger request is built alone). Each worker then builds one batch of
+Admission is by free device memory, read again whenever a batch is formed. At start the server
+reads the free HBM, keeps `mem_fraction` of it, and gives every worker an equal share: its warm
+capacity, share / bytes_per_key keys (at most `max_batch_keys`). Each worker builds one batch of
 that size before serving, so that its device buffers and its pinned result block exist before the
-first request arrives: growing them later would allocate and free device and pinned memory, which
-synchronises the whole device and stalls the other workers. Each result is bit-identical to
-building that request alone.
+first request arrives. When a worker forms a batch, it takes, in arrival order, requests up to its
+warm capacity plus what the device's free memory at that moment allows beyond it (`mem_fraction`
+of the free bytes, less what other workers have reserved for batches in flight, divided by
+bytes_per_key); a batch beyond the warm capacity grows that worker's buffers once, and the new
+size becomes its capacity. A request larger than every limit is built alone. Each result is
+bit-identical to building that request alone.
 
     python -m shockhash_b200.serve --requests 400
 prints one JSON line with p50/p99 build latency, aggregate keys/s and device utilisation for a
-Poisson stream (mean 200 requests/s) of log-uniform sizes between 10^3 and 10^7 keys.
+Poisson stream (mean 200 requests/s) of log-uniform sizes between 10^3 and 10^7 keys. Each
+request's keys are drawn when it is submitted (keys_mix of the request's sub-seed), so a stream of
+any length runs in bounded host memory; the latency clock starts at submission.
 """
 import argparse
 import json
@@ -30,7 +35,7 @@ from collections import deque
 
 import numpy as np
 
-from . import SHOCKHASH2, Engine, device_memory, keys_mt19937_64
+from . import SHOCKHASH2, Engine, device_memory, keys_mix, keys_mt19937_64
 
 
 class Request:
@@ -57,25 +62,32 @@ class Request:
 
 class BuildServer:
     def __init__(self, variant=SHOCKHASH2, leaf=64, bucket=2000, workers=2, device=0, mem_fraction=0.5,
-                 bytes_per_key=96, max_batch_keys=32_000_000, keep_results=True, warm=True):
+                 bytes_per_key=96, max_batch_keys=32_000_000, keep_results=True, warm=True, free_memory=None):
         self.variant, self.leaf, self.bucket = variant, leaf, bucket
         self.keep_results = keep_results
-        free, _ = device_memory(device)
-        share = free * mem_fraction / workers
+        self.device, self.mem_fraction, self.bytes_per_key = device, mem_fraction, bytes_per_key
+        self.max_batch_keys = max_batch_keys
+        # free device bytes now (a callable; tests substitute their own)
+        self._free_memory = free_memory or (lambda: device_memory(device)[0])
+        share = self._free_memory() * mem_fraction / workers
         self.batch_keys = int(min(max_batch_keys or share // bytes_per_key, share // bytes_per_key))
         self._q = deque()
         self._cv = threading.Condition()
         self._stop = False
+        self._reserved = 0  # bytes of growth admitted for batches in flight
         self.busy_s = 0.0
         self.batches = []
+        self.grown = 0  # batches admitted beyond their worker's warm capacity
         self._engines = [Engine(device) for _ in range(workers)]
+        self._cap = [self.batch_keys] * workers  # keys each worker's buffers fit
         if warm:  # size every worker's buffers for a full batch before serving
             sample = keys_mt19937_64(0x5EED, self.batch_keys)
             for e in self._engines:
                 for r in e.build_batch_u64(variant, leaf, [sample], bucket):
                     r.free()
             del sample
-        self._threads = [threading.Thread(target=self._worker, args=(e,), daemon=True) for e in self._engines]
+        self._threads = [threading.Thread(target=self._worker, args=(w, e), daemon=True)
+                         for w, e in enumerate(self._engines)]
         for t in self._threads:
             t.start()
 
@@ -86,25 +98,36 @@ class BuildServer:
             self._cv.notify()
         return req
 
-    def _take(self):
-        """Arrival-ordered prefix of the queue that fits one batch (at least one request)."""
+    def batch_limit(self, w):
+        """Keys worker `w` may take now: its capacity plus the growth the free device memory allows
+        (call with the lock held)."""
+        extra = max(0, int(self._free_memory() * self.mem_fraction) - self._reserved) // self.bytes_per_key
+        limit = self._cap[w] + extra
+        return min(limit, self.max_batch_keys) if self.max_batch_keys else limit
+
+    def _take(self, w):
+        """Arrival-ordered prefix of the queue that fits worker w's limit (at least one request), and
+        the bytes of growth it reserves."""
+        limit = self.batch_limit(w)
         batch, total = [], 0
         while self._q:
             n = len(self._q[0].keys)
-            if batch and total + n > self.batch_keys:
+            if batch and total + n > limit:
                 break
             batch.append(self._q.popleft())
             total += n
-        return batch
+        grow = max(0, total - self._cap[w]) * self.bytes_per_key
+        self._reserved += grow
+        return batch, total, grow
 
-    def _worker(self, eng):
+    def _worker(self, w, eng):
         while True:
             with self._cv:
                 while not self._q and not self._stop:
                     self._cv.wait()
                 if self._stop and not self._q:
                     return
-                batch = self._take()
+                batch, total, grow = self._take(w)
             t0 = time.perf_counter()
             for r in batch:
                 r.t_start = t0
@@ -117,7 +140,11 @@ class BuildServer:
             t1 = time.perf_counter()
             with self._cv:
                 self.busy_s += t1 - t0
-                self.batches.append((t0, t1, len(batch), sum(len(r.keys) for r in batch)))
+                self.batches.append((t0, t1, len(batch), total))
+                self._reserved -= grow
+                if total > self._cap[w]:
+                    self._cap[w] = total  # the engine's buffers now fit this batch
+                    self.grown += 1
             for r, res in zip(batch, results):
                 try:
                     r.t_done = t1
@@ -154,19 +181,25 @@ def poisson_stream(n_requests, rate=200.0, seed=31, lo_exp=3.0, hi_exp=7.0):
 
 
 def run_stream(stream, workers=2, leaf=64, bucket=2000, mem_fraction=0.5, max_batch_keys=32_000_000):
-    # every request's keys exist before the clock starts, as a client's would when it submits
-    all_keys = [keys_mt19937_64(kseed, size) for _, size, kseed in stream]
+    """Replay `stream` against a fresh server. Each request's keys are drawn just before it is
+    submitted (keys_mix of its sub-seed, on the host); it is submitted at its arrival time, or as
+    soon as its keys exist if drawing them ran past that time, and its latency runs from submission
+    to the end of its batch."""
     srv = BuildServer(leaf=leaf, bucket=bucket, workers=workers, mem_fraction=mem_fraction,
                       max_batch_keys=max_batch_keys, keep_results=False)
     reqs = []
+    late = 0.0
     t0 = time.perf_counter()
     for i, (at, size, kseed) in enumerate(stream):
-        keys = all_keys[i]
-        all_keys[i] = None
-        delay = t0 + at - time.perf_counter()
+        keys = keys_mix(kseed, size)
+        now = time.perf_counter()
+        delay = t0 + at - now
         if delay > 0:
             time.sleep(delay)
-        reqs.append(srv.submit(i, keys, t_arrival=t0 + at))
+        else:
+            late = max(late, -delay)
+        reqs.append(srv.submit(i, keys, t_arrival=max(t0 + at, now)))
+        del keys
     for r in reqs:
         r.wait()
     t_end = max(r.t_done for r in reqs)
@@ -176,6 +209,7 @@ def run_stream(stream, workers=2, leaf=64, bucket=2000, mem_fraction=0.5, max_ba
     span = t_end - t0
     return {
         "requests": len(reqs), "total_keys": int(total_keys), "workers": workers,
+        "max_submit_lag_ms": round(late * 1e3, 3), "batches_grown": srv.grown,
         "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
         "mean_ms": round(float(lat.mean()), 3), "max_ms": round(float(lat.max()), 3),
         "aggregate_keys_per_s": round(total_keys / span, 1), "wall_s": round(span, 3),
@@ -203,6 +237,7 @@ def main():
                 "config": {"variant": "ShockHash2", "leaf_size": args.leaf, "bucket_size": args.bucket,
                            "arrivals": f"Poisson, mean {args.rate}/s, seed {args.seed}",
                            "sizes": "round(10^(3+4u)) uint64 keys per request",
+                           "keys": "remix(sub_seed ^ j * 0x9E3779B97F4A7C15), drawn at submission",
                            "sample": f"first {args.requests} requests of the 10,000-request stream"}})
     print(json.dumps(out), flush=True)
 

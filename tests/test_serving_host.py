@@ -131,3 +131,54 @@ def test_poisson_stream_is_deterministic_and_in_range():
     assert min(sizes) >= 10 ** 3 and max(sizes) <= 10 ** 7
     assert 1.0 < arrivals[-1] < 5.0  # 500 arrivals at a mean of 200/s
     assert len({s for _, _, s in a}) == 500
+
+
+def test_admission_reads_free_memory_per_batch(fake):
+    free = {"bytes": 96 * 1000 * 2}  # half kept, one worker: a warm capacity of 1000 keys
+    srv = serve.BuildServer(workers=1, warm=False, max_batch_keys=0, free_memory=lambda: free["bytes"])
+    assert srv.batch_keys == 1000
+    # the device's free memory is gone: batches stay within the worker's capacity
+    fake.gate = threading.Event()
+    free["bytes"] = 0
+    blocker = srv.submit(0, _keys(10))
+    assert fake.entered.wait(5)
+    a = [srv.submit(1, _keys(600, 100)), srv.submit(2, _keys(600, 1000))]
+    fake.gate.set()
+    for r in [blocker] + a:
+        r.wait(5)
+    assert fake.batches == [[10], [600], [600]]
+    assert srv.grown == 0
+    # memory frees up: the next batch may grow the worker's buffers, once, by what is free now
+    fake.gate = threading.Event()
+    fake.entered = threading.Event()
+    free["bytes"] = 96 * 2000 * 2
+    blocker = srv.submit(3, _keys(10, 5000))
+    assert fake.entered.wait(5)
+    b = [srv.submit(4, _keys(600, 6000)), srv.submit(5, _keys(600, 7000))]
+    fake.gate.set()
+    for r in [blocker] + b:
+        r.wait(5)
+    srv.close()
+    assert fake.batches[3:] == [[10], [600, 600]]
+    assert srv.grown == 1 and srv._cap == [1200] and srv._reserved == 0
+
+
+def test_stream_draws_keys_at_submission(fake):
+    stream = serve.poisson_stream(20, rate=2000.0, seed=5, lo_exp=2.0, hi_exp=3.0)
+    out = serve.run_stream(stream, workers=2, max_batch_keys=2000)
+    assert out["requests"] == 20 and out["total_keys"] == sum(s for _, s, _ in stream)
+    served = fake.batches[2:]  # after one warm-up batch per worker
+    assert sorted(n for b in served for n in b) == sorted(s for _, s, _ in stream)
+    assert out["p99_ms"] >= out["p50_ms"] >= 0
+
+
+def test_request_keys_are_distinct_and_deterministic():
+    import shockhash_b200 as shg
+    a = shg.keys_mix(12345, 300_000, threads=4)
+    assert len(np.unique(a)) == len(a)
+    assert np.array_equal(a, shg.keys_mix(12345, 300_000, threads=1))
+    j = np.arange(5, dtype=np.uint64)
+    z = np.uint64(12345) ^ (j * np.uint64(0x9E3779B97F4A7C15))
+    z = (z ^ (z >> np.uint64(30))) * np.uint64(0xbf58476d1ce4e5b9)
+    z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94d049bb133111eb)
+    assert np.array_equal(a[:5], z ^ (z >> np.uint64(31)))
