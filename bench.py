@@ -64,7 +64,9 @@ def config_dict(args):
             "key_encoding": "each uint64 key hashed as its 8-byte little-endian string (SpookyV2-128, seed 0)",
             "l2": "inputs (10M keys: 80 MB keys, 160 MB fingerprints, 240 MB partition buffers) exceed the 126 MB L2, "
                   "and a 256 MB buffer is written before every timed step, outside the timing",
-            "parallelism": f"{args.gpus} independent bucket shards, no data-path collective"}
+            "parallelism": (f"one structure over {args.gpus} ranks: bucket-range shards after a device partition and "
+                            "an NCCL all-to-all of 16-byte fingerprints" if getattr(args, "sharded", False) else
+                            f"{args.gpus} independent bucket shards, no data-path collective")}
 
 
 class _Summary:
@@ -279,6 +281,9 @@ def main():
                     help="keys of the north-star size leg (0 skips it)")
     ap.add_argument("--serve-requests", type=int, default=int(os.environ.get("SHG_SERVE_REQUESTS", "400")),
                     help="requests of the serving leg (0 skips it)")
+    ap.add_argument("--sharded", action="store_true",
+                    help="build ONE structure over all ranks: every step exchanges the ranks' keys by bucket range "
+                         "(device partition + NCCL all-to-all) and builds each rank's buckets on its GPU")
     args = ap.parse_args()
     _workload(args)
     if args.impl == "reference":
@@ -310,8 +315,20 @@ def main():
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
+    args.sharded = args.sharded and ws > 1  # one rank: the sharded build is the plain build
+    if args.sharded:  # fingerprints of this rank's keys, device-resident (the exchange moves 16 B per key)
+        d_first = torch.empty(n, dtype=torch.int64, device=dev)
+        d_second = torch.empty(n, dtype=torch.int64, device=dev)
+        eng.hash_u64_device(d_keys.data_ptr(), n, d_first.data_ptr(), d_second.data_ptr())
+
     def step_device():
-        return eng.build_u64_device(VARIANT, LEAF, d_keys.data_ptr(), n, BUCKET, args.mode)
+        if not args.sharded:
+            return eng.build_u64_device(VARIANT, LEAF, d_keys.data_ptr(), n, BUCKET, args.mode)
+        from shockhash_b200 import shard
+        build = lambda f, s, nbg, b0, b1: eng.build_shard_hash128_device(VARIANT, LEAF, f.data_ptr(), s.data_ptr(),
+                                                                        f.numel(), nbg, b0, b1, BUCKET, args.mode)
+        part, _, _ = shard.build_sharded_tensors(build, d_first, d_second, BUCKET, engine=eng)
+        return part
 
     for _ in range(args.warmup):
         step_device().free()

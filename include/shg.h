@@ -141,6 +141,25 @@ shg_status shg_result_load(const char *path, shg_params *p, shg_result *out);
 shg_status shg_build_shard_hash128(shg_engine *e, const shg_params *p, const uint64_t *first,
                                    const uint64_t *second, uint64_t n, uint64_t nb_global, uint64_t b0,
                                    uint64_t b1, shg_result *out);
+/* Same with the fingerprints in DEVICE memory on the engine's device (the keys a rank received
+ * from the exchange stay on its GPU). */
+shg_status shg_build_shard_hash128_device(shg_engine *e, const shg_params *p, const uint64_t *d_first,
+                                          const uint64_t *d_second, uint64_t n, uint64_t nb_global, uint64_t b0,
+                                          uint64_t b1, shg_result *out);
+/* The 128-bit fingerprints of uint64 keys (each hashed as its 8-byte string, SpookyV2 seed 0) from
+ * and into DEVICE memory on the engine's device; synchronous. What a rank exchanges before a
+ * sharded build. */
+shg_status shg_hash_u64_device(shg_engine *e, const uint64_t *d_keys, uint64_t n, uint64_t *d_first, uint64_t *d_second);
+/* The send side of the exchange before a sharded build: every key's (first, second) pair written to
+ * pairs[2 i], pairs[2 i + 1] in owner-rank order, stable (input order inside a rank), with the key
+ * count per rank in counts[world]. Rank g of `world` owns buckets [floor(nb g / world),
+ * floor(nb (g + 1) / world)) of remap128(first, nb). shg_shard_partition runs on the host (host
+ * pointers); shg_shard_partition_device on the engine's device (device pointers; counts in host
+ * memory; synchronous). Both give the same order. 1 <= world <= 64, 1 <= nb < 2^32. */
+shg_status shg_shard_partition(const uint64_t *first, const uint64_t *second, uint64_t n, uint64_t nb, int world,
+                               uint64_t *pairs, uint64_t *counts);
+shg_status shg_shard_partition_device(shg_engine *e, const uint64_t *d_first, const uint64_t *d_second, uint64_t n,
+                                      uint64_t nb, int world, uint64_t *d_pairs, uint64_t *counts);
 shg_status shg_merge_shards(const shg_params *p, const shg_result *shards, uint64_t nshards, shg_result *out);
 
 /* Hash n string keys (bytes + offsets[n+1], host memory) to 128-bit fingerprints on the device:
@@ -333,6 +352,22 @@ int shg_int_peak_kind(int device, int kind, uint64_t iters, double *evals_per_s,
  * [5] bipartite leaves' candidate-scan mask-pair tests (for each raw seed, the earlier raw seeds
  * it is paired with), [6..7] zero. */
 shg_status shg_engine_last_work(const shg_engine *e, uint64_t *out, int n);
+
+/* Launch parameters of the search kernels per configuration (no counterpart in the reference; they
+ * change speed only, never a result). variant is an shg_variant (SHG_SHOCKHASH_ROTATION shares
+ * SHG_SHOCKHASH's entry) or 4 for ShockHash2Flat<k> with leaf_size = k. Names and ranges:
+ *   split_seeds_per_lane 1, 2, 4; split_threads 128, 256, 512; split_round_div 1..64 (a round of
+ *   seeds aims at 1/round_div of a split node's expected trials); leaf_blocks_per_sm 0..16 (0 =
+ *   as many as shared memory allows); leaf_min_blocks 4, 6, 8 (bipartite leaves up to 64 keys:
+ *   register bound); sh1_seeds_per_lane 1, 2 (original leaves).
+ * At creation an engine loads the table shockhash_b200/tuning.tsv beside the library (or the file
+ * named by the SHG_TUNING_TABLE environment variable; empty = none), written by the autotuner
+ * (python -m shockhash_b200.tune); lines "<variant> <leaf> <name> <value>", '#' comments. */
+shg_status shg_engine_set_tuning(shg_engine *e, int variant, int leaf_size, const char *name, int64_t value);
+shg_status shg_engine_get_tuning(shg_engine *e, int variant, int leaf_size, const char *name, int64_t *value);
+shg_status shg_engine_load_tuning(shg_engine *e, const char *path);
+/* Path of the table the engine loaded ("" if none). */
+const char *shg_engine_tuning_source(const shg_engine *e);
 
 /* Free and total device memory (cudaMemGetInfo), for admission control. */
 shg_status shg_device_memory(int device, uint64_t *free_bytes, uint64_t *total_bytes);

@@ -94,6 +94,10 @@ def lib():
         "shg_result_load": ([ctypes.c_char_p, P, R], ctypes.c_int),
         "shg_build_batch_u64": ([_vp, P, _vp, _vp, _u64, _vp], ctypes.c_int),
         "shg_build_shard_hash128": ([_vp, P, _vp, _vp, _u64, _u64, _u64, _u64, R], ctypes.c_int),
+        "shg_build_shard_hash128_device": ([_vp, P, _vp, _vp, _u64, _u64, _u64, _u64, R], ctypes.c_int),
+        "shg_shard_partition": ([_vp, _vp, _u64, _u64, ctypes.c_int, _vp, _vp], ctypes.c_int),
+        "shg_hash_u64_device": ([_vp, _vp, _u64, _vp, _vp], ctypes.c_int),
+        "shg_shard_partition_device": ([_vp, _vp, _vp, _u64, _u64, ctypes.c_int, _vp, _vp], ctypes.c_int),
         "shg_merge_shards": ([P, _vp, _u64, R], ctypes.c_int),
         "shg_hash_strings": ([_vp, ctypes.c_char_p, _vp, _u64, _vp, _vp], ctypes.c_int),
         "shg_sh2_construct_leaves": ([_vp, _vp, _vp, _u64, _vp, _vp], ctypes.c_int),
@@ -147,6 +151,11 @@ def lib():
         "shg_retrieval_query_ms": ([_vp], ctypes.c_float),
         "shg_device_memory": ([ctypes.c_int, ctypes.POINTER(_u64), ctypes.POINTER(_u64)], ctypes.c_int),
         "shg_engine_last_work": ([_vp, _vp, ctypes.c_int], ctypes.c_int),
+        "shg_engine_set_tuning": ([_vp, ctypes.c_int, ctypes.c_int, ctypes.c_char_p, ctypes.c_int64], ctypes.c_int),
+        "shg_engine_get_tuning": ([_vp, ctypes.c_int, ctypes.c_int, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)],
+                                  ctypes.c_int),
+        "shg_engine_load_tuning": ([_vp, ctypes.c_char_p], ctypes.c_int),
+        "shg_engine_tuning_source": ([_vp], ctypes.c_char_p),
         "shg_keys_mt19937_64": ([_u64, _u64, _vp], None),
         "shg_keys_mix": ([_u64, _u64, _vp, ctypes.c_int], None),
         "shg_int_peak": ([ctypes.c_int, _u64, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)],
@@ -216,6 +225,11 @@ def int_peak(device=0, iters=1 << 16, kind=0):
 
 
 SPLIT_KINDS = ("thresholds_1", "thresholds_2", "thresholds_3", "quarter_moments")
+# Launch parameters of the search kernels (shg_engine_set_tuning); FLAT is the tuning table's
+# variant key of ShockHash2Flat<k>.
+TUNING_PARAMS = ("split_seeds_per_lane", "split_threads", "split_round_div", "leaf_blocks_per_sm", "leaf_min_blocks",
+                 "sh1_seeds_per_lane")
+TUNING_FLAT = 4
 
 
 def split_peaks(device=0, iters=1 << 15):
@@ -335,6 +349,27 @@ class Engine:
         except Exception:
             pass
 
+    def set_tuning(self, variant, leaf_size, **params):
+        """Set launch parameters of one configuration (names in TUNING_PARAMS; speed only)."""
+        for name, v in params.items():
+            _check(lib().shg_engine_set_tuning(self._h, variant, leaf_size, name.encode(), int(v)))
+
+    def get_tuning(self, variant, leaf_size):
+        """The launch parameters this engine uses for a configuration, as a dict."""
+        out = {}
+        for name in TUNING_PARAMS:
+            v = ctypes.c_int64()
+            _check(lib().shg_engine_get_tuning(self._h, variant, leaf_size, name.encode(), ctypes.byref(v)))
+            out[name] = int(v.value)
+        return out
+
+    def load_tuning(self, path):
+        _check(lib().shg_engine_load_tuning(self._h, os.fsencode(path)))
+
+    def tuning_source(self):
+        """Path of the tuning table loaded at creation ("" if none)."""
+        return lib().shg_engine_tuning_source(self._h).decode()
+
     def last_work(self):
         """Work counts of this engine's last build beyond BuildResult.work: useful split evaluations
         by inner loop (SPLIT_KINDS), split level launches, bipartite candidate-scan mask tests."""
@@ -397,6 +432,18 @@ class Engine:
         p, res = self.params(variant, leaf_size, bucket_size, mode, 0), _Result()
         st = lib().shg_build_shard_hash128(self._h, ctypes.byref(p), _ptr(first), _ptr(second), len(first), nb_global,
                                            b0, b1, ctypes.byref(res))
+        return self._finish(p, st, res)
+
+    def hash_u64_device(self, d_keys_ptr, n, d_first_ptr, d_second_ptr):
+        """Fingerprints of n device-resident uint64 keys into device buffers (synchronous)."""
+        _check(lib().shg_hash_u64_device(self._h, _vp(d_keys_ptr), n, _vp(d_first_ptr), _vp(d_second_ptr)))
+
+    def build_shard_hash128_device(self, variant, leaf_size, d_first_ptr, d_second_ptr, n, nb_global, b0, b1,
+                                   bucket_size=2000, mode=MODE_DEFAULT):
+        """build_shard_hash128 with the fingerprints in device memory (pointers on the engine's device)."""
+        p, res = self.params(variant, leaf_size, bucket_size, mode, 0), _Result()
+        st = lib().shg_build_shard_hash128_device(self._h, ctypes.byref(p), _vp(d_first_ptr), _vp(d_second_ptr), n,
+                                                  nb_global, b0, b1, ctypes.byref(res))
         return self._finish(p, st, res)
 
     def build_u64_device(self, variant, leaf_size, d_keys_ptr, n, bucket_size=2000, mode=MODE_DEFAULT):

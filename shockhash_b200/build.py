@@ -59,7 +59,7 @@ def build(verbose=False, force=False, jobs=8):
     if failed:
         raise RuntimeError("nvcc failed")
     if force or _stale([LIB], objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-ldl"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.check_call(cmd)

@@ -13,9 +13,11 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
+#include <dlfcn.h>
 #include <cuda_runtime.h>
 #include "shg.h"
 #include "shg_common.cuh"
@@ -25,11 +27,12 @@ namespace shg {
 uint64_t sh2_scratch_bytes(uint32_t smax, uint32_t cmax, int max_leaf);
 void launch_leaves_sh1_ctr(const Node *nodes, const uint32_t *ids, uint32_t count, const uint64_t *keys, uint64_t *codes,
                            uint64_t *rib_keys, uint8_t *rib_bits, uint64_t max_trials, uint32_t *err,
-                           unsigned long long *work, unsigned int *ctr, int grid, cudaStream_t s, uint32_t rot_leaf = 0);
+                           unsigned long long *work, unsigned int *ctr, int grid, cudaStream_t s, uint32_t rot_leaf = 0,
+                           int spl = 2);
 void launch_leaves_sh2_ctr(const Node *nodes, const uint32_t *ids, uint32_t count, const uint64_t *keys, uint64_t *codes,
                            uint8_t *rib_bits, uint8_t *scratch, uint64_t scratch_per_warp, uint32_t smax, uint32_t cmax,
                            uint32_t *err, unsigned long long *work, unsigned int *ctr, int grid, cudaStream_t s,
-                           int max_leaf, uint32_t quad_min = kQuadMinRecSplit);
+                           int max_leaf, uint32_t quad_min = kQuadMinRecSplit, int minb = 6);
 int sh2_smem_per_warp(int max_leaf);
 int leaves_sh1_warps_per_block();
 } // namespace shg
@@ -133,6 +136,16 @@ struct shg_engine {
     int pipe_chunks = 8;
     unsigned long long split_kind[4] = {};  // of the last build (shg_engine_last_work)
     uint64_t split_launches = 0, leaf_scan = 0;
+    // launch parameters per configuration (variant, leaf size); absent = the Tuning defaults
+    std::map<std::pair<int, int>, Tuning> tuning;
+    std::mutex tuning_mu;
+    std::string tuning_source;  // the table file loaded at creation, or ""
+    Tuning tuning_of(int variant, int leaf) {
+        std::lock_guard<std::mutex> lock(tuning_mu);
+        if (variant == SHG_SHOCKHASH_ROTATION) variant = SHG_SHOCKHASH;  // same searches
+        auto it = tuning.find({variant, leaf});
+        return it == tuning.end() ? Tuning() : it->second;
+    }
     ~shg_engine() {
         DevBuf *all[] = {&in_keys, &in_bytes, &in_offsets, &first, &second, &sfirst, &sidx, &counts, &cursor,
                          &acc, &keys, &nodes, &ids, &codes, &fixed_off, &bucket_bits, &pos_acc, &words,
@@ -460,21 +473,25 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
     const uint32_t smax = maxm > 64 ? 16384 : 4096, cmax = maxm > 64 ? 16384 : 2048;
     const uint64_t per_warp = (sh2_scratch_bytes(smax, cmax, maxm) + 255) & ~255ull;
     int leaf_grid;
+    const Tuning tun = e->tuning_of(p->variant, p->leaf_size);
     if (sh2) {
         const int per_block_smem = 4 * sh2_smem_per_warp(maxm);
-        const int blocks_per_sm = std::max(1, std::min(8, (228 * 1024) / (per_block_smem + 1024)));
+        int blocks_per_sm = std::max(1, std::min(8, (228 * 1024) / (per_block_smem + 1024)));
+        if (tun.leaf_bps > 0) blocks_per_sm = std::min(blocks_per_sm, tun.leaf_bps);
         // next to running split launches, leaves take part of each SM (the splits are ALU bound,
         // the leaves latency bound, so the two interleave)
         const int bps = pipelined ? std::max(1, blocks_per_sm / 2) : blocks_per_sm;
         leaf_grid = p->mode == SHG_MODE_PER_LEAF ? 1 : std::max(1, std::min<int>(e->sms * bps, (int)((nleaves + 3) / 4)));
     } else {
         const int wpb = leaves_sh1_warps_per_block();
-        leaf_grid = std::max(1, std::min<int>(e->sms * (pipelined ? 4 : 8), (int)((nleaves + wpb - 1) / wpb)));
+        const int bps = tun.leaf_bps > 0 ? tun.leaf_bps : 8;
+        leaf_grid = std::max(1, std::min<int>(e->sms * (pipelined ? std::max(1, bps / 2) : bps), (int)((nleaves + wpb - 1) / wpb)));
     }
     auto split_range = [&](size_t lv, uint64_t a, uint64_t b, cudaStream_t st) {
         if (b <= a) return;
         launch_split_level(e->nodes.as<Node>(), d_ids + level_off[lv] + a, (uint32_t)(b - a), e->keys.as<uint64_t>(),
-                           e->codes.as<uint64_t>(), p->max_trials, &misc->err, &misc->work[0], misc->split_kind, st);
+                           e->codes.as<uint64_t>(), p->max_trials, &misc->err, &misc->work[0], misc->split_kind, tun.split,
+                           st);
         launches++;
     };
     auto leaf_range = [&](uint64_t a, uint64_t b, cudaStream_t st, int grid) {
@@ -482,12 +499,13 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
         if (sh2)
             launch_leaves_sh2_ctr(e->nodes.as<Node>(), d_ids + leaf_off + a, (uint32_t)(b - a), e->keys.as<uint64_t>(),
                                   e->codes.as<uint64_t>(), e->rib_bits.as<uint8_t>(), e->scratch.as<uint8_t>(), per_warp, smax,
-                                  cmax, &misc->err, misc->work, &misc->leaf_ctr, grid, st, maxm);
+                                  cmax, &misc->err, misc->work, &misc->leaf_ctr, grid, st, maxm, kQuadMinRecSplit,
+                                  tun.leaf_minb);
         else
             launch_leaves_sh1_ctr(e->nodes.as<Node>(), d_ids + leaf_off + a, (uint32_t)(b - a), e->keys.as<uint64_t>(),
                                   e->codes.as<uint64_t>(), e->rib_keys.as<uint64_t>(), e->rib_bits.as<uint8_t>(), p->max_trials,
                                   &misc->err, misc->work, &misc->leaf_ctr, grid, st,
-                                  p->variant == SHG_SHOCKHASH_ROTATION ? (uint32_t)p->leaf_size : 0);
+                                  p->variant == SHG_SHOCKHASH_ROTATION ? (uint32_t)p->leaf_size : 0, tun.sh1_spl);
         launches++;
     };
     if (pipelined) {
@@ -874,12 +892,14 @@ shg_status build_flat(shg_engine *e, uint64_t k, const char *bytes, const uint64
         CU(cudaMemcpyAsync(e->f_ids.p, ids.data(), nbuckets * 4, cudaMemcpyHostToDevice, s));
         const uint32_t smax = k > 64 ? 16384 : 4096, cmax = k > 64 ? 16384 : 2048;
         const uint64_t per_warp = (sh2_scratch_bytes(smax, cmax, (int)k) + 255) & ~255ull;
-        const int bps = std::max(1, std::min(8, (228 * 1024) / (4 * sh2_smem_per_warp((int)k) + 1024)));
+        const Tuning ftun = e->tuning_of(kTuningFlat, (int)k);
+        int bps = std::max(1, std::min(8, (228 * 1024) / (4 * sh2_smem_per_warp((int)k) + 1024)));
+        if (ftun.leaf_bps > 0) bps = std::min(bps, ftun.leaf_bps);
         const int grid = std::max(1, std::min<int>(e->sms * bps, (int)((nbuckets + 3) / 4)));
         CU(e->scratch.ensure(per_warp * (uint64_t)grid * 4));
         launch_leaves_sh2_ctr(e->f_nodes.as<Node>(), e->f_ids.as<uint32_t>(), (uint32_t)nbuckets, e->f_leaf_keys.as<uint64_t>(),
                               e->f_codes.as<uint64_t>(), e->f_bits.as<uint8_t>(), e->scratch.as<uint8_t>(), per_warp, smax, cmax,
-                              &misc->err, misc->work, &misc->leaf_ctr, grid, s, (int)k, kQuadMinFlat);
+                              &misc->err, misc->work, &misc->leaf_ctr, grid, s, (int)k, kQuadMinFlat, ftun.leaf_minb);
         CU(cudaGetLastError());
     }
     uint32_t err = 0;
@@ -960,6 +980,85 @@ void *engine_scratch(shg_engine *e, int slot, size_t bytes, cudaError_t &err) {
 
 extern "C" {
 
+// ------------------------------------------------------------------ tuning table
+// One parameter per line: "<variant> <leaf size> <name> <value>" (variant as shg_variant, or 4 for
+// ShockHash2Flat<k>); '#' starts a comment. Unknown names or out-of-range values reject the file.
+static shg_status set_tuning(shg_engine *e, int variant, int leaf, const std::string &name, int64_t v) {
+    if (variant < 1 || variant > kTuningFlat || leaf < 1 || leaf > kMaxLeaf2)
+        return fail(SHG_ERR_ARG, "tuning: no configuration variant " + std::to_string(variant) + " leaf " + std::to_string(leaf));
+    if (variant == SHG_SHOCKHASH_ROTATION) variant = SHG_SHOCKHASH;
+    std::lock_guard<std::mutex> lock(e->tuning_mu);
+    Tuning t = e->tuning.count({variant, leaf}) ? e->tuning[{variant, leaf}] : Tuning();
+    if (name == "split_seeds_per_lane") t.split.spl = (int)v;
+    else if (name == "split_threads") t.split.threads = (int)v;
+    else if (name == "split_round_div") t.split.round_div = (int)v;
+    else if (name == "leaf_blocks_per_sm" && v >= 0 && v <= 16) t.leaf_bps = (int)v;
+    else if (name == "leaf_min_blocks" && (v == 4 || v == 6 || v == 8)) t.leaf_minb = (int)v;
+    else if (name == "sh1_seeds_per_lane" && (v == 1 || v == 2)) t.sh1_spl = (int)v;
+    else return fail(SHG_ERR_ARG, "tuning: bad parameter " + name + " = " + std::to_string(v));
+    if (!split_tuning_valid(t.split.spl, t.split.threads, t.split.round_div))
+        return fail(SHG_ERR_ARG, "tuning: bad parameter " + name + " = " + std::to_string(v));
+    e->tuning[{variant, leaf}] = t;
+    return SHG_OK;
+}
+
+static shg_status load_tuning(shg_engine *e, const char *path) {
+    FILE *f = fopen(path, "r");
+    if (!f) return fail(SHG_ERR_ARG, std::string("tuning: cannot open ") + path);
+    char line[512];
+    shg_status st = SHG_OK;
+    while (st == SHG_OK && fgets(line, sizeof line, f)) {
+        if (char *hash = strchr(line, '#')) *hash = 0;
+        int variant = 0, leaf = 0;
+        char name[128];
+        long long v = 0;
+        const int got = sscanf(line, "%d %d %127s %lld", &variant, &leaf, name, &v);
+        if (got <= 0) continue;  // blank or comment
+        st = got == 4 ? set_tuning(e, variant, leaf, name, v) : fail(SHG_ERR_ARG, std::string("tuning: malformed line in ") + path);
+    }
+    fclose(f);
+    if (st == SHG_OK) e->tuning_source = path;
+    return st;
+}
+
+// The table next to the package (shockhash_b200/tuning.tsv beside _lib/libshg.so), or the file
+// named by SHG_TUNING_TABLE (empty: none).
+static std::string default_tuning_path() {
+    if (const char *env = getenv("SHG_TUNING_TABLE")) return env;
+    Dl_info info;
+    if (!dladdr((void *)&default_tuning_path, &info) || !info.dli_fname) return "";
+    std::string so = info.dli_fname;
+    const size_t slash = so.rfind('/');
+    const std::string dir = slash == std::string::npos ? "." : so.substr(0, slash);
+    return dir + "/../tuning.tsv";
+}
+
+shg_status shg_engine_set_tuning(shg_engine *e, int variant, int leaf_size, const char *name, int64_t value) {
+    if (!e || !name) return fail(SHG_ERR_ARG, "null argument");
+    return set_tuning(e, variant, leaf_size, name, value);
+}
+
+shg_status shg_engine_get_tuning(shg_engine *e, int variant, int leaf_size, const char *name, int64_t *value) {
+    if (!e || !name || !value) return fail(SHG_ERR_ARG, "null argument");
+    const Tuning t = e->tuning_of(variant, leaf_size);
+    const std::string n = name;
+    if (n == "split_seeds_per_lane") *value = t.split.spl;
+    else if (n == "split_threads") *value = t.split.threads;
+    else if (n == "split_round_div") *value = t.split.round_div;
+    else if (n == "leaf_blocks_per_sm") *value = t.leaf_bps;
+    else if (n == "leaf_min_blocks") *value = t.leaf_minb;
+    else if (n == "sh1_seeds_per_lane") *value = t.sh1_spl;
+    else return fail(SHG_ERR_ARG, "tuning: unknown parameter " + n);
+    return SHG_OK;
+}
+
+shg_status shg_engine_load_tuning(shg_engine *e, const char *path) {
+    if (!e || !path) return fail(SHG_ERR_ARG, "null argument");
+    return load_tuning(e, path);
+}
+
+const char *shg_engine_tuning_source(const shg_engine *e) { return e ? e->tuning_source.c_str() : ""; }
+
 shg_status shg_engine_create(int device, shg_engine **out) {
     if (!out) return fail(SHG_ERR_ARG, "null output");
     *out = nullptr;
@@ -985,6 +1084,17 @@ shg_status shg_engine_create(int device, shg_engine **out) {
         return fail(SHG_ERR_CUDA, "stream creation failed");
     }
     if (const char *c = getenv("SHG_PIPE_CHUNKS")) e->pipe_chunks = std::max(1, std::min(shg_engine::kMaxChunks, atoi(c)));
+    const std::string tpath = default_tuning_path();
+    if (!tpath.empty()) {
+        if (FILE *f = fopen(tpath.c_str(), "r")) {  // a table that exists must be valid
+            fclose(f);
+            const shg_status st = load_tuning(e, tpath.c_str());
+            if (st != SHG_OK) {
+                delete e;
+                return st;
+            }
+        }
+    }
     *out = e;
     return SHG_OK;
 }
@@ -1051,6 +1161,28 @@ shg_status shg_build_shard_hash128(shg_engine *e, const shg_params *p, const uin
     }
     const ShardSpec shard{nb_global, b0, b1};
     return build_batch(e, p, e->first.as<uint64_t>(), e->second.as<uint64_t>(), std::vector<uint64_t>{n}, out, 0.f, &shard);
+}
+
+shg_status shg_hash_u64_device(shg_engine *e, const uint64_t *d_keys, uint64_t n, uint64_t *d_first, uint64_t *d_second) {
+    if (!e || (n && (!d_keys || !d_first || !d_second))) return fail(SHG_ERR_ARG, "null argument");
+    if (!n) return SHG_OK;
+    CU(cudaSetDevice(e->device));
+    launch_spooky_u64(d_keys, n, d_first, d_second, e->stream);
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(e->stream));
+    return SHG_OK;
+}
+
+shg_status shg_build_shard_hash128_device(shg_engine *e, const shg_params *p, const uint64_t *d_first,
+                                          const uint64_t *d_second, uint64_t n, uint64_t nb_global, uint64_t b0,
+                                          uint64_t b1, shg_result *out) {
+    if (!e || !out || (n && (!d_first || !d_second))) return fail(SHG_ERR_ARG, "null argument");
+    if (b0 >= b1 || b1 > nb_global) return fail(SHG_ERR_ARG, "bucket range must satisfy b0 < b1 <= nb_global");
+    shg_status st = check_params(p, n);
+    if (st) return st;
+    CU(cudaSetDevice(e->device));
+    const ShardSpec shard{nb_global, b0, b1};
+    return build_batch(e, p, d_first, d_second, std::vector<uint64_t>{n}, out, 0.f, &shard);
 }
 
 // On-disk form of a build result (no counterpart in the reference classes, which persist only the

@@ -134,11 +134,27 @@ void launch_bucket_scatter(const uint64_t *first, uint64_t n, uint64_t nb, uint6
                            uint64_t *sfirst, uint32_t *sidx, uint64_t idx_base, cudaStream_t s);
 void launch_bucket_sort(const uint64_t *acc, uint64_t nb, const uint64_t *sfirst, const uint32_t *sidx,
                         const uint64_t *second, uint64_t *keys, cudaStream_t s);
+// Speed-only launch parameters of the search kernels for one configuration (variant, leaf size):
+// every choice gives identical results. The defaults are the untuned values; a tuning table
+// (shg_engine_load_tuning) replaces them per configuration.
+struct SplitTuning {
+    int spl = 2;         // seeds per lane: 1, 2 or 4
+    int threads = 256;   // threads per split block (one node per block): 128, 256 or 512
+    int round_div = 8;   // warp groups make a round about 1/round_div of a node's expected trials (1..64)
+};
+struct Tuning {
+    SplitTuning split;
+    int leaf_bps = 0;    // leaf grid in blocks per SM (0: as many as shared memory allows, at most 8)
+    int leaf_minb = 6;   // bipartite leaves of up to 64 keys: launch bound of 4, 6 or 8 blocks per SM
+    int sh1_spl = 2;     // original leaves: seeds per lane, 1 or 2
+};
+bool split_tuning_valid(int spl, int threads, int round_div);
+constexpr int kTuningFlat = 4;  // tuning-table variant key of ShockHash2Flat<k> (leaf size = k)
 // work[0] += useful evaluations; kind_work[k] += the same per inner loop (k = compared thresholds
 // - 1, or 3 for quarter-split moments)
 void launch_split_level(const Node *nodes, const uint32_t *ids, uint32_t count, uint64_t *keys,
                         uint64_t *codes, uint64_t max_trials, uint32_t *err, unsigned long long *work,
-                        unsigned long long *kind_work, cudaStream_t s);
+                        unsigned long long *kind_work, const SplitTuning &t, cudaStream_t s);
 int leaves_sh1_warps_per_block();
 // Inner-loop peaks of the bipartite leaf search (kind 0 scan, 1 pair filter, 2 pseudoforest edges),
 // 256-thread blocks; operations per thread and iteration from sh2_op_peak_per_iter.

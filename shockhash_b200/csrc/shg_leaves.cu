@@ -1,7 +1,7 @@
 // ShockHash leaf searches, one warp per leaf, leaves pulled from a device counter.
 //
-// Original ShockHash (ShockHash.h:404-434): lanes take consecutive seeds x (two per lane, x and
-// x + 32, per round of 64); a lane's seed passes
+// Original ShockHash (ShockHash.h:404-434): lanes take consecutive seeds x (SPL per lane, x, x + 32,
+// ..., per round of 32 * SPL); a lane's seed passes
 // when the two candidate cells of all m keys cover all m cells (64-bit OR) and the cuckoo graph
 // (cells = vertices, keys = edges) is a pseudoforest. The pseudoforest test is a per-lane
 // union-find with a cycle flag per root; the reference inserts into a cuckoo table instead, and
@@ -211,6 +211,8 @@ __device__ bool rotation_leaf(Sh1WarpSmem &sm, uint16_t *cells, LaneUF &uf, int 
     return false;
 }
 
+// SPL: seeds per lane and round (1 or 2; a tuning parameter, the same seed is found either way).
+template <int SPL>
 __global__ void __launch_bounds__(kLeafWarps * 32) k_leaves_sh1(const Node *__restrict__ nodes, const uint32_t *__restrict__ ids,
                                                                 uint32_t count, const uint64_t *__restrict__ keys,
                                                                 uint64_t *__restrict__ codes, uint64_t *__restrict__ rib_keys,
@@ -281,31 +283,35 @@ __global__ void __launch_bounds__(kLeafWarps * 32) k_leaves_sh1(const Node *__re
             }
             return ok;
         };
-        // Two seeds per lane (x and x + 32): one shared-memory key read feeds two evaluations.
-        for (uint64_t base = 0; base < cap; base += 64) {
-            const uint64_t xa = seed0 + base + lane, xb = xa + 32;
-            uint32_t a1 = 0, a2 = 0, b1 = 0, b2 = 0;
+        // SPL seeds per lane (x, x + 32, ...): one shared-memory key read feeds SPL evaluations.
+        for (uint64_t base = 0; base < cap && found == ~0ull; base += 32 * SPL) {
+            uint32_t c1m[SPL], c2m[SPL];
+#pragma unroll
+            for (int t = 0; t < SPL; t++) c1m[t] = c2m[t] = 0;
             for (uint32_t k = 0; k < m; k++) {
                 const uint64_t key = sm.keys[k];
-                const uint64_t ra = remix(key + xa), rb = remix(key + xb);
-                a1 |= 1u << fastrange32((uint32_t)ra, h1);
-                a2 |= 1u << fastrange32((uint32_t)(ra >> 32), h2);
-                b1 |= 1u << fastrange32((uint32_t)rb, h1);
-                b2 |= 1u << fastrange32((uint32_t)(rb >> 32), h2);
-            }
-            bool oka = a1 == all1 && a2 == all2, okb = b1 == all1 && b2 == all2;
-            if (__any_sync(0xffffffffu, oka || okb)) {
-                if (oka) oka = pseudoforest(xa);
-                unsigned bal = __ballot_sync(0xffffffffu, oka);
-                if (bal) {
-                    found = base + (__ffs(bal) - 1);
-                    break;
+#pragma unroll
+                for (int t = 0; t < SPL; t++) {
+                    const uint64_t r = remix(key + seed0 + base + lane + 32 * t);
+                    c1m[t] |= 1u << fastrange32((uint32_t)r, h1);
+                    c2m[t] |= 1u << fastrange32((uint32_t)(r >> 32), h2);
                 }
-                if (okb) okb = pseudoforest(xb);
-                bal = __ballot_sync(0xffffffffu, okb);
-                if (bal) {
-                    found = base + 32 + (__ffs(bal) - 1);
-                    break;
+            }
+            bool ok[SPL], any = false;
+#pragma unroll
+            for (int t = 0; t < SPL; t++) {
+                ok[t] = c1m[t] == all1 && c2m[t] == all2;
+                any |= ok[t];
+            }
+            if (__any_sync(0xffffffffu, any)) {
+#pragma unroll
+                for (int t = 0; t < SPL; t++) {  // seeds in order: all lanes' x + 32 t before x + 32 (t + 1)
+                    bool pass = ok[t] && pseudoforest(seed0 + base + lane + 32 * t);
+                    const unsigned bal = __ballot_sync(0xffffffffu, pass);
+                    if (bal) {
+                        found = base + 32 * t + (__ffs(bal) - 1);
+                        break;
+                    }
                 }
             }
         }
@@ -343,12 +349,17 @@ int leaves_sh1_warps_per_block() { return kLeafWarps; }
 
 void launch_leaves_sh1_ctr(const Node *nodes, const uint32_t *ids, uint32_t count, const uint64_t *keys, uint64_t *codes,
                            uint64_t *rib_keys, uint8_t *rib_bits, uint64_t max_trials, uint32_t *err,
-                           unsigned long long *work, unsigned int *ctr, int grid, cudaStream_t s, uint32_t rot_leaf) {
+                           unsigned long long *work, unsigned int *ctr, int grid, cudaStream_t s, uint32_t rot_leaf,
+                           int spl) {
     if (!count) return;
     cudaMemsetAsync(ctr, 0, sizeof(unsigned int), s);
     const size_t dyn = rot_leaf ? (size_t)kLeafWarps * 64 * 32 * sizeof(uint16_t) : 0;  // 16 KB per block
-    k_leaves_sh1<<<grid, kLeafWarps * 32, dyn, s>>>(nodes, ids, count, keys, codes, rib_keys, rib_bits, max_trials, err,
-                                                    work, ctr, rot_leaf);
+    if (spl == 1)
+        k_leaves_sh1<1><<<grid, kLeafWarps * 32, dyn, s>>>(nodes, ids, count, keys, codes, rib_keys, rib_bits, max_trials,
+                                                           err, work, ctr, rot_leaf);
+    else
+        k_leaves_sh1<2><<<grid, kLeafWarps * 32, dyn, s>>>(nodes, ids, count, keys, codes, rib_keys, rib_bits, max_trials,
+                                                           err, work, ctr, rot_leaf);
 }
 
 } // namespace shg

@@ -232,8 +232,10 @@ template <int MAXM> struct OffsetLeaves {
     }
 };
 
-template <int MAXM, class Src>
-__global__ void __launch_bounds__(128, MAXM <= 64 ? 6 : 1) k_leaves_sh2_v2(Src src, uint32_t count, const uint64_t *__restrict__ keys,
+// MINB: blocks per SM the register allocation is bounded for (a tuning parameter; any value gives
+// the same results).
+template <int MAXM, class Src, int MINB = (MAXM <= 64 ? 6 : 1)>
+__global__ void __launch_bounds__(128, MINB) k_leaves_sh2_v2(Src src, uint32_t count, const uint64_t *__restrict__ keys,
                                                        uint8_t *__restrict__ rib_bits,
                                                        uint8_t *__restrict__ scratch, uint64_t scratch_per_warp,
                                                        uint32_t smax, uint32_t cmax, uint32_t *__restrict__ err,
@@ -660,16 +662,17 @@ __global__ void __launch_bounds__(128, MAXM <= 64 ? 6 : 1) k_leaves_sh2_v2(Src s
     }
 }
 
-template <int MAXM>
+template <int MAXM, int MINB>
 void launch_v2(const Node *nodes, const uint32_t *ids, uint32_t count, const uint64_t *keys, uint64_t *codes,
                uint8_t *rib_bits, uint8_t *scratch, uint64_t scratch_per_warp, uint32_t smax, uint32_t cmax,
                uint32_t *err, unsigned long long *work, unsigned int *ctr, int grid, cudaStream_t s, uint32_t quad_min) {
     const size_t smem = sizeof(Sh2Smem<MAXM>) * 4;
     // The shared-memory limit is an attribute of the kernel on the current device: set it on every
     // launch (a cheap host call), so engines on several devices and threads each get it.
-    cudaFuncSetAttribute(k_leaves_sh2_v2<MAXM, NodeLeaves>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_leaves_sh2_v2<MAXM, NodeLeaves><<<grid, 128, smem, s>>>(NodeLeaves{nodes, ids, codes}, count, keys, rib_bits, scratch,
-                                                              scratch_per_warp, smax, cmax, err, work, ctr, quad_min);
+    cudaFuncSetAttribute(k_leaves_sh2_v2<MAXM, NodeLeaves, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_leaves_sh2_v2<MAXM, NodeLeaves, MINB><<<grid, 128, smem, s>>>(NodeLeaves{nodes, ids, codes}, count, keys, rib_bits,
+                                                                    scratch, scratch_per_warp, smax, cmax, err, work, ctr,
+                                                                    quad_min);
 }
 
 } // namespace
@@ -684,15 +687,21 @@ uint64_t sh2_scratch_bytes(uint32_t smax, uint32_t cmax, int max_leaf) {
 void launch_leaves_sh2_ctr(const Node *nodes, const uint32_t *ids, uint32_t count, const uint64_t *keys, uint64_t *codes,
                            uint8_t *rib_bits, uint8_t *scratch, uint64_t scratch_per_warp, uint32_t smax, uint32_t cmax,
                            uint32_t *err, unsigned long long *work, unsigned int *ctr, int grid, cudaStream_t s,
-                           int max_leaf, uint32_t quad_min) {
+                           int max_leaf, uint32_t quad_min, int minb) {
     if (!count) return;
     cudaMemsetAsync(ctr, 0, sizeof(unsigned int), s);
-    if (max_leaf <= 64)
-        launch_v2<64>(nodes, ids, count, keys, codes, rib_bits, scratch, scratch_per_warp, smax, cmax, err, work, ctr, grid, s,
-                      quad_min);
+    if (max_leaf > 64)
+        launch_v2<128, 1>(nodes, ids, count, keys, codes, rib_bits, scratch, scratch_per_warp, smax, cmax, err, work, ctr, grid,
+                          s, quad_min);
+    else if (minb == 4)
+        launch_v2<64, 4>(nodes, ids, count, keys, codes, rib_bits, scratch, scratch_per_warp, smax, cmax, err, work, ctr, grid,
+                         s, quad_min);
+    else if (minb == 8)
+        launch_v2<64, 8>(nodes, ids, count, keys, codes, rib_bits, scratch, scratch_per_warp, smax, cmax, err, work, ctr, grid,
+                         s, quad_min);
     else
-        launch_v2<128>(nodes, ids, count, keys, codes, rib_bits, scratch, scratch_per_warp, smax, cmax, err, work, ctr, grid, s,
-                       quad_min);
+        launch_v2<64, 6>(nodes, ids, count, keys, codes, rib_bits, scratch, scratch_per_warp, smax, cmax, err, work, ctr, grid,
+                         s, quad_min);
 }
 
 int sh2_smem_per_warp(int max_leaf) { return max_leaf <= 64 ? (int)sizeof(Sh2Smem<64>) : (int)sizeof(Sh2Smem<128>); }

@@ -1,7 +1,7 @@
 // RecSplit split-seed search and stable partition (ShockHash.h:451-547, ShockHash2.h:290-386).
 //
 // One thread block per split node. The node's keys (<= 3000 x 8 B) sit in shared memory and are
-// read as warp-wide broadcasts; each lane owns kSeedsPerLane consecutive-in-round seeds and keeps
+// read as warp-wide broadcasts; each lane owns SPL consecutive-in-round seeds and keeps
 // per-seed part counts in registers. A seed x is valid when every part but the last receives
 // exactly its size under  part(k) = remap16(remix(k + x), m) / unit  (fanout 2: h >= split).
 //
@@ -9,11 +9,12 @@
 // r16 the low 16 bits of remix, so each part boundary becomes one 16-bit threshold and only the
 // low 47 bits of remix's second product are needed.
 //
-// Rounds: the block evaluates 64*G seeds per round (G warp groups; a group's warps split the
-// node's keys and merge counts in shared memory). G is picked from the node's expected trial count
-// 1/p (the same p the Golomb-Rice memo uses) so the overshoot past the answer stays small. The
-// smallest valid seed of the first round that has one is the answer, identical to the reference's
-// sequential `for (;;) x++` search.
+// Rounds: the block evaluates 32*SPL*G seeds per round (SPL seeds per lane, G warp groups; a
+// group's warps split the node's keys and merge counts in shared memory). G is picked from the
+// node's expected trial count 1/p (the same p the Golomb-Rice memo uses) so that a round stays near
+// 1/round_div of it and the overshoot past the answer stays small. The smallest valid seed of the
+// first round that has one is the answer, identical to the reference's sequential `for (;;) x++`
+// search, for every choice of SPL, block size and round_div (the tuning parameters).
 #include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -22,29 +23,25 @@
 
 namespace shg {
 
-constexpr int kSplitThreads = 256;
-constexpr int kSplitWarps = kSplitThreads / 32;
-constexpr int kSeedsPerLane = 2;
-constexpr int kSeedsPerWarp = 32 * kSeedsPerLane;
-
-struct SplitSmem {
+template <int SPL, int THREADS> struct SplitSmem {
+    static constexpr int kWarps = THREADS / 32;
     uint64_t keys[kMaxBucket];
-    uint32_t part_counts[kSplitWarps][kSeedsPerWarp][3];
-    uint64_t scan[kSplitWarps];
+    uint32_t part_counts[kWarps][32 * SPL][3];
+    uint64_t scan[kWarps];
     uint32_t best;
 };
 
-// Counts of keys below each of NT thresholds, for kSeedsPerLane seeds, over keys [lo, hi).
-template <int NT>
+// Counts of keys below each of NT thresholds, for SPL seeds, over keys [lo, hi).
+template <int NT, int SPL>
 __device__ __forceinline__ void count_range(const uint64_t *__restrict__ sk, uint32_t lo, uint32_t hi, uint64_t x0,
                                             const uint32_t T0, const uint32_t T1, const uint32_t T2,
-                                            uint32_t (&c)[kSeedsPerLane][3]) {
+                                            uint32_t (&c)[SPL][3]) {
     const uint32_t T[3] = {T0, T1, T2};
     uint32_t i = lo;
     for (; i + 2 <= hi; i += 2) {
         const uint64_t k0 = sk[i], k1 = sk[i + 1];
 #pragma unroll
-        for (int s = 0; s < kSeedsPerLane; s++) {
+        for (int s = 0; s < SPL; s++) {
             const uint64_t x = x0 + (uint64_t)(s * 32);
             const uint32_t r0 = remix_low16(k0 + x);
             const uint32_t r1 = remix_low16(k1 + x);
@@ -55,7 +52,7 @@ __device__ __forceinline__ void count_range(const uint64_t *__restrict__ sk, uin
     for (; i < hi; i++) {
         const uint64_t k0 = sk[i];
 #pragma unroll
-        for (int s = 0; s < kSeedsPerLane; s++) {
+        for (int s = 0; s < SPL; s++) {
             const uint32_t r0 = remix_low16(k0 + x0 + (uint64_t)(s * 32));
 #pragma unroll
             for (int t = 0; t < NT; t++) c[s][t] += (r0 < T[t]);
@@ -68,13 +65,14 @@ __device__ __forceinline__ void count_range(const uint64_t *__restrict__ sk, uin
 // accumulates the moments sum p, sum p^2, sum p^3 (multiply-adds); part counts (u, u, u, u) are the
 // only counts with moments (6u, 14u, 36u) because the system matrix [[1,2,3],[1,4,9],[1,8,27]] is
 // invertible.
+template <int SPL>
 __device__ __forceinline__ void moments_range(const uint64_t *__restrict__ sk, uint32_t lo, uint32_t hi, uint64_t x0,
-                                              uint32_t (&c)[kSeedsPerLane][3]) {
+                                              uint32_t (&c)[SPL][3]) {
     uint32_t i = lo;
     for (; i + 2 <= hi; i += 2) {
         const uint64_t k0 = sk[i], k1 = sk[i + 1];
 #pragma unroll
-        for (int s = 0; s < kSeedsPerLane; s++) {
+        for (int s = 0; s < SPL; s++) {
             const uint64_t x = x0 + (uint64_t)(s * 32);
             const uint32_t p0 = remix_low16(k0 + x) >> 14;
             const uint32_t p1 = remix_low16(k1 + x) >> 14;
@@ -87,7 +85,7 @@ __device__ __forceinline__ void moments_range(const uint64_t *__restrict__ sk, u
     for (; i < hi; i++) {
         const uint64_t k0 = sk[i];
 #pragma unroll
-        for (int s = 0; s < kSeedsPerLane; s++) {
+        for (int s = 0; s < SPL; s++) {
             const uint32_t p0 = remix_low16(k0 + x0 + (uint64_t)(s * 32)) >> 14;
             c[s][0] += p0;
             c[s][1] += p0 * p0;
@@ -98,31 +96,32 @@ __device__ __forceinline__ void moments_range(const uint64_t *__restrict__ sk, u
 
 // Smallest valid trial index (seed - seed0), or ~0 when `cap` trials were exhausted.
 // NT = number of part thresholds compared (1..3); NT = 4 selects the quarter-split moments.
-template <int NT>
-__device__ uint64_t search_seeds(SplitSmem &sm, uint32_t m, uint64_t seed0, const uint32_t T0, const uint32_t T1,
-                                 const uint32_t T2, const uint32_t N0, const uint32_t N1, const uint32_t N2, int G,
-                                 uint64_t cap) {
+template <int NT, int SPL, int THREADS>
+__device__ uint64_t search_seeds(SplitSmem<SPL, THREADS> &sm, uint32_t m, uint64_t seed0, const uint32_t T0,
+                                 const uint32_t T1, const uint32_t T2, const uint32_t N0, const uint32_t N1,
+                                 const uint32_t N2, int G, uint64_t cap) {
+    constexpr int kWarps = THREADS / 32, kSeedsPerWarp = 32 * SPL;
     const uint32_t need[3] = {N0, N1, N2};
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int wpg = kSplitWarps / G;  // warps per group
+    const int wpg = kWarps / G;  // warps per group
     const int group = warp / wpg, sub = warp % wpg;
     const uint32_t lo = (uint32_t)((uint64_t)m * sub / wpg), hi = (uint32_t)((uint64_t)m * (sub + 1) / wpg);
     const uint32_t per_round = (uint32_t)(kSeedsPerWarp * G);
     for (uint64_t base = 0; base < cap; base += per_round) {
         const uint32_t slot0 = (uint32_t)group * kSeedsPerWarp + lane;  // seed slot s is slot0 + 32 s
-        uint32_t c[kSeedsPerLane][3] = {};
-        if (NT == 4) moments_range(sm.keys, lo, hi, seed0 + base + slot0, c);
-        else count_range<NT>(sm.keys, lo, hi, seed0 + base + slot0, T0, T1, T2, c);
+        uint32_t c[SPL][3] = {};
+        if (NT == 4) moments_range<SPL>(sm.keys, lo, hi, seed0 + base + slot0, c);
+        else count_range<NT, SPL>(sm.keys, lo, hi, seed0 + base + slot0, T0, T1, T2, c);
         constexpr int NC = NT == 4 ? 3 : NT;  // counters per seed
         if (wpg > 1) {
 #pragma unroll
-            for (int s = 0; s < kSeedsPerLane; s++)
+            for (int s = 0; s < SPL; s++)
 #pragma unroll
                 for (int t = 0; t < NC; t++) sm.part_counts[warp][s * 32 + lane][t] = c[s][t];
             __syncthreads();
             if (sub == 0) {
 #pragma unroll
-                for (int s = 0; s < kSeedsPerLane; s++)
+                for (int s = 0; s < SPL; s++)
 #pragma unroll
                     for (int t = 0; t < NC; t++) {
                         uint32_t tot = 0;
@@ -133,7 +132,7 @@ __device__ uint64_t search_seeds(SplitSmem &sm, uint32_t m, uint64_t seed0, cons
         }
         if (sub == 0) {
 #pragma unroll
-            for (int s = 0; s < kSeedsPerLane; s++) {
+            for (int s = 0; s < SPL; s++) {
                 bool ok = true;
 #pragma unroll
                 for (int t = 0; t < NC; t++) ok &= c[s][t] == need[t];
@@ -147,13 +146,15 @@ __device__ uint64_t search_seeds(SplitSmem &sm, uint32_t m, uint64_t seed0, cons
     return ~0ull;
 }
 
-__global__ void __launch_bounds__(kSplitThreads) k_split(const Node *__restrict__ nodes, const uint32_t *__restrict__ ids,
-                                                         uint64_t *__restrict__ keys, uint64_t *__restrict__ codes,
-                                                         uint64_t max_trials, uint32_t *__restrict__ err,
-                                                         unsigned long long *__restrict__ work,
-                                                         unsigned long long *__restrict__ kind_work) {
+template <int SPL, int THREADS>
+__global__ void __launch_bounds__(THREADS) k_split(const Node *__restrict__ nodes, const uint32_t *__restrict__ ids,
+                                                   uint64_t *__restrict__ keys, uint64_t *__restrict__ codes,
+                                                   uint64_t max_trials, uint32_t *__restrict__ err,
+                                                   unsigned long long *__restrict__ work,
+                                                   unsigned long long *__restrict__ kind_work, int round_div) {
+    constexpr int kWarps = THREADS / 32, kSeedsPerWarp = 32 * SPL;
     extern __shared__ __align__(16) uint8_t smem_raw[];
-    SplitSmem &sm = *reinterpret_cast<SplitSmem *>(smem_raw);
+    SplitSmem<SPL, THREADS> &sm = *reinterpret_cast<SplitSmem<SPL, THREADS> *>(smem_raw);
     const uint32_t id = ids[blockIdx.x];
     const Node nd = nodes[id];
     const uint32_t m = nd.m;
@@ -181,10 +182,10 @@ __global__ void __launch_bounds__(kSplitThreads) k_split(const Node *__restrict_
         sp *= sqrt((double)(m - (uint32_t)NT * nd.unit));
         p = sqrt((double)m) / (pow(2 * M_PI, NT / 2.0) * sp);
     }
-    // Warp groups: aim for a round of ~1/8 of the expected trials.
+    // Warp groups: aim for a round of ~1/round_div of the expected trials.
     const double expect = 1.0 / p;
     int G = 1;
-    while (G < kSplitWarps && (double)(kSeedsPerWarp * G * 2) * 8.0 <= expect) G <<= 1;
+    while (G < kWarps && (double)(kSeedsPerWarp * G * 2) * (double)round_div <= expect) G <<= 1;
     if (threadIdx.x == 0) sm.best = 0xffffffffu;
     __syncthreads();
 
@@ -202,10 +203,10 @@ __global__ void __launch_bounds__(kSplitThreads) k_split(const Node *__restrict_
         need[2] = 36u * nd.unit;
     }
     switch (NT) {
-        case 1: trial = search_seeds<1>(sm, m, seed0, T[0], T[1], T[2], need[0], need[1], need[2], G, cap); break;
-        case 2: trial = search_seeds<2>(sm, m, seed0, T[0], T[1], T[2], need[0], need[1], need[2], G, cap); break;
-        case 3: trial = search_seeds<3>(sm, m, seed0, T[0], T[1], T[2], need[0], need[1], need[2], G, cap); break;
-        default: trial = search_seeds<4>(sm, m, seed0, T[0], T[1], T[2], need[0], need[1], need[2], G, cap); break;
+        case 1: trial = search_seeds<1, SPL, THREADS>(sm, m, seed0, T[0], T[1], T[2], need[0], need[1], need[2], G, cap); break;
+        case 2: trial = search_seeds<2, SPL, THREADS>(sm, m, seed0, T[0], T[1], T[2], need[0], need[1], need[2], G, cap); break;
+        case 3: trial = search_seeds<3, SPL, THREADS>(sm, m, seed0, T[0], T[1], T[2], need[0], need[1], need[2], G, cap); break;
+        default: trial = search_seeds<4, SPL, THREADS>(sm, m, seed0, T[0], T[1], T[2], need[0], need[1], need[2], G, cap); break;
     }
     if (trial == ~0ull) {
         if (threadIdx.x == 0) atomicOr(err, kErrTrialLimit);
@@ -216,7 +217,7 @@ __global__ void __launch_bounds__(kSplitThreads) k_split(const Node *__restrict_
     // Stable partition (counting sort by part, original order inside a part). Each thread owns a
     // contiguous chunk; per-part counts are packed 16 bits per part into one 64-bit word and
     // exclusive-scanned across the block.
-    const uint32_t chunk = (m + kSplitThreads - 1) / kSplitThreads;
+    const uint32_t chunk = (m + THREADS - 1) / THREADS;
     const uint32_t lo = min(m, threadIdx.x * chunk), hi = min(m, lo + chunk);
     uint64_t mine = 0;
     for (uint32_t i = lo; i < hi; i++) {
@@ -255,13 +256,32 @@ __global__ void __launch_bounds__(kSplitThreads) k_split(const Node *__restrict_
     }
 }
 
+template <int SPL, int THREADS>
+static void launch_split_t(const Node *nodes, const uint32_t *ids, uint32_t count, uint64_t *keys, uint64_t *codes,
+                           uint64_t max_trials, uint32_t *err, unsigned long long *work, unsigned long long *kind_work,
+                           int round_div, cudaStream_t s) {
+    const size_t smem = sizeof(SplitSmem<SPL, THREADS>);
+    cudaFuncSetAttribute(k_split<SPL, THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_split<SPL, THREADS><<<count, THREADS, smem, s>>>(nodes, ids, keys, codes, max_trials, err, work, kind_work, round_div);
+}
+
+bool split_tuning_valid(int spl, int threads, int round_div) {
+    return (spl == 1 || spl == 2 || spl == 4) && (threads == 128 || threads == 256 || threads == 512) && round_div >= 1 &&
+           round_div <= 64;
+}
+
 void launch_split_level(const Node *nodes, const uint32_t *ids, uint32_t count, uint64_t *keys, uint64_t *codes,
                         uint64_t max_trials, uint32_t *err, unsigned long long *work, unsigned long long *kind_work,
-                        cudaStream_t s) {
+                        const SplitTuning &t, cudaStream_t s) {
     if (!count) return;
-    const size_t smem = sizeof(SplitSmem);
-    cudaFuncSetAttribute(k_split, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_split<<<count, kSplitThreads, smem, s>>>(nodes, ids, keys, codes, max_trials, err, work, kind_work);
+#define SHG_SPLIT_CASE(SPL, TH)                                                                                  \
+    if (t.spl == SPL && t.threads == TH)                                                                        \
+        return launch_split_t<SPL, TH>(nodes, ids, count, keys, codes, max_trials, err, work, kind_work, t.round_div, s);
+    SHG_SPLIT_CASE(1, 128) SHG_SPLIT_CASE(1, 256) SHG_SPLIT_CASE(1, 512)
+    SHG_SPLIT_CASE(2, 128) SHG_SPLIT_CASE(2, 256) SHG_SPLIT_CASE(2, 512)
+    SHG_SPLIT_CASE(4, 128) SHG_SPLIT_CASE(4, 256) SHG_SPLIT_CASE(4, 512)
+#undef SHG_SPLIT_CASE
+    launch_split_t<2, 256>(nodes, ids, count, keys, codes, max_trials, err, work, kind_work, t.round_div, s);
 }
 
 } // namespace shg

@@ -45,3 +45,43 @@ def test_shard_rejects_keys_outside_its_range(engine):
     ok = shard.owners(f, nb, 2) == 0
     r = engine.build_shard_hash128(2, 64, f[ok], s[ok], nb, 0, nb // 2)  # the engine stays usable
     assert r.nbuckets == nb // 2 and r.n == int(ok.sum())
+
+
+@pytest.mark.parametrize("world,nb", [(1, 5000), (2, 5000), (3, 7), (8, 50_000), (64, 100_003), (5, 1)])
+def test_device_partition_equals_host_partition(engine, world, nb):
+    import torch
+    from shockhash_b200 import shard
+    rng = np.random.default_rng(world * 7 + nb)
+    n = 1_000_003
+    f = rng.integers(0, 2**64, size=n, dtype=np.uint64)
+    s = rng.integers(0, 2**64, size=n, dtype=np.uint64)
+    ft, st = torch.from_numpy(f.view(np.int64)), torch.from_numpy(s.view(np.int64))
+    host_pairs, host_counts = shard.partition(ft, st, nb, world)
+    dev_pairs, dev_counts = shard.partition(ft.cuda(), st.cuda(), nb, world, engine)
+    assert np.array_equal(dev_counts, host_counts)
+    assert torch.equal(dev_pairs.cpu(), host_pairs)
+
+
+def test_device_shard_builds_merge_to_one_build(engine):
+    import torch
+    from shockhash_b200 import shard
+    rng = np.random.default_rng(5)
+    n, b, world = 300_000, 2000, 3
+    f = rng.integers(0, 2**64, size=n, dtype=np.uint64)
+    s = np.unique(rng.integers(0, 2**64, size=n + 64, dtype=np.uint64))[:n]
+    full = engine.build_hash128(2, 64, f, s, b)
+    nb = shard.nbuckets(n, b)
+    pairs, counts = shard.partition(torch.from_numpy(f.view(np.int64)).cuda(), torch.from_numpy(s.view(np.int64)).cuda(),
+                                    nb, world, engine)
+    parts, at = [], 0
+    for g, (b0, b1) in enumerate(shard.bucket_ranges(nb, world)):
+        seg = pairs[at:at + int(counts[g])]
+        at += int(counts[g])
+        fg, sg = seg[:, 0].contiguous(), seg[:, 1].contiguous()
+        torch.cuda.synchronize()  # torch's copies are done before the engine's stream reads them
+        r = engine.build_shard_hash128_device(2, 64, fg.data_ptr(), sg.data_ptr(), fg.numel(), nb, b0, b1, b)
+        parts.append(shard._arrays(r))
+        r.free()
+    m = shg.merge_shards(2, 64, parts, b)
+    for name in ("bucket_size_acc", "bucket_pos_acc", "descriptors", "ribbon_keys", "ribbon_bits"):
+        assert np.array_equal(getattr(m, name), getattr(full, name)), name

@@ -96,3 +96,49 @@ def test_two_gloo_ranks_exchange_build_and_merge(tmp_path):
     import torch.multiprocessing as mp
     mp.spawn(_rank_main, args=(2, _free_port(), 2, 24, 12000, 600, str(tmp_path)), nprocs=2, join=True)
     assert (tmp_path / "ok").exists()
+
+
+@pytest.mark.parametrize("world,nb", [(1, 5), (2, 5000), (3, 7), (8, 1), (5, 123457), (64, 1000)])
+def test_host_partition_is_the_stable_owner_order(world, nb):
+    import torch
+    f, s = _keys(world * 31 + nb, 20_011)
+    pairs, counts = shard.partition(torch.from_numpy(f.view(np.int64)), torch.from_numpy(s.view(np.int64)), nb, world)
+    own = shard.owners(f, nb, world)
+    order = np.argsort(own, kind="stable")
+    got = pairs.numpy().view(np.uint64)
+    assert np.array_equal(got[:, 0], f[order]) and np.array_equal(got[:, 1], s[order])
+    assert np.array_equal(counts, np.bincount(own, minlength=world))
+
+
+def _tensor_rank_main(rank, world, port_no, variant, leaf, n, b, out_dir):
+    import torch
+    import torch.distributed as dist
+    from oracle.bindings import PortLib
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port_no)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        P = PortLib()
+        f, s = _keys(78, n)
+        mine = slice(rank, None, world)
+        ft = torch.from_numpy(np.ascontiguousarray(f[mine]).view(np.int64))
+        st = torch.from_numpy(np.ascontiguousarray(s[mine]).view(np.int64))
+        build = lambda ff, ss, nbg, x0, x1: P.build_shard(variant, leaf, ff.numpy().view(np.uint64),
+                                                          ss.numpy().view(np.uint64), nbg, x0, x1, b)
+        part, nb, (b0, b1) = shard.build_sharded_tensors(build, ft, st, b)
+        own = shard.owners(f, nb, world)
+        assert (part.n if part is not None else 0) == int((own == rank).sum())
+        merged = shard.gather_merge_tensors(part, variant, leaf, b)
+        if rank == 0:
+            _same(merged, P.build_hash(variant, leaf, f, s, b))
+            open(os.path.join(out_dir, "ok"), "w").write("ok")
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,n,b", [(2, 12000, 600), (3, 900, 500)])
+def test_gloo_ranks_tensor_exchange_build_and_merge(tmp_path, world, n, b):
+    # (3, 900, 500): two buckets over three ranks, so one rank owns none
+    import torch.multiprocessing as mp
+    mp.spawn(_tensor_rank_main, args=(world, _free_port(), 2, 24, n, b, str(tmp_path)), nprocs=world, join=True)
+    assert (tmp_path / "ok").exists()
