@@ -342,7 +342,9 @@ int shg_int_peak(int device, uint64_t iters, double *evals_per_s, double *ms);
  * 1 = original leaf coverage (remix, two fastrange32 cells, half masks), 2 = bipartite raw seeds
  * (remix, fastrange64, mask), 3 / 4 / 5 = split compare-and-count against 1 / 2 / 3 part
  * thresholds (fanout-2 and uneven split nodes), 6 = bipartite candidate-scan mask pairs,
- * 7 = bipartite isolated-key pair filter, 8 = bipartite pseudoforest edges (union-find). */
+ * 7 = bipartite isolated-key pair filter, 8 = bipartite pseudoforest edges (union-find),
+ * 9 / 10 / 11 / 12 = kinds 0 / 3 / 4 / 5 with the split kernel's pipe-split arithmetic
+ * (tuning parameter split_arith 1). */
 int shg_int_peak_kind(int device, int kind, uint64_t iters, double *evals_per_s, double *ms);
 
 /* Work counts of the engine's last RecSplit build beyond shg_result.work (measurement utility, no
@@ -357,7 +359,9 @@ shg_status shg_engine_last_work(const shg_engine *e, uint64_t *out, int n);
  * change speed only, never a result). variant is an shg_variant (SHG_SHOCKHASH_ROTATION shares
  * SHG_SHOCKHASH's entry) or 4 for ShockHash2Flat<k> with leaf_size = k. Names and ranges:
  *   split_seeds_per_lane 1, 2, 4; split_threads 128, 256, 512; split_round_div 1..64 (a round of
- *   seeds aims at 1/round_div of a split node's expected trials); leaf_blocks_per_sm 0..16 (0 =
+ *   seeds aims at 1/round_div of a split node's expected trials); split_arith 0, 1 (1: remix's
+ *   shifts partly as multiply-highs, moving work from the integer to the multiply pipe);
+ *   leaf_blocks_per_sm 0..16 (0 =
  *   as many as shared memory allows); leaf_min_blocks 4, 6, 8 (bipartite leaves up to 64 keys:
  *   register bound); sh1_seeds_per_lane 1, 2 (original leaves).
  * At creation an engine loads the table shockhash_b200/tuning.tsv beside the library (or the file

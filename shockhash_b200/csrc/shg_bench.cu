@@ -60,6 +60,37 @@ __global__ void __launch_bounds__(kPeakThreads) k_int_peak_cmp(uint64_t iters, u
     if ((c[0][0] ^ c[0][1] ^ c[0][2] ^ c[1][0] ^ c[1][1] ^ c[1][2]) == 0xFFFFFFFFu) atomicAdd(sink, 1ull);
 }
 
+// The same two loops with remix split between the integer and multiply pipes (the split kernel's
+// arithmetic option 1): quarter moments (NT = 4) or compare-and-count against NT thresholds.
+template <int NT>
+__global__ void __launch_bounds__(kPeakThreads) k_int_peak_pipes(uint64_t iters, uint32_t T0, uint32_t T1, uint32_t T2,
+                                                                 const shg::PipeK K, unsigned long long *sink) {
+    const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    uint64_t k0 = shg::remix(tid * 0x9E3779B97F4A7C15ULL), k1 = shg::remix(k0);
+    const uint64_t x0 = 0x643e521ddbd2be98ULL + tid;
+    const uint32_t T[3] = {T0, T1, T2};
+    uint32_t c[2][3] = {};
+    for (uint64_t i = 0; i < iters; i++) {
+        uint32_t a0, b0, a1, b1;
+        shg::remix_lo32_pipes(k0 + x0 + i, K, a0, b0);
+        shg::remix_lo32_pipes(k1 + x0 + i, K, a1, b1);
+        if (NT == 4) {
+            const uint32_t p0 = __umulhi((a0 ^ b0) & 0xC000u, K.c18), p1 = __umulhi((a1 ^ b1) & 0xC000u, K.c18);
+            const uint32_t q0 = p0 * p0, q1 = p1 * p1;
+            c[0][0] += p0; c[0][1] += q0; c[0][2] += q0 * p0;
+            c[1][0] += p1; c[1][1] += q1; c[1][2] += q1 * p1;
+        } else {
+            const uint32_t r0 = (a0 ^ b0) & 0xFFFFu, r1 = (a1 ^ b1) & 0xFFFFu;
+#pragma unroll
+            for (int t = 0; t < NT; t++) {
+                c[0][t] = shg::add_sign_bit(c[0][t], r0 - T[t], K.two);
+                c[1][t] = shg::add_sign_bit(c[1][t], r1 - T[t], K.two);
+            }
+        }
+    }
+    if ((c[0][0] ^ c[0][1] ^ c[0][2] ^ c[1][0] ^ c[1][1] ^ c[1][2]) == 0xFFFFFFFFu) atomicAdd(sink, 1ull);
+}
+
 // The arithmetic of the original leaf search's coverage loop: full 64-bit remix, both cells by
 // fastrange32 on its halves, one bit each into two 32-bit half masks; two seeds per lane.
 __global__ void __launch_bounds__(kPeakThreads) k_int_peak_sh1(uint64_t iters, uint32_t h1, uint32_t h2,
@@ -183,10 +214,11 @@ int shg_int_peak(int device, uint64_t iters, double *evals_per_s, double *ms_out
 
 // Integer-pipe peak of one search's inner loop (0 = split quarter moments, 1 = original leaf,
 // 2 = bipartite leaf hashing, 3..5 = split compare-and-count with 1..3 thresholds, 6..8 = bipartite
-// candidate scan, pair filter and pseudoforest edges).
+// candidate scan, pair filter and pseudoforest edges, 9..12 = kinds 0 and 3..5 with the split
+// kernel's pipe-split arithmetic).
 int shg_int_peak_kind(int device, int kind, uint64_t iters, double *evals_per_s, double *ms_out) {
     if (kind == 0) return shg_int_peak(device, iters, evals_per_s, ms_out);
-    if (kind < 1 || kind > 8) return SHG_ERR_ARG;
+    if (kind < 1 || kind > 12) return SHG_ERR_ARG;
     if (cudaSetDevice(device) != cudaSuccess) return SHG_ERR_CUDA;
     cudaDeviceProp prop;
     cudaGetDeviceProperties(&prop, device);
@@ -210,8 +242,15 @@ int shg_int_peak_kind(int device, int kind, uint64_t iters, double *evals_per_s,
             k_int_peak_cmp<2><<<blocks, kPeakThreads>>>(it, 21846, 43691, 65536, sink);
         else if (kind == 5)
             k_int_peak_cmp<3><<<blocks, kPeakThreads>>>(it, 16384, 32768, 49152, sink);
-        else  // the bipartite leaf's scan, pair filter and pseudoforest loops (64 edges per iteration)
+        else if (kind <= 8)  // the bipartite leaf's scan, pair filter and pseudoforest loops (64 edges per iteration)
             shg::launch_sh2_op_peak(kind - 6, blocks, kind == 8 ? it / 64 + 1 : it, sink);
+        else {  // 9: quarter moments, 10..12: 1..3 thresholds, with the split kernel's pipe-split arithmetic
+            const shg::PipeK K{4u, 32u, 1u << 18, 2u};
+            if (kind == 9) k_int_peak_pipes<4><<<blocks, kPeakThreads>>>(it, 16384, 32768, 49152, K, sink);
+            else if (kind == 10) k_int_peak_pipes<1><<<blocks, kPeakThreads>>>(it, 50331, 65536, 65536, K, sink);
+            else if (kind == 11) k_int_peak_pipes<2><<<blocks, kPeakThreads>>>(it, 21846, 43691, 65536, K, sink);
+            else k_int_peak_pipes<3><<<blocks, kPeakThreads>>>(it, 16384, 32768, 49152, K, sink);
+        }
         if (rep) cudaEventRecord(b);
     }
     cudaEventSynchronize(b);

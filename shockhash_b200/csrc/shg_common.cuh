@@ -51,6 +51,36 @@ SHG_HD uint32_t remix_low16(uint64_t z) {
     return (uint32_t)((z ^ (z >> 31)) & 0xFFFF);
 }
 
+#ifdef __CUDACC__
+// remix's low 32 bits with the work split between the integer and multiply pipes: the high words
+// of the two xor-shifts are taken as multiply-highs by the runtime constants K.four (4) and
+// K.thirtytwo (32), which the compiler cannot turn back into shifts, so that they run on the
+// multiply-add pipe next to the 64-bit products. Returns (lo, t): remix(z) = lo ^ t in the low 32
+// bits, left unmerged so that the caller folds its own mask into the same logic operation.
+struct PipeK {
+    uint32_t four, thirtytwo, c18, two;  // 4, 32, 2^18, 2 (kernel arguments)
+};
+__device__ __forceinline__ void remix_lo32_pipes(uint64_t z, const PipeK &K, uint32_t &lo4, uint32_t &t) {
+    uint32_t lo = (uint32_t)z, hi = (uint32_t)(z >> 32);
+    lo ^= __funnelshift_r(lo, hi, 30);  // z ^= z >> 30
+    hi ^= __umulhi(hi, K.four);
+    uint64_t w = (uint64_t)lo * 0x1ce4e5b9u;  // z *= 0xbf58476d1ce4e5b9
+    uint32_t lo2 = (uint32_t)w, hi2 = (uint32_t)(w >> 32) + lo * 0xbf58476du + hi * 0x1ce4e5b9u;
+    lo2 ^= __funnelshift_r(lo2, hi2, 27);  // z ^= z >> 27
+    hi2 ^= __umulhi(hi2, K.thirtytwo);
+    w = (uint64_t)lo2 * 0x133111ebu;  // z *= 0x94d049bb133111eb (bits 0..46 matter)
+    lo4 = (uint32_t)w;
+    const uint32_t hi4 = (uint32_t)(w >> 32) + lo2 * 0x94d049bbu + hi2 * 0x133111ebu;
+    t = __funnelshift_r(lo4, hi4, 31);  // z ^ (z >> 31)
+}
+// c + (x >> 31) as one multiply-add-high (x * 2 >> 32), on the multiply-add pipe.
+__device__ __forceinline__ uint32_t add_sign_bit(uint32_t c, uint32_t x, uint32_t two) {
+    uint32_t d;
+    asm("mad.hi.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(x), "r"(two), "r"(c));
+    return d;
+}
+#endif
+
 // Lemire range reduction. fastrange32 takes the low 32 bits of its argument
 // (TinyBinaryCuckooHashTable.h:140-141, SimdUtils.h:48-51).
 SHG_HD uint32_t fastrange32(uint32_t word, uint32_t p) { return (uint32_t)(((uint64_t)word * (uint64_t)p) >> 32); }

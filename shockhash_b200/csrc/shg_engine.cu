@@ -992,11 +992,12 @@ static shg_status set_tuning(shg_engine *e, int variant, int leaf, const std::st
     if (name == "split_seeds_per_lane") t.split.spl = (int)v;
     else if (name == "split_threads") t.split.threads = (int)v;
     else if (name == "split_round_div") t.split.round_div = (int)v;
+    else if (name == "split_arith") t.split.arith = (int)v;
     else if (name == "leaf_blocks_per_sm" && v >= 0 && v <= 16) t.leaf_bps = (int)v;
     else if (name == "leaf_min_blocks" && (v == 4 || v == 6 || v == 8)) t.leaf_minb = (int)v;
     else if (name == "sh1_seeds_per_lane" && (v == 1 || v == 2)) t.sh1_spl = (int)v;
     else return fail(SHG_ERR_ARG, "tuning: bad parameter " + name + " = " + std::to_string(v));
-    if (!split_tuning_valid(t.split.spl, t.split.threads, t.split.round_div))
+    if (!split_tuning_valid(t.split.spl, t.split.threads, t.split.round_div, t.split.arith))
         return fail(SHG_ERR_ARG, "tuning: bad parameter " + name + " = " + std::to_string(v));
     e->tuning[{variant, leaf}] = t;
     return SHG_OK;
@@ -1045,6 +1046,7 @@ shg_status shg_engine_get_tuning(shg_engine *e, int variant, int leaf_size, cons
     if (n == "split_seeds_per_lane") *value = t.split.spl;
     else if (n == "split_threads") *value = t.split.threads;
     else if (n == "split_round_div") *value = t.split.round_div;
+    else if (n == "split_arith") *value = t.split.arith;
     else if (n == "leaf_blocks_per_sm") *value = t.leaf_bps;
     else if (n == "leaf_min_blocks") *value = t.leaf_minb;
     else if (n == "sh1_seeds_per_lane") *value = t.sh1_spl;

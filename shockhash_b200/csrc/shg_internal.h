@@ -141,6 +141,7 @@ struct SplitTuning {
     int spl = 2;         // seeds per lane: 1, 2 or 4
     int threads = 256;   // threads per split block (one node per block): 128, 256 or 512
     int round_div = 8;   // warp groups make a round about 1/round_div of a node's expected trials (1..64)
+    int arith = 0;       // 0: remix as the compiler schedules it; 1: split between integer and multiply pipes
 };
 struct Tuning {
     SplitTuning split;
@@ -148,7 +149,7 @@ struct Tuning {
     int leaf_minb = 6;   // bipartite leaves of up to 64 keys: launch bound of 4, 6 or 8 blocks per SM
     int sh1_spl = 2;     // original leaves: seeds per lane, 1 or 2
 };
-bool split_tuning_valid(int spl, int threads, int round_div);
+bool split_tuning_valid(int spl, int threads, int round_div, int arith);
 constexpr int kTuningFlat = 4;  // tuning-table variant key of ShockHash2Flat<k> (leaf size = k)
 // work[0] += useful evaluations; kind_work[k] += the same per inner loop (k = compared thresholds
 // - 1, or 3 for quarter-split moments)

@@ -32,30 +32,46 @@ template <int SPL, int THREADS> struct SplitSmem {
 };
 
 // Counts of keys below each of NT thresholds, for SPL seeds, over keys [lo, hi).
-template <int NT, int SPL>
+// ARITH 1 computes the same counts with remix_lo32_pipes and multiply-add-high counting (r < T is
+// the sign bit of r - T), trading integer-pipe instructions for multiply-pipe ones.
+template <int NT, int SPL, int ARITH>
 __device__ __forceinline__ void count_range(const uint64_t *__restrict__ sk, uint32_t lo, uint32_t hi, uint64_t x0,
                                             const uint32_t T0, const uint32_t T1, const uint32_t T2,
-                                            uint32_t (&c)[SPL][3]) {
+                                            uint32_t (&c)[SPL][3], const PipeK &K) {
     const uint32_t T[3] = {T0, T1, T2};
     uint32_t i = lo;
-    for (; i + 2 <= hi; i += 2) {
-        const uint64_t k0 = sk[i], k1 = sk[i + 1];
+    if constexpr (ARITH == 1) {
+        for (; i < hi; i++) {
+            const uint64_t k0 = sk[i];
 #pragma unroll
-        for (int s = 0; s < SPL; s++) {
-            const uint64_t x = x0 + (uint64_t)(s * 32);
-            const uint32_t r0 = remix_low16(k0 + x);
-            const uint32_t r1 = remix_low16(k1 + x);
+            for (int s = 0; s < SPL; s++) {
+                uint32_t a, b;
+                remix_lo32_pipes(k0 + x0 + (uint64_t)(s * 32), K, a, b);
+                const uint32_t r = (a ^ b) & 0xFFFFu;
 #pragma unroll
-            for (int t = 0; t < NT; t++) c[s][t] += (r0 < T[t]) + (r1 < T[t]);
+                for (int t = 0; t < NT; t++) c[s][t] = add_sign_bit(c[s][t], r - T[t], K.two);
+            }
         }
-    }
-    for (; i < hi; i++) {
-        const uint64_t k0 = sk[i];
+    } else {
+        for (; i + 2 <= hi; i += 2) {
+            const uint64_t k0 = sk[i], k1 = sk[i + 1];
 #pragma unroll
-        for (int s = 0; s < SPL; s++) {
-            const uint32_t r0 = remix_low16(k0 + x0 + (uint64_t)(s * 32));
+            for (int s = 0; s < SPL; s++) {
+                const uint64_t x = x0 + (uint64_t)(s * 32);
+                const uint32_t r0 = remix_low16(k0 + x);
+                const uint32_t r1 = remix_low16(k1 + x);
 #pragma unroll
-            for (int t = 0; t < NT; t++) c[s][t] += (r0 < T[t]);
+                for (int t = 0; t < NT; t++) c[s][t] += (r0 < T[t]) + (r1 < T[t]);
+            }
+        }
+        for (; i < hi; i++) {
+            const uint64_t k0 = sk[i];
+#pragma unroll
+            for (int s = 0; s < SPL; s++) {
+                const uint32_t r0 = remix_low16(k0 + x0 + (uint64_t)(s * 32));
+#pragma unroll
+                for (int t = 0; t < NT; t++) c[s][t] += (r0 < T[t]);
+            }
         }
     }
 }
@@ -65,41 +81,57 @@ __device__ __forceinline__ void count_range(const uint64_t *__restrict__ sk, uin
 // accumulates the moments sum p, sum p^2, sum p^3 (multiply-adds); part counts (u, u, u, u) are the
 // only counts with moments (6u, 14u, 36u) because the system matrix [[1,2,3],[1,4,9],[1,8,27]] is
 // invertible.
-template <int SPL>
+template <int SPL, int ARITH>
 __device__ __forceinline__ void moments_range(const uint64_t *__restrict__ sk, uint32_t lo, uint32_t hi, uint64_t x0,
-                                              uint32_t (&c)[SPL][3]) {
+                                              uint32_t (&c)[SPL][3], const PipeK &K) {
     uint32_t i = lo;
-    for (; i + 2 <= hi; i += 2) {
-        const uint64_t k0 = sk[i], k1 = sk[i + 1];
+    if constexpr (ARITH == 1) {  // part p = bits 14..15 of r, taken as a multiply-high of r & 0xC000 by 2^18
+        for (; i < hi; i++) {
+            const uint64_t k0 = sk[i];
 #pragma unroll
-        for (int s = 0; s < SPL; s++) {
-            const uint64_t x = x0 + (uint64_t)(s * 32);
-            const uint32_t p0 = remix_low16(k0 + x) >> 14;
-            const uint32_t p1 = remix_low16(k1 + x) >> 14;
-            const uint32_t q0 = p0 * p0, q1 = p1 * p1;
-            c[s][0] += p0 + p1;
-            c[s][1] += q0 + q1;
-            c[s][2] += q0 * p0 + q1 * p1;
+            for (int s = 0; s < SPL; s++) {
+                uint32_t a, b;
+                remix_lo32_pipes(k0 + x0 + (uint64_t)(s * 32), K, a, b);
+                const uint32_t p0 = __umulhi((a ^ b) & 0xC000u, K.c18);
+                const uint32_t q0 = p0 * p0;
+                c[s][0] += p0;
+                c[s][1] += q0;
+                c[s][2] += q0 * p0;
+            }
         }
-    }
-    for (; i < hi; i++) {
-        const uint64_t k0 = sk[i];
+    } else {
+        for (; i + 2 <= hi; i += 2) {
+            const uint64_t k0 = sk[i], k1 = sk[i + 1];
 #pragma unroll
-        for (int s = 0; s < SPL; s++) {
-            const uint32_t p0 = remix_low16(k0 + x0 + (uint64_t)(s * 32)) >> 14;
-            c[s][0] += p0;
-            c[s][1] += p0 * p0;
-            c[s][2] += p0 * p0 * p0;
+            for (int s = 0; s < SPL; s++) {
+                const uint64_t x = x0 + (uint64_t)(s * 32);
+                const uint32_t p0 = remix_low16(k0 + x) >> 14;
+                const uint32_t p1 = remix_low16(k1 + x) >> 14;
+                const uint32_t q0 = p0 * p0, q1 = p1 * p1;
+                c[s][0] += p0 + p1;
+                c[s][1] += q0 + q1;
+                c[s][2] += q0 * p0 + q1 * p1;
+            }
+        }
+        for (; i < hi; i++) {
+            const uint64_t k0 = sk[i];
+#pragma unroll
+            for (int s = 0; s < SPL; s++) {
+                const uint32_t p0 = remix_low16(k0 + x0 + (uint64_t)(s * 32)) >> 14;
+                c[s][0] += p0;
+                c[s][1] += p0 * p0;
+                c[s][2] += p0 * p0 * p0;
+            }
         }
     }
 }
 
 // Smallest valid trial index (seed - seed0), or ~0 when `cap` trials were exhausted.
 // NT = number of part thresholds compared (1..3); NT = 4 selects the quarter-split moments.
-template <int NT, int SPL, int THREADS>
+template <int NT, int SPL, int THREADS, int ARITH>
 __device__ uint64_t search_seeds(SplitSmem<SPL, THREADS> &sm, uint32_t m, uint64_t seed0, const uint32_t T0,
                                  const uint32_t T1, const uint32_t T2, const uint32_t N0, const uint32_t N1,
-                                 const uint32_t N2, int G, uint64_t cap) {
+                                 const uint32_t N2, int G, uint64_t cap, const PipeK &K) {
     constexpr int kWarps = THREADS / 32, kSeedsPerWarp = 32 * SPL;
     const uint32_t need[3] = {N0, N1, N2};
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -110,8 +142,8 @@ __device__ uint64_t search_seeds(SplitSmem<SPL, THREADS> &sm, uint32_t m, uint64
     for (uint64_t base = 0; base < cap; base += per_round) {
         const uint32_t slot0 = (uint32_t)group * kSeedsPerWarp + lane;  // seed slot s is slot0 + 32 s
         uint32_t c[SPL][3] = {};
-        if (NT == 4) moments_range<SPL>(sm.keys, lo, hi, seed0 + base + slot0, c);
-        else count_range<NT, SPL>(sm.keys, lo, hi, seed0 + base + slot0, T0, T1, T2, c);
+        if constexpr (NT == 4) moments_range<SPL, ARITH>(sm.keys, lo, hi, seed0 + base + slot0, c, K);
+        else count_range<NT, SPL, ARITH>(sm.keys, lo, hi, seed0 + base + slot0, T0, T1, T2, c, K);
         constexpr int NC = NT == 4 ? 3 : NT;  // counters per seed
         if (wpg > 1) {
 #pragma unroll
@@ -146,12 +178,13 @@ __device__ uint64_t search_seeds(SplitSmem<SPL, THREADS> &sm, uint32_t m, uint64
     return ~0ull;
 }
 
-template <int SPL, int THREADS>
+template <int SPL, int THREADS, int ARITH>
 __global__ void __launch_bounds__(THREADS) k_split(const Node *__restrict__ nodes, const uint32_t *__restrict__ ids,
                                                    uint64_t *__restrict__ keys, uint64_t *__restrict__ codes,
                                                    uint64_t max_trials, uint32_t *__restrict__ err,
                                                    unsigned long long *__restrict__ work,
-                                                   unsigned long long *__restrict__ kind_work, int round_div) {
+                                                   unsigned long long *__restrict__ kind_work, int round_div,
+                                                   const PipeK K) {
     constexpr int kWarps = THREADS / 32, kSeedsPerWarp = 32 * SPL;
     extern __shared__ __align__(16) uint8_t smem_raw[];
     SplitSmem<SPL, THREADS> &sm = *reinterpret_cast<SplitSmem<SPL, THREADS> *>(smem_raw);
@@ -203,10 +236,10 @@ __global__ void __launch_bounds__(THREADS) k_split(const Node *__restrict__ node
         need[2] = 36u * nd.unit;
     }
     switch (NT) {
-        case 1: trial = search_seeds<1, SPL, THREADS>(sm, m, seed0, T[0], T[1], T[2], need[0], need[1], need[2], G, cap); break;
-        case 2: trial = search_seeds<2, SPL, THREADS>(sm, m, seed0, T[0], T[1], T[2], need[0], need[1], need[2], G, cap); break;
-        case 3: trial = search_seeds<3, SPL, THREADS>(sm, m, seed0, T[0], T[1], T[2], need[0], need[1], need[2], G, cap); break;
-        default: trial = search_seeds<4, SPL, THREADS>(sm, m, seed0, T[0], T[1], T[2], need[0], need[1], need[2], G, cap); break;
+        case 1: trial = search_seeds<1, SPL, THREADS, ARITH>(sm, m, seed0, T[0], T[1], T[2], need[0], need[1], need[2], G, cap, K); break;
+        case 2: trial = search_seeds<2, SPL, THREADS, ARITH>(sm, m, seed0, T[0], T[1], T[2], need[0], need[1], need[2], G, cap, K); break;
+        case 3: trial = search_seeds<3, SPL, THREADS, ARITH>(sm, m, seed0, T[0], T[1], T[2], need[0], need[1], need[2], G, cap, K); break;
+        default: trial = search_seeds<4, SPL, THREADS, ARITH>(sm, m, seed0, T[0], T[1], T[2], need[0], need[1], need[2], G, cap, K); break;
     }
     if (trial == ~0ull) {
         if (threadIdx.x == 0) atomicOr(err, kErrTrialLimit);
@@ -256,32 +289,38 @@ __global__ void __launch_bounds__(THREADS) k_split(const Node *__restrict__ node
     }
 }
 
-template <int SPL, int THREADS>
+template <int SPL, int THREADS, int ARITH>
 static void launch_split_t(const Node *nodes, const uint32_t *ids, uint32_t count, uint64_t *keys, uint64_t *codes,
                            uint64_t max_trials, uint32_t *err, unsigned long long *work, unsigned long long *kind_work,
                            int round_div, cudaStream_t s) {
     const size_t smem = sizeof(SplitSmem<SPL, THREADS>);
-    cudaFuncSetAttribute(k_split<SPL, THREADS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_split<SPL, THREADS><<<count, THREADS, smem, s>>>(nodes, ids, keys, codes, max_trials, err, work, kind_work, round_div);
+    cudaFuncSetAttribute(k_split<SPL, THREADS, ARITH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const PipeK K{4u, 32u, 1u << 18, 2u};
+    k_split<SPL, THREADS, ARITH><<<count, THREADS, smem, s>>>(nodes, ids, keys, codes, max_trials, err, work, kind_work,
+                                                              round_div, K);
 }
 
-bool split_tuning_valid(int spl, int threads, int round_div) {
+bool split_tuning_valid(int spl, int threads, int round_div, int arith) {
     return (spl == 1 || spl == 2 || spl == 4) && (threads == 128 || threads == 256 || threads == 512) && round_div >= 1 &&
-           round_div <= 64;
+           round_div <= 64 && (arith == 0 || arith == 1);
 }
 
 void launch_split_level(const Node *nodes, const uint32_t *ids, uint32_t count, uint64_t *keys, uint64_t *codes,
                         uint64_t max_trials, uint32_t *err, unsigned long long *work, unsigned long long *kind_work,
                         const SplitTuning &t, cudaStream_t s) {
     if (!count) return;
-#define SHG_SPLIT_CASE(SPL, TH)                                                                                  \
-    if (t.spl == SPL && t.threads == TH)                                                                        \
-        return launch_split_t<SPL, TH>(nodes, ids, count, keys, codes, max_trials, err, work, kind_work, t.round_div, s);
-    SHG_SPLIT_CASE(1, 128) SHG_SPLIT_CASE(1, 256) SHG_SPLIT_CASE(1, 512)
-    SHG_SPLIT_CASE(2, 128) SHG_SPLIT_CASE(2, 256) SHG_SPLIT_CASE(2, 512)
-    SHG_SPLIT_CASE(4, 128) SHG_SPLIT_CASE(4, 256) SHG_SPLIT_CASE(4, 512)
+#define SHG_SPLIT_CASE(SPL, TH, AR)                                                                              \
+    if (t.spl == SPL && t.threads == TH && t.arith == AR)                                                       \
+        return launch_split_t<SPL, TH, AR>(nodes, ids, count, keys, codes, max_trials, err, work, kind_work,     \
+                                           t.round_div, s);
+    SHG_SPLIT_CASE(1, 128, 0) SHG_SPLIT_CASE(1, 256, 0) SHG_SPLIT_CASE(1, 512, 0)
+    SHG_SPLIT_CASE(2, 128, 0) SHG_SPLIT_CASE(2, 256, 0) SHG_SPLIT_CASE(2, 512, 0)
+    SHG_SPLIT_CASE(4, 128, 0) SHG_SPLIT_CASE(4, 256, 0) SHG_SPLIT_CASE(4, 512, 0)
+    SHG_SPLIT_CASE(1, 128, 1) SHG_SPLIT_CASE(1, 256, 1) SHG_SPLIT_CASE(1, 512, 1)
+    SHG_SPLIT_CASE(2, 128, 1) SHG_SPLIT_CASE(2, 256, 1) SHG_SPLIT_CASE(2, 512, 1)
+    SHG_SPLIT_CASE(4, 128, 1) SHG_SPLIT_CASE(4, 256, 1) SHG_SPLIT_CASE(4, 512, 1)
 #undef SHG_SPLIT_CASE
-    launch_split_t<2, 256>(nodes, ids, count, keys, codes, max_trials, err, work, kind_work, t.round_div, s);
+    launch_split_t<2, 256, 0>(nodes, ids, count, keys, codes, max_trials, err, work, kind_work, t.round_div, s);
 }
 
 } // namespace shg

@@ -3,7 +3,8 @@
 The split-seed search and the leaf searches have launch parameters that change their speed and
 never their results (shg_engine_set_tuning): seeds per lane, threads per split block and the size
 of a split round relative to a node's expected trials, the leaf grid's blocks per SM, the register
-bound of the bipartite leaf kernel and the original leaf kernel's seeds per lane. The best values
+bound of the bipartite leaf kernel, the original leaf kernel's seeds per lane, and which pipes the
+split search's remix runs on. The best values
 depend on the leaf size (the reference's own search loops are ShockHash.h:404-434 for the original
 leaves, ShockHash2-internal.h:386-483 for the bipartite finder and ShockHash.h:451-547 /
 ShockHash2.h:290-386 for the splits).
@@ -33,7 +34,7 @@ from . import SHOCKHASH, SHOCKHASH2, TUNING_FLAT, Engine, keys_mt19937_64
 HERE = os.path.dirname(os.path.abspath(__file__))
 TABLE = os.path.join(HERE, "tuning.tsv")
 
-SPLIT_CANDIDATES = {"split_seeds_per_lane": (1, 2, 4), "split_threads": (128, 256, 512),
+SPLIT_CANDIDATES = {"split_arith": (0, 1), "split_seeds_per_lane": (1, 2, 4), "split_threads": (128, 256, 512),
                     "split_round_div": (2, 4, 8, 16, 32)}
 LEAF_CANDIDATES = {
     SHOCKHASH2: {"leaf_blocks_per_sm": (3, 4, 5, 6, 7, 8), "leaf_min_blocks": (4, 6, 8)},
@@ -102,8 +103,8 @@ class Tuner:
 def tune_config(eng, variant, leaf, n, reps=2, min_gain=0.01, log=print):
     tu = Tuner(eng, variant, leaf, n, reps=reps)
     # start from the library's untuned defaults, whatever table the engine loaded
-    base = {"split_seeds_per_lane": 2, "split_threads": 256, "split_round_div": 8, "leaf_blocks_per_sm": 0,
-            "leaf_min_blocks": 6, "sh1_seeds_per_lane": 2}
+    base = {"split_seeds_per_lane": 2, "split_threads": 256, "split_round_div": 8, "split_arith": 0,
+            "leaf_blocks_per_sm": 0, "leaf_min_blocks": 6, "sh1_seeds_per_lane": 2}
     t0_split, t0_leaf = tu.measure(base)
     params = dict(base)
     if variant != TUNING_FLAT:

@@ -22,8 +22,9 @@ def test_every_parameter_value_gives_identical_products(variant, leaf):
     keys = shg.keys_mt19937_64(77, 150_000)
     eng = shg.Engine(0)
     base = products(eng.build_u64(variant, leaf, keys, 2000))
-    settings = [dict(split_seeds_per_lane=s, split_threads=t, split_round_div=d)
-                for s, t, d in ((1, 128, 2), (4, 512, 32), (4, 128, 1), (1, 512, 64), (2, 256, 16))]
+    settings = [dict(split_seeds_per_lane=s, split_threads=t, split_round_div=d, split_arith=a)
+                for s, t, d, a in ((1, 128, 2, 0), (4, 512, 32, 1), (4, 128, 1, 0), (1, 512, 64, 1), (2, 256, 16, 1),
+                                   (2, 256, 8, 1))]
     if variant == shg.SHOCKHASH2:
         settings += [dict(leaf_blocks_per_sm=b, leaf_min_blocks=mb) for b, mb in ((1, 4), (3, 8), (8, 6))]
     else:
