@@ -41,7 +41,7 @@ LEAF, BUCKET, VARIANT = 64, 2000, 2
 SEED = 7
 METRIC = "build ns/key on 1 B200, batched vs per-leaf GPU vs CPU, bit-exact; p99 latency"
 CONFIG_NAME = "ShockHash2<64> b=2000, 10M uint64 keys (mt19937_64 seed 7) hashed to 128-bit"
-MODES = ["default (levels)", "levels", "per_leaf", "pipelined"]
+MODES = ["default (levels)", "levels", "per_leaf", "pipelined", "queue"]
 # DRAM bytes per key of the split stage (all level launches), from one ncu capture of the 1M-key
 # case scaled by keys (the node keys are read once per level and written back once)
 SPLIT_DRAM_BYTES_PER_KEY = None
@@ -410,7 +410,7 @@ def main():
             b.free()
         forms = {"default_ns_per_key": round(ms * 1e6 / n, 3)}
         if ws == 1 and not args.no_forms:
-            for name, mode in (("levels", shg.MODE_LEVELS), ("pipelined", shg.MODE_PIPELINED)):
+            for name, mode in (("levels", shg.MODE_LEVELS), ("pipelined", shg.MODE_PIPELINED), ("queue", shg.MODE_QUEUE)):
                 t, _, _ = timed_device_builds(eng, d_keys.data_ptr(), n, mode, flush, reps=3)
                 forms[f"{name}_device_ns_per_key"] = round(t * 1e6 / n, 3)
             # the per-leaf-launch comparison form on the first 1M keys of the same stream

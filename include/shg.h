@@ -51,8 +51,12 @@ typedef enum shg_mode {
     SHG_MODE_LEVELS = 1,      /* one launch per RecSplit level (a block per split node), then one persistent
                                  leaf launch whose warps drain all leaves from a device counter */
     SHG_MODE_PER_LEAF = 2,    /* comparison form: per-level split launches and one launch per leaf */
-    SHG_MODE_PIPELINED = 3    /* buckets in chunks; a chunk's leaf launch (second stream) overlaps the next
+    SHG_MODE_PIPELINED = 3,   /* buckets in chunks; a chunk's leaf launch (second stream) overlaps the next
                                  chunk's split launches (measured slower on B200: both compete for issue slots) */
+    SHG_MODE_QUEUE = 4        /* ShockHash2 with leaves of up to 64 keys: every split node and leaf in ONE
+                                 persistent launch that takes them from a device work list, a node as soon as
+                                 its bucket's levels above it are done, leaves once their bucket's splits are;
+                                 other variants run the level schedule */
 } shg_mode;
 
 typedef struct shg_params {

@@ -27,7 +27,7 @@ __all__ = ["ShgError", "Engine", "BuildResult", "ShockHash", "ShockHash2", "Shoc
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libshg.so")
 
 SHOCKHASH, SHOCKHASH2, SHOCKHASH_ROTATION = 1, 2, 3
-MODE_DEFAULT, MODE_LEVELS, MODE_PER_LEAF, MODE_PIPELINED = 0, 1, 2, 3
+MODE_DEFAULT, MODE_LEVELS, MODE_PER_LEAF, MODE_PIPELINED, MODE_QUEUE = 0, 1, 2, 3, 4
 _STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_OOM", 3: "ERR_TRIAL_LIMIT", 4: "ERR_CUDA", 5: "ERR_BUCKET",
            6: "ERR_NO_DEVICE"}
 STAGES = ("hash", "partition", "plan", "splits", "leaves", "encode", "copy_out", "total")

@@ -127,7 +127,7 @@ struct shg_engine {
         DevBuf cnt, nodes, node_off, singles, single_off, skip_bits;
     };
     std::vector<Shapes *> shapes;
-    DevBuf plan_offs, ret_scratch;
+    DevBuf plan_offs, ret_scratch, qdone;
     cudaEvent_t ev[8] = {};
     cudaStream_t stream2 = nullptr;  // leaves of the pipelined mode
     static constexpr int kMaxChunks = 64;
@@ -156,6 +156,7 @@ struct shg_engine {
         for (DevBuf *b : all) b->release();
         plan_offs.release();
         ret_scratch.release();
+        qdone.release();
         for (Shapes *sh : shapes) {
             DevBuf *sb[] = {&sh->cnt, &sh->nodes, &sh->node_off, &sh->singles, &sh->single_off, &sh->skip_bits};
             for (DevBuf *b : sb) b->release();
@@ -214,6 +215,7 @@ struct Misc {  // small device-side counters, one allocation
     unsigned int pad;
     unsigned long long work[8];
     unsigned long long split_kind[4];  // useful split evaluations by inner loop (see launch_split_level)
+    unsigned int qctr[2];              // work-queue schedule: split and leaf items taken
 };
 
 // Memo tables are cached per configuration (they cost ~3000 transcendental evaluations).
@@ -277,7 +279,7 @@ shg_status check_params(const shg_params *p, uint64_t n) {
     if (p->leaf_size < 2 || p->leaf_size > maxleaf) return fail(SHG_ERR_ARG, "leaf size out of range");
     if (p->bucket_size < 1) return fail(SHG_ERR_ARG, "bucket size must be >= 1");
     if (n >= (1ull << 32)) return fail(SHG_ERR_ARG, "at most 2^32 - 1 keys per build");
-    if (p->mode < SHG_MODE_DEFAULT || p->mode > SHG_MODE_PIPELINED) return fail(SHG_ERR_ARG, "unknown mode");
+    if (p->mode < SHG_MODE_DEFAULT || p->mode > SHG_MODE_QUEUE) return fail(SHG_ERR_ARG, "unknown mode");
     return SHG_OK;
 }
 
@@ -438,7 +440,9 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
     // runs. The pinned block is then taken before the splits, with room for descriptor words
     // bounded by the fixed bits plus 8 unary bits per node; a longer stream (not seen in
     // practice) takes a new block after encoding.
-    const bool early_keys = p->variant == SHG_SHOCKHASH2 && p->mode != SHG_MODE_PIPELINED;
+    // the work-queue schedule: bipartite leaves of up to 64 keys (other builds take the level schedule)
+    const bool queue = p->mode == SHG_MODE_QUEUE && p->variant == SHG_SHOCKHASH2 && p->leaf_size <= 64;
+    const bool early_keys = p->variant == SHG_SHOCKHASH2 && p->mode != SHG_MODE_PIPELINED && !queue;
     std::vector<uint64_t> wcap(R, 0);
     std::vector<size_t> roff(R + 1, 0);
     auto layout = [&]() {
@@ -508,7 +512,23 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
                                   p->variant == SHG_SHOCKHASH_ROTATION ? (uint32_t)p->leaf_size : 0, tun.sh1_spl);
         launches++;
     };
-    if (pipelined) {
+    if (queue) {
+        // one persistent launch: splits level by level, then leaves, each item once its bucket allows
+        const int qsmem = tree_queue_smem_per_block(tun.split.spl);
+        int qbps = std::max(1, std::min(3, (228 * 1024) / (qsmem + 1024)));
+        if (tun.leaf_bps > 0) qbps = std::min(qbps, tun.leaf_bps);
+        const int qgrid = std::max(1, std::min<int>(e->sms * qbps, (int)std::max<uint64_t>(leaf_off, (nleaves + 7) / 8)));
+        CU(e->scratch.ensure(per_warp * (uint64_t)qgrid * tree_queue_warps_per_block()));
+        CU(e->qdone.ensure(std::max<uint64_t>(nb, 1) * 4));
+        CU(cudaMemsetAsync(e->qdone.p, 0, nb * 4, s));
+        CU(cudaMemsetAsync(misc->qctr, 0, sizeof(misc->qctr), s));
+        launch_tree_queue(e->nodes.as<Node>(), d_ids, (uint32_t)leaf_off, nleaves, e->plan_offs.as<uint32_t>(), offs_stride,
+                          (uint32_t)nlevels, e->qdone.as<uint32_t>(), e->keys.as<uint64_t>(), e->codes.as<uint64_t>(),
+                          e->rib_bits.as<uint8_t>(), e->scratch.as<uint8_t>(), per_warp, smax, cmax, p->max_trials,
+                          &misc->err, misc->work, misc->split_kind, misc->qctr, tun.split, qgrid, s);
+        launches++;
+        CU(cudaEventRecord(e->ev[3], s));  // the split stage's time covers the whole queue launch
+    } else if (pipelined) {
         // Buckets in chunks: chunk c's split levels run on the engine stream, its leaves on the
         // second stream as soon as those splits are done, overlapping the next chunk's splits.
         // Node and leaf lists are in bucket order, so a chunk is a contiguous range of each list.

@@ -161,6 +161,17 @@ int leaves_sh1_warps_per_block();
 // 256-thread blocks; operations per thread and iteration from sh2_op_peak_per_iter.
 void launch_sh2_op_peak(int kind, int blocks, uint64_t iters, unsigned long long *sink);
 int sh2_op_peak_per_iter(int kind);
+// The work-queue schedule of a ShockHash2 build with leaves of up to 64 keys (shg_leaves_sh2.cu):
+// split nodes then leaves of the launch lists `ids` ([0, nsplit) the split levels in order, then
+// nleaf leaves) in one persistent launch of `grid` blocks; offs/stride/nlevels are the plan's
+// per-bucket list offsets, done[nbuckets] zeroed counters, ctr[2] zeroed item counters.
+int tree_queue_warps_per_block();
+int tree_queue_smem_per_block(int spl);
+void launch_tree_queue(const Node *nodes, const uint32_t *ids, uint32_t nsplit, uint32_t nleaf, const uint32_t *offs,
+                       uint64_t stride, uint32_t nlevels, uint32_t *done, uint64_t *keys, uint64_t *codes, uint8_t *rib_bits,
+                       uint8_t *scratch, uint64_t per_warp, uint32_t smax, uint32_t cmax, uint64_t max_trials,
+                       uint32_t *err, unsigned long long *work, unsigned long long *kind_work, unsigned int *ctr,
+                       const SplitTuning &t, int grid, cudaStream_t s);
 void launch_gr_bucket_bits(const Node *nodes, const uint32_t *bnb, uint64_t nb, const uint64_t *acc,
                            const uint64_t *codes, const uint32_t *memo_skip_bits, uint64_t *bucket_bits,
                            cudaStream_t s);

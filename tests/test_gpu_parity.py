@@ -40,7 +40,7 @@ def test_build_matches_golden(engine, name):
 def test_modes_identical(engine):
     g = load("sh2_l64_b2000")
     outs = [engine.build_hash128(2, 64, g["first"], g["second"], 2000, mode=m) for m in
-            (shg.MODE_DEFAULT, shg.MODE_LEVELS, shg.MODE_PER_LEAF, shg.MODE_PIPELINED)]
+            (shg.MODE_DEFAULT, shg.MODE_LEVELS, shg.MODE_PER_LEAF, shg.MODE_PIPELINED, shg.MODE_QUEUE)]
     for r in outs:
         assert_same(r, g)
     g = load("sh1_l30_b2000")
@@ -218,3 +218,17 @@ def test_rotation_fitting_at_scale_is_mphf(engine, leaf):
     assert np.array_equal(np.sort(out), np.arange(len(keys), dtype=np.uint64))
     idx = np.random.default_rng(2).choice(len(keys), 5000, replace=False)
     assert np.array_equal(r._mphf.query_strings([int(k).to_bytes(8, "little") for k in keys[idx]]), out[idx])
+
+
+@pytest.mark.parametrize("leaf,n,b", [(64, 300_000, 2000), (24, 60_000, 700), (9, 20_000, 50), (64, 3, 2000)])
+def test_queue_schedule_equals_levels(engine, leaf, n, b):
+    # every split node and leaf in one persistent launch gives the level schedule's products
+    rng = np.random.default_rng(leaf + n)
+    f, s = rand_u64(rng, n), unique_u64(rng, n)
+    lv = engine.build_hash128(2, leaf, f, s, b, mode=shg.MODE_LEVELS)
+    q = engine.build_hash128(2, leaf, f, s, b, mode=shg.MODE_QUEUE)
+    assert_same(q, type("G", (), {"__getitem__": lambda self, k: {"size_acc": lv.bucket_size_acc,
+                                                                  "pos_acc": lv.bucket_pos_acc, "desc": lv.descriptors,
+                                                                  "ribbon_keys": lv.ribbon_keys,
+                                                                  "ribbon_bits": lv.ribbon_bits}[k]})())
+    assert q.work["split_evals"] == lv.work["split_evals"] and q.work["uf_edges"] == lv.work["uf_edges"]
