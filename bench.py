@@ -52,6 +52,10 @@ def _workload(args):
     original ShockHash<40> with seed 11 for profiling); the defaults are the configuration above."""
     global VARIANT, LEAF, SEED, CONFIG_NAME
     VARIANT, LEAF, SEED = args.variant, args.leaf, args.seed
+    if VARIANT == 4:
+        CONFIG_NAME = (f"ShockHash2Flat<{LEAF}>, {args.n / 1e6:g}M uint64 keys (mt19937_64 seed {SEED}) as 8-byte "
+                       "strings")
+        return
     name = "ShockHash2" if VARIANT == 2 else "ShockHash"
     CONFIG_NAME = (f"{name}<{LEAF}> b={BUCKET}, {args.n / 1e6:g}M uint64 keys (mt19937_64 seed {SEED}) "
                    "hashed to 128-bit")
@@ -247,6 +251,45 @@ def leaf_report(last, leaf_ms, leaf_peak, lpeaks, extra):
     return out
 
 
+def run_flat(args):
+    """ShockHash2Flat<k> (ShockHash2Flat.h:66-171) over n uint64 keys as 8-byte strings on one GPU:
+    build time per key from host strings, and its leaf stage (k keys per bucket, one persistent leaf
+    launch) against the bipartite work model's ceiling for leaves of its size."""
+    import shockhash_b200 as shg
+    n, k = args.n, LEAF
+    keys = shg.keys_mt19937_64(SEED, n)
+    strings = u64_as_strings(keys)
+    eng = shg.Engine(0)
+    lpeaks = shg.leaf_peaks(0, large=k > 64)
+    for _ in range(args.warmup):
+        eng.build_flat_strings(k, strings).free()
+    totals, leaves = [], []
+    with ClockSampler(0) as clocks:
+        for _ in range(args.steps):
+            f = eng.build_flat_strings(k, strings)
+            totals.append(f.stage_ms[7])
+            leaves.append(f.stage_ms[4])
+            f.free()
+    w = eng.last_work()["flat_leaves"]
+    counts = {"hash_evals": w["hash_evals"], "scan_tests": w["scan_tests"], "pair_tests": w["pair_tests"],
+              "uf_edges": w["uf_edges"]}
+    leaf_ms = statistics.mean(leaves)
+    ceil_s = shg.leaf_ceiling_s(counts, lpeaks)
+    ms = statistics.mean(totals)
+    line = {"metric": METRIC, "value": round(ms * 1e6 / n, 3), "unit": "ns/key", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": CONFIG_NAME, "keys": n, "k": k, "input": "host strings (8 bytes each)"},
+            "leaf_stage": {"ms": round(leaf_ms, 3), "counts": counts,
+                           "peaks_g_per_s": {x: round(v / 1e9, 3) for x, v in lpeaks.items()},
+                           "ceiling_ms": round(ceil_s * 1e3, 3),
+                           "ceiling_ms_by_op": {x: round(counts[x] / lpeaks[x] * 1e3, 3) for x in shg.LEAF_OPS},
+                           "frac": round(ceil_s * 1e3 / leaf_ms, 4)},
+            "clocks": clocks.summary(), "tuning": eng.get_tuning(shg.TUNING_FLAT, k)}
+    eng.close()
+    print(json.dumps(line), flush=True)
+
+
 def timed_device_builds(eng, d_ptr, n, mode, flush, reps, warm=1):
     """Device-resident builds: `warm` untimed, then `reps` with the L2 flushed before each; returns
     (mean device ms, stage means, last result summary)."""
@@ -272,7 +315,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_KEYS)
     ap.add_argument("--mode", type=int, default=0)
-    ap.add_argument("--variant", type=int, default=VARIANT, choices=[1, 2])
+    ap.add_argument("--variant", type=int, default=VARIANT, choices=[1, 2, 4],
+                    help="1 ShockHash, 2 ShockHash2, 4 ShockHash2Flat (leaf = k; a profiling and C4 line)")
     ap.add_argument("--leaf", type=int, default=LEAF)
     ap.add_argument("--seed", type=int, default=SEED)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and parity leg")
@@ -288,6 +332,8 @@ def main():
     _workload(args)
     if args.impl == "reference":
         return run_reference_arm(args)
+    if VARIANT == 4:
+        return run_flat(args)
 
     import torch
     import shockhash_b200 as shg
@@ -348,6 +394,8 @@ def main():
             results.append(_Summary(r))
         barrier()
     split_kinds = eng.last_work()
+    tuning = {"table": os.path.relpath(eng.tuning_source(), ROOT) if eng.tuning_source() else None,
+              "params": eng.get_tuning(VARIANT, LEAF)}
     dev_ms = [x.stage_ms["total"] for x in results]
     # ---- end to end through the public API, host (pinned) input, host outputs (e2e)
     e2e_ms = []
@@ -511,7 +559,7 @@ def main():
             "work": last.work, "bits_per_key_trees": round(bits_per_key, 4),
             "gpu_launches": int(last.work["launches"] * args.steps),
             "clocks": clocks.summary(),
-            "cpu_baseline": cpu, "parity": parity, "forms": forms,
+            "cpu_baseline": cpu, "parity": parity, "forms": forms, "tuning": tuning,
         }
     r.free()
     if ws > 1:

@@ -348,15 +348,18 @@ int shg_int_peak(int device, uint64_t iters, double *evals_per_s, double *ms);
  * thresholds (fanout-2 and uneven split nodes), 6 = bipartite candidate-scan mask pairs,
  * 7 = bipartite isolated-key pair filter, 8 = bipartite pseudoforest edges (union-find),
  * 9 / 10 / 11 / 12 = kinds 0 / 3 / 4 / 5 with the split kernel's pipe-split arithmetic
- * (tuning parameter split_arith 1). */
+ * (tuning parameter split_arith 1), 13 / 14 / 15 = kinds 6 / 7 / 8 for bipartite leaves of more
+ * than 64 keys (64-bit masks, 100-edge tests). */
 int shg_int_peak_kind(int device, int kind, uint64_t iters, double *evals_per_s, double *ms);
 
 /* Work counts of the engine's last RecSplit build beyond shg_result.work (measurement utility, no
  * counterpart in the reference; the weights of the search stages' roofline denominators). Writes
- * min(n, 8) values: [0..2] useful split evaluations of nodes comparing 1, 2 or 3 part thresholds
+ * min(n, 13) values: [0..2] useful split evaluations of nodes comparing 1, 2 or 3 part thresholds
  * (fanout-2 and uneven nodes), [3] of quarter splits (moment sums), [4] split level launches,
  * [5] bipartite leaves' candidate-scan mask-pair tests (for each raw seed, the earlier raw seeds
- * it is paired with), [6..7] zero. */
+ * it is paired with), [6..7] zero; [8..12] the last ShockHash2Flat build's leaf search: hash
+ * evaluations, candidate pairs, pairs left by the isolated-key filter, union-find edges,
+ * candidate-scan mask-pair tests. */
 shg_status shg_engine_last_work(const shg_engine *e, uint64_t *out, int n);
 
 /* Launch parameters of the search kernels per configuration (no counterpart in the reference; they

@@ -243,11 +243,12 @@ def split_peaks(device=0, iters=1 << 15):
 LEAF_OPS = ("hash_evals", "scan_tests", "pair_tests", "uf_edges")
 
 
-def leaf_peaks(device=0, iters=1 << 15):
+def leaf_peaks(device=0, iters=1 << 15, large=False):
     """Measured operations/s of the bipartite leaf search's inner loops, keyed as LEAF_OPS:
     hashing (remix, fastrange64, mask), candidate-scan mask pairs, isolated-key pair filter,
-    pseudoforest (union-find) edges."""
-    return {name: int_peak(device, iters, k)[0] for name, k in zip(LEAF_OPS, (2, 6, 7, 8))}
+    pseudoforest (union-find) edges; `large` for leaves of more than 64 keys."""
+    kinds = (2, 13, 14, 15) if large else (2, 6, 7, 8)
+    return {name: int_peak(device, iters, k)[0] for name, k in zip(LEAF_OPS, kinds)}
 
 
 def leaf_ceiling_s(counts, peaks):
@@ -375,11 +376,13 @@ class Engine:
     def last_work(self):
         """Work counts of this engine's last build beyond BuildResult.work: useful split evaluations
         by inner loop (SPLIT_KINDS), split level launches, bipartite candidate-scan mask tests."""
-        k = np.zeros(8, np.uint64)
-        _check(lib().shg_engine_last_work(self._h, _ptr(k), 8))
+        k = np.zeros(13, np.uint64)
+        _check(lib().shg_engine_last_work(self._h, _ptr(k), 13))
         out = {name: int(v) for name, v in zip(SPLIT_KINDS, k[:4])}
         out["split_launches"] = int(k[4])
         out["leaf_scan_tests"] = int(k[5])
+        out["flat_leaves"] = {"hash_evals": int(k[8]), "pair_tests": int(k[9]), "pairs_filtered": int(k[10]),
+                              "uf_edges": int(k[11]), "scan_tests": int(k[12])}
         return out
 
     @staticmethod

@@ -215,10 +215,10 @@ int shg_int_peak(int device, uint64_t iters, double *evals_per_s, double *ms_out
 // Integer-pipe peak of one search's inner loop (0 = split quarter moments, 1 = original leaf,
 // 2 = bipartite leaf hashing, 3..5 = split compare-and-count with 1..3 thresholds, 6..8 = bipartite
 // candidate scan, pair filter and pseudoforest edges, 9..12 = kinds 0 and 3..5 with the split
-// kernel's pipe-split arithmetic).
+// kernel's pipe-split arithmetic, 13..15 = kinds 6..8 for leaves of more than 64 keys).
 int shg_int_peak_kind(int device, int kind, uint64_t iters, double *evals_per_s, double *ms_out) {
     if (kind == 0) return shg_int_peak(device, iters, evals_per_s, ms_out);
-    if (kind < 1 || kind > 12) return SHG_ERR_ARG;
+    if (kind < 1 || kind > 15) return SHG_ERR_ARG;
     if (cudaSetDevice(device) != cudaSuccess) return SHG_ERR_CUDA;
     cudaDeviceProp prop;
     cudaGetDeviceProperties(&prop, device);
@@ -244,6 +244,8 @@ int shg_int_peak_kind(int device, int kind, uint64_t iters, double *evals_per_s,
             k_int_peak_cmp<3><<<blocks, kPeakThreads>>>(it, 16384, 32768, 49152, sink);
         else if (kind <= 8)  // the bipartite leaf's scan, pair filter and pseudoforest loops (64 edges per iteration)
             shg::launch_sh2_op_peak(kind - 6, blocks, kind == 8 ? it / 64 + 1 : it, sink);
+        else if (kind >= 13)  // the same for leaves of more than 64 keys (100 edges per iteration)
+            shg::launch_sh2_op_peak(kind - 10, blocks, kind == 15 ? it / 100 + 1 : it, sink);
         else {  // 9: quarter moments, 10..12: 1..3 thresholds, with the split kernel's pipe-split arithmetic
             const shg::PipeK K{4u, 32u, 1u << 18, 2u};
             if (kind == 9) k_int_peak_pipes<4><<<blocks, kPeakThreads>>>(it, 16384, 32768, 49152, K, sink);
@@ -262,9 +264,12 @@ int shg_int_peak_kind(int device, int kind, uint64_t iters, double *evals_per_s,
     if (cudaGetLastError() != cudaSuccess) return SHG_ERR_CUDA;
     double per_iter = 2.0;
     uint64_t timed_iters = iters;
-    if (kind >= 6) {
+    if (kind >= 6 && kind <= 8) {
         per_iter = shg::sh2_op_peak_per_iter(kind - 6);
         if (kind == 8) timed_iters = iters / 64 + 1;
+    } else if (kind >= 13) {
+        per_iter = shg::sh2_op_peak_per_iter(kind - 10);
+        if (kind == 15) timed_iters = iters / 100 + 1;
     }
     *evals_per_s = per_iter * (double)timed_iters * blocks * kPeakThreads / (ms * 1e-3);
     if (ms_out) *ms_out = ms;

@@ -136,6 +136,7 @@ struct shg_engine {
     int pipe_chunks = 8;
     unsigned long long split_kind[4] = {};  // of the last build (shg_engine_last_work)
     uint64_t split_launches = 0, leaf_scan = 0;
+    unsigned long long flat_work[5] = {};  // leaf work of the last ShockHash2Flat build (shg_engine_last_work)
     // launch parameters per configuration (variant, leaf size); absent = the Tuning defaults
     std::map<std::pair<int, int>, Tuning> tuning;
     std::mutex tuning_mu;
@@ -917,10 +918,14 @@ shg_status build_flat(shg_engine *e, uint64_t k, const char *bytes, const uint64
         if (ftun.leaf_bps > 0) bps = std::min(bps, ftun.leaf_bps);
         const int grid = std::max(1, std::min<int>(e->sms * bps, (int)((nbuckets + 3) / 4)));
         CU(e->scratch.ensure(per_warp * (uint64_t)grid * 4));
+        CU(cudaMemsetAsync(&misc->work[1], 0, 5 * sizeof(unsigned long long), s));  // the fallback build's counts
         launch_leaves_sh2_ctr(e->f_nodes.as<Node>(), e->f_ids.as<uint32_t>(), (uint32_t)nbuckets, e->f_leaf_keys.as<uint64_t>(),
                               e->f_codes.as<uint64_t>(), e->f_bits.as<uint8_t>(), e->scratch.as<uint8_t>(), per_warp, smax, cmax,
                               &misc->err, misc->work, &misc->leaf_ctr, grid, s, (int)k, kQuadMinFlat, ftun.leaf_minb);
         CU(cudaGetLastError());
+        CU(cudaMemcpyAsync(e->flat_work, &misc->work[1], sizeof(e->flat_work), cudaMemcpyDeviceToHost, s));
+    } else {
+        for (auto &w : e->flat_work) w = 0;
     }
     uint32_t err = 0;
     CU(cudaMemcpyAsync(&err, &misc->err, 4, cudaMemcpyDeviceToHost, s));
@@ -1626,9 +1631,10 @@ shg_status shg_memo_table(int variant, int leaf_size, uint64_t *out) {
 
 shg_status shg_engine_last_work(const shg_engine *e, uint64_t *out, int n) {
     if (!e || !out || n < 0) return fail(SHG_ERR_ARG, "null argument");
-    const uint64_t v[8] = {e->split_kind[0], e->split_kind[1], e->split_kind[2], e->split_kind[3], e->split_launches,
-                           e->leaf_scan, 0, 0};
-    for (int k = 0; k < n && k < 8; k++) out[k] = v[k];
+    const uint64_t v[13] = {e->split_kind[0], e->split_kind[1], e->split_kind[2], e->split_kind[3], e->split_launches,
+                            e->leaf_scan, 0, 0, e->flat_work[0], e->flat_work[1], e->flat_work[2], e->flat_work[3],
+                            e->flat_work[4]};
+    for (int k = 0; k < n && k < 13; k++) out[k] = v[k];
     return SHG_OK;
 }
 

@@ -872,21 +872,27 @@ void launch_tree_queue(const Node *nodes, const uint32_t *ids, uint32_t nsplit, 
 //   kind 2: one pseudoforest edge of a 64-key leaf (LaneUF2::add on shared-memory parents; each
 //           test initialises the parents and adds 64 edges).
 namespace {
-template <int KIND>
+// W = 64: the loops of leaves of up to 64 keys (32-bit half masks, two raw seeds per 16-byte load,
+// one isolated-key word, 64-edge tests); W = 128: of larger leaves (64-bit half masks, one raw seed
+// per 16-byte load, two isolated-key words, 100-edge tests on 100 vertices).
+template <int KIND, int W>
 __global__ void __launch_bounds__(256) k_sh2_op_peak(uint64_t iters, unsigned long long *sink) {
     __shared__ uint4 masks[128];
-    __shared__ uint64_t iso[256];
-    __shared__ uint8_t par[8][64 * 32];
+    __shared__ uint64_t iso[2][256];
+    __shared__ uint8_t par[8][(W == 64 ? 64 : 128) * 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     for (int i = threadIdx.x; i < 128; i += blockDim.x) {
         const uint64_t a = remix(0x51ull * i + 7), b = remix(a);
         masks[i] = make_uint4((uint32_t)a, (uint32_t)(a >> 32), (uint32_t)b, (uint32_t)(b >> 32));
     }
-    for (int i = threadIdx.x; i < 256; i += blockDim.x) iso[i] = remix(0x93ull * i + 3) & remix(0x77ull * i + 1);
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+        iso[0][i] = remix(0x93ull * i + 3) & remix(0x77ull * i + 1);
+        iso[1][i] = remix(0x95ull * i + 5) & remix(0x79ull * i + 2);
+    }
     __syncthreads();
     uint64_t acc = 0;
-    if (KIND == 0) {
+    if (KIND == 0 && W == 64) {
         const uint64_t r = remix(tid);
         const uint32_t tA = (uint32_t)r, tB = (uint32_t)(r >> 32), full = 0xFFFFFFFFu;
         uint32_t hits = 0;
@@ -896,10 +902,21 @@ __global__ void __launch_bounds__(256) k_sh2_op_peak(uint64_t iters, unsigned lo
             hits += z == 0;
         }
         acc = hits;
+    } else if (KIND == 0) {
+        const uint64_t tA = remix(tid), tB = remix(tA), full = ~0ull;
+        uint32_t hits = 0;
+        for (uint64_t i = 0; i < iters; i++) {
+            const uint4 w = masks[i & 127];
+            const uint64_t a = (uint64_t)w.y << 32 | w.x, b = (uint64_t)w.w << 32 | w.z;
+            hits += (((a | tB) ^ full) == 0) | (((b | tA) ^ full) == 0);
+        }
+        acc = hits;
     } else if (KIND == 1) {
         uint32_t j = 1 + (uint32_t)(tid & 63), i = (uint32_t)(tid >> 6) % j, hits = 0;
         for (uint64_t q = 0; q < iters; q++) {
-            hits += (iso[j & 255] & iso[i & 255]) == 0;
+            uint64_t x = iso[0][j & 255] & iso[0][i & 255];
+            if (W == 128) x |= iso[1][j & 255] & iso[1][i & 255];
+            hits += x == 0;
             if (++i == j) {  // (j, i) in lexicographic order, as the pair enumeration steps
                 i = 0;
                 j++;
@@ -907,13 +924,14 @@ __global__ void __launch_bounds__(256) k_sh2_op_peak(uint64_t iters, unsigned lo
         }
         acc = hits;
     } else {
-        LaneUF2<64> uf{par[warp], lane, 0, 0};
+        constexpr uint32_t M = W == 64 ? 64 : 100, H = W == 64 ? 32 : 50;
+        LaneUF2<W> uf{par[warp], lane, 0, 0};
         uint64_t x = remix(tid), ok = 0;
         for (uint64_t t = 0; t < iters; t++) {
-            uf.init(64);
-            for (int k = 0; k < 64; k++) {
+            uf.init(M);
+            for (uint32_t k = 0; k < M; k++) {
                 x = x * 0x9E3779B97F4A7C15ull + 1;
-                ok += uf.add(32 + (uint32_t)((x >> 20) & 31), (uint32_t)((x >> 40) & 31));
+                ok += uf.add(H + (uint32_t)(((x >> 20) & 0xFFFF) * H >> 16), (uint32_t)(((x >> 40) & 0xFFFF) * H >> 16));
             }
         }
         acc = ok;
@@ -922,12 +940,21 @@ __global__ void __launch_bounds__(256) k_sh2_op_peak(uint64_t iters, unsigned lo
 }
 }  // namespace
 
-// Operations per launch thread and iteration: 2 (kind 0), 1 (kind 1), 64 (kind 2).
-int sh2_op_peak_per_iter(int kind) { return kind == 0 ? 2 : kind == 1 ? 1 : 64; }
+// Operations per launch thread and iteration: kinds 0..2 for leaves of up to 64 keys (2 scan tests,
+// 1 pair filter, 64 edges), kinds 3..5 for larger leaves (1 scan test, 1 pair filter, 100 edges).
+int sh2_op_peak_per_iter(int kind) {
+    static const int per[6] = {2, 1, 64, 1, 1, 100};
+    return per[kind];
+}
 void launch_sh2_op_peak(int kind, int blocks, uint64_t iters, unsigned long long *sink) {
-    if (kind == 0) k_sh2_op_peak<0><<<blocks, 256>>>(iters, sink);
-    else if (kind == 1) k_sh2_op_peak<1><<<blocks, 256>>>(iters, sink);
-    else k_sh2_op_peak<2><<<blocks, 256>>>(iters, sink);
+    switch (kind) {
+        case 0: k_sh2_op_peak<0, 64><<<blocks, 256>>>(iters, sink); break;
+        case 1: k_sh2_op_peak<1, 64><<<blocks, 256>>>(iters, sink); break;
+        case 2: k_sh2_op_peak<2, 64><<<blocks, 256>>>(iters, sink); break;
+        case 3: k_sh2_op_peak<0, 128><<<blocks, 256>>>(iters, sink); break;
+        case 4: k_sh2_op_peak<1, 128><<<blocks, 256>>>(iters, sink); break;
+        default: k_sh2_op_peak<2, 128><<<blocks, 256>>>(iters, sink); break;
+    }
 }
 
 // ------------------------------------------------------------------ no-allocation variant
