@@ -936,7 +936,7 @@ __global__ void __launch_bounds__(256) k_sh2_op_peak(uint64_t iters, unsigned lo
         }
         acc = ok;
     }
-    if ((uint32_t)acc == 0x9E3779B9u + (uint32_t)tid) atomicAdd(sink, 1ull);  // keeps the loops live
+    sink[tid] = acc;  // every thread's result is stored: no loop can fold
 }
 }  // namespace
 

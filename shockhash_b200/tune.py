@@ -48,7 +48,7 @@ NAMES = {SHOCKHASH: "ShockHash<{}>", SHOCKHASH2: "ShockHash2<{}>", TUNING_FLAT: 
 
 
 class Tuner:
-    def __init__(self, eng, variant, leaf, n, seed=7, reps=2, bucket=2000):
+    def __init__(self, eng, variant, leaf, n, seed=7, reps=3, bucket=2000):
         self.eng, self.variant, self.leaf, self.bucket, self.reps = eng, variant, leaf, bucket, reps
         keys = keys_mt19937_64(seed, n)
         if variant == TUNING_FLAT:
@@ -57,6 +57,7 @@ class Tuner:
         self.keys = keys
         self.reference = None
         self.builds = 0
+        self.trials = []
 
     def _build(self):
         """One build: (split ms, leaf ms, fingerprint of the products)."""
@@ -86,7 +87,8 @@ class Tuner:
         return best_s, best_l
 
     def descend(self, params, candidates, stage, min_gain):
-        """Coordinate descent over `candidates`, timing `stage` (0 split, 1 leaves)."""
+        """Coordinate descent over `candidates`, timing `stage` (0 split, 1 leaves); every candidate's
+        time goes to self.trials."""
         best = self.measure(params)[stage]
         for name, values in candidates.items():
             for v in values:
@@ -94,13 +96,15 @@ class Tuner:
                     continue
                 trial = dict(params, **{name: v})
                 t = self.measure(trial)[stage]
+                self.trials.append({"stage": ("splits", "leaves")[stage], name: v, "ms": round(t, 3),
+                                    "incumbent_ms": round(best, 3)})
                 if t < best * (1.0 - min_gain):
                     params, best = trial, t
             self.eng.set_tuning(self.variant, self.leaf, **params)
         return params, best
 
 
-def tune_config(eng, variant, leaf, n, reps=2, min_gain=0.01, log=print):
+def tune_config(eng, variant, leaf, n, reps=3, min_gain=0.02, log=print):
     tu = Tuner(eng, variant, leaf, n, reps=reps)
     # start from the library's untuned defaults, whatever table the engine loaded
     base = {"split_seeds_per_lane": 2, "split_threads": 256, "split_round_div": 8, "split_arith": 0,
@@ -113,7 +117,8 @@ def tune_config(eng, variant, leaf, n, reps=2, min_gain=0.01, log=print):
     t1_split, t1_leaf = tu.measure(params)
     res = {"variant": variant, "leaf": leaf, "keys": n, "params": params,
            "default_ms": {"splits": round(t0_split, 3), "leaves": round(t0_leaf, 3)},
-           "tuned_ms": {"splits": round(t1_split, 3), "leaves": round(t1_leaf, 3)}, "builds": tu.builds}
+           "tuned_ms": {"splits": round(t1_split, 3), "leaves": round(t1_leaf, 3)}, "builds": tu.builds,
+           "trials": tu.trials}
     log(json.dumps(res))
     return res
 
@@ -143,8 +148,8 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--out", default=TABLE)
     ap.add_argument("--device", type=int, default=0)
-    ap.add_argument("--reps", type=int, default=2)
-    ap.add_argument("--min-gain", type=float, default=0.01)
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--min-gain", type=float, default=0.02, help="relative gain a value must show to be kept")
     ap.add_argument("--only", default="", help="comma-separated variant:leaf pairs (default: all configurations)")
     a = ap.parse_args(argv)
     prev = os.environ.get("SHG_TUNING_TABLE")
