@@ -351,7 +351,8 @@ def main():
     d_keys = torch.from_numpy(keys.view(np.int64)).to(dev)
     h_keys = torch.from_numpy(keys.view(np.int64)).pin_memory()
     eng = shg.Engine(local)
-    peaks = shg.split_peaks(local)
+    peak_forms = {}
+    peaks = shg.split_peaks(local, detail=peak_forms)
     leaf_peak, _ = shg.int_peak(local, 1 << 15, 1 if VARIANT == 1 else 2)
     lpeaks = shg.leaf_peaks(local) if VARIANT == 2 else None
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
@@ -549,6 +550,8 @@ def main():
                          "traffic": (None if SPLIT_DRAM_BYTES_PER_KEY is None else
                                      round(SPLIT_DRAM_BYTES_PER_KEY * n / max(1, split_kinds["split_launches"]))),
                          "peaks_by_kind_gevals": {k: round(v / 1e9, 3) for k, v in peaks.items()},
+                         "peaks_by_form_gevals": {k: {f: round(x / 1e9, 3) for f, x in v.items()}
+                                                  for k, v in peak_forms.items()},
                          "evals_by_kind": {k: split_kinds[k] for k in shg.SPLIT_KINDS},
                          "launches": split_kinds["split_launches"],
                          "note": "useful split evaluations (the reference's sequential count) / device time of the "

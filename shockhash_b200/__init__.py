@@ -232,12 +232,18 @@ TUNING_PARAMS = ("split_seeds_per_lane", "split_threads", "split_round_div", "sp
 TUNING_FLAT = 4
 
 
-def split_peaks(device=0, iters=1 << 15):
+def split_peaks(device=0, iters=1 << 15, detail=None):
     """Measured evaluations/s of each split inner loop, keyed as SPLIT_KINDS: the faster of the two
-    arithmetic forms the split kernel can run (split_arith 0 and 1), so the ceiling holds for both."""
+    arithmetic forms the split kernel can run (split_arith 0 and 1), so the ceiling holds for both.
+    `detail`, a dict, receives both forms' rates per kind."""
     plain, pipes = (3, 4, 5, 0), (10, 11, 12, 9)
-    return {name: max(int_peak(device, iters, a)[0], int_peak(device, iters, b)[0])
-            for name, a, b in zip(SPLIT_KINDS, plain, pipes)}
+    out = {}
+    for name, a, b in zip(SPLIT_KINDS, plain, pipes):
+        ra, rb = int_peak(device, iters, a)[0], int_peak(device, iters, b)[0]
+        out[name] = max(ra, rb)
+        if detail is not None:
+            detail[name] = {"arith_0": ra, "arith_1": rb}
+    return out
 
 
 LEAF_OPS = ("hash_evals", "scan_tests", "pair_tests", "uf_edges")

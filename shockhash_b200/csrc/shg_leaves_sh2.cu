@@ -710,7 +710,7 @@ void launch_v2(const Node *nodes, const uint32_t *ids, uint32_t count, const uin
 // Keys rewritten by another SM's partition are read past L1.
 constexpr int kQueueThreads = 256;
 constexpr int kQueueWarps = kQueueThreads / 32;
-constexpr uint32_t kQueueWaitLimit = 1u << 20;  // polls of at least 64 ns: about a second, far beyond any node
+constexpr uint32_t kQueueWaitLimit = 1u << 18;  // polls of at least 64 ns: a fifth of a second or more, far beyond any node
 
 __device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t *p) {
     uint32_t v;
@@ -718,10 +718,12 @@ __device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t *p) {
     return v;
 }
 
-// Waits until *done >= need (one thread); false when the wait ran out.
-__device__ bool wait_done(const uint32_t *done, uint32_t need) {
+// Waits until *done >= need (one thread); false when the wait ran out, or at once when another wait
+// of the launch has run out already (kErrInternal in *err), so that a fault ends the launch quickly.
+__device__ bool wait_done(const uint32_t *done, uint32_t need, const uint32_t *err) {
     for (uint32_t it = 0; it < kQueueWaitLimit; it++) {
         if (ld_acquire_gpu(done) >= need) return true;
+        if ((it & 255) == 255 && (ld_acquire_gpu(err) & kErrInternal)) return false;
         __nanosleep(64);
     }
     return false;
@@ -759,7 +761,7 @@ __global__ void __launch_bounds__(kQueueThreads, 3)
         if (i >= nsplit) break;
         const uint32_t id = ids[i];
         const Node nd = nodes[id];
-        if (threadIdx.x == 0 && !wait_done(&done[nd.bucket], splits_above(offs, stride, nd.bucket, nd.level)))
+        if (threadIdx.x == 0 && !wait_done(&done[nd.bucket], splits_above(offs, stride, nd.bucket, nd.level), err))
             atomicOr(err, kErrInternal);
         __syncthreads();
         split_node<SPL, kQueueThreads, ARITH, true>(ssm, nd, id, keys, codes, max_trials, err, work, kind_work,
@@ -782,7 +784,7 @@ __global__ void __launch_bounds__(kQueueThreads, 3)
         li = __shfl_sync(0xffffffffu, li, 0);
         if (li >= nleaf) break;
         const uint32_t b = nodes[ids[nsplit + li]].bucket;
-        if (lane == 0 && !wait_done(&done[b], splits_above(offs, stride, b, nlevels))) atomicOr(err, kErrInternal);
+        if (lane == 0 && !wait_done(&done[b], splits_above(offs, stride, b, nlevels), err)) atomicOr(err, kErrInternal);
         __syncwarp();
         sh2_leaf<64, NodeLeaves, true>(leaves, li, keys, rib_bits, sm, g, uf, lane, smax, cmax, kQuadMinRecSplit, err, lw);
     }
