@@ -118,6 +118,13 @@ SHG_HD bool float_accurate_elegant(uint64_t x, uint64_t y) {  // :93-96
     unpair_elegant(pair_elegant(x, y), a, b);
     return a == x && b == y;
 }
+// The same test for raw seeds of a leaf search: below 2^24 it always holds, so the square root is
+// skipped there. z = pair_elegant(x, y) lies in [f^2, (f + 1)^2 - 1] with f <= 2^24; sqrt(f^2) = f
+// is exact, and sqrt((f + 1)^2 - 1) stays more than 2^-26 below f + 1 while doubles near f are at
+// most 2^-28 apart, so the correctly rounded square root floors to f and unpairing is exact.
+SHG_HD bool float_accurate_elegant_seeds(uint64_t x, uint64_t y) {
+    return (x | y) < (1ull << 24) || float_accurate_elegant(x, y);
+}
 
 // ------------------------------------------------------------------ leaf cell hashes
 // Original ShockHash candidate cells (TinyBinaryCuckooHashTable.h:138-149).

@@ -369,12 +369,12 @@ __device__ __forceinline__ void sh2_leaf(const Src &src, uint32_t li, const uint
                 const auto ts = cx.mp(s);
                 const auto tA = ts.a, tB = ts.b;
                 auto visit = [&](uint64_t p, MaskPair<typename LeafCtx<MAXM>::Mask> w) {
-                    if (p < s && (w.a | tB) == cx.full && float_accurate_elegant(p, s)) {
+                    if (p < s && (w.a | tB) == cx.full && float_accurate_elegant_seeds(p, s)) {
                         ha0 = mineA == 0 ? (uint32_t)p : ha0;
                         ha1 = mineA == 1 ? (uint32_t)p : ha1;
                         mineA++;
                     }
-                    if ((w.b | tA) == cx.full && float_accurate_elegant(s, p)) {
+                    if ((w.b | tA) == cx.full && float_accurate_elegant_seeds(s, p)) {
                         hb0 = mineB == 0 ? (uint32_t)p : hb0;
                         hb1 = mineB == 1 ? (uint32_t)p : hb1;
                         mineB++;
@@ -466,13 +466,13 @@ __device__ __forceinline__ void sh2_leaf(const Src &src, uint32_t li, const uint
             } else if (cx.quad) {  // more than two partners on a side (rare): scan again
                 const auto tA = cx.maskA(s), tB = cx.maskB(s);
                 for (uint64_t a = 0; a < s && mine; a++)
-                    if ((cx.maskA(a) | tB) == cx.full && float_accurate_elegant(a, s)) {
+                    if ((cx.maskA(a) | tB) == cx.full && float_accurate_elegant_seeds(a, s)) {
                         cx.csa(pos) = (uint32_t)a;
                         cx.csb(pos) = (uint32_t)s;
                         pos++;
                     }
                 for (uint64_t b = 0; b <= s && mine; b++)
-                    if ((cx.maskB(b) | tA) == cx.full && float_accurate_elegant(s, b)) {
+                    if ((cx.maskB(b) | tA) == cx.full && float_accurate_elegant_seeds(s, b)) {
                         cx.csa(pos) = (uint32_t)s;
                         cx.csb(pos) = (uint32_t)b;
                         pos++;

@@ -223,3 +223,29 @@ def test_ref_stats_phase_times(ref):
     assert res["keys"] == 20000 and res["threads"] == 1
     assert 0 < res["leaves_ms"] and 0 < res["splits_ms"]
     assert res["leaves_ms"] + res["splits_ms"] <= res["total_ms"] * 1.02
+
+
+def test_elegant_pairing_of_raw_seeds_is_float_accurate():
+    # The bipartite leaf kernel skips isFloatAccurateElegant (PairingFunction.h:93-96) for raw seeds
+    # below 2^24, where unpairing with an IEEE double square root is always exact: checked here
+    # exhaustively below 2^11, around every power of two, and on random pairs below 2^24.
+    def accurate(x, y):
+        x, y = x.astype(np.uint64), y.astype(np.uint64)
+        z = np.where(x < y, y * y + x, x * x + x + y)
+        f = np.floor(np.sqrt(z.astype(np.float64))).astype(np.uint64)
+        sq = f * f
+        first = z - sq < f
+        a = np.where(first, z - sq, f)
+        b = np.where(first, f, z - sq - f)
+        return (a == x) & (b == y)
+    g = np.arange(2048, dtype=np.uint64)
+    xs, ys = np.meshgrid(g, g)
+    assert accurate(xs.ravel(), ys.ravel()).all()
+    rng = np.random.default_rng(5)
+    r = rng.integers(0, 1 << 24, size=(2, 4_000_000), dtype=np.uint64)
+    assert accurate(r[0], r[1]).all()
+    edges = np.array([(1 << e) + d for e in range(1, 25) for d in (-2, -1, 0, 1) if (1 << e) + d < (1 << 24)],
+                     dtype=np.uint64)
+    other = rng.integers(0, 1 << 24, size=(len(edges), 2000), dtype=np.uint64)
+    ee = np.repeat(edges, 2000)
+    assert accurate(ee, other.ravel()).all() and accurate(other.ravel(), ee).all()
