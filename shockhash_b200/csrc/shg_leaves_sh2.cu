@@ -384,16 +384,40 @@ __device__ __forceinline__ void sh2_leaf(const Src &src, uint32_t li, const uint
                 uint32_t p = 0;
                 if constexpr (sizeof(typename LeafCtx<MAXM>::Mask) == 4) {
                     // two raw seeds per 16-byte load; one combined test rejects the common case
-                    // that neither side of either seed covers the half table
+                    // that neither side of either seed covers the half table. A hit only
+                    // appends its 16-byte slot (p / 2 < 128) to a register queue of up to 8;
+                    // the hits are visited after the loop, in the same ascending order, so the
+                    // loop itself stays free of the recording path. Past 8 hits the scan
+                    // resumes, visiting directly, from the 9th hit's slot on.
                     const uint4 *m2 = reinterpret_cast<const uint4 *>(sm.mask);
                     const uint32_t full = cx.full;
+                    uint64_t hq = 0;
+                    uint32_t nh = 0, resume = 0;
                     for (; p + 2 <= in_sm; p += 2) {
                         const uint4 w = m2[p >> 1];
                         const uint32_t z = min(min((w.x | tB) ^ full, (w.y | tA) ^ full),
                                                min((w.z | tB) ^ full, (w.w | tA) ^ full));
                         if (z == 0) {
-                            visit(p, MaskPair<uint32_t>{w.x, w.y});
-                            visit(p + 1, MaskPair<uint32_t>{w.z, w.w});
+                            if (nh < 8) hq |= (uint64_t)(p >> 1) << (8 * nh);
+                            else if (nh == 8) resume = p;
+                            nh++;
+                        }
+                    }
+                    for (uint32_t h = 0; h < min(nh, 8u); h++) {
+                        const uint32_t q = (uint32_t)((hq >> (8 * h)) & 0xFF) * 2;
+                        const uint4 w = m2[q >> 1];
+                        visit(q, MaskPair<uint32_t>{w.x, w.y});
+                        visit(q + 1, MaskPair<uint32_t>{w.z, w.w});
+                    }
+                    if (nh > 8) {
+                        for (uint32_t q = resume; q + 2 <= in_sm; q += 2) {
+                            const uint4 w = m2[q >> 1];
+                            const uint32_t z = min(min((w.x | tB) ^ full, (w.y | tA) ^ full),
+                                                   min((w.z | tB) ^ full, (w.w | tA) ^ full));
+                            if (z == 0) {
+                                visit(q, MaskPair<uint32_t>{w.x, w.y});
+                                visit(q + 1, MaskPair<uint32_t>{w.z, w.w});
+                            }
                         }
                     }
                 }
