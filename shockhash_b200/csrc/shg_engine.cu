@@ -1258,9 +1258,15 @@ shg_status shg_result_load(const char *path, shg_params *p, shg_result *out) {
     if (fseek(f, 0, SEEK_END) != 0) return bad("seek failed");
     const uint64_t fsize = (uint64_t)ftell(f);
     const uint64_t fixed = 8 + 8 + 40;
-    if (nb == 0 || nb > fsize / 16 || rn > n || bits < 1) return bad("inconsistent sizes");
+    {  // the configuration must be one this library builds
+        shg_params cp{(int)vl[0], (int)vl[1], head[0], SHG_MODE_DEFAULT, 0};
+        if (vl[0] > 16 || vl[1] > 4096 || check_params(&cp, 0) != SHG_OK) return bad("unknown configuration");
+    }
+    // every count is bounded by the file size before any product is formed
+    if (nb == 0 || nb > fsize / 16 || rn > n || rn > fsize / 9 || bits < 1 || bits > 8 * fsize)
+        return bad("inconsistent sizes");
     if (fseek(f, (long)(fixed + 16 * (nb + 1)), SEEK_SET) != 0 || fread(&words, 8, 1, f) != 1) return bad("truncated");
-    if (words != ((bits + 7) / 8 + 14) / 8) return bad("descriptor word count does not match its bit count");
+    if (words > fsize / 8 || words != ((bits + 7) / 8 + 14) / 8) return bad("descriptor word count does not match its bit count");
     if (fsize != fixed + 16 * (nb + 1) + 8 + 8 * words + 9 * rn) return bad("file size does not match its header");
     const size_t acc_bytes = (nb + 1) * 8;
     const size_t bytes = 2 * acc_bytes + words * 8 + rn * 9 + 64;
@@ -1291,7 +1297,11 @@ shg_status shg_result_load(const char *path, shg_params *p, shg_result *out) {
                     fseek(f, 8, SEEK_CUR) == 0 && fread(out->descriptors, 8, words, f) == words &&
                     fread(out->ribbon_keys, 8, rn, f) == rn && fread(out->ribbon_bits, 1, rn, f) == rn;
     fclose(f);
-    if (!ok || out->bucket_size_acc[nb] != n) {
+    // the accumulators start at zero, never decrease, end at n keys and within the code bits
+    bool mono = ok && out->bucket_size_acc[0] == 0 && out->bucket_pos_acc[0] == 0;
+    for (uint64_t b = 0; mono && b < nb; b++)
+        mono = out->bucket_size_acc[b] <= out->bucket_size_acc[b + 1] && out->bucket_pos_acc[b] <= out->bucket_pos_acc[b + 1];
+    if (!mono || out->bucket_size_acc[nb] != n || out->bucket_pos_acc[nb] >= bits) {
         release_pinned(blk);
         memset(out, 0, sizeof(shg_result));
         return fail(SHG_ERR_ARG, std::string(path) + ": truncated or inconsistent arrays");

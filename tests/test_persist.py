@@ -64,6 +64,20 @@ def test_damaged_files_are_rejected(tmp_path, port):
     raw = open(path, "rb").read()
     cases = {"magic": b"XXXXXXXX" + raw[8:], "truncated": raw[:-3], "longer": raw + b"\0",
              "words": raw[:56 + 16 * (res.nbuckets + 1)] + struct.pack("<Q", 1) + raw[56 + 16 * (res.nbuckets + 1) + 8:]}
+    nb = res.nbuckets
+    acc0 = 56  # bucket_size_acc, then bucket_pos_acc, (nb + 1) words each
+    def put(data, off, value):
+        return data[:off] + struct.pack("<Q", value) + data[off + 8:]
+    cases.update({
+        "variant": raw[:8] + struct.pack("<I", 9) + raw[12:],
+        "leaf_size": raw[:12] + struct.pack("<I", 500) + raw[16:],
+        "size_acc_decreases": put(raw, acc0 + 8 * 2, 0),
+        "size_acc_start": put(raw, acc0, 1),
+        "pos_acc_decreases": put(raw, acc0 + 8 * (nb + 1) + 8 * 2, 0),
+        "pos_acc_past_bits": put(raw, acc0 + 8 * (nb + 1) + 8 * nb, res.desc_bits + 64),
+        "huge_ribbon_count": raw[:48] + struct.pack("<Q", (1 << 63) + 5) + raw[56:],
+        "huge_bit_count": raw[:40] + struct.pack("<Q", (1 << 62)) + raw[48:],
+    })
     for name, data in cases.items():
         p = str(tmp_path / (name + ".shg"))
         with open(p, "wb") as fh:
