@@ -41,10 +41,15 @@ LEAF, BUCKET, VARIANT = 64, 2000, 2
 SEED = 7
 METRIC = "build ns/key on 1 B200, batched vs per-leaf GPU vs CPU, bit-exact; p99 latency"
 CONFIG_NAME = "ShockHash2<64> b=2000, 10M uint64 keys (mt19937_64 seed 7) hashed to 128-bit"
-MODES = ["default (levels)", "levels", "per_leaf", "pipelined", "queue"]
-# DRAM bytes per key of the split stage (all level launches), from one ncu capture of the 1M-key
-# case scaled by keys (the node keys are read once per level and written back once)
-SPLIT_DRAM_BYTES_PER_KEY = None
+MODES = ["default (work queue for ShockHash2 with leaves of up to 64 keys, else levels)", "levels", "per_leaf",
+         "pipelined", "queue"]
+# DRAM bytes (read + write) per key of one launch, from one ncu capture of the 1M-key case
+# (profiles/k_tree_queue_sh2_l64.md, profiles/k_split_sh2_l64.md) scaled by keys: the work-queue
+# kernel (the whole search: node keys read, retrieval bits and spilled leaf scratch written) and a
+# quarter-split level launch of the level schedule (node keys read once; the partition's writes
+# stay in L2).
+QUEUE_DRAM_BYTES_PER_KEY = (9_491_200 + 43_116_288) / 1_000_000
+SPLIT_DRAM_BYTES_PER_KEY = (6_560_256 + 512) / 1_000_000
 
 
 def _workload(args):
@@ -221,6 +226,30 @@ def compare_products(r, b):
     }
     return {"bit_exact": all(checks.values()), "compared": sorted(checks), "mismatch": sorted(k for k, v in checks.items() if not v),
             "descriptor_words": int(len(b.desc)), "retrieval_keys": int(len(b.ribbon_keys))}
+
+
+def search_roofline(queue_used, achieved, peak_eff, split_ms, split_ceil_s, leaf_ceil_s, n):
+    """The dominant kernel against its ceiling. Level schedule: k_split, useful split evaluations per
+    second against the evaluation-weighted peak of the node kinds' loops. Work-queue schedule:
+    k_tree_queue, which runs both searches; its ceiling is the split ceiling plus the leaf ceiling
+    (section 5 of the work model), expressed in split-evaluation equivalents so that `achieved` and
+    `peak` keep the split kernel's unit."""
+    if not queue_used:
+        return {"kernel": "k_split (RecSplit split-seed search, level schedule)", "bound": "int",
+                "achieved": round(achieved / 1e9, 3), "peak": round(peak_eff / 1e9, 3), "unit": "Gevals/s",
+                "frac": round(achieved / peak_eff, 4), "traffic": round(SPLIT_DRAM_BYTES_PER_KEY * n),
+                "traffic_note": "DRAM bytes of a quarter-split level launch (ncu, 1M keys, scaled by keys)",
+                "note": "useful split evaluations (the reference's sequential count) / device time of the split "
+                        "stage; peak = each node kind's evaluations at its inner loop's measured rate"}
+    t = split_ms * 1e-3
+    equiv = (split_ceil_s + leaf_ceil_s) * peak_eff  # split-evaluation equivalents of all the search work
+    return {"kernel": "k_tree_queue (split nodes and leaves in one persistent launch)", "bound": "int",
+            "achieved": round(equiv / t / 1e9, 3), "peak": round(peak_eff / 1e9, 3),
+            "unit": "Gevals/s (split-evaluation equivalents)", "frac": round((split_ceil_s + leaf_ceil_s) / t, 4),
+            "traffic": round(QUEUE_DRAM_BYTES_PER_KEY * n),
+            "traffic_note": "DRAM bytes of the launch (ncu, 1M keys, scaled by keys)",
+            "note": "frac = (split evaluations per node kind at that kind's measured loop peak + the bipartite leaf "
+                    "work model's ceiling) / the launch's device time"}
 
 
 def leaf_report(last, leaf_ms, leaf_peak, lpeaks, extra):
@@ -417,6 +446,13 @@ def main():
     barrier()
     r2.free()
 
+    # the level schedule's stages, measured apart for the per-kernel fractions when the default build
+    # runs both searches in the work-queue kernel
+    lv = None
+    if VARIANT == 2 and LEAF <= 64 and args.mode in (0, 4):
+        t_lv, st_lv, last_lv = timed_device_builds(eng, d_keys.data_ptr(), n, shg.MODE_LEVELS, flush, reps=2)
+        lv = (st_lv, last_lv, eng.last_work())
+
     def maxed(x):
         if ws == 1:
             return x
@@ -435,6 +471,13 @@ def main():
     achieved = last.work["split_evals"] / (split_ms * 1e-3)
     # denominator: each node kind's useful evaluations at that kind's measured loop peak
     peak_eff = shg.weighted_split_peak(split_kinds, peaks)
+    # the default ShockHash2 build (leaves <= 64) runs both searches in the one work-queue kernel,
+    # whose time is the split stage's: its ceiling is the split ceiling plus the leaf ceiling
+    queue_used = VARIANT == 2 and LEAF <= 64 and args.mode in (0, 4)
+    split_ceil_s = sum(split_kinds[k] / peaks[k] for k in shg.SPLIT_KINDS if split_kinds[k])
+    leaf_ceil_s = (shg.leaf_ceiling_s({"hash_evals": last.work["leaf_evals"], "scan_tests": split_kinds["leaf_scan_tests"],
+                                       "pair_tests": last.work["pairs"], "uf_edges": last.work["uf_edges"]}, lpeaks)
+                   if lpeaks else 0.0)
     bits_per_key = (r.descriptors.size * 64) / n
 
     line = None
@@ -465,9 +508,9 @@ def main():
             # the per-leaf-launch comparison form on the first 1M keys of the same stream
             pl_n = min(n, int(os.environ.get("SHG_PER_LEAF_SAMPLE", "1000000")))
             t_pl, st_pl, _ = timed_device_builds(eng, d_keys.data_ptr(), pl_n, shg.MODE_PER_LEAF, flush, reps=1)
-            t_b, st_b, _ = timed_device_builds(eng, d_keys.data_ptr(), pl_n, shg.MODE_LEVELS, flush, reps=3)
+            t_b, st_b, _ = timed_device_builds(eng, d_keys.data_ptr(), pl_n, args.mode, flush, reps=3)
             rp = eng.build_u64_device(VARIANT, LEAF, d_keys.data_ptr(), pl_n, BUCKET, shg.MODE_PER_LEAF)
-            rl = eng.build_u64_device(VARIANT, LEAF, d_keys.data_ptr(), pl_n, BUCKET, shg.MODE_LEVELS)
+            rl = eng.build_u64_device(VARIANT, LEAF, d_keys.data_ptr(), pl_n, BUCKET, args.mode)
             forms["per_leaf"] = {"keys": pl_n, "per_leaf_launch_ns_per_key": round(t_pl * 1e6 / pl_n, 3),
                                  "batched_ns_per_key": round(t_b * 1e6 / pl_n, 3),
                                  "batched_speedup": round(t_pl / t_b, 2),
@@ -520,8 +563,13 @@ def main():
             del t_keys
             t, st, lw = timed_device_builds(eng, d_t.data_ptr(), tn, args.mode, flush, reps=2)
             sk = eng.last_work()
+            t_split_ceil = sum(sk[k] / peaks[k] for k in shg.SPLIT_KINDS if sk[k])
+            t_leaf_ceil = (shg.leaf_ceiling_s({"hash_evals": lw.work["leaf_evals"], "scan_tests": sk["leaf_scan_tests"],
+                                               "pair_tests": lw.work["pairs"], "uf_edges": lw.work["uf_edges"]}, lpeaks)
+                           if lpeaks else 0.0)
+            searches_ms = st["splits"] + st["leaves"]  # one work-queue launch, or the split and leaf launches
             tgt = {"keys": tn, "device_ns_per_key": round(t * 1e6 / tn, 3), "stage_ms": st,
-                   "split_frac": round(lw.work["split_evals"] / (st["splits"] * 1e-3) / shg.weighted_split_peak(sk, peaks), 4)}
+                   "search_frac": round((t_split_ceil + t_leaf_ceil) * 1e3 / searches_ms, 4)}
             if cpu:
                 tgt["vs_cpu_reference"] = round(cpu["value"] / (t * 1e6 / tn), 1)
             if "per_leaf" in forms:
@@ -544,21 +592,20 @@ def main():
             "stage_ms": {k: round(statistics.mean(x.stage_ms[k] for x in results), 3) for k in shg.STAGES},
             "e2e": {"value": round(ms_e2e * 1e6 / total_keys, 3), "unit": "ns/key", "p99_ms": round(p99, 3),
                     "h2d_bytes_per_step": int(n * 8), "d2h_bytes_per_step": int(d2h)},
-            "roofline": {"kernel": "k_split (RecSplit split-seed search)", "bound": "int",
-                         "achieved": round(achieved / 1e9, 3), "peak": round(peak_eff / 1e9, 3),
-                         "unit": "Gevals/s", "frac": round(achieved / peak_eff, 4),
-                         "traffic": (None if SPLIT_DRAM_BYTES_PER_KEY is None else
-                                     round(SPLIT_DRAM_BYTES_PER_KEY * n / max(1, split_kinds["split_launches"]))),
+            "roofline": search_roofline(queue_used, achieved, peak_eff, split_ms, split_ceil_s, leaf_ceil_s, n) | {
                          "peaks_by_kind_gevals": {k: round(v / 1e9, 3) for k, v in peaks.items()},
                          "peaks_by_form_gevals": {k: {f: round(x / 1e9, 3) for f, x in v.items()}
                                                   for k, v in peak_forms.items()},
                          "evals_by_kind": {k: split_kinds[k] for k in shg.SPLIT_KINDS},
-                         "launches": split_kinds["split_launches"],
-                         "note": "useful split evaluations (the reference's sequential count) / device time of the "
-                                 "split stage; peak = each node kind's useful evaluations at the measured rate of "
-                                 "that kind's inner loop run with no memory traffic (compare-and-count for 1..3 "
-                                 "thresholds, moment sums for quarter splits)"},
-            "leaf_stage": leaf_report(last, leaf_ms, leaf_peak, lpeaks, split_kinds),
+                         "split_ceiling_ms": round(split_ceil_s * 1e3, 3), "leaf_ceiling_ms": round(leaf_ceil_s * 1e3, 3)},
+            "leaf_stage": (leaf_report(last, leaf_ms, leaf_peak, lpeaks, split_kinds) if lv is None else
+                           dict(leaf_report(lv[1], lv[0]["leaves"], leaf_peak, lpeaks, lv[2]),
+                                schedule="level schedule, measured apart (2 builds)")),
+            "split_stage": ({"ms": round(split_ms, 3), "frac": round(achieved / peak_eff, 4)} if lv is None else
+                            {"ms": lv[0]["splits"], "schedule": "level schedule, measured apart (2 builds)",
+                             "achieved_gevals": round(lv[1].work["split_evals"] / (lv[0]["splits"] * 1e-3) / 1e9, 3),
+                             "peak_gevals": round(peak_eff / 1e9, 3),
+                             "frac": round(lv[1].work["split_evals"] / (lv[0]["splits"] * 1e-3) / peak_eff, 4)}),
             "work": last.work, "bits_per_key_trees": round(bits_per_key, 4),
             "gpu_launches": int(last.work["launches"] * args.steps),
             "clocks": clocks.summary(),

@@ -47,7 +47,8 @@ typedef enum shg_variant {
 
 /* How the search stages are scheduled on the device. All modes give identical results. */
 typedef enum shg_mode {
-    SHG_MODE_DEFAULT = 0,     /* the fastest measured schedule: currently SHG_MODE_LEVELS */
+    SHG_MODE_DEFAULT = 0,     /* the fastest measured schedule: SHG_MODE_QUEUE for ShockHash2 with leaves of up
+                                 to 64 keys, SHG_MODE_LEVELS otherwise */
     SHG_MODE_LEVELS = 1,      /* one launch per RecSplit level (a block per split node), then one persistent
                                  leaf launch whose warps drain all leaves from a device counter */
     SHG_MODE_PER_LEAF = 2,    /* comparison form: per-level split launches and one launch per leaf */

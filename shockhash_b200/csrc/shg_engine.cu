@@ -442,7 +442,9 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
     // bounded by the fixed bits plus 8 unary bits per node; a longer stream (not seen in
     // practice) takes a new block after encoding.
     // the work-queue schedule: bipartite leaves of up to 64 keys (other builds take the level schedule)
-    const bool queue = p->mode == SHG_MODE_QUEUE && p->variant == SHG_SHOCKHASH2 && p->leaf_size <= 64;
+    // (the default schedule for these builds: measured faster than the level schedule on B200)
+    const bool queue = (p->mode == SHG_MODE_QUEUE || p->mode == SHG_MODE_DEFAULT) && p->variant == SHG_SHOCKHASH2 &&
+                       p->leaf_size <= 64;
     const bool early_keys = p->variant == SHG_SHOCKHASH2 && p->mode != SHG_MODE_PIPELINED && !queue;
     std::vector<uint64_t> wcap(R, 0);
     std::vector<size_t> roff(R + 1, 0);

@@ -444,6 +444,20 @@ __device__ __forceinline__ void sh2_leaf(const Src &src, uint32_t li, const uint
                 uint64_t q = in_sm;
                 if constexpr (sizeof(typename LeafCtx<MAXM>::Mask) == 8) {  // spilled masks: same paired test
                     const uint64_t full = cx.full;
+                    // eight raw seeds' masks requested before any is tested, so that eight L2 or DRAM
+                    // loads are in flight per warp instead of two (these loads dominate large leaves)
+                    for (; q + 8 <= s + 1; q += 8) {
+                        MaskPair<uint64_t> w8[8];
+#pragma unroll
+                        for (int t = 0; t < 8; t++) w8[t] = g.mask[q + t];
+                        bool any = false;
+#pragma unroll
+                        for (int t = 0; t < 8; t++) any |= (((w8[t].a | tB) ^ full) == 0) | (((w8[t].b | tA) ^ full) == 0);
+                        if (any) {
+#pragma unroll 1
+                            for (uint32_t t = 0; t < 8; t++) visit(q + t, g.mask[q + t]);
+                        }
+                    }
                     for (; q + 2 <= s + 1; q += 2) {
                         const MaskPair<uint64_t> w = g.mask[q], v = g.mask[q + 1];
                         const bool any = (((w.a | tB) ^ full) == 0) | (((w.b | tA) ^ full) == 0) |
