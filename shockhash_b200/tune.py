@@ -12,8 +12,9 @@ ShockHash2.h:290-386 for the splits).
 For each configuration this module builds one synthetic key set (uint64 keys of the benchmark
 stream, hashed as 8-byte strings; ShockHash2Flat<k> gets the same keys as 8-byte strings) and
 tunes by coordinate descent: the split parameters first, then the leaf parameters, one parameter
-at a time over its candidate values, each candidate timed by the CUDA-event time of its stage
-(the best of `reps` builds after one warm-up). A value replaces the incumbent only when it is
+at a time over its candidate values, each candidate timed by the CUDA-event time of the two search
+stages together (the best of `reps` builds after one warm-up; the default ShockHash2 schedule runs
+both searches in one launch). A value replaces the incumbent only when it is
 faster by more than `min_gain`. Every build's products are compared with the first build's: a
 parameter that changed a result would be a bug, and the tuner stops with an error.
 
@@ -87,16 +88,17 @@ class Tuner:
         return best_s, best_l
 
     def descend(self, params, candidates, stage, min_gain):
-        """Coordinate descent over `candidates`, timing `stage` (0 split, 1 leaves); every candidate's
-        time goes to self.trials."""
-        best = self.measure(params)[stage]
+        """Coordinate descent over `candidates`, timing both search stages together (the default
+        ShockHash2 schedule runs them in one launch, so its time is all in the split stage); `stage`
+        names the parameter group in self.trials, which receives every candidate's time."""
+        best = sum(self.measure(params))
         for name, values in candidates.items():
             for v in values:
                 if v == params[name]:
                     continue
                 trial = dict(params, **{name: v})
-                t = self.measure(trial)[stage]
-                self.trials.append({"stage": ("splits", "leaves")[stage], name: v, "ms": round(t, 3),
+                t = sum(self.measure(trial))
+                self.trials.append({"group": ("split", "leaf")[stage], name: v, "ms": round(t, 3),
                                     "incumbent_ms": round(best, 3)})
                 if t < best * (1.0 - min_gain):
                     params, best = trial, t
@@ -111,9 +113,14 @@ def tune_config(eng, variant, leaf, n, reps=3, min_gain=0.02, log=print):
             "leaf_blocks_per_sm": 0, "leaf_min_blocks": 6, "sh1_seeds_per_lane": 2}
     t0_split, t0_leaf = tu.measure(base)
     params = dict(base)
+    split_c, leaf_c = dict(SPLIT_CANDIDATES), dict(LEAF_CANDIDATES[variant])
+    if variant == SHOCKHASH2 and leaf <= 64:
+        # the work-queue schedule (the default here): 256-thread blocks, at most 3 per SM
+        split_c.pop("split_threads", None)
+        leaf_c = {"leaf_blocks_per_sm": (1, 2, 3)}
     if variant != TUNING_FLAT:
-        params, _ = tu.descend(params, SPLIT_CANDIDATES, 0, min_gain)
-    params, _ = tu.descend(params, LEAF_CANDIDATES[variant], 1, min_gain)
+        params, _ = tu.descend(params, split_c, 0, min_gain)
+    params, _ = tu.descend(params, leaf_c, 1, min_gain)
     t1_split, t1_leaf = tu.measure(params)
     res = {"variant": variant, "leaf": leaf, "keys": n, "params": params,
            "default_ms": {"splits": round(t0_split, 3), "leaves": round(t0_leaf, 3)},
