@@ -582,7 +582,10 @@ def main():
             eng.close()  # the serving leg's workers hold their own engines
             eng = None
             torch.cuda.empty_cache()
-            forms["serving"] = serve.run_stream(serve.poisson_stream(args.serve_requests, 200.0, 31), workers=2)
+            stream = serve.poisson_stream(args.serve_requests, 200.0, 31)
+            forms["serving"] = serve.run_stream(stream, workers=2)
+            # the same stream with requests above 2M keys built as bucket-range pieces
+            forms["serving_chunked"] = serve.run_stream(stream, workers=2, chunk_keys=2_000_000)
         line = {
             "metric": METRIC, "value": round(ms * 1e6 / total_keys, 3), "unit": "ns/key", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False,

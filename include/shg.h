@@ -123,6 +123,24 @@ shg_status shg_build_u64_device(shg_engine *e, const shg_params *p, const uint64
 shg_status shg_build_batch_u64(shg_engine *e, const shg_params *p, const uint64_t *const *keys, const uint64_t *n,
                                uint64_t nreq, shg_result *outs);
 
+/* One item of a mixed batch (shg_build_batch_items): n uint64 keys (`keys`, hashed on the device as
+ * 8-byte strings) or n 128-bit fingerprints (`first`/`second` when `keys` is NULL), in HOST memory;
+ * with b1 > b0 the item is one piece of a larger structure of nb_global buckets and holds exactly
+ * the keys of its buckets [b0, b1) (as shg_build_shard_hash128), else a whole structure. */
+typedef struct shg_batch_item {
+    const uint64_t *keys;
+    const uint64_t *first, *second;
+    uint64_t n;
+    uint64_t nb_global, b0, b1;
+} shg_batch_item;
+
+/* Batched construction of mixed items (no counterpart in the reference): whole key sets and pieces
+ * of larger ones share the kernel launches; outs[i] is what building item i alone gives (for a
+ * piece, what shg_build_shard_hash128 gives, to be joined by shg_merge_shards). The build service
+ * uses it to interleave the bucket-range pieces of large requests with smaller requests. */
+shg_status shg_build_batch_items(shg_engine *e, const shg_params *p, const shg_batch_item *items, uint64_t nitems,
+                                 shg_result *outs);
+
 void shg_result_free(shg_result *r);
 
 /* A build result on disk and back (no counterpart in the reference classes, which persist only
@@ -163,6 +181,9 @@ shg_status shg_hash_u64_device(shg_engine *e, const uint64_t *d_keys, uint64_t n
  * memory; synchronous). Both give the same order. 1 <= world <= 64, 1 <= nb < 2^32. */
 shg_status shg_shard_partition(const uint64_t *first, const uint64_t *second, uint64_t n, uint64_t nb, int world,
                                uint64_t *pairs, uint64_t *counts);
+/* The same fingerprints as shg_hash_u64_device, on the host with up to `threads` threads (the build
+ * service splits large requests into bucket-range pieces before they reach a GPU). */
+shg_status shg_hash_u64_host(const uint64_t *keys, uint64_t n, uint64_t *first, uint64_t *second, int threads);
 shg_status shg_shard_partition_device(shg_engine *e, const uint64_t *d_first, const uint64_t *d_second, uint64_t n,
                                       uint64_t nb, int world, uint64_t *d_pairs, uint64_t *counts);
 shg_status shg_merge_shards(const shg_params *p, const shg_result *shards, uint64_t nshards, shg_result *out);

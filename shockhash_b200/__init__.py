@@ -55,6 +55,11 @@ class _Result(ctypes.Structure):
                 ("stage_ms", ctypes.c_double * 8), ("work", ctypes.c_uint64 * 8), ("owner", ctypes.c_void_p)]
 
 
+class _BatchItem(ctypes.Structure):
+    _fields_ = [("keys", ctypes.c_void_p), ("first", ctypes.c_void_p), ("second", ctypes.c_void_p),
+                ("n", ctypes.c_uint64), ("nb_global", ctypes.c_uint64), ("b0", ctypes.c_uint64), ("b1", ctypes.c_uint64)]
+
+
 class _FlatResult(ctypes.Structure):
     _fields_ = [("n", ctypes.c_uint64), ("k", ctypes.c_uint64), ("nbuckets", ctypes.c_uint64), ("layers", ctypes.c_uint64),
                 ("layer_bases", ctypes.c_uint64 * 3), ("threshold_bits", ctypes.c_uint32), ("seed_bits", ctypes.c_uint32),
@@ -97,6 +102,8 @@ def lib():
         "shg_build_shard_hash128_device": ([_vp, P, _vp, _vp, _u64, _u64, _u64, _u64, R], ctypes.c_int),
         "shg_shard_partition": ([_vp, _vp, _u64, _u64, ctypes.c_int, _vp, _vp], ctypes.c_int),
         "shg_hash_u64_device": ([_vp, _vp, _u64, _vp, _vp], ctypes.c_int),
+        "shg_hash_u64_host": ([_vp, _u64, _vp, _vp, ctypes.c_int], ctypes.c_int),
+        "shg_build_batch_items": ([_vp, P, _vp, _u64, _vp], ctypes.c_int),
         "shg_shard_partition_device": ([_vp, _vp, _vp, _u64, _u64, ctypes.c_int, _vp, _vp], ctypes.c_int),
         "shg_merge_shards": ([P, _vp, _u64, R], ctypes.c_int),
         "shg_hash_strings": ([_vp, ctypes.c_char_p, _vp, _u64, _vp, _vp], ctypes.c_int),
@@ -198,6 +205,15 @@ def keys_mt19937_64(seed, n):
     out = np.zeros(n, dtype=np.uint64)
     lib().shg_keys_mt19937_64(seed, n, _ptr(out))
     return out
+
+
+def hash_u64_host(keys, threads=8):
+    """128-bit fingerprints (first, second) of uint64 keys hashed as 8-byte strings, on the host."""
+    keys = np.ascontiguousarray(keys, dtype=np.uint64)
+    f = np.empty(len(keys), np.uint64)
+    s = np.empty(len(keys), np.uint64)
+    _check(lib().shg_hash_u64_host(_ptr(keys), len(keys), _ptr(f), _ptr(s), threads))
+    return f, s
 
 
 def keys_mix(seed, n, threads=8):
@@ -430,6 +446,32 @@ class Engine:
         _check(st)
         results = []
         for r in range(R):
+            res = _Result()
+            ctypes.memmove(ctypes.byref(res), ctypes.byref(outs[r]), ctypes.sizeof(_Result))
+            results.append(BuildResult(p, res, self))
+        return results
+
+    def build_batch_items(self, variant, leaf_size, items, bucket_size=2000, mode=MODE_DEFAULT):
+        """One batched construction of mixed items (shg_build_batch_items): each item a dict with
+        "keys" (uint64 keys) or "first"/"second" (fingerprints), optionally "nb_global", "b0", "b1"
+        for a bucket-range piece of a larger structure. Returns one BuildResult per item."""
+        keep, arr = [], (_BatchItem * len(items))()
+        for it, d in zip(arr, items):
+            if d.get("keys") is not None:
+                k = np.ascontiguousarray(d["keys"], dtype=np.uint64)
+                keep.append(k)
+                it.keys, it.n = k.ctypes.data, len(k)
+            else:
+                f = np.ascontiguousarray(d["first"], dtype=np.uint64)
+                sc = np.ascontiguousarray(d["second"], dtype=np.uint64)
+                keep += [f, sc]
+                it.first, it.second, it.n = f.ctypes.data, sc.ctypes.data, len(f)
+            it.nb_global, it.b0, it.b1 = d.get("nb_global", 0), d.get("b0", 0), d.get("b1", 0)
+        outs = (_Result * len(items))()
+        p = self.params(variant, leaf_size, bucket_size, mode, 0)
+        _check(lib().shg_build_batch_items(self._h, ctypes.byref(p), arr, len(items), outs))
+        results = []
+        for r in range(len(items)):
             res = _Result()
             ctypes.memmove(ctypes.byref(res), ctypes.byref(outs[r]), ctypes.sizeof(_Result))
             results.append(BuildResult(p, res, self))

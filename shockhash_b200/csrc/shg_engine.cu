@@ -289,27 +289,28 @@ shg_status check_params(const shg_params *p, uint64_t n) {
 // back in d_first / d_second (request r holds nr[r] keys). Every request gets its own bucket range
 // and its own products (as if built alone); the partition, the split levels and the leaf search of
 // all requests share the same launches.
-// A request that is one shard of a larger structure: it owns buckets [b0, b1) of nb_global.
+// A request that is one shard of a larger structure: it owns buckets [b0, b1) of nb_global
+// (nb_global 0: the request is a whole structure). `shards` holds one entry per request, or is null.
 struct ShardSpec {
     uint64_t nb_global, b0, b1;
 };
 
 shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_first, const uint64_t *d_second,
                        const std::vector<uint64_t> &nr, shg_result *outs, float hash_ms,
-                       const ShardSpec *shard = nullptr) {
+                       const ShardSpec *shards = nullptr) {
     const Config &cfg = config_of(p->variant, p->leaf_size);
     cudaStream_t s = e->stream;
     const size_t R = nr.size();
-    if (shard && R != 1) return fail(SHG_ERR_ARG, "a shard build holds one request");
+
     std::vector<uint64_t> off(R + 1, 0), nbr(R), boff(R + 1, 0), nb_map(R), b0(R, 0);
     for (size_t r = 0; r < R; r++) {
         off[r + 1] = off[r] + nr[r];
         nbr[r] = std::max<uint64_t>(1, (nr[r] + p->bucket_size - 1) / p->bucket_size);  // ShockHash.h:616
         nb_map[r] = nbr[r];
-        if (shard) {
-            nbr[r] = shard->b1 - shard->b0;
-            nb_map[r] = shard->nb_global;
-            b0[r] = shard->b0;
+        if (shards && shards[r].nb_global) {  // request r holds buckets [b0, b1) of a larger structure
+            nbr[r] = shards[r].b1 - shards[r].b0;
+            nb_map[r] = shards[r].nb_global;
+            b0[r] = shards[r].b0;
         }
         boff[r + 1] = boff[r] + nbr[r];
         memset(&outs[r], 0, sizeof(shg_result));
@@ -1200,6 +1201,54 @@ shg_status shg_hash_u64_device(shg_engine *e, const uint64_t *d_keys, uint64_t n
     CU(cudaGetLastError());
     CU(cudaStreamSynchronize(e->stream));
     return SHG_OK;
+}
+
+shg_status shg_build_batch_items(shg_engine *e, const shg_params *p, const shg_batch_item *items, uint64_t nitems,
+                                 shg_result *outs) {
+    if (!e || !outs || !items || nitems == 0) return fail(SHG_ERR_ARG, "null argument or empty batch");
+    uint64_t total = 0, nkeys = 0;
+    std::vector<uint64_t> nr(nitems);
+    std::vector<ShardSpec> specs(nitems, ShardSpec{0, 0, 0});
+    for (uint64_t r = 0; r < nitems; r++) {
+        const shg_batch_item &it = items[r];
+        if (it.n && !it.keys && (!it.first || !it.second)) return fail(SHG_ERR_ARG, "item without keys or fingerprints");
+        if (it.b1 > it.b0) {
+            if (it.b1 > it.nb_global) return fail(SHG_ERR_ARG, "bucket range must satisfy b0 < b1 <= nb_global");
+            specs[r] = ShardSpec{it.nb_global, it.b0, it.b1};
+        }
+        nr[r] = it.n;
+        total += it.n;
+        if (it.keys) nkeys += it.n;
+    }
+    shg_status st = check_params(p, total);
+    if (st) return st;
+    CU(cudaSetDevice(e->device));
+    cudaStream_t s = e->stream;
+    CU(e->first.ensure(std::max<uint64_t>(total, 1) * 8));
+    CU(e->second.ensure(std::max<uint64_t>(total, 1) * 8));
+    CU(e->in_keys.ensure(std::max<uint64_t>(nkeys, 1) * 8));
+    CU(cudaEventRecord(e->ev[7], s));
+    uint64_t off = 0, koff = 0;
+    for (uint64_t r = 0; r < nitems; r++) {
+        const shg_batch_item &it = items[r];
+        if (!it.n) continue;
+        if (it.keys) {  // uint64 keys, hashed on the device as 8-byte strings
+            CU(cudaMemcpyAsync(e->in_keys.as<uint64_t>() + koff, it.keys, it.n * 8, cudaMemcpyHostToDevice, s));
+            launch_spooky_u64(e->in_keys.as<uint64_t>() + koff, it.n, e->first.as<uint64_t>() + off,
+                              e->second.as<uint64_t>() + off, s);
+            koff += it.n;
+        } else {
+            CU(cudaMemcpyAsync(e->first.as<uint64_t>() + off, it.first, it.n * 8, cudaMemcpyHostToDevice, s));
+            CU(cudaMemcpyAsync(e->second.as<uint64_t>() + off, it.second, it.n * 8, cudaMemcpyHostToDevice, s));
+        }
+        off += it.n;
+    }
+    CU(cudaGetLastError());
+    CU(cudaEventRecord(e->ev[0], s));
+    CU(cudaEventSynchronize(e->ev[0]));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e->ev[7], e->ev[0]);
+    return build_batch(e, p, e->first.as<uint64_t>(), e->second.as<uint64_t>(), nr, outs, ms, specs.data());
 }
 
 shg_status shg_build_shard_hash128_device(shg_engine *e, const shg_params *p, const uint64_t *d_first,

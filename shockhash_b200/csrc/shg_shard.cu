@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <string>
+#include <thread>
 #include <vector>
 #include <cuda_runtime.h>
 #include "shg.h"
@@ -138,6 +139,26 @@ shg_status shg_shard_partition(const uint64_t *first, const uint64_t *second, ui
         pairs[2 * d] = first[i];
         pairs[2 * d + 1] = second[i];
     }
+    return SHG_OK;
+}
+
+shg_status shg_hash_u64_host(const uint64_t *keys, uint64_t n, uint64_t *first, uint64_t *second, int threads) {
+    if (n && (!keys || !first || !second)) return shg_set_error(SHG_ERR_ARG, "null argument");
+    const uint64_t T = (uint64_t)std::max(1, std::min(threads, 64));
+    const uint64_t chunk = (n + T - 1) / T;
+    auto run = [&](uint64_t a, uint64_t b) {
+        for (uint64_t i = a; i < b; i++) spooky128_u64(keys[i], 0, first[i], second[i]);
+    };
+    if (T == 1 || n < (1u << 15)) {
+        run(0, n);
+        return SHG_OK;
+    }
+    std::vector<std::thread> pool;
+    for (uint64_t t = 0; t < T; t++) {
+        const uint64_t a = std::min(n, t * chunk), b = std::min(n, a + chunk);
+        if (a < b) pool.emplace_back(run, a, b);
+    }
+    for (auto &th : pool) th.join();
     return SHG_OK;
 }
 

@@ -20,6 +20,12 @@ bytes_per_key); a batch beyond the warm capacity grows that worker's buffers onc
 size becomes its capacity. A request larger than every limit is built alone. Each result is
 bit-identical to building that request alone.
 
+With `chunk_keys` set, a request of more keys than that is split at submission into bucket-range
+pieces (host fingerprints, partitioned by bucket range like the shards of a multi-GPU build). The
+pieces queue as separate items, so they fit the batch limits, spread over the workers and share
+batches with other requests; the last piece to finish joins them (shg_merge_shards), which gives
+the same bits as building the request alone.
+
     python -m shockhash_b200.serve --requests 400
 prints one JSON line with p50/p99 build latency, aggregate keys/s and device utilisation for a
 Poisson stream (mean 200 requests/s) of log-uniform sizes between 10^3 and 10^7 keys. Each
@@ -35,17 +41,19 @@ from collections import deque
 
 import numpy as np
 
-from . import SHOCKHASH2, Engine, device_memory, keys_mix, keys_mt19937_64
+from . import SHOCKHASH2, Engine, _check, _ptr, device_memory, hash_u64_host, keys_mix, keys_mt19937_64, lib, merge_shards
 
 
 class Request:
-    __slots__ = ("rid", "keys", "t_arrival", "t_start", "t_done", "result", "error", "_event", "batch_size")
+    __slots__ = ("rid", "keys", "t_arrival", "t_start", "t_done", "result", "error", "_event", "batch_size",
+                 "parts", "remaining")
 
     def __init__(self, rid, keys, t_arrival):
         self.rid, self.keys, self.t_arrival = rid, keys, t_arrival
         self.t_start = self.t_done = None
         self.result = self.error = None
         self.batch_size = 0
+        self.parts, self.remaining = None, 0  # bucket-range pieces of a chunked request
         self._event = threading.Event()
 
     def wait(self, timeout=None):
@@ -60,10 +68,47 @@ class Request:
         return None if self.t_done is None else self.t_done - self.t_arrival
 
 
+class Piece:
+    """Buckets [b0, b1) of a chunked request's structure (nb_global buckets): the fingerprints of
+    exactly its keys, built like a shard and joined with the request's other pieces at the end."""
+    __slots__ = ("parent", "idx", "first", "second", "nb_global", "b0", "b1")
+
+    def __init__(self, parent, idx, first, second, nb_global, b0, b1):
+        self.parent, self.idx, self.first, self.second = parent, idx, first, second
+        self.nb_global, self.b0, self.b1 = nb_global, b0, b1
+
+    @property
+    def keys(self):  # the size the admission counts
+        return self.first
+
+
+def split_request(keys, bucket, chunk_keys, threads=8):
+    """The bucket-range pieces of a request of more than `chunk_keys` keys: its fingerprints (host),
+    partitioned by range of their bucket remap128(first, nb) into ceil(n / chunk_keys) ranges (at most
+    64), stable. Returns [(first, second, nb_global, b0, b1)] in bucket order, empty ranges left out."""
+    n = len(keys)
+    first, second = hash_u64_host(keys, threads)
+    nb = max(1, (n + bucket - 1) // bucket)
+    parts = max(1, min(64, -(-n // chunk_keys), nb))
+    pairs = np.empty((n, 2), dtype=np.uint64)
+    counts = np.zeros(parts, dtype=np.uint64)
+    _check(lib().shg_shard_partition(_ptr(first), _ptr(second), n, nb, parts, _ptr(pairs), _ptr(counts)))
+    out, at = [], 0
+    for g in range(parts):
+        b0, b1 = nb * g // parts, nb * (g + 1) // parts
+        c = int(counts[g])
+        if b1 > b0:
+            out.append((np.ascontiguousarray(pairs[at:at + c, 0]), np.ascontiguousarray(pairs[at:at + c, 1]), nb, b0, b1))
+        at += c
+    return out
+
+
 class BuildServer:
     def __init__(self, variant=SHOCKHASH2, leaf=64, bucket=2000, workers=2, device=0, mem_fraction=0.5,
-                 bytes_per_key=96, max_batch_keys=32_000_000, keep_results=True, warm=True, free_memory=None):
+                 bytes_per_key=96, max_batch_keys=32_000_000, keep_results=True, warm=True, free_memory=None,
+                 chunk_keys=0):
         self.variant, self.leaf, self.bucket = variant, leaf, bucket
+        self.chunk_keys = chunk_keys  # requests above this size are built in bucket-range pieces
         self.keep_results = keep_results
         self.device, self.mem_fraction, self.bytes_per_key = device, mem_fraction, bytes_per_key
         self.max_batch_keys = max_batch_keys
@@ -93,9 +138,17 @@ class BuildServer:
 
     def submit(self, rid, keys, t_arrival=None):
         req = Request(rid, np.ascontiguousarray(keys, dtype=np.uint64), time.perf_counter() if t_arrival is None else t_arrival)
+        items = [req]
+        if self.chunk_keys and len(req.keys) > self.chunk_keys:
+            # pieces enter the queue one after another; other requests can be admitted between them,
+            # and the finished pieces' products wait for the last one
+            pieces = split_request(req.keys, self.bucket, self.chunk_keys)
+            req.parts, req.remaining = [None] * len(pieces), len(pieces)
+            items = [Piece(req, i, *pc) for i, pc in enumerate(pieces)]
+            req.keys = None
         with self._cv:
-            self._q.append(req)
-            self._cv.notify()
+            self._q.extend(items)
+            self._cv.notify_all()
         return req
 
     def batch_limit(self, w):
@@ -130,10 +183,17 @@ class BuildServer:
                 batch, total, grow = self._take(w)
             t0 = time.perf_counter()
             for r in batch:
-                r.t_start = t0
-                r.batch_size = len(batch)
+                owner = r.parent if isinstance(r, Piece) else r
+                if owner.t_start is None:
+                    owner.t_start = t0
+                owner.batch_size = max(owner.batch_size, len(batch))
             try:
-                results = eng.build_batch_u64(self.variant, self.leaf, [r.keys for r in batch], self.bucket)
+                if any(isinstance(r, Piece) for r in batch):
+                    items = [dict(first=r.first, second=r.second, nb_global=r.nb_global, b0=r.b0, b1=r.b1)
+                             if isinstance(r, Piece) else dict(keys=r.keys) for r in batch]
+                    results = eng.build_batch_items(self.variant, self.leaf, items, self.bucket)
+                else:
+                    results = eng.build_batch_u64(self.variant, self.leaf, [r.keys for r in batch], self.bucket)
                 err = None
             except Exception as ex:  # reported per request
                 results, err = [None] * len(batch), ex
@@ -146,6 +206,9 @@ class BuildServer:
                     self._cap[w] = total  # the engine's buffers now fit this batch
                     self.grown += 1
             for r, res in zip(batch, results):
+                if isinstance(r, Piece):
+                    self._piece_done(r, res, err)
+                    continue
                 try:
                     r.t_done = t1
                     r.error = err
@@ -159,6 +222,36 @@ class BuildServer:
                     r.error = ex
                 finally:
                     r._event.set()
+
+    def _piece_done(self, piece, res, err):
+        """Keeps a finished piece's products; the last piece of a request joins them all
+        (shg_merge_shards: accumulators offset, codes concatenated at bit granularity), which gives
+        exactly the result of building the request alone."""
+        req = piece.parent
+        with self._cv:
+            req.parts[piece.idx] = res
+            if err is not None:
+                req.error = err
+            req.remaining -= 1
+            last = req.remaining == 0
+        if not last:
+            return
+        try:
+            if req.error is None:
+                merged = merge_shards(self.variant, self.leaf, req.parts, self.bucket)
+                if self.keep_results:
+                    req.result = merged
+                else:
+                    merged.free()
+        except Exception as ex:
+            req.error = ex
+        finally:
+            for x in req.parts:
+                if x is not None:
+                    x.free()
+            req.parts = None
+            req.t_done = time.perf_counter()
+            req._event.set()
 
     def close(self):
         with self._cv:
@@ -180,13 +273,13 @@ def poisson_stream(n_requests, rate=200.0, seed=31, lo_exp=3.0, hi_exp=7.0):
     return [(float(arrivals[i]), int(sizes[i]), seed * 1000003 + i) for i in range(n_requests)]
 
 
-def run_stream(stream, workers=2, leaf=64, bucket=2000, mem_fraction=0.5, max_batch_keys=32_000_000):
+def run_stream(stream, workers=2, leaf=64, bucket=2000, mem_fraction=0.5, max_batch_keys=32_000_000, chunk_keys=0):
     """Replay `stream` against a fresh server. Each request's keys are drawn just before it is
     submitted (keys_mix of its sub-seed, on the host); it is submitted at its arrival time, or as
     soon as its keys exist if drawing them ran past that time, and its latency runs from submission
     to the end of its batch."""
     srv = BuildServer(leaf=leaf, bucket=bucket, workers=workers, mem_fraction=mem_fraction,
-                      max_batch_keys=max_batch_keys, keep_results=False)
+                      max_batch_keys=max_batch_keys, keep_results=False, chunk_keys=chunk_keys)
     reqs = []
     late = 0.0
     t0 = time.perf_counter()
@@ -205,6 +298,7 @@ def run_stream(stream, workers=2, leaf=64, bucket=2000, mem_fraction=0.5, max_ba
     t_end = max(r.t_done for r in reqs)
     srv.close()
     lat = np.array([r.latency for r in reqs]) * 1e3
+    small = np.array([s <= 100_000 for _, s, _ in stream])
     total_keys = sum(s for _, s, _ in stream)
     span = t_end - t0
     return {
@@ -212,6 +306,8 @@ def run_stream(stream, workers=2, leaf=64, bucket=2000, mem_fraction=0.5, max_ba
         "max_submit_lag_ms": round(late * 1e3, 3), "batches_grown": srv.grown,
         "p50_ms": round(float(np.percentile(lat, 50)), 3), "p99_ms": round(float(np.percentile(lat, 99)), 3),
         "mean_ms": round(float(lat.mean()), 3), "max_ms": round(float(lat.max()), 3),
+        "p99_ms_small": round(float(np.percentile(lat[small], 99)), 3) if small.any() else None,
+        "chunk_keys": chunk_keys,
         "aggregate_keys_per_s": round(total_keys / span, 1), "wall_s": round(span, 3),
         "offered_keys_per_s": round(total_keys / max(stream[-1][0], 1e-9), 1),
         "device_busy_fraction": round(min(1.0, srv.busy_s / (span * workers)), 4),
@@ -229,10 +325,11 @@ def main():
     ap.add_argument("--leaf", type=int, default=64)
     ap.add_argument("--bucket", type=int, default=2000)
     ap.add_argument("--max-batch-keys", type=int, default=32_000_000)
+    ap.add_argument("--chunk-keys", type=int, default=0, help="build requests above this size in bucket-range pieces")
     args = ap.parse_args()
     stream = poisson_stream(args.requests, args.rate, args.seed)
     out = run_stream(stream, workers=args.workers, leaf=args.leaf, bucket=args.bucket,
-                     max_batch_keys=args.max_batch_keys)
+                     max_batch_keys=args.max_batch_keys, chunk_keys=args.chunk_keys)
     out.update({"metric": "ShockHash2 build service: p50/p99 build latency and aggregate keys/s",
                 "config": {"variant": "ShockHash2", "leaf_size": args.leaf, "bucket_size": args.bucket,
                            "arrivals": f"Poisson, mean {args.rate}/s, seed {args.seed}",

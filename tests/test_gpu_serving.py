@@ -45,6 +45,38 @@ def test_server_results_equal_alone_builds(engine):
         r.result.free()
 
 
+def test_batch_items_equal_alone_and_shard_builds(engine):
+    keys_a = shg.keys_mt19937_64(41, 30_000)
+    keys_b = shg.keys_mt19937_64(42, 200_000)
+    pieces = serve.split_request(keys_b, 2000, 70_000)
+    items = [dict(keys=keys_a)] + [dict(first=f, second=s, nb_global=nb, b0=b0, b1=b1) for f, s, nb, b0, b1 in pieces]
+    items.append(dict(keys=keys_a[:5]))
+    got = engine.build_batch_items(2, 64, items, 2000)
+    assert same(got[0], engine.build_u64(2, 64, keys_a, 2000))
+    assert same(got[-1], engine.build_u64(2, 64, keys_a[:5], 2000))
+    for (f, s, nb, b0, b1), r in zip(pieces, got[1:-1]):
+        assert same(r, engine.build_shard_hash128(2, 64, f, s, nb, b0, b1, 2000))
+    whole = shg.merge_shards(2, 64, got[1:-1], 2000)
+    assert same(whole, engine.build_u64(2, 64, keys_b, 2000))
+
+
+def test_chunked_server_results_equal_alone_builds(engine):
+    sizes = [3_000, 260_000, 40_000, 1, 180_001, 9_999]
+    srv = serve.BuildServer(workers=2, max_batch_keys=150_000, chunk_keys=60_000)
+    try:
+        reqs = [srv.submit(i, shg.keys_mt19937_64(500 + i, n)) for i, n in enumerate(sizes)]
+        for r in reqs:
+            r.wait(timeout=120)
+            assert r.error is None, r.error
+        for i, (n, r) in enumerate(zip(sizes, reqs)):
+            alone = engine.build_u64(2, 64, shg.keys_mt19937_64(500 + i, n), 2000)
+            assert same(r.result, alone), r.rid
+            alone.free()
+            r.result.free()
+    finally:
+        srv.close()
+
+
 def test_serving_stream_reports_latency():
     out = serve.run_stream(serve.poisson_stream(30, rate=500.0, seed=31, hi_exp=5.0), workers=2)
     assert out["requests"] == 30 and out["p99_ms"] >= out["p50_ms"] > 0 and out["aggregate_keys_per_s"] > 0

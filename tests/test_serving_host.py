@@ -38,6 +38,15 @@ class _FakeEngine:
             raise RuntimeError("device build failed")
         return [_FakeResult(k) for k in key_arrays]
 
+    def build_batch_items(self, variant, leaf, items, bucket):
+        _FakeEngine.entered.set()
+        if _FakeEngine.gate is not None:
+            _FakeEngine.gate.wait(5)
+        sizes = [len(d["keys"]) if d.get("keys") is not None else len(d["first"]) for d in items]
+        with _FakeEngine.lock:
+            _FakeEngine.batches.append(sizes)
+        return [_FakeResult(np.zeros(n)) for n in sizes]
+
     def close(self):
         self.closed = True
 
@@ -182,3 +191,47 @@ def test_request_keys_are_distinct_and_deterministic():
     z = (z ^ (z >> np.uint64(30))) * np.uint64(0xbf58476d1ce4e5b9)
     z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94d049bb133111eb)
     assert np.array_equal(a[:5], z ^ (z >> np.uint64(31)))
+
+
+def test_split_request_covers_every_key_by_bucket_range():
+    from shockhash_b200 import shard
+    keys = serve.keys_mix(5, 250_000)
+    pieces = serve.split_request(keys, 2000, 60_000, threads=4)
+    nb = shard.nbuckets(len(keys), 2000)
+    assert len(pieces) == 5 and pieces[0][3] == 0 and pieces[-1][4] == nb
+    assert all(a[4] == b[3] for a, b in zip(pieces, pieces[1:]))  # contiguous bucket ranges
+    import shockhash_b200 as shg
+    f_all, s_all = shg.hash_u64_host(keys)
+    got = set()
+    for first, second, nbg, b0, b1 in pieces:
+        assert nbg == nb
+        b = shard.remap128(first, nb)
+        assert b.min() >= b0 and b.max() < b1
+        got.update(zip(first.tolist(), second.tolist()))
+    assert got == set(zip(f_all.tolist(), s_all.tolist()))
+    assert sum(len(p[0]) for p in pieces) == len(keys)
+
+
+def test_chunked_request_joins_its_pieces(fake, monkeypatch):
+    merged = []
+
+    def fake_merge(variant, leaf, parts, bucket):
+        merged.append([p.n for p in parts])
+        return _FakeResult(np.zeros(sum(p.n for p in parts)))
+
+    monkeypatch.setattr(serve, "merge_shards", fake_merge)
+    srv = serve.BuildServer(workers=1, max_batch_keys=100_000, chunk_keys=40_000, warm=False)
+    try:
+        small = srv.submit("a", _keys(10))
+        big = srv.submit("b", serve.keys_mix(3, 130_000))
+        tail = srv.submit("c", _keys(20, 100))
+        for r in (small, big, tail):
+            r.wait(timeout=30)
+            assert r.error is None
+    finally:
+        srv.close()
+    assert big.result.n == 130_000 and len(merged) == 1 and len(merged[0]) == 4
+    assert sum(merged[0]) == 130_000 and small.result.n == 10 and tail.result.n == 20
+    # pieces were admitted like requests: batches never exceed the cap unless a single item does
+    assert all(sum(b) <= 100_000 or len(b) == 1 for b in fake.batches)
+    assert big.t_done >= big.t_start and big.batch_size >= 1
