@@ -473,7 +473,8 @@ def main():
     peak_eff = shg.weighted_split_peak(split_kinds, peaks)
     # the default ShockHash2 build (leaves <= 64) runs both searches in the one work-queue kernel,
     # whose time is the split stage's: its ceiling is the split ceiling plus the leaf ceiling
-    queue_used = VARIANT == 2 and LEAF <= 64 and args.mode in (0, 4)
+    # (the library reports the whole launch as the split stage and no separate leaf stage then)
+    queue_used = VARIANT == 2 and LEAF <= 64 and args.mode in (0, 4) and leaf_ms < 0.05 * split_ms
     split_ceil_s = sum(split_kinds[k] / peaks[k] for k in shg.SPLIT_KINDS if split_kinds[k])
     leaf_ceil_s = (shg.leaf_ceiling_s({"hash_evals": last.work["leaf_evals"], "scan_tests": split_kinds["leaf_scan_tests"],
                                        "pair_tests": last.work["pairs"], "uf_edges": last.work["uf_edges"]}, lpeaks)
@@ -582,10 +583,7 @@ def main():
             eng.close()  # the serving leg's workers hold their own engines
             eng = None
             torch.cuda.empty_cache()
-            stream = serve.poisson_stream(args.serve_requests, 200.0, 31)
-            forms["serving"] = serve.run_stream(stream, workers=2)
-            # the same stream with requests above 2M keys built as bucket-range pieces
-            forms["serving_chunked"] = serve.run_stream(stream, workers=2, chunk_keys=2_000_000)
+            forms["serving"] = serve.run_stream(serve.poisson_stream(args.serve_requests, 200.0, 31), workers=2)
         line = {
             "metric": METRIC, "value": round(ms * 1e6 / total_keys, 3), "unit": "ns/key", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False,

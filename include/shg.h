@@ -181,9 +181,14 @@ shg_status shg_hash_u64_device(shg_engine *e, const uint64_t *d_keys, uint64_t n
  * memory; synchronous). Both give the same order. 1 <= world <= 64, 1 <= nb < 2^32. */
 shg_status shg_shard_partition(const uint64_t *first, const uint64_t *second, uint64_t n, uint64_t nb, int world,
                                uint64_t *pairs, uint64_t *counts);
-/* The same fingerprints as shg_hash_u64_device, on the host with up to `threads` threads (the build
- * service splits large requests into bucket-range pieces before they reach a GPU). */
+/* The same fingerprints as shg_hash_u64_device, on the host with up to `threads` threads. */
 shg_status shg_hash_u64_host(const uint64_t *keys, uint64_t n, uint64_t *first, uint64_t *second, int threads);
+/* Host uint64 keys in, host (first, second) pairs out in bucket-range order: the keys are copied to
+ * the engine's device, hashed (shg_hash_u64_device) and partitioned into `parts` bucket ranges of
+ * nb buckets (shg_shard_partition_device), and the pairs and per-range counts copied back. The
+ * build service splits large requests this way into pieces for shg_build_batch_items. */
+shg_status shg_partition_u64(shg_engine *e, const uint64_t *keys, uint64_t n, uint64_t nb, int parts, uint64_t *pairs,
+                             uint64_t *counts);
 shg_status shg_shard_partition_device(shg_engine *e, const uint64_t *d_first, const uint64_t *d_second, uint64_t n,
                                       uint64_t nb, int world, uint64_t *d_pairs, uint64_t *counts);
 shg_status shg_merge_shards(const shg_params *p, const shg_result *shards, uint64_t nshards, shg_result *out);
@@ -211,7 +216,7 @@ shg_status shg_sh2_construct_leaves(shg_engine *e, const uint64_t *keys, const u
  * device image, held by every GPU that loads the library until the process exits; a leaf needing
  * more than 512 raw seeds or 512 candidates fails with SHG_ERR_TRIAL_LIMIT, a leaf outside 2..64
  * keys with SHG_ERR_ARG. The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture. All calls share the
+ * (cudaGetSymbolAddress). All calls share the
  * array, so calls that overlap on the GPU (other streams, other host threads) race. */
 shg_status shg_sh2_construct_leaves_noalloc(const uint64_t *d_keys, const uint64_t *d_leaf_offsets, uint64_t nleaves,
                                             uint64_t *d_seeds, uint8_t *d_bits, void *stream);
@@ -392,7 +397,9 @@ shg_status shg_engine_last_work(const shg_engine *e, uint64_t *out, int n);
  *   shifts partly as multiply-highs, moving work from the integer to the multiply pipe);
  *   leaf_blocks_per_sm 0..16 (0 =
  *   as many as shared memory allows); leaf_min_blocks 4, 6, 8 (bipartite leaves up to 64 keys:
- *   register bound); sh1_seeds_per_lane 1, 2 (original leaves).
+ *   register bound); sh1_seeds_per_lane 1, 2 (original leaves); queue_lag_rounds 0..64 (work-queue
+ *   schedule: lag between a bucket's tree levels in the item order, in rounds of the grid; default
+ *   8; 0 = the levels one after another, then the leaves).
  * At creation an engine loads the table shockhash_b200/tuning.tsv beside the library (or the file
  * named by the SHG_TUNING_TABLE environment variable; empty = none), written by the autotuner
  * (python -m shockhash_b200.tune); lines "<variant> <leaf> <name> <value>", '#' comments. */

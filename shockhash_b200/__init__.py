@@ -103,6 +103,7 @@ def lib():
         "shg_shard_partition": ([_vp, _vp, _u64, _u64, ctypes.c_int, _vp, _vp], ctypes.c_int),
         "shg_hash_u64_device": ([_vp, _vp, _u64, _vp, _vp], ctypes.c_int),
         "shg_hash_u64_host": ([_vp, _u64, _vp, _vp, ctypes.c_int], ctypes.c_int),
+        "shg_partition_u64": ([_vp, _vp, _u64, _u64, ctypes.c_int, _vp, _vp], ctypes.c_int),
         "shg_build_batch_items": ([_vp, P, _vp, _u64, _vp], ctypes.c_int),
         "shg_shard_partition_device": ([_vp, _vp, _vp, _u64, _u64, ctypes.c_int, _vp, _vp], ctypes.c_int),
         "shg_merge_shards": ([P, _vp, _u64, R], ctypes.c_int),
@@ -244,7 +245,7 @@ SPLIT_KINDS = ("thresholds_1", "thresholds_2", "thresholds_3", "quarter_moments"
 # Launch parameters of the search kernels (shg_engine_set_tuning); FLAT is the tuning table's
 # variant key of ShockHash2Flat<k>.
 TUNING_PARAMS = ("split_seeds_per_lane", "split_threads", "split_round_div", "split_arith", "leaf_blocks_per_sm",
-                 "leaf_min_blocks", "sh1_seeds_per_lane")
+                 "leaf_min_blocks", "sh1_seeds_per_lane", "queue_lag_rounds")
 TUNING_FLAT = 4
 
 
@@ -486,6 +487,16 @@ class Engine:
         st = lib().shg_build_shard_hash128(self._h, ctypes.byref(p), _ptr(first), _ptr(second), len(first), nb_global,
                                            b0, b1, ctypes.byref(res))
         return self._finish(p, st, res)
+
+    def partition_u64(self, keys, nb, parts):
+        """Fingerprints of host uint64 keys made and ordered by bucket range on this engine's GPU
+        (shg_partition_u64): an (n, 2) uint64 array of (first, second) pairs, range by range in
+        input order, and the key count of each of the `parts` ranges of nb buckets."""
+        keys = np.ascontiguousarray(keys, dtype=np.uint64)
+        pairs = np.empty((len(keys), 2), np.uint64)
+        counts = np.zeros(parts, np.uint64)
+        _check(lib().shg_partition_u64(self._h, _ptr(keys), len(keys), nb, parts, _ptr(pairs), _ptr(counts)))
+        return pairs, counts
 
     def hash_u64_device(self, d_keys_ptr, n, d_first_ptr, d_second_ptr):
         """Fingerprints of n device-resident uint64 keys into device buffers (synchronous)."""

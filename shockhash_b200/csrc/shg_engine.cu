@@ -127,7 +127,7 @@ struct shg_engine {
         DevBuf cnt, nodes, node_off, singles, single_off, skip_bits;
     };
     std::vector<Shapes *> shapes;
-    DevBuf plan_offs, ret_scratch, qdone;
+    DevBuf plan_offs, ret_scratch, qdone, qorder;
     cudaEvent_t ev[8] = {};
     cudaStream_t stream2 = nullptr;  // leaves of the pipelined mode
     static constexpr int kMaxChunks = 64;
@@ -158,6 +158,7 @@ struct shg_engine {
         plan_offs.release();
         ret_scratch.release();
         qdone.release();
+        qorder.release();
         for (Shapes *sh : shapes) {
             DevBuf *sb[] = {&sh->cnt, &sh->nodes, &sh->node_off, &sh->singles, &sh->single_off, &sh->skip_bits};
             for (DevBuf *b : sb) b->release();
@@ -446,6 +447,10 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
     // (the default schedule for these builds: measured faster than the level schedule on B200)
     const bool queue = (p->mode == SHG_MODE_QUEUE || p->mode == SHG_MODE_DEFAULT) && p->variant == SHG_SHOCKHASH2 &&
                        p->leaf_size <= 64;
+    const Tuning tun = e->tuning_of(p->variant, p->leaf_size);
+    // with per-bucket leaf groups, the queue kernel writes each bucket's retrieval keys and bits
+    // straight into the pinned result block as the bucket's leaves finish
+    const bool stream_out = queue && tun.queue_lag > 0;
     const bool early_keys = p->variant == SHG_SHOCKHASH2 && p->mode != SHG_MODE_PIPELINED && !queue;
     std::vector<uint64_t> wcap(R, 0);
     std::vector<size_t> roff(R + 1, 0);
@@ -456,7 +461,7 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
         }
     };
     PinnedBlock *blk = nullptr;
-    if (early_keys) {
+    if (early_keys || stream_out) {
         for (size_t r = 0; r < R; r++) {
             const uint64_t bits = rfixed[r] + 8 * rnodes[r] + 1;
             wcap[r] = ((bits + 7) / 8 + 14) / 8;
@@ -481,7 +486,6 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
     const uint32_t smax = maxm > 64 ? 16384 : 4096, cmax = maxm > 64 ? 16384 : 2048;
     const uint64_t per_warp = (sh2_scratch_bytes(smax, cmax, maxm) + 255) & ~255ull;
     int leaf_grid;
-    const Tuning tun = e->tuning_of(p->variant, p->leaf_size);
     if (sh2) {
         const int per_block_smem = 4 * sh2_smem_per_warp(maxm);
         int blocks_per_sm = std::max(1, std::min(8, (228 * 1024) / (per_block_smem + 1024)));
@@ -517,19 +521,46 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
         launches++;
     };
     if (queue) {
-        // one persistent launch: splits level by level, then leaves, each item once its bucket allows
+        // one persistent launch over the staggered item order: split nodes and per-bucket leaf groups
         const int qsmem = tree_queue_smem_per_block(tun.split.spl);
         int qbps = std::max(1, std::min(3, (228 * 1024) / (qsmem + 1024)));
         if (tun.leaf_bps > 0) qbps = std::min(qbps, tun.leaf_bps);
-        const int qgrid = std::max(1, std::min<int>(e->sms * qbps, (int)std::max<uint64_t>(leaf_off, (nleaves + 7) / 8)));
+        const int qgrid = std::max(1, std::min<int>(e->sms * qbps, (int)std::max<uint64_t>(leaf_off + nb, 1)));
+        // lag between a bucket's levels: queue_lag rounds of the grid's blocks, in buckets of
+        // (split nodes + one leaf group) each, so that a node's parent has finished when it is
+        // taken; none (0): lag nb, the levels one after another, then the leaf groups
+        const uint64_t per_bucket = std::max<uint64_t>(1, (leaf_off + nb) / std::max<uint64_t>(nb, 1));
+        const uint64_t lag_b = tun.queue_lag > 0 ? ((uint64_t)tun.queue_lag * qgrid + per_bucket - 1) / per_bucket : nb;
+        const uint32_t lag = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(nb, 1), std::max<uint64_t>(1, lag_b));
+        const uint64_t T = queue_order_slots(nb, (uint32_t)nlevels, lag);
+        const uint64_t seq_words = leaf_off + nb;
+        const uint64_t order_words = (2 * T + 1 + seq_words + 1) & ~1ull;  // the request table after it, 8-byte aligned
+        CU(e->qorder.ensure(order_words * 4 + (stream_out ? R * sizeof(QueueOut) : 0) + 256));
+        uint32_t *q_cnt = e->qorder.as<uint32_t>(), *q_pos = q_cnt + T, *q_seq = q_pos + T + 1;
+        QueueOut *q_out = nullptr;
+        if (stream_out) {
+            // where each request's compacted retrieval keys and bits go in the pinned block
+            std::vector<QueueOut> qo(R);
+            for (size_t r = 0; r < R; r++)
+                qo[r] = QueueOut{boff[r], off[r], soff[r], keys_host(blk, r), (uint8_t *)keys_host(blk, r) + rnv[r] * 8};
+            q_out = (QueueOut *)(e->qorder.as<uint32_t>() + order_words);
+            CU(cudaMemcpyAsync(q_out, qo.data(), R * sizeof(QueueOut), cudaMemcpyHostToDevice, s));
+            CU(cudaStreamSynchronize(s));  // qo is pageable and leaves scope
+        }
         CU(e->scratch.ensure(per_warp * (uint64_t)qgrid * tree_queue_warps_per_block()));
         CU(e->qdone.ensure(std::max<uint64_t>(nb, 1) * 4));
         CU(cudaMemsetAsync(e->qdone.p, 0, nb * 4, s));
         CU(cudaMemsetAsync(misc->qctr, 0, sizeof(misc->qctr), s));
-        launch_tree_queue(e->nodes.as<Node>(), d_ids, (uint32_t)leaf_off, nleaves, e->plan_offs.as<uint32_t>(), offs_stride,
-                          (uint32_t)nlevels, e->qdone.as<uint32_t>(), e->keys.as<uint64_t>(), e->codes.as<uint64_t>(),
-                          e->rib_bits.as<uint8_t>(), e->scratch.as<uint8_t>(), per_warp, smax, cmax, p->max_trials,
-                          &misc->err, misc->work, misc->split_kind, misc->qctr, tun.split, qgrid, s);
+        const bool groups = tun.queue_lag > 0;
+        launch_queue_order(e->plan_offs.as<uint32_t>(), offs_stride, nb, (uint32_t)nlevels, lag, groups, lists,
+                           (uint32_t)leaf_off, q_cnt, q_pos, q_seq, s);
+        launches += T ? 3 : 0;
+        if (T == 0) CU(cudaMemsetAsync(q_pos, 0, 4, s));  // no buckets: no items
+        launch_tree_queue(e->nodes.as<Node>(), d_ids, q_seq, q_pos + T, (uint32_t)leaf_off, e->plan_offs.as<uint32_t>(),
+                          offs_stride, (uint32_t)nlevels, e->qdone.as<uint32_t>(), e->keys.as<uint64_t>(),
+                          e->codes.as<uint64_t>(), e->rib_bits.as<uint8_t>(), e->scratch.as<uint8_t>(), per_warp, smax, cmax,
+                          p->max_trials, &misc->err, misc->work, misc->split_kind, misc->qctr, groups ? 0u : nleaves,
+                          e->acc.as<uint64_t>(), e->singles.as<uint64_t>(), q_out, (uint32_t)R, tun.split, qgrid, s);
         launches++;
         CU(cudaEventRecord(e->ev[3], s));  // the split stage's time covers the whole queue launch
     } else if (pipelined) {
@@ -625,15 +656,15 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
 
     // ---- copy-out: the products of each request into the pinned block (one block per batch,
     // each result holding a reference); the retrieval input is compacted on the device first.
-    bool keys_done = early_keys;
-    if (early_keys) {
+    bool keys_done = early_keys || stream_out, bits_done = stream_out;
+    if (early_keys || stream_out) {
         bool fits = true;
         for (size_t r = 0; r < R; r++) fits = fits && words[r] <= wcap[r];
-        if (!fits) {  // descriptor stream longer than the bound: a new block, keys copied again
+        if (!fits) {  // descriptor stream longer than the bound: a new block, keys (and bits) copied again
             CU(cudaStreamSynchronize(e->stream2));
             release_all(blk);
             blk = nullptr;
-            keys_done = false;
+            keys_done = bits_done = false;
         }
     }
     if (!blk) {
@@ -646,8 +677,10 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
     for (size_t r = 0; r < R; r++) {
         shg_result *out = &outs[r];
         const uint64_t ns = soff[r + 1] - soff[r], rn = rnv[r];
-        launch_compact_ribbon(src_keys + off[r], e->rib_bits.as<uint8_t>() + off[r], nr[r], e->singles.as<uint64_t>() + soff[r], ns,
-                              off[r], keys_done ? nullptr : e->ckeys.as<uint64_t>() + off[r], e->cbits.as<uint8_t>() + off[r], s);
+        if (!bits_done)
+            launch_compact_ribbon(src_keys + off[r], e->rib_bits.as<uint8_t>() + off[r], nr[r], e->singles.as<uint64_t>() + soff[r],
+                                  ns, off[r], keys_done ? nullptr : e->ckeys.as<uint64_t>() + off[r],
+                                  e->cbits.as<uint8_t>() + off[r], s);
         const size_t acc_bytes = (nbr[r] + 1) * 8;
         uint8_t *hp = (uint8_t *)blk->p + roff[r];
         out->owner = blk;
@@ -662,13 +695,14 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
         if (rn) {
             if (!keys_done)
                 CU(cudaMemcpyAsync(out->ribbon_keys, e->ckeys.as<uint64_t>() + off[r], rn * 8, cudaMemcpyDeviceToHost, s));
-            CU(cudaMemcpyAsync(out->ribbon_bits, e->cbits.as<uint8_t>() + off[r], rn, cudaMemcpyDeviceToHost, s));
+            if (!bits_done)
+                CU(cudaMemcpyAsync(out->ribbon_bits, e->cbits.as<uint8_t>() + off[r], rn, cudaMemcpyDeviceToHost, s));
         }
         out->desc_words = words[r];
         out->desc_bits = total[r] + 1;
         out->ribbon_n = rn;
     }
-    if (keys_done) CU(cudaStreamWaitEvent(s, e->join_ev, 0));  // the keys copied during the leaves
+    if (keys_done && early_keys) CU(cudaStreamWaitEvent(s, e->join_ev, 0));  // the keys copied during the leaves
     unsigned long long work[8];
     CU(cudaMemcpyAsync(work, misc->work, sizeof(work), cudaMemcpyDeviceToHost, s));
     CU(cudaMemcpyAsync(e->split_kind, misc->split_kind, sizeof(e->split_kind), cudaMemcpyDeviceToHost, s));
@@ -696,7 +730,8 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
         // (count and scatter per request, one scan, one sort), plan (offset scan and expansion),
         // split levels and leaves, Golomb-Rice encoding (4 per request, counted above), retrieval
         // compaction (keys and bits together, or keys before the leaves and bits after them)
-        out->work[7] = (hash_ms > 0.f ? 1 : 0) + 2 * R + 2 + plan_launches + launches + R * (early_keys ? 2 : 1);
+        out->work[7] = (hash_ms > 0.f ? 1 : 0) + 2 * R + 2 + plan_launches + launches +
+                      R * ((early_keys ? 1 : 0) + (bits_done ? 0 : 1));
     }
     return SHG_OK;
 }
@@ -1024,6 +1059,7 @@ static shg_status set_tuning(shg_engine *e, int variant, int leaf, const std::st
     else if (name == "leaf_blocks_per_sm" && v >= 0 && v <= 16) t.leaf_bps = (int)v;
     else if (name == "leaf_min_blocks" && (v == 4 || v == 6 || v == 8)) t.leaf_minb = (int)v;
     else if (name == "sh1_seeds_per_lane" && (v == 1 || v == 2)) t.sh1_spl = (int)v;
+    else if (name == "queue_lag_rounds" && v >= 0 && v <= 64) t.queue_lag = (int)v;
     else return fail(SHG_ERR_ARG, "tuning: bad parameter " + name + " = " + std::to_string(v));
     if (!split_tuning_valid(t.split.spl, t.split.threads, t.split.round_div, t.split.arith))
         return fail(SHG_ERR_ARG, "tuning: bad parameter " + name + " = " + std::to_string(v));
@@ -1078,6 +1114,7 @@ shg_status shg_engine_get_tuning(shg_engine *e, int variant, int leaf_size, cons
     else if (n == "leaf_blocks_per_sm") *value = t.leaf_bps;
     else if (n == "leaf_min_blocks") *value = t.leaf_minb;
     else if (n == "sh1_seeds_per_lane") *value = t.sh1_spl;
+    else if (n == "queue_lag_rounds") *value = t.queue_lag;
     else return fail(SHG_ERR_ARG, "tuning: unknown parameter " + n);
     return SHG_OK;
 }

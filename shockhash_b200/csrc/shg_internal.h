@@ -148,6 +148,8 @@ struct Tuning {
     int leaf_bps = 0;    // leaf grid in blocks per SM (0: as many as shared memory allows, at most 8)
     int leaf_minb = 6;   // bipartite leaves of up to 64 keys: launch bound of 4, 6 or 8 blocks per SM
     int sh1_spl = 2;     // original leaves: seeds per lane, 1 or 2
+    int queue_lag = 8;   // work-queue item order: lag between a bucket's levels in rounds of the grid
+                         // (0: none, the levels one after another and the leaves last; 1..64)
 };
 bool split_tuning_valid(int spl, int threads, int round_div, int arith);
 constexpr int kTuningFlat = 4;  // tuning-table variant key of ShockHash2Flat<k> (leaf size = k)
@@ -162,16 +164,34 @@ int leaves_sh1_warps_per_block();
 void launch_sh2_op_peak(int kind, int blocks, uint64_t iters, unsigned long long *sink);
 int sh2_op_peak_per_iter(int kind);
 // The work-queue schedule of a ShockHash2 build with leaves of up to 64 keys (shg_leaves_sh2.cu):
-// split nodes then leaves of the launch lists `ids` ([0, nsplit) the split levels in order, then
-// nleaf leaves) in one persistent launch of `grid` blocks; offs/stride/nlevels are the plan's
-// per-bucket list offsets, done[nbuckets] zeroed counters, ctr[2] zeroed item counters.
+// the split nodes and leaves of the launch lists `ids` ([0, nsplit) the split levels in order, then
+// the leaves) in one persistent launch of `grid` blocks, taken in the order of `seq` (*nitems items,
+// both from launch_queue_order); offs/stride/nlevels are the plan's per-bucket list offsets,
+// done[nbuckets] zeroed counters, ctr[2] zeroed item counters.
+// Where the queue kernel writes request r's retrieval input (out[r]; buckets from b_first on, keys
+// from key_off, size-1 positions from single_off in the batch's arrays): compacted keys and bits,
+// host-mapped pinned memory.
+struct QueueOut {
+    uint64_t b_first, key_off, single_off;
+    uint64_t *keys;
+    uint8_t *bits;
+};
 int tree_queue_warps_per_block();
 int tree_queue_smem_per_block(int spl);
-void launch_tree_queue(const Node *nodes, const uint32_t *ids, uint32_t nsplit, uint32_t nleaf, const uint32_t *offs,
-                       uint64_t stride, uint32_t nlevels, uint32_t *done, uint64_t *keys, uint64_t *codes, uint8_t *rib_bits,
-                       uint8_t *scratch, uint64_t per_warp, uint32_t smax, uint32_t cmax, uint64_t max_trials,
-                       uint32_t *err, unsigned long long *work, unsigned long long *kind_work, unsigned int *ctr,
-                       const SplitTuning &t, int grid, cudaStream_t s);
+// Time slots T of the staggered item order (nb + nlevels * lag); launch_queue_order writes the items
+// into seq[0 .. nsplit + buckets with leaves), with scratch cnt[T] and pos[T + 1] (pos[T]: the
+// item count). Without groups the sequence holds the split nodes only, and the queue kernel is
+// given nleaf_tail = the leaf count: its warps take the leaves one by one after the last item.
+uint64_t queue_order_slots(uint64_t nb, uint32_t nlevels, uint32_t lag);
+void launch_queue_order(const uint32_t *offs, uint64_t stride, uint64_t nb, uint32_t nlevels, uint32_t lag, bool groups,
+                        const ListOffsets &lists, uint32_t nsplit, uint32_t *cnt, uint32_t *pos, uint32_t *seq,
+                        cudaStream_t s);
+void launch_tree_queue(const Node *nodes, const uint32_t *ids, const uint32_t *seq, const uint32_t *nitems, uint32_t nsplit,
+                       const uint32_t *offs, uint64_t stride, uint32_t nlevels, uint32_t *done, uint64_t *keys,
+                       uint64_t *codes, uint8_t *rib_bits, uint8_t *scratch, uint64_t per_warp, uint32_t smax, uint32_t cmax,
+                       uint64_t max_trials, uint32_t *err, unsigned long long *work, unsigned long long *kind_work,
+                       unsigned int *ctr, uint32_t nleaf_tail, const uint64_t *acc, const uint64_t *singles,
+                       const QueueOut *out, uint32_t nreq, const SplitTuning &t, int grid, cudaStream_t s);
 void launch_gr_bucket_bits(const Node *nodes, const uint32_t *bnb, uint64_t nb, const uint64_t *acc,
                            const uint64_t *codes, const uint32_t *memo_skip_bits, uint64_t *bucket_bits,
                            cudaStream_t s);

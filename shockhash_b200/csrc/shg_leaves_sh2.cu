@@ -338,18 +338,24 @@ __device__ __forceinline__ void sh2_leaf(const Src &src, uint32_t li, const uint
                 break;
             }
             const uint64_t s = S + lane;
-            typename LeafCtx<MAXM>::Mask tA = 0, tB = 0;
+            using Mask = typename LeafCtx<MAXM>::Mask;
+            Mask tA = 0, tB = 0;
             uint64_t *rrow = s < g.rawcap ? g.raw + s * (MAXM / 8) : nullptr;
-            uint64_t word = 0;
-            for (uint32_t k = 0; k < m; k++) {
-                const uint32_t h = half_hash(sm.keys[k], s, half);
-                const auto bit = (typename LeafCtx<MAXM>::Mask)1 << h;
-                if (k < cx.sizeA) tA |= bit; else tB |= bit;
-                word |= (uint64_t)h << (8 * (k & 7));
-                if ((k & 7) == 7 || k + 1 == m) {
-                    if (rrow) rrow[k >> 3] = word;
-                    word = 0;
+            const uint32_t sizeA = cx.sizeA;
+            // eight independent hash chains per row word (keys 8w..8w+7; MAXM is a multiple of 8, so
+            // sm.keys[8w + 7] is in bounds, and the cells of keys past m are dropped)
+            for (uint32_t k0 = 0; k0 < m; k0 += 8) {
+                uint64_t word = 0;
+#pragma unroll
+                for (uint32_t t = 0; t < 8; t++) {
+                    const uint32_t k = k0 + t;
+                    const uint32_t h = half_hash(sm.keys[k], s, half);
+                    const Mask bit = k < m ? (Mask)1 << h : (Mask)0;
+                    tA |= k < sizeA ? bit : (Mask)0;
+                    tB |= k < sizeA ? (Mask)0 : bit;
+                    word |= k < m ? (uint64_t)h << (8 * t) : 0ull;
                 }
+                if (rrow) rrow[k0 >> 3] = word;
             }
             cx.mp(s) = MaskPair<typename LeafCtx<MAXM>::Mask>{tA, tB};
             w_evals += m;
@@ -737,15 +743,19 @@ void launch_v2(const Node *nodes, const uint32_t *ids, uint32_t count, const uin
 
 // ------------------------------------------------------------------ work-queue schedule
 // All split nodes and leaves of a ShockHash2 build (leaves of up to 64 keys) in ONE persistent
-// launch. Items are taken in the order of the launch lists: the split nodes level by level (buckets
-// in order inside a level), then the leaves (buckets in order). A block takes one split node at a
-// time and searches it with all its warps (split_node); once every split node has been taken, its
-// warps take leaves one at a time (sh2_leaf). A node may start when its bucket's split nodes of the
-// levels above it are done, a leaf when all of its bucket's split nodes are: a per-bucket counter
-// of finished split nodes, compared with the counts of the plan (offs: per list column and bucket).
-// Everything an item waits for was taken earlier by a block that is running, so the waits end;
-// each is still bounded, and one that runs out sets kErrInternal (the build then fails).
-// Keys rewritten by another SM's partition are read past L1.
+// launch. Blocks take items from one sequence: a split node (searched and partitioned by the whole
+// block, split_node) or the leaves of one bucket (the block's warps take them one at a time from a
+// shared counter, sh2_leaf). The sequence is staggered by bucket: time slot t holds the level-lv
+// split nodes of bucket t - lv * lag for every level, then the leaves of bucket t - nlevels * lag.
+// So at any moment the running blocks mix the deep split levels of some buckets, the upper levels
+// of later ones and the leaves of earlier ones: the integer-bound split search and the latency-bound
+// leaf search share every SM, instead of the leaves starting after the last split level.
+// A node may start when its bucket's split nodes of the levels above it are done, a leaf group when
+// all of its bucket's split nodes are: a per-bucket counter of finished split nodes, compared with
+// the plan's counts (offs: per list column and bucket). Everything an item waits for sits earlier in
+// the sequence, so it was taken by a block that is running, and the waits end; each is still
+// bounded, and one that runs out sets kErrInternal (the build then fails). Keys rewritten by another
+// SM's partition are read past L1.
 constexpr int kQueueThreads = 256;
 constexpr int kQueueWarps = kQueueThreads / 32;
 constexpr uint32_t kQueueWaitLimit = 1u << 18;  // polls of at least 64 ns: a fifth of a second or more, far beyond any node
@@ -778,37 +788,130 @@ __device__ __forceinline__ uint32_t splits_above(const uint32_t *__restrict__ of
     return t;
 }
 
+// The item sequence. Items are indices into the launch lists' id array for split nodes
+// (< nsplit) and nsplit + b for the leaves of bucket b (buckets without leaves have no item; with
+// groups = 0 no leaf items at all: the kernel's warps then take the leaves one by one after the
+// last item). cnt[t]: items of time slot t.
+__global__ void k_qorder_count(const uint32_t *__restrict__ offs, uint64_t stride, uint32_t nb, uint32_t nlevels,
+                               uint32_t lag, uint32_t T, uint32_t groups, uint32_t *__restrict__ cnt) {
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T) return;
+    uint32_t c = 0;
+    for (uint32_t lv = 0; lv < nlevels + groups; lv++) {
+        const uint64_t sh = (uint64_t)lv * lag;
+        if (t < sh || t - sh >= nb) continue;
+        const uint64_t b = t - sh;
+        if (lv < nlevels) {
+            const uint32_t *col = offs + (uint64_t)(kColLevel0 + lv) * stride;
+            c += col[b + 1] - col[b];
+        } else {
+            const uint32_t *col = offs + (uint64_t)kColLeaves * stride;
+            c += col[b + 1] > col[b];
+        }
+    }
+    cnt[t] = c;
+}
+
+// Exclusive scan of cnt[0..T) into pos, the total into pos[T] (one block: a sequential run per
+// thread, then the runs' sums).
+__global__ void __launch_bounds__(1024) k_qorder_scan(const uint32_t *__restrict__ cnt, uint32_t T,
+                                                      uint32_t *__restrict__ pos) {
+    __shared__ uint32_t part[1024];
+    const uint32_t per = (T + blockDim.x - 1) / blockDim.x;
+    const uint32_t lo = min(T, threadIdx.x * per), hi = min(T, lo + per);
+    uint32_t sum = 0;
+    for (uint32_t i = lo; i < hi; i++) sum += cnt[i];
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (uint32_t w = 0; w < blockDim.x; w++) {
+            const uint32_t v = part[w];
+            part[w] = run;
+            run += v;
+        }
+    }
+    __syncthreads();
+    uint32_t run = part[threadIdx.x];
+    for (uint32_t i = lo; i < hi; i++) {
+        pos[i] = run;
+        run += cnt[i];
+    }
+    if (threadIdx.x == blockDim.x - 1) pos[T] = run;
+}
+
+__global__ void k_qorder_scatter(const uint32_t *__restrict__ offs, uint64_t stride, uint32_t nb, uint32_t nlevels,
+                                 uint32_t lag, uint32_t T, uint32_t groups, ListOffsets lists, uint32_t nsplit,
+                                 const uint32_t *__restrict__ pos, uint32_t *__restrict__ seq) {
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T) return;
+    uint32_t p = pos[t];
+    for (uint32_t lv = 0; lv < nlevels + groups; lv++) {
+        const uint64_t sh = (uint64_t)lv * lag;
+        if (t < sh || t - sh >= nb) continue;
+        const uint64_t b = t - sh;
+        if (lv < nlevels) {
+            const uint32_t *col = offs + (uint64_t)(kColLevel0 + lv) * stride;
+            for (uint32_t j = col[b]; j < col[b + 1]; j++) seq[p++] = lists.level[lv] + j;
+        } else {
+            const uint32_t *col = offs + (uint64_t)kColLeaves * stride;
+            if (col[b + 1] > col[b]) seq[p++] = nsplit + (uint32_t)b;
+        }
+    }
+}
+
+// Bucket b's retrieval input (its keys in tree order and their bits, without the size-1 positions,
+// which have no bit) written by the calling block to its request's compacted arrays in host-mapped
+// pinned memory, once the bucket's splits and leaves are done. Size-1 positions of the batch are
+// singles[] (ascending), bucket b's at singles[scol[b] .. scol[b + 1]).
+__device__ void write_bucket_out(uint32_t b, const uint64_t *__restrict__ acc, const uint64_t *__restrict__ keys,
+                                 const uint8_t *__restrict__ rib_bits, const uint64_t *__restrict__ singles,
+                                 const uint32_t *__restrict__ scol, const QueueOut *__restrict__ out, uint32_t nreq) {
+    uint32_t lo = 0, hi = nreq;  // the request of bucket b: the last with b_first <= b
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (out[mid].b_first <= b) lo = mid; else hi = mid;
+    }
+    const QueueOut o = out[lo];
+    const uint64_t k0 = acc[b], k1 = acc[b + 1], s0 = scol[b], s1 = scol[b + 1];
+    const uint64_t base = (k0 - o.key_off) - (s0 - o.single_off);  // compacted index of the bucket's first kept key
+    for (uint64_t i = k0 + threadIdx.x; i < k1; i += blockDim.x) {
+        uint64_t below = 0;
+        bool single = false;
+        for (uint64_t t = s0; t < s1; t++) {  // a bucket has few size-1 positions
+            const uint64_t sp = singles[t];
+            below += sp < i;
+            single |= sp == i;
+        }
+        if (single) continue;
+        const uint64_t j = base + (i - k0) - below;
+        o.keys[j] = __ldcg(&keys[i]);
+        o.bits[j] = rib_bits[i];
+    }
+}
+
+// The queue kernel's leaf search, out of line: called once per leaf, it keeps the split loop's
+// register allocation apart from the leaf search's.
+__device__ __noinline__ void queue_leaf(const NodeLeaves &leaves, uint32_t li, const uint64_t *__restrict__ keys,
+                                        uint8_t *__restrict__ rib_bits, Sh2Smem<64> &sm, Sh2Global<64> &g, LaneUF2<64> &uf,
+                                        int lane, uint32_t smax, uint32_t cmax, uint32_t *__restrict__ err, LeafWork &lw) {
+    sh2_leaf<64, NodeLeaves, true>(leaves, li, keys, rib_bits, sm, g, uf, lane, smax, cmax, kQuadMinRecSplit, err, lw);
+}
+
 template <int SPL, int ARITH>
 __global__ void __launch_bounds__(kQueueThreads, 3)
-    k_tree_queue(const Node *__restrict__ nodes, const uint32_t *__restrict__ ids, uint32_t nsplit, uint32_t nleaf,
-                 const uint32_t *__restrict__ offs, uint64_t stride, uint32_t nlevels, uint32_t *__restrict__ done,
-                 uint64_t *__restrict__ keys, uint64_t *__restrict__ codes, uint8_t *__restrict__ rib_bits,
-                 uint8_t *__restrict__ scratch, uint64_t scratch_per_warp, uint32_t smax, uint32_t cmax,
-                 uint64_t max_trials, uint32_t *__restrict__ err, unsigned long long *__restrict__ work,
-                 unsigned long long *__restrict__ kind_work, unsigned int *__restrict__ ctr, int round_div,
-                 const PipeK K) {
+    k_tree_queue(const Node *__restrict__ nodes, const uint32_t *__restrict__ ids, const uint32_t *__restrict__ seq,
+                 const uint32_t *__restrict__ nitems_p, uint32_t nsplit, const uint32_t *__restrict__ offs, uint64_t stride, uint32_t nlevels,
+                 uint32_t *__restrict__ done, uint64_t *__restrict__ keys, uint64_t *__restrict__ codes,
+                 uint8_t *__restrict__ rib_bits, uint8_t *__restrict__ scratch, uint64_t scratch_per_warp, uint32_t smax,
+                 uint32_t cmax, uint64_t max_trials, uint32_t *__restrict__ err, unsigned long long *__restrict__ work,
+                 unsigned long long *__restrict__ kind_work, unsigned int *__restrict__ ctr, uint32_t nleaf_tail,
+                 const uint64_t *__restrict__ acc, const uint64_t *__restrict__ singles,
+                 const QueueOut *__restrict__ out, uint32_t nreq, int round_div, const PipeK K) {
     extern __shared__ __align__(16) uint8_t smem_raw[];
-    __shared__ uint32_t item;
-    // split phase: the block's shared memory is one SplitSmem
+    __shared__ uint32_t item, leaf_next;
+    // the block's shared memory is one SplitSmem for a split node, one Sh2Smem per warp for leaves
     SplitSmem<SPL, kQueueThreads> &ssm = *reinterpret_cast<SplitSmem<SPL, kQueueThreads> *>(smem_raw);
-    for (;;) {
-        if (threadIdx.x == 0) item = atomicAdd(&ctr[0], 1u);
-        __syncthreads();
-        const uint32_t i = item;
-        __syncthreads();
-        if (i >= nsplit) break;
-        const uint32_t id = ids[i];
-        const Node nd = nodes[id];
-        if (threadIdx.x == 0 && !wait_done(&done[nd.bucket], splits_above(offs, stride, nd.bucket, nd.level), err))
-            atomicOr(err, kErrInternal);
-        __syncthreads();
-        split_node<SPL, kQueueThreads, ARITH, true>(ssm, nd, id, keys, codes, max_trials, err, work, kind_work,
-                                                    round_div, K);
-        __threadfence();  // this thread's part of the partition before the bucket's counter moves
-        __syncthreads();
-        if (threadIdx.x == 0) atomicAdd(&done[nd.bucket], 1u);
-    }
-    // leaf phase: the same shared memory as one Sh2Smem per warp
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     Sh2Smem<64> &sm = reinterpret_cast<Sh2Smem<64> *>(smem_raw)[warp];
     Sh2Global<64> g;
@@ -816,15 +919,54 @@ __global__ void __launch_bounds__(kQueueThreads, 3)
     LaneUF2<64> uf{sm.uf, lane, 0, 0};
     LeafWork lw;
     const NodeLeaves leaves{nodes, ids + nsplit, codes};
+    const uint32_t *leaf_col = offs + (uint64_t)kColLeaves * stride;
+    const uint32_t nitems = *nitems_p;
     for (;;) {
-        uint32_t li = 0;
-        if (lane == 0) li = atomicAdd(&ctr[1], 1u);
-        li = __shfl_sync(0xffffffffu, li, 0);
-        if (li >= nleaf) break;
-        const uint32_t b = nodes[ids[nsplit + li]].bucket;
-        if (lane == 0 && !wait_done(&done[b], splits_above(offs, stride, b, nlevels), err)) atomicOr(err, kErrInternal);
-        __syncwarp();
-        sh2_leaf<64, NodeLeaves, true>(leaves, li, keys, rib_bits, sm, g, uf, lane, smax, cmax, kQuadMinRecSplit, err, lw);
+        if (threadIdx.x == 0) item = atomicAdd(&ctr[0], 1u);
+        __syncthreads();
+        const uint32_t i = item;
+        __syncthreads();
+        const uint32_t it = i < nitems ? seq[i] : 0xffffffffu;
+        if (it < nsplit) {
+            const uint32_t id = ids[it];
+            const Node nd = nodes[id];
+            if (threadIdx.x == 0 && !wait_done(&done[nd.bucket], splits_above(offs, stride, nd.bucket, nd.level), err))
+                atomicOr(err, kErrInternal);
+            __syncthreads();
+            split_node<SPL, kQueueThreads, ARITH, true>(ssm, nd, id, keys, codes, max_trials, err, work, kind_work,
+                                                        round_div, K);
+            __threadfence();  // this thread's part of the partition before the bucket's counter moves
+            __syncthreads();
+            if (threadIdx.x == 0) atomicAdd(&done[nd.bucket], 1u);
+            continue;
+        }
+        // leaves: the group of bucket b (the block's warps share a counter), or, once the items are
+        // all taken, the leaves left out of the sequence (every warp on its own from ctr[1])
+        const bool group = i < nitems;
+        const uint32_t b = group ? it - nsplit : 0, end = group ? leaf_col[b + 1] : nleaf_tail;
+        if (group) {
+            if (threadIdx.x == 0) {
+                if (!wait_done(&done[b], splits_above(offs, stride, b, nlevels), err)) atomicOr(err, kErrInternal);
+                leaf_next = leaf_col[b];
+            }
+            __syncthreads();
+        }
+        for (;;) {
+            uint32_t li = 0;
+            if (lane == 0) li = atomicAdd(group ? &leaf_next : &ctr[1], 1u);
+            li = __shfl_sync(0xffffffffu, li, 0);
+            if (li >= end) break;
+            if (!group) {
+                const uint32_t lb = nodes[ids[nsplit + li]].bucket;
+                if (lane == 0 && !wait_done(&done[lb], splits_above(offs, stride, lb, nlevels), err))
+                    atomicOr(err, kErrInternal);
+                __syncwarp();
+            }
+            queue_leaf(leaves, li, keys, rib_bits, sm, g, uf, lane, smax, cmax, err, lw);
+        }
+        if (!group) break;
+        __syncthreads();  // every warp is done with its Sh2Smem before a split node reuses the memory
+        if (out) write_bucket_out(b, acc, keys, rib_bits, singles, offs + (uint64_t)kColSingles * stride, out, nreq);
     }
     unsigned long long w[5] = {lw.evals, lw.pairs, lw.filtered, lw.edges, lw.scan};
 #pragma unroll
@@ -835,17 +977,19 @@ __global__ void __launch_bounds__(kQueueThreads, 3)
 }
 
 template <int SPL, int ARITH>
-void launch_queue_t(const Node *nodes, const uint32_t *ids, uint32_t nsplit, uint32_t nleaf, const uint32_t *offs,
-                    uint64_t stride, uint32_t nlevels, uint32_t *done, uint64_t *keys, uint64_t *codes, uint8_t *rib_bits,
-                    uint8_t *scratch, uint64_t per_warp, uint32_t smax, uint32_t cmax, uint64_t max_trials, uint32_t *err,
-                    unsigned long long *work, unsigned long long *kind_work, unsigned int *ctr, int round_div, int grid,
-                    cudaStream_t s) {
+void launch_queue_t(const Node *nodes, const uint32_t *ids, const uint32_t *seq, const uint32_t *nitems, uint32_t nsplit,
+                    const uint32_t *offs, uint64_t stride, uint32_t nlevels, uint32_t *done, uint64_t *keys, uint64_t *codes,
+                    uint8_t *rib_bits, uint8_t *scratch, uint64_t per_warp, uint32_t smax, uint32_t cmax,
+                    uint64_t max_trials, uint32_t *err, unsigned long long *work, unsigned long long *kind_work,
+                    unsigned int *ctr, uint32_t nleaf_tail, const uint64_t *acc, const uint64_t *singles,
+                    const QueueOut *out, uint32_t nreq, int round_div, int grid, cudaStream_t s) {
     const size_t smem = std::max(sizeof(SplitSmem<SPL, kQueueThreads>), kQueueWarps * sizeof(Sh2Smem<64>));
     cudaFuncSetAttribute(k_tree_queue<SPL, ARITH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const PipeK K{4u, 32u, 1u << 18, 2u};
-    k_tree_queue<SPL, ARITH><<<grid, kQueueThreads, smem, s>>>(nodes, ids, nsplit, nleaf, offs, stride, nlevels, done, keys,
-                                                               codes, rib_bits, scratch, per_warp, smax, cmax, max_trials,
-                                                               err, work, kind_work, ctr, round_div, K);
+    k_tree_queue<SPL, ARITH><<<grid, kQueueThreads, smem, s>>>(nodes, ids, seq, nitems, nsplit, offs, stride, nlevels, done,
+                                                               keys, codes, rib_bits, scratch, per_warp, smax, cmax,
+                                                               max_trials, err, work, kind_work, ctr, nleaf_tail, acc,
+                                                               singles, out, nreq, round_div, K);
 }
 
 } // namespace
@@ -887,16 +1031,31 @@ int tree_queue_smem_per_block(int spl) {
     return (int)std::max(leaf, split);
 }
 
-void launch_tree_queue(const Node *nodes, const uint32_t *ids, uint32_t nsplit, uint32_t nleaf, const uint32_t *offs,
-                       uint64_t stride, uint32_t nlevels, uint32_t *done, uint64_t *keys, uint64_t *codes, uint8_t *rib_bits,
-                       uint8_t *scratch, uint64_t per_warp, uint32_t smax, uint32_t cmax, uint64_t max_trials,
-                       uint32_t *err, unsigned long long *work, unsigned long long *kind_work, unsigned int *ctr,
-                       const SplitTuning &t, int grid, cudaStream_t s) {
+uint64_t queue_order_slots(uint64_t nb, uint32_t nlevels, uint32_t lag) { return nb + (uint64_t)nlevels * lag; }
+
+void launch_queue_order(const uint32_t *offs, uint64_t stride, uint64_t nb, uint32_t nlevels, uint32_t lag, bool groups,
+                        const ListOffsets &lists, uint32_t nsplit, uint32_t *cnt, uint32_t *pos, uint32_t *seq,
+                        cudaStream_t s) {
+    const uint64_t T = queue_order_slots(nb, nlevels, lag);
+    if (!T) return;
+    const uint32_t blocks = (uint32_t)((T + 255) / 256);
+    k_qorder_count<<<blocks, 256, 0, s>>>(offs, stride, (uint32_t)nb, nlevels, lag, (uint32_t)T, groups ? 1u : 0u, cnt);
+    k_qorder_scan<<<1, 1024, 0, s>>>(cnt, (uint32_t)T, pos);
+    k_qorder_scatter<<<blocks, 256, 0, s>>>(offs, stride, (uint32_t)nb, nlevels, lag, (uint32_t)T, groups ? 1u : 0u, lists,
+                                            nsplit, pos, seq);
+}
+
+void launch_tree_queue(const Node *nodes, const uint32_t *ids, const uint32_t *seq, const uint32_t *nitems, uint32_t nsplit,
+                       const uint32_t *offs, uint64_t stride, uint32_t nlevels, uint32_t *done, uint64_t *keys,
+                       uint64_t *codes, uint8_t *rib_bits, uint8_t *scratch, uint64_t per_warp, uint32_t smax, uint32_t cmax,
+                       uint64_t max_trials, uint32_t *err, unsigned long long *work, unsigned long long *kind_work,
+                       unsigned int *ctr, uint32_t nleaf_tail, const uint64_t *acc, const uint64_t *singles,
+                       const QueueOut *out, uint32_t nreq, const SplitTuning &t, int grid, cudaStream_t s) {
 #define SHG_QUEUE_CASE(SPL, AR)                                                                                          \
     if (t.spl == SPL && t.arith == AR)                                                                                  \
-        return launch_queue_t<SPL, AR>(nodes, ids, nsplit, nleaf, offs, stride, nlevels, done, keys, codes, rib_bits,   \
-                                       scratch, per_warp, smax, cmax, max_trials, err, work, kind_work, ctr, t.round_div, \
-                                       grid, s);
+        return launch_queue_t<SPL, AR>(nodes, ids, seq, nitems, nsplit, offs, stride, nlevels, done, keys, codes,        \
+                                       rib_bits, scratch, per_warp, smax, cmax, max_trials, err, work, kind_work, ctr,   \
+                                       nleaf_tail, acc, singles, out, nreq, t.round_div, grid, s);
     SHG_QUEUE_CASE(1, 0) SHG_QUEUE_CASE(2, 0) SHG_QUEUE_CASE(4, 0) SHG_QUEUE_CASE(1, 1) SHG_QUEUE_CASE(2, 1)
     SHG_QUEUE_CASE(4, 1)
 #undef SHG_QUEUE_CASE
@@ -1000,7 +1159,7 @@ void launch_sh2_op_peak(int kind, int blocks, uint64_t iters, unsigned long long
 // ------------------------------------------------------------------ no-allocation variant
 // Some callers cannot allocate device memory at the moment they need leaf seeds: code running
 // under a host-side allocator that forbids cudaMalloc (a memory pool owned by another framework,
-// a region being captured, a real-time or embedded host path), or code that already owns every
+// a real-time or embedded host path), or code that already owns every
 // buffer it may touch. For them the bipartite leaf search also runs from a fixed scratch area that
 // lives in this library's own device image: kNoAllocScratchBytes (16 MiB) per device that loads the
 // library, held until the process exits. Its layout: 256 bytes of counters (error flags, the leaf

@@ -195,4 +195,33 @@ shg_status shg_shard_partition_device(shg_engine *e, const uint64_t *d_first, co
     return SHG_OK;
 }
 
+shg_status shg_partition_u64(shg_engine *e, const uint64_t *keys, uint64_t n, uint64_t nb, int parts, uint64_t *pairs,
+                             uint64_t *counts) {
+    if (!e || parts < 1 || parts > kMaxWorld || nb == 0 || nb >= (1ull << 32) || !counts || (n && (!keys || !pairs)))
+        return shg_set_error(SHG_ERR_ARG, "partition: bad arguments (1 <= parts <= 64, 1 <= nb < 2^32)");
+    if (!n) {
+        for (int g = 0; g < parts; g++) counts[g] = 0;
+        return SHG_OK;
+    }
+    int device = 0;
+    cudaStream_t s = engine_stream(e, &device);
+    cudaError_t err = cudaSetDevice(device);
+    if (err != cudaSuccess) return shg_set_error(SHG_ERR_CUDA, cudaGetErrorString(err));
+    // scratch: the keys in one engine buffer, fingerprints and pairs in another (32 bytes per key)
+    uint64_t *d_keys = (uint64_t *)engine_scratch(e, 1, n * 8, err);
+    if (!d_keys) return shg_set_error(SHG_ERR_OOM, "partition: key buffer");
+    uint64_t *d_fp = (uint64_t *)engine_scratch(e, 2, n * 32, err);
+    if (!d_fp) return shg_set_error(SHG_ERR_OOM, "partition: fingerprint buffer");
+    uint64_t *d_first = d_fp, *d_second = d_fp + n, *d_pairs = d_fp + 2 * n;
+    if ((err = cudaMemcpyAsync(d_keys, keys, n * 8, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+        return shg_set_error(SHG_ERR_CUDA, cudaGetErrorString(err));
+    launch_spooky_u64(d_keys, n, d_first, d_second, s);
+    const shg_status st = shg_shard_partition_device(e, d_first, d_second, n, nb, parts, d_pairs, counts);
+    if (st != SHG_OK) return st;
+    if ((err = cudaMemcpyAsync(pairs, d_pairs, n * 16, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (err = cudaStreamSynchronize(s)) != cudaSuccess)
+        return shg_set_error(SHG_ERR_CUDA, cudaGetErrorString(err));
+    return SHG_OK;
+}
+
 } // extern "C"

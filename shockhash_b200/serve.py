@@ -20,11 +20,12 @@ bytes_per_key); a batch beyond the warm capacity grows that worker's buffers onc
 size becomes its capacity. A request larger than every limit is built alone. Each result is
 bit-identical to building that request alone.
 
-With `chunk_keys` set, a request of more keys than that is split at submission into bucket-range
-pieces (host fingerprints, partitioned by bucket range like the shards of a multi-GPU build). The
-pieces queue as separate items, so they fit the batch limits, spread over the workers and share
-batches with other requests; the last piece to finish joins them (shg_merge_shards), which gives
-the same bits as building the request alone.
+With `chunk_keys` set, a request of more keys than that is split into bucket-range pieces by the
+first worker that reaches it in the queue: its keys are hashed and partitioned by bucket range on
+that worker's GPU (shg_partition_u64, the partition of a multi-GPU build) and the pieces go back to
+the head of the queue as separate items, so they fit the batch limits, spread over the workers and
+share batches with other requests; the last piece to finish joins them (shg_merge_shards), which
+gives the same bits as building the request alone.
 
     python -m shockhash_b200.serve --requests 400
 prints one JSON line with p50/p99 build latency, aggregate keys/s and device utilisation for a
@@ -38,6 +39,7 @@ import math
 import threading
 import time
 from collections import deque
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
@@ -46,7 +48,7 @@ from . import SHOCKHASH2, Engine, _check, _ptr, device_memory, hash_u64_host, ke
 
 class Request:
     __slots__ = ("rid", "keys", "t_arrival", "t_start", "t_done", "result", "error", "_event", "batch_size",
-                 "parts", "remaining")
+                 "parts", "remaining", "to_split")
 
     def __init__(self, rid, keys, t_arrival):
         self.rid, self.keys, self.t_arrival = rid, keys, t_arrival
@@ -54,6 +56,7 @@ class Request:
         self.result = self.error = None
         self.batch_size = 0
         self.parts, self.remaining = None, 0  # bucket-range pieces of a chunked request
+        self.to_split = False  # queued whole, split into pieces by the first worker that reaches it
         self._event = threading.Event()
 
     def wait(self, timeout=None):
@@ -82,17 +85,22 @@ class Piece:
         return self.first
 
 
-def split_request(keys, bucket, chunk_keys, threads=8):
-    """The bucket-range pieces of a request of more than `chunk_keys` keys: its fingerprints (host),
+def split_request(keys, bucket, chunk_keys, engine=None, threads=8):
+    """The bucket-range pieces of a request of more than `chunk_keys` keys: its fingerprints
     partitioned by range of their bucket remap128(first, nb) into ceil(n / chunk_keys) ranges (at most
-    64), stable. Returns [(first, second, nb_global, b0, b1)] in bucket order, empty ranges left out."""
+    64), stable. With an engine the keys are hashed and partitioned on its GPU (shg_partition_u64),
+    otherwise on the host (shg_hash_u64_host, shg_shard_partition); both give the same pieces.
+    Returns [(first, second, nb_global, b0, b1)] in bucket order, empty ranges left out."""
     n = len(keys)
-    first, second = hash_u64_host(keys, threads)
     nb = max(1, (n + bucket - 1) // bucket)
     parts = max(1, min(64, -(-n // chunk_keys), nb))
-    pairs = np.empty((n, 2), dtype=np.uint64)
-    counts = np.zeros(parts, dtype=np.uint64)
-    _check(lib().shg_shard_partition(_ptr(first), _ptr(second), n, nb, parts, _ptr(pairs), _ptr(counts)))
+    if engine is not None:
+        pairs, counts = engine.partition_u64(keys, nb, parts)
+    else:
+        first, second = hash_u64_host(keys, threads)
+        pairs = np.empty((n, 2), dtype=np.uint64)
+        counts = np.zeros(parts, dtype=np.uint64)
+        _check(lib().shg_shard_partition(_ptr(first), _ptr(second), n, nb, parts, _ptr(pairs), _ptr(counts)))
     out, at = [], 0
     for g in range(parts):
         b0, b1 = nb * g // parts, nb * (g + 1) // parts
@@ -131,6 +139,7 @@ class BuildServer:
                 for r in e.build_batch_u64(variant, leaf, [sample], bucket):
                     r.free()
             del sample
+        self._merger = ThreadPoolExecutor(max_workers=2) if chunk_keys else None
         self._threads = [threading.Thread(target=self._worker, args=(w, e), daemon=True)
                          for w, e in enumerate(self._engines)]
         for t in self._threads:
@@ -138,18 +147,28 @@ class BuildServer:
 
     def submit(self, rid, keys, t_arrival=None):
         req = Request(rid, np.ascontiguousarray(keys, dtype=np.uint64), time.perf_counter() if t_arrival is None else t_arrival)
-        items = [req]
-        if self.chunk_keys and len(req.keys) > self.chunk_keys:
-            # pieces enter the queue one after another; other requests can be admitted between them,
-            # and the finished pieces' products wait for the last one
-            pieces = split_request(req.keys, self.bucket, self.chunk_keys)
-            req.parts, req.remaining = [None] * len(pieces), len(pieces)
-            items = [Piece(req, i, *pc) for i, pc in enumerate(pieces)]
-            req.keys = None
+        # a large request queues whole; the worker that reaches it splits it on its GPU and puts the
+        # pieces back at the head of the queue (its latency clock runs from here, split included)
+        req.to_split = bool(self.chunk_keys) and len(req.keys) > self.chunk_keys
         with self._cv:
-            self._q.extend(items)
-            self._cv.notify_all()
+            self._q.append(req)
+            self._cv.notify()
         return req
+
+    def _split(self, req, eng):
+        """Replaces a large request at the head of the queue by its pieces (worker thread)."""
+        try:
+            pieces = split_request(req.keys, self.bucket, self.chunk_keys, engine=eng)
+        except Exception as ex:
+            req.error, req.t_done = ex, time.perf_counter()
+            req._event.set()
+            return
+        req.parts, req.remaining = [None] * len(pieces), len(pieces)
+        req.keys = None
+        with self._cv:
+            # pieces go first, in bucket order; other requests are admitted beside them
+            self._q.extendleft(reversed([Piece(req, i, *pc) for i, pc in enumerate(pieces)]))
+            self._cv.notify_all()
 
     def batch_limit(self, w):
         """Keys worker `w` may take now: its capacity plus the growth the free device memory allows
@@ -180,7 +199,19 @@ class BuildServer:
                     self._cv.wait()
                 if self._stop and not self._q:
                     return
-                batch, total, grow = self._take(w)
+                head = self._q[0]
+                if isinstance(head, Request) and head.to_split:
+                    self._q.popleft()
+                    head.to_split = False
+                    if head.t_start is None:
+                        head.t_start = time.perf_counter()
+                    split = head
+                else:
+                    split = None
+                    batch, total, grow = self._take(w)
+            if split is not None:
+                self._split(split, eng)
+                continue
             t0 = time.perf_counter()
             for r in batch:
                 owner = r.parent if isinstance(r, Piece) else r
@@ -234,8 +265,10 @@ class BuildServer:
                 req.error = err
             req.remaining -= 1
             last = req.remaining == 0
-        if not last:
-            return
+        if last:  # the join runs beside the workers, which go on building
+            self._merger.submit(self._join, req)
+
+    def _join(self, req):
         try:
             if req.error is None:
                 merged = merge_shards(self.variant, self.leaf, req.parts, self.bucket)
@@ -259,6 +292,8 @@ class BuildServer:
             self._cv.notify_all()
         for t in self._threads:
             t.join()
+        if self._merger is not None:
+            self._merger.shutdown(wait=True)
         for e in self._engines:
             e.close()
 

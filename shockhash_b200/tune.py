@@ -110,14 +110,14 @@ def tune_config(eng, variant, leaf, n, reps=3, min_gain=0.02, log=print):
     tu = Tuner(eng, variant, leaf, n, reps=reps)
     # start from the library's untuned defaults, whatever table the engine loaded
     base = {"split_seeds_per_lane": 2, "split_threads": 256, "split_round_div": 8, "split_arith": 0,
-            "leaf_blocks_per_sm": 0, "leaf_min_blocks": 6, "sh1_seeds_per_lane": 2}
+            "leaf_blocks_per_sm": 0, "leaf_min_blocks": 6, "sh1_seeds_per_lane": 2, "queue_lag_rounds": 8}
     t0_split, t0_leaf = tu.measure(base)
     params = dict(base)
     split_c, leaf_c = dict(SPLIT_CANDIDATES), dict(LEAF_CANDIDATES[variant])
     if variant == SHOCKHASH2 and leaf <= 64:
         # the work-queue schedule (the default here): 256-thread blocks, at most 3 per SM
         split_c.pop("split_threads", None)
-        leaf_c = {"leaf_blocks_per_sm": (1, 2, 3)}
+        leaf_c = {"leaf_blocks_per_sm": (1, 2, 3), "queue_lag_rounds": (0, 2, 4, 16, 32)}
     if variant != TUNING_FLAT:
         params, _ = tu.descend(params, split_c, 0, min_gain)
     params, _ = tu.descend(params, leaf_c, 1, min_gain)

@@ -60,6 +60,15 @@ def test_batch_items_equal_alone_and_shard_builds(engine):
     assert same(whole, engine.build_u64(2, 64, keys_b, 2000))
 
 
+def test_device_split_equals_host_split(engine):
+    keys = shg.keys_mt19937_64(43, 333_333)
+    host = serve.split_request(keys, 2000, 50_000)
+    dev = serve.split_request(keys, 2000, 50_000, engine=engine)
+    assert len(host) == len(dev) == 7
+    for a, b in zip(host, dev):
+        assert a[2:] == b[2:] and np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
 def test_chunked_server_results_equal_alone_builds(engine):
     sizes = [3_000, 260_000, 40_000, 1, 180_001, 9_999]
     srv = serve.BuildServer(workers=2, max_batch_keys=150_000, chunk_keys=60_000)

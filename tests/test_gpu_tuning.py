@@ -27,6 +27,7 @@ def test_every_parameter_value_gives_identical_products(variant, leaf):
                                    (2, 256, 8, 1))]
     if variant == shg.SHOCKHASH2:
         settings += [dict(leaf_blocks_per_sm=b, leaf_min_blocks=mb) for b, mb in ((1, 4), (3, 8), (8, 6))]
+        settings += [dict(leaf_blocks_per_sm=0, queue_lag_rounds=q) for q in (1, 3, 64, 0)]
     else:
         settings += [dict(leaf_blocks_per_sm=b, sh1_seeds_per_lane=sp) for b, sp in ((1, 1), (16, 1), (4, 2))]
     for st in settings:

@@ -47,6 +47,15 @@ class _FakeEngine:
             _FakeEngine.batches.append(sizes)
         return [_FakeResult(np.zeros(n)) for n in sizes]
 
+    def partition_u64(self, keys, nb, parts):  # the device partition's host twin
+        import shockhash_b200 as shg
+        first, second = shg.hash_u64_host(keys)
+        pairs = np.empty((len(keys), 2), np.uint64)
+        counts = np.zeros(parts, np.uint64)
+        shg._check(shg.lib().shg_shard_partition(shg._ptr(first), shg._ptr(second), len(keys), nb, parts,
+                                                 shg._ptr(pairs), shg._ptr(counts)))
+        return pairs, counts
+
     def close(self):
         self.closed = True
 
