@@ -41,8 +41,14 @@ typedef enum shg_status {
 typedef enum shg_variant {
     SHG_SHOCKHASH = 1,   /* shockhash::ShockHash<leaf_size, false>            (include/ShockHash.h:134) */
     SHG_SHOCKHASH2 = 2,  /* shockhash::ShockHash2<leaf_size>                  (include/ShockHash2.h:117) */
-    SHG_SHOCKHASH_ROTATION = 3  /* shockhash::ShockHash<leaf_size, true>: leaves of exactly leaf_size keys
+    SHG_SHOCKHASH_ROTATION = 3, /* shockhash::ShockHash<leaf_size, true>: leaves of exactly leaf_size keys
                                    use rotation fitting (ShockHash.h:316-399); leaf_size 2..60 */
+    SHG_SIMDSHOCKHASH = 5,      /* shockhash::SIMDShockHash<leaf_size, false> (include/SIMDShockHash.hpp:105), the
+                                   class the reference's SIMD benchmark builds as ShockHash<l>: the same tree and
+                                   leaves as ShockHash<l, false>, with its own split hash (remixAndRemap,
+                                   SIMDShockHash.hpp:762-766) and start seeds (:209, :582, :593, :411); leaf_size 2..60 */
+    SHG_SIMDSHOCKHASH_ROTATION = 6 /* shockhash::SIMDShockHash<leaf_size, true>: rotation fitting for leaves of
+                                   exactly leaf_size keys (SIMDShockHash.hpp:419-512) */
 } shg_variant;
 
 /* How the search stages are scheduled on the device. All modes give identical results. */
@@ -62,7 +68,7 @@ typedef enum shg_mode {
 
 typedef struct shg_params {
     int variant;              /* shg_variant */
-    int leaf_size;            /* ShockHash: 2..60; ShockHash2: 2..128 */
+    int leaf_size;            /* ShockHash, SIMDShockHash: 2..60; ShockHash2: 2..128 */
     uint64_t bucket_size;     /* expected keys per bucket (the reference's bucket_size argument) */
     int mode;                 /* shg_mode */
     uint64_t max_trials;      /* seeds tried at most per split node / original leaf; 0 = library default,
@@ -376,7 +382,8 @@ int shg_int_peak(int device, uint64_t iters, double *evals_per_s, double *ms);
  * 7 = bipartite isolated-key pair filter, 8 = bipartite pseudoforest edges (union-find),
  * 9 / 10 / 11 / 12 = kinds 0 / 3 / 4 / 5 with the split kernel's pipe-split arithmetic
  * (tuning parameter split_arith 1), 13 / 14 / 15 = kinds 6 / 7 / 8 for bipartite leaves of more
- * than 64 keys (64-bit masks, 100-edge tests). */
+ * than 64 keys (64-bit masks, 100-edge tests), 16 / 17 / 18 / 19 = kinds 0 / 3 / 4 / 5 under
+ * SIMDShockHash's split hash (SIMDShockHash.hpp:762-766). */
 int shg_int_peak_kind(int device, int kind, uint64_t iters, double *evals_per_s, double *ms);
 
 /* Work counts of the engine's last RecSplit build beyond shg_result.work (measurement utility, no

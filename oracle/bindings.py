@@ -32,6 +32,8 @@ REF_DIR = _V4_DIR if host_has_avx512() and os.path.exists(os.path.join(_V4_DIR, 
 REF_SO = os.path.join(REF_DIR, "libshref.so")
 STATS_SO = os.path.join(REF_DIR, "libshref_stats.so")
 PORT_SO = os.path.join(HERE, "_port", "libshgport.so")
+# SIMDShockHash.hpp built for 4 lanes of 64 bits (x86-64-v3) and for 8 (x86-64-v4)
+SIMD_SO = {4: os.path.join(HERE, "_ref", "libshref_simd.so"), 8: os.path.join(_V4_DIR, "libshref_simd.so")}
 
 
 def ref_build_info():
@@ -110,6 +112,59 @@ class _Lib:
             if fn is not None:
                 fn.restype = ctypes.c_uint64
                 fn.argtypes = [_vp]
+
+
+class RefSimdLib(_Lib):
+    """The reference's SIMDShockHash<leaf, rotation> (oracle/ref_simd_capi.cpp), built for `lanes`
+    64-bit lanes (4: AVX2, 8: AVX-512; the 8-lane build needs an AVX-512 host)."""
+    prefix = "refsimd_"
+
+    def __init__(self, lanes=None):
+        if lanes is None:
+            lanes = 8 if host_has_avx512() and os.path.exists(SIMD_SO[8]) else 4
+        super().__init__(SIMD_SO[lanes])
+        L = self.lib
+        L.refsimd_lanes.restype = ctypes.c_uint64
+        L.refsimd_build_hash.restype = _vp
+        L.refsimd_build_hash.argtypes = [ctypes.c_int, ctypes.c_int, _vp, _vp, _sz, _sz, _sz]
+        L.refsimd_build_strings.restype = _vp
+        L.refsimd_build_strings.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_char_p, _vp, _sz, _sz, _sz]
+        L.refsimd_query_strings.argtypes = [_vp, ctypes.c_char_p, _vp, _sz, _vp]
+        L.refsimd_remix_and_remap.argtypes = [_vp, _sz, ctypes.c_uint32, _vp]
+        self.lanes = int(L.refsimd_lanes())
+
+    def _built(self, h, leaf):
+        if not h:
+            raise ValueError(f"leaf size {leaf} not instantiated in the SIMDShockHash oracle")
+        b = Built(self.lib, "refsimd_", h)
+        b.bits = int(self.lib.refsimd_get_bits(_vp(h)))
+        return b
+
+    def build_hash(self, rotation, leaf, first, second, bucket_size=2000, threads=1):
+        first = np.ascontiguousarray(first, dtype=np.uint64)
+        second = np.ascontiguousarray(second, dtype=np.uint64)
+        return self._built(self.lib.refsimd_build_hash(int(rotation), leaf, _ptr(first), _ptr(second), len(first),
+                                                       bucket_size, threads), leaf)
+
+    def build_strings(self, rotation, leaf, keys, bucket_size=2000, threads=1):
+        data, offs = pack_strings(keys)
+        b = self._built(self.lib.refsimd_build_strings(int(rotation), leaf, data, _ptr(offs), len(keys), bucket_size,
+                                                       threads), leaf)
+        b._strings = (data, offs)
+        return b
+
+    def query_strings(self, built, keys):
+        data, offs = pack_strings(keys)
+        out = np.zeros(len(keys), dtype=np.uint64)
+        self.lib.refsimd_query_strings(_vp(built.h), data, _ptr(offs), len(keys), _ptr(out))
+        return out
+
+    def remix_and_remap(self, x, n):
+        """The format's split hash of each value for range n (SIMDShockHash.hpp:762-766)."""
+        x = np.ascontiguousarray(x, dtype=np.uint64)
+        out = np.zeros(len(x), np.uint32)
+        self.lib.refsimd_remix_and_remap(_ptr(x), len(x), n, _ptr(out))
+        return out
 
 
 class RefLib(_Lib):

@@ -52,13 +52,29 @@ struct Work {
     uint64_t split_evals = 0, leaf_evals = 0, pairs = 0, pairs_filtered = 0, uf_edges = 0, leaves = 0, splits = 0;
 };
 
-// Splitting thresholds: ShockHash.h:63-72 (variant 1) and ShockHash2.h:49-56 (variant 2).
+// Variant 5 is SIMDShockHash<l, false> (SIMDShockHash.hpp): ShockHash's tree, memo and leaves, with
+// its own split hash and start seeds.
+inline bool sh1_like(int variant) { return variant == 1 || variant == 5; }
+
+// MurmurHash3's 32-bit finalizer (SIMDShockHash.hpp:76-83, remix32).
+inline uint32_t fmix32(uint32_t z) {
+    z ^= z >> 16;
+    z *= 0x85ebca6bu;
+    z ^= z >> 13;
+    z *= 0xc2b2ae35u;
+    z ^= z >> 16;
+    return z;
+}
+// SIMDShockHash's split hash of z (= key + seed) onto [0, m): remixAndRemap, SIMDShockHash.hpp:762-766.
+inline size_t simd_remap(uint64_t z, uint32_t m) { return remap16(fmix32(uint32_t(z >> 32) ^ uint32_t(z)), m); }
+
+// Splitting thresholds: ShockHash.h:63-72 (variants 1, 5) and ShockHash2.h:49-56 (variant 2).
 struct Config {
     int variant, leaf;
     size_t lower, upper;
     std::vector<uint64_t> memo;
     Config(int variant, int leaf) : variant(variant), leaf(leaf) {
-        if (variant == 1) {
+        if (sh1_like(variant)) {
             lower = leaf * (leaf > 24 ? 4 : 2);
             upper = lower * (leaf > 24 ? 3 : 2);
         } else {
@@ -69,7 +85,7 @@ struct Config {
         // fill_golomb_rice (ShockHash.h:121-127) / fill_golomb_rice2 (ShockHash2.h:106-115)
         size_t s = 0;
         for (; s <= (size_t)leaf; ++s) {
-            uint64_t b = variant == 1 ? BIJ_MEMO[s] : BIJ_MEMO2[s];
+            uint64_t b = sh1_like(variant) ? BIJ_MEMO[s] : BIJ_MEMO2[s];
             memo[s] = b << 27 | (uint64_t)(s > 1) << 16 | b;
         }
         for (; s < (size_t)MAX_BUCKET; ++s) fill(s);
@@ -414,12 +430,15 @@ struct Builder {
     // takes the rest; for the fanout-2 case the split point is `unit`.
     // Part of a key under seed x: fanout 2 splits at `unit` (h >= split goes right); otherwise
     // h / unit (the last part takes the remainder).
-    static inline size_t part_of(uint64_t key, uint64_t x, size_t m, size_t unit, size_t fanout) {
-        size_t h = remap16(remix(key + x), (uint32_t)m);
+    // SIMDShockHash searches with its own hash (higherLevel, aggrLevel: SIMDShockHash.hpp:201-364).
+    inline size_t part_of(uint64_t key, uint64_t x, size_t m, size_t unit, size_t fanout) const {
+        size_t h = cfg.variant == 5 ? simd_remap(key + x, (uint32_t)m) : remap16(remix(key + x), (uint32_t)m);
         return fanout == 2 ? (h >= unit ? 1 : 0) : h / unit;
     }
-    uint64_t split(uint64_t *b, size_t m, size_t unit, size_t fanout, int level) {
-        uint64_t x = START_SEED[level];
+    // `seed`: the index into START_SEED the search starts from (the depth, except for SIMDShockHash's
+    // aggregation levels, SIMDShockHash.hpp:582, 593)
+    uint64_t split(uint64_t *b, size_t m, size_t unit, size_t fanout, int seed) {
+        uint64_t x = START_SEED[seed];
         size_t count[32];
         for (;;) {
             std::fill(count, count + 32, 0);
@@ -435,15 +454,16 @@ struct Builder {
         for (size_t i = 0; i < m; i++) temp[pos[part_of(b[i], x, m, unit, fanout)]++] = b[i];
         std::copy(temp.begin(), temp.begin() + m, b);
         work.splits++;
-        return x - START_SEED[level];
+        return x - START_SEED[seed];
     }
 
     void rec(uint64_t *b, size_t m, int level) {
         const size_t leaf = cfg.leaf;
         if (m <= leaf) {
             uint64_t code;
-            if (cfg.variant == 1) {
-                code = sh1_leaf(b, (uint32_t)m, level, ribbon, work);
+            if (sh1_like(cfg.variant)) {
+                // SIMDShockHash's leaves start at START_SEED[19] (SIMDShockHash.hpp:411)
+                code = sh1_leaf(b, (uint32_t)m, cfg.variant == 5 ? 19 : level, ribbon, work);
             } else {
                 code = sh2_find_seed(b, (uint32_t)m, work);
                 sh2_retrieval(b, (uint32_t)m, code, ribbon);
@@ -462,7 +482,8 @@ struct Builder {
         } else {
             const size_t unit = m > cfg.lower ? cfg.lower : leaf;
             const size_t fanout = uint16_t(m + unit - 1) / unit;
-            uint64_t x = split(b, m, unit, fanout, level);
+            const int seed = cfg.variant == 5 ? (unit == leaf ? 18 : 17) : level;
+            uint64_t x = split(b, m, unit, fanout, seed);
             emit(x, m);
             size_t i;
             for (i = 0; i < m - unit; i += unit) rec(b + i, unit, level + 1);
@@ -596,9 +617,13 @@ uint64_t query(const PortResult *r, uint64_t first, uint64_t second) {
     Reader rd(r->desc);
     rd.reset(r->pos_acc[bucket], c.skip_bits(m));
     int level = 0;
+    const bool simd = r->variant == 5;  // SIMDShockHash.hpp:779-844
+    auto hsplit = [simd](uint64_t z, size_t range) {
+        return simd ? simd_remap(z, (uint32_t)range) : remap16(remix(z), (uint32_t)range);
+    };
     while (m > c.upper) {
         uint64_t d = rd.next(c.golomb(m));
-        size_t h = remap16(remix(second + d + START_SEED[level]), (uint32_t)m);
+        size_t h = hsplit(second + d + START_SEED[level], m);
         const size_t sp = (uint16_t(m / 2 + c.upper - 1) / c.upper) * c.upper;
         if (h < sp) m = sp;
         else { rd.skip(c.skip_nodes(sp), c.skip_bits(sp)); m -= sp; cum += sp; }
@@ -606,7 +631,7 @@ uint64_t query(const PortResult *r, uint64_t first, uint64_t second) {
     }
     if (m > c.lower) {
         uint64_t d = rd.next(c.golomb(m));
-        size_t h = remap16(remix(second + d + START_SEED[level]), (uint32_t)m);
+        size_t h = hsplit(second + d + START_SEED[simd ? 17 : level], m);
         size_t part = uint16_t(h) / c.lower;
         m = std::min(c.lower, m - part * c.lower);
         cum += c.lower * part;
@@ -615,7 +640,7 @@ uint64_t query(const PortResult *r, uint64_t first, uint64_t second) {
     }
     if (m > (size_t)c.leaf) {
         uint64_t d = rd.next(c.golomb(m));
-        size_t h = remap16(remix(second + d + START_SEED[level]), (uint32_t)m);
+        size_t h = hsplit(second + d + START_SEED[simd ? 18 : level], m);
         size_t part = uint16_t(h) / c.leaf;
         m = std::min((size_t)c.leaf, m - part * c.leaf);
         cum += c.leaf * part;
@@ -624,9 +649,9 @@ uint64_t query(const PortResult *r, uint64_t first, uint64_t second) {
     }
     uint64_t b = rd.next(c.golomb(m));
     uint64_t ret = retrieve(r, second);
-    if (r->variant == 1) {
+    if (sh1_like(r->variant)) {
         uint32_t c1, c2;
-        cells_sh1(second, b + START_SEED[level], (uint32_t)m, c1, c2);
+        cells_sh1(second, b + START_SEED[simd ? 19 : level], (uint32_t)m, c1, c2);
         return cum + (ret == 0 ? c1 : c2);
     }
     return cum + sh2_query_leaf((uint32_t)m, b, second, ret);

@@ -20,13 +20,14 @@ import os
 
 import numpy as np
 
-__all__ = ["ShgError", "Engine", "BuildResult", "ShockHash", "ShockHash2", "ShockHash2Flat", "lib", "LIB_PATH",
-           "SHOCKHASH", "SHOCKHASH2", "SHOCKHASH_ROTATION", "MODE_DEFAULT", "MODE_LEVELS", "MODE_PER_LEAF",
-           "MODE_PIPELINED"]
+__all__ = ["ShgError", "Engine", "BuildResult", "ShockHash", "ShockHash2", "ShockHash2Flat", "SIMDShockHash", "lib",
+           "LIB_PATH", "SHOCKHASH", "SHOCKHASH2", "SHOCKHASH_ROTATION", "SIMDSHOCKHASH", "SIMDSHOCKHASH_ROTATION",
+           "MODE_DEFAULT", "MODE_LEVELS", "MODE_PER_LEAF", "MODE_PIPELINED"]
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libshg.so")
 
 SHOCKHASH, SHOCKHASH2, SHOCKHASH_ROTATION = 1, 2, 3
+SIMDSHOCKHASH, SIMDSHOCKHASH_ROTATION = 5, 6  # shg_variant (4 is ShockHash2Flat's tuning-table key)
 MODE_DEFAULT, MODE_LEVELS, MODE_PER_LEAF, MODE_PIPELINED, MODE_QUEUE = 0, 1, 2, 3, 4
 _STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_OOM", 3: "ERR_TRIAL_LIMIT", 4: "ERR_CUDA", 5: "ERR_BUCKET",
            6: "ERR_NO_DEVICE"}
@@ -924,9 +925,10 @@ class _Templated(type):
         if key not in _Templated._cache:
             attrs = {"LEAF": int(leaf)}
             if rot:
-                if cls.VARIANT != SHOCKHASH:
-                    raise TypeError("rotation fitting exists for ShockHash<l, true> only")
-                attrs["VARIANT"] = SHOCKHASH_ROTATION
+                rotated = {SHOCKHASH: SHOCKHASH_ROTATION, SIMDSHOCKHASH: SIMDSHOCKHASH_ROTATION}
+                if cls.VARIANT not in rotated:
+                    raise TypeError("rotation fitting exists for ShockHash<l, true> and SIMDShockHash<l, true> only")
+                attrs["VARIANT"] = rotated[cls.VARIANT]
             _Templated._cache[key] = type(f"{cls.__name__}[{leaf}{', True' if rot else ''}]", (cls,), attrs)
         return _Templated._cache[key]
 
@@ -935,6 +937,13 @@ class ShockHash(_RecSplitBase, metaclass=_Templated):
     """shockhash::ShockHash<LEAF_SIZE, ROTATION_FITTING> (include/ShockHash.h:134); use ShockHash[l](keys, b)
     or ShockHash[l, True](keys, b) for rotation fitting."""
     VARIANT = SHOCKHASH
+
+
+class SIMDShockHash(_RecSplitBase, metaclass=_Templated):
+    """shockhash::SIMDShockHash<LEAF_SIZE, ROTATION_FITTING> (include/SIMDShockHash.hpp:105), the class the
+    reference's SIMD benchmark builds as ShockHash<l>; use SIMDShockHash[l](keys, b) or
+    SIMDShockHash[l, True](keys, b) for rotation fitting."""
+    VARIANT = SIMDSHOCKHASH
 
 
 class ShockHash2(_RecSplitBase, metaclass=_Templated):

@@ -91,6 +91,34 @@ __global__ void __launch_bounds__(kPeakThreads) k_int_peak_pipes(uint64_t iters,
     sink[tid] = c[0][0] ^ c[0][1] ^ c[0][2] ^ c[1][0] ^ c[1][1] ^ c[1][2];
 }
 
+// The split loops under SIMDShockHash's split hash (fmix32 of the xor-folded halves): quarter
+// moments (NT = 4) or compare-and-count against NT thresholds; two seeds per key pair.
+template <int NT>
+__global__ void __launch_bounds__(kPeakThreads) k_int_peak_simd(uint64_t iters, uint32_t T0, uint32_t T1, uint32_t T2,
+                                                                unsigned long long *sink) {
+    const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    uint64_t k0 = shg::remix(tid * 0x9E3779B97F4A7C15ULL), k1 = shg::remix(k0);
+    const uint64_t x0 = 0x643e521ddbd2be98ULL + tid;
+    const uint32_t T[3] = {T0, T1, T2};
+    uint32_t c[2][3] = {};
+    for (uint64_t i = 0; i < iters; i++) {
+        const uint32_t r0 = shg::simd_split_low16(k0 + x0 + i), r1 = shg::simd_split_low16(k1 + x0 + i);
+        if (NT == 4) {
+            const uint32_t p0 = r0 >> 14, p1 = r1 >> 14;
+            const uint32_t q0 = p0 * p0, q1 = p1 * p1;
+            c[0][0] += p0; c[0][1] += q0; c[0][2] += q0 * p0;
+            c[1][0] += p1; c[1][1] += q1; c[1][2] += q1 * p1;
+        } else {
+#pragma unroll
+            for (int t = 0; t < NT; t++) {
+                c[0][t] += r0 < T[t];
+                c[1][t] += r1 < T[t];
+            }
+        }
+    }
+    sink[tid] = c[0][0] ^ c[0][1] ^ c[0][2] ^ c[1][0] ^ c[1][1] ^ c[1][2];
+}
+
 // The arithmetic of the original leaf search's coverage loop: full 64-bit remix, both cells by
 // fastrange32 on its halves, one bit each into two 32-bit half masks; two seeds per lane.
 __global__ void __launch_bounds__(kPeakThreads) k_int_peak_sh1(uint64_t iters, uint32_t h1, uint32_t h2,
@@ -214,10 +242,11 @@ int shg_int_peak(int device, uint64_t iters, double *evals_per_s, double *ms_out
 // Integer-pipe peak of one search's inner loop (0 = split quarter moments, 1 = original leaf,
 // 2 = bipartite leaf hashing, 3..5 = split compare-and-count with 1..3 thresholds, 6..8 = bipartite
 // candidate scan, pair filter and pseudoforest edges, 9..12 = kinds 0 and 3..5 with the split
-// kernel's pipe-split arithmetic, 13..15 = kinds 6..8 for leaves of more than 64 keys).
+// kernel's pipe-split arithmetic, 13..15 = kinds 6..8 for leaves of more than 64 keys, 16..19 = kinds
+// 0 and 3..5 under SIMDShockHash's split hash).
 int shg_int_peak_kind(int device, int kind, uint64_t iters, double *evals_per_s, double *ms_out) {
     if (kind == 0) return shg_int_peak(device, iters, evals_per_s, ms_out);
-    if (kind < 1 || kind > 15) return SHG_ERR_ARG;
+    if (kind < 1 || kind > 19) return SHG_ERR_ARG;
     if (cudaSetDevice(device) != cudaSuccess) return SHG_ERR_CUDA;
     cudaDeviceProp prop;
     cudaGetDeviceProperties(&prop, device);
@@ -242,6 +271,14 @@ int shg_int_peak_kind(int device, int kind, uint64_t iters, double *evals_per_s,
             k_int_peak_cmp<3><<<blocks, kPeakThreads>>>(it, 16384, 32768, 49152, sink);
         else if (kind <= 8)  // the bipartite leaf's scan, pair filter and pseudoforest loops (64 edges per iteration)
             shg::launch_sh2_op_peak(kind - 6, blocks, kind == 8 ? it / 64 + 1 : it, sink);
+        else if (kind == 16)
+            k_int_peak_simd<4><<<blocks, kPeakThreads>>>(it, 16384, 32768, 49152, sink);
+        else if (kind == 17)
+            k_int_peak_simd<1><<<blocks, kPeakThreads>>>(it, 50331, 65536, 65536, sink);
+        else if (kind == 18)
+            k_int_peak_simd<2><<<blocks, kPeakThreads>>>(it, 21846, 43691, 65536, sink);
+        else if (kind == 19)
+            k_int_peak_simd<3><<<blocks, kPeakThreads>>>(it, 16384, 32768, 49152, sink);
         else if (kind >= 13)  // the same for leaves of more than 64 keys (100 edges per iteration)
             shg::launch_sh2_op_peak(kind - 10, blocks, kind == 15 ? it / 100 + 1 : it, sink);
         else {  // 9: quarter moments, 10..12: 1..3 thresholds, with the split kernel's pipe-split arithmetic
@@ -265,7 +302,7 @@ int shg_int_peak_kind(int device, int kind, uint64_t iters, double *evals_per_s,
     if (kind >= 6 && kind <= 8) {
         per_iter = shg::sh2_op_peak_per_iter(kind - 6);
         if (kind == 8) timed_iters = iters / 64 + 1;
-    } else if (kind >= 13) {
+    } else if (kind >= 13 && kind <= 15) {
         per_iter = shg::sh2_op_peak_per_iter(kind - 10);
         if (kind == 15) timed_iters = iters / 100 + 1;
     }

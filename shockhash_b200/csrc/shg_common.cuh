@@ -51,6 +51,20 @@ SHG_HD uint32_t remix_low16(uint64_t z) {
     return (uint32_t)((z ^ (z >> 31)) & 0xFFFF);
 }
 
+// MurmurHash3's 32-bit finalizer (fmix32), as SIMDShockHash.hpp:76-83 (remix32) writes it.
+SHG_HD uint32_t fmix32(uint32_t z) {
+    z ^= z >> 16;
+    z *= 0x85ebca6bu;
+    z ^= z >> 13;
+    z *= 0xc2b2ae35u;
+    z ^= z >> 16;
+    return z;
+}
+// SIMDShockHash's split hash before remap16: fmix32 of the xor of z's two 32-bit halves
+// (remixAndRemap, SIMDShockHash.hpp:762-766; the vector form remap() at :58-71 combines the same
+// halves lane by lane). Only the low 16 bits reach remap16.
+SHG_HD uint32_t simd_split_low16(uint64_t z) { return fmix32((uint32_t)(z >> 32) ^ (uint32_t)z) & 0xFFFFu; }
+
 #ifdef __CUDACC__
 // remix's low 32 bits with the work split between the integer and multiply pipes: the high words
 // of the two xor-shifts are taken as multiply-highs by the runtime constants K.four (4) and

@@ -136,9 +136,15 @@ __device__ uint64_t dquery_one(const DView &v, uint64_t first, uint64_t second, 
     DReader rd;
     rd.reset(v, __ldg(v.pos_acc + bucket), skip_bits(v, m));
     int level = 0;
+    // SIMDShockHash: its own split hash and fixed start seeds below the fanout-2 levels
+    // (SIMDShockHash.hpp:785-843)
+    const bool simd = is_simd(v.variant);
+    auto split_hash = [simd](uint64_t z, uint32_t range) {
+        return simd ? remap16(simd_split_low16(z), range) : remap16(remix(z), range);
+    };
     while (m > v.upper) {
         const uint64_t d = rd.next(v, golomb(v, m));
-        const uint32_t h = remap16(remix(second + d + start_seed(level)), m);
+        const uint32_t h = split_hash(second + d + start_seed(level), m);
         const uint32_t sp = (uint16_t(m / 2 + v.upper - 1) / v.upper) * v.upper;
         if (h < sp) {
             m = sp;
@@ -151,7 +157,7 @@ __device__ uint64_t dquery_one(const DView &v, uint64_t first, uint64_t second, 
     }
     if (m > v.lower) {
         const uint64_t d = rd.next(v, golomb(v, m));
-        const uint32_t h = remap16(remix(second + d + start_seed(level)), m);
+        const uint32_t h = split_hash(second + d + start_seed(simd ? kSimdSeedLower : level), m);
         const uint32_t part = uint16_t(h) / v.lower;
         m = min(v.lower, m - part * v.lower);
         cum += (uint64_t)v.lower * part;
@@ -160,7 +166,7 @@ __device__ uint64_t dquery_one(const DView &v, uint64_t first, uint64_t second, 
     }
     if (m > v.leaf) {
         const uint64_t d = rd.next(v, golomb(v, m));
-        const uint32_t h = remap16(remix(second + d + start_seed(level)), m);
+        const uint32_t h = split_hash(second + d + start_seed(simd ? kSimdSeedLeafAggr : level), m);
         const uint32_t part = uint16_t(h) / v.leaf;
         m = min(v.leaf, m - part * v.leaf);
         cum += (uint64_t)v.leaf * part;
@@ -170,9 +176,10 @@ __device__ uint64_t dquery_one(const DView &v, uint64_t first, uint64_t second, 
     const uint64_t b = rd.next(v, golomb(v, m));
     bad = bad || rd.bad;
     const uint64_t ret = dretrieve(v, second);
-    if (v.variant == SHG_SHOCKHASH_ROTATION && m == v.leaf) {  // rotation fitting (ShockHash.h:251-265)
+    const int leaf_seed = simd ? kSimdSeedLeaf : level;
+    if (is_rotation(v.variant) && m == v.leaf) {  // rotation fitting (ShockHash.h:251-265, SIMDShockHash.hpp:826-840)
         const uint32_t r = (uint32_t)(b % m);
-        const uint64_t x = b / m + start_seed(level);
+        const uint64_t x = b / m + start_seed(leaf_seed);
         uint32_t c1, c2;
         if ((second & 1) == 0) {
             sh1_cells(second, x & ~(uint64_t)(m > 32 ? 7 : 0), m, c1, c2);
@@ -183,7 +190,7 @@ __device__ uint64_t dquery_one(const DView &v, uint64_t first, uint64_t second, 
     }
     if (is_sh1(v.variant)) {
         uint32_t c1, c2;
-        sh1_cells(second, b + start_seed(level), m, c1, c2);  // TinyBinaryCuckooHashTable.h:116-123
+        sh1_cells(second, b + start_seed(leaf_seed), m, c1, c2);  // TinyBinaryCuckooHashTable.h:116-123
         return cum + (ret == 0 ? c1 : c2);
     }
     return cum + sh2_leaf_query(m, b, second, ret);

@@ -144,8 +144,11 @@ struct shg_engine {
     Tuning tuning_of(int variant, int leaf) {
         std::lock_guard<std::mutex> lock(tuning_mu);
         if (variant == SHG_SHOCKHASH_ROTATION) variant = SHG_SHOCKHASH;  // same searches
+        if (variant == SHG_SIMDSHOCKHASH_ROTATION) variant = SHG_SIMDSHOCKHASH;
         auto it = tuning.find({variant, leaf});
-        return it == tuning.end() ? Tuning() : it->second;
+        Tuning t = it == tuning.end() ? Tuning() : it->second;
+        if (is_simd(variant)) t.split.arith = kSplitArithSimd;  // the format's own split hash
+        return t;
     }
     ~shg_engine() {
         DevBuf *all[] = {&in_keys, &in_bytes, &in_offsets, &first, &second, &sfirst, &sidx, &counts, &cursor,
@@ -517,7 +520,7 @@ shg_status build_batch(shg_engine *e, const shg_params *p, const uint64_t *d_fir
             launch_leaves_sh1_ctr(e->nodes.as<Node>(), d_ids + leaf_off + a, (uint32_t)(b - a), e->keys.as<uint64_t>(),
                                   e->codes.as<uint64_t>(), e->rib_keys.as<uint64_t>(), e->rib_bits.as<uint8_t>(), p->max_trials,
                                   &misc->err, misc->work, &misc->leaf_ctr, grid, st,
-                                  p->variant == SHG_SHOCKHASH_ROTATION ? (uint32_t)p->leaf_size : 0, tun.sh1_spl);
+                                  is_rotation(p->variant) ? (uint32_t)p->leaf_size : 0, tun.sh1_spl);
         launches++;
     };
     if (queue) {
@@ -1047,9 +1050,10 @@ extern "C" {
 // One parameter per line: "<variant> <leaf size> <name> <value>" (variant as shg_variant, or 4 for
 // ShockHash2Flat<k>); '#' starts a comment. Unknown names or out-of-range values reject the file.
 static shg_status set_tuning(shg_engine *e, int variant, int leaf, const std::string &name, int64_t v) {
-    if (variant < 1 || variant > kTuningFlat || leaf < 1 || leaf > kMaxLeaf2)
+    if (variant < 1 || variant > SHG_SIMDSHOCKHASH_ROTATION || leaf < 1 || leaf > kMaxLeaf2)
         return fail(SHG_ERR_ARG, "tuning: no configuration variant " + std::to_string(variant) + " leaf " + std::to_string(leaf));
     if (variant == SHG_SHOCKHASH_ROTATION) variant = SHG_SHOCKHASH;
+    if (variant == SHG_SIMDSHOCKHASH_ROTATION) variant = SHG_SIMDSHOCKHASH;
     std::lock_guard<std::mutex> lock(e->tuning_mu);
     Tuning t = e->tuning.count({variant, leaf}) ? e->tuning[{variant, leaf}] : Tuning();
     if (name == "split_seeds_per_lane") t.split.spl = (int)v;

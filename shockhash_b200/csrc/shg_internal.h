@@ -18,7 +18,8 @@ enum NodeKind : uint8_t { kLeaf = 0, kSplit2 = 1, kSplitK = 2 };
 struct __align__(16) Node {
     uint32_t start;
     uint16_t m;
-    uint8_t level;
+    uint8_t level;  // index into start_seed of the node's search: its depth, except SIMDShockHash's
+                    // aggregation nodes and leaves (kSimdSeed*)
     uint8_t kind;
     uint32_t bucket;
     uint16_t unit;
@@ -31,7 +32,17 @@ static_assert(sizeof(Node) == 16, "Node must stay 16 bytes");
 // ShockHash<l>: lower = l*(l>24?4:2), upper = lower*(l>24?3:2) (ShockHash.h:63-72);
 // ShockHash2<l>: lower = 4l, upper = 12l (ShockHash2.h:49-56).
 // ShockHash<l, true> shares the tree, memo tables and retrieval layout of ShockHash<l, false>.
-SHG_HD bool is_sh1(int variant) { return variant == SHG_SHOCKHASH || variant == SHG_SHOCKHASH_ROTATION; }
+// SIMDShockHash<l, rot> shares them too; it differs in the split hash and the start seeds.
+SHG_HD bool is_simd(int variant) { return variant == SHG_SIMDSHOCKHASH || variant == SHG_SIMDSHOCKHASH_ROTATION; }
+SHG_HD bool is_sh1(int variant) {
+    return variant == SHG_SHOCKHASH || variant == SHG_SHOCKHASH_ROTATION || is_simd(variant);
+}
+SHG_HD bool is_rotation(int variant) { return variant == SHG_SHOCKHASH_ROTATION || variant == SHG_SIMDSHOCKHASH_ROTATION; }
+// The index into start_seed of a node's search. ShockHash and ShockHash2 start every node at its
+// depth (ShockHash.h:309); SIMDShockHash starts fanout-2 nodes at their depth (SIMDShockHash.hpp:209)
+// and uses fixed entries for the lower aggregation level (:582, start_seed[17]), the leaf
+// aggregation level (:593, start_seed[18]) and the leaves (:411, start_seed[19]).
+constexpr int kSimdSeedLower = kMaxLevels - 3, kSimdSeedLeafAggr = kMaxLevels - 2, kSimdSeedLeaf = kMaxLevels - 1;
 
 struct ShapeCache;  // tree shapes by bucket size, built on first use (shg_plan.cpp)
 struct Config {
@@ -51,6 +62,7 @@ struct TNode {
     uint16_t rel;        // first key relative to the bucket start
     uint16_t m;
     uint8_t level, kind, fanout, g;
+    uint8_t seed;        // index into start_seed of the node's search
     uint16_t unit;
     uint16_t fixed_off;  // bit offset of the node's fixed part within the bucket
 };
@@ -73,7 +85,7 @@ constexpr int kMaxPlanCols = kColLevel0 + kMaxLevels;
 struct __align__(16) ShapeNode {
     uint16_t rel, m;
     uint8_t level, kind, fanout, g;
-    uint16_t unit, fixed_off, rank, pad;
+    uint16_t unit, fixed_off, rank, seed;  // seed: index into start_seed of the node's search
 };
 static_assert(sizeof(ShapeNode) == 16, "ShapeNode must stay 16 bytes");
 struct ShapeTables {
@@ -141,8 +153,10 @@ struct SplitTuning {
     int spl = 2;         // seeds per lane: 1, 2 or 4
     int threads = 256;   // threads per split block (one node per block): 128, 256 or 512
     int round_div = 8;   // warp groups make a round about 1/round_div of a node's expected trials (1..64)
-    int arith = 0;       // 0: remix as the compiler schedules it; 1: split between integer and multiply pipes
+    int arith = 0;       // 0: remix as the compiler schedules it; 1: split between integer and multiply pipes;
+                         // kSplitArithSimd: SIMDShockHash's split hash (set by the engine, not by the table)
 };
+constexpr int kSplitArithSimd = 2;
 struct Tuning {
     SplitTuning split;
     int leaf_bps = 0;    // leaf grid in blocks per SM (0: as many as shared memory allows, at most 8)

@@ -343,7 +343,7 @@ __global__ void k_plan_expand(const uint64_t *__restrict__ acc, uint64_t nb, uin
             Node n;
             n.start = (uint32_t)(a0 + t.rel);
             n.m = t.m;
-            n.level = t.level;
+            n.level = (uint8_t)t.seed;  // start-seed index (the depth, except SIMDShockHash's fixed entries)
             n.kind = t.kind;
             n.bucket = (uint32_t)b;
             n.unit = t.unit;

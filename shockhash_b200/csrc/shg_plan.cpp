@@ -92,9 +92,12 @@ struct ShapeBuilder {
         t.level = (uint8_t)level;
         t.g = (uint8_t)c.golomb(m);
         t.fixed_off = (uint16_t)fixed;
+        t.seed = (uint8_t)level;
         fixed += t.g;
+        const bool simd = is_simd(c.variant);
         if (m <= (uint32_t)c.leaf) {
             t.kind = kLeaf;
+            if (simd) t.seed = kSimdSeedLeaf;
             sh.nodes.push_back(t);
             return;
         }
@@ -111,6 +114,7 @@ struct ShapeBuilder {
             const uint32_t unit = m > c.lower ? c.lower : (uint32_t)c.leaf;
             t.kind = kSplitK;
             t.unit = (uint16_t)unit;
+            if (simd) t.seed = unit == (uint32_t)c.leaf ? kSimdSeedLeafAggr : kSimdSeedLower;
             t.fanout = (uint8_t)(uint16_t(m + unit - 1) / unit);
             sh.nodes.push_back(t);
             uint32_t i;
@@ -165,6 +169,7 @@ void make_shape_tables(const Config &c, uint32_t rows, ShapeTables &t) {
             n.g = tn.g;
             n.unit = tn.unit;
             n.fixed_off = tn.fixed_off;
+            n.seed = tn.seed;
             const int col = tn.kind == kLeaf ? kColLeaves : kColLevel0 + tn.level;
             n.rank = (uint16_t)row[col]++;
             t.nodes.push_back(n);

@@ -111,9 +111,15 @@ uint64_t query_one(const shg_mphf *f, uint64_t first, uint64_t second) {
     Reader rd{f->desc.data(), (uint64_t)f->desc.size()};
     rd.reset(f->pos_acc[bucket], c.skip_bits(m));
     int level = 0;
+    // SIMDShockHash: its own split hash and fixed start seeds below the fanout-2 levels
+    // (SIMDShockHash.hpp:785-843)
+    const bool simd = is_simd(f->variant);
+    auto split_hash = [simd](uint64_t z, uint32_t range) {
+        return simd ? remap16(simd_split_low16(z), range) : remap16(remix(z), range);
+    };
     while (m > c.upper) {
         const uint64_t d = rd.next(c.golomb(m));
-        const uint32_t h = remap16(remix(second + d + start_seed(level)), m);
+        const uint32_t h = split_hash(second + d + start_seed(level), m);
         const uint32_t sp = (uint16_t(m / 2 + c.upper - 1) / c.upper) * c.upper;
         if (h < sp) {
             m = sp;
@@ -126,7 +132,7 @@ uint64_t query_one(const shg_mphf *f, uint64_t first, uint64_t second) {
     }
     if (m > c.lower) {
         const uint64_t d = rd.next(c.golomb(m));
-        const uint32_t h = remap16(remix(second + d + start_seed(level)), m);
+        const uint32_t h = split_hash(second + d + start_seed(simd ? kSimdSeedLower : level), m);
         const uint32_t part = uint16_t(h) / c.lower;
         m = std::min(c.lower, m - part * c.lower);
         cum += (uint64_t)c.lower * part;
@@ -135,7 +141,7 @@ uint64_t query_one(const shg_mphf *f, uint64_t first, uint64_t second) {
     }
     if (m > (uint32_t)c.leaf) {
         const uint64_t d = rd.next(c.golomb(m));
-        const uint32_t h = remap16(remix(second + d + start_seed(level)), m);
+        const uint32_t h = split_hash(second + d + start_seed(simd ? kSimdSeedLeafAggr : level), m);
         const uint32_t part = uint16_t(h) / c.leaf;
         m = std::min((uint32_t)c.leaf, m - part * c.leaf);
         cum += (uint64_t)c.leaf * part;
@@ -144,10 +150,12 @@ uint64_t query_one(const shg_mphf *f, uint64_t first, uint64_t second) {
     }
     const uint64_t b = rd.next(c.golomb(m));
     const uint64_t ret = retrieve(f, second);
-    if (f->variant == SHG_SHOCKHASH_ROTATION && m == (uint32_t)f->leaf) {
-        // rotation fitting (ShockHash.h:251-265): code = x * L + r; set B's cells rotate by r
+    const int leaf_seed = simd ? kSimdSeedLeaf : level;
+    if (is_rotation(f->variant) && m == (uint32_t)f->leaf) {
+        // rotation fitting (ShockHash.h:251-265, SIMDShockHash.hpp:826-840): code = x * L + r; set
+        // B's cells rotate by r
         const uint32_t r = (uint32_t)(b % m);
-        const uint64_t x = b / m + start_seed(level);
+        const uint64_t x = b / m + start_seed(leaf_seed);
         const uint64_t gmask = m > 32 ? 7 : 0;
         uint32_t c1, c2;
         if ((second & 1) == 0) {
@@ -160,7 +168,7 @@ uint64_t query_one(const shg_mphf *f, uint64_t first, uint64_t second) {
     if (is_sh1(f->variant)) {
         // hashToCell (TinyBinaryCuckooHashTable.h:116-123)
         uint32_t c1, c2;
-        sh1_cells(second, b + start_seed(level), m, c1, c2);
+        sh1_cells(second, b + start_seed(leaf_seed), m, c1, c2);
         return cum + (ret == 0 ? c1 : c2);
     }
     return cum + sh2_leaf_query(m, b, second, ret);

@@ -28,6 +28,7 @@ static void launch_split_t(const Node *nodes, const uint32_t *ids, uint32_t coun
                                                               round_div, K);
 }
 
+// Parameters a tuning table may set (the SIMDShockHash form is chosen by the engine, not the table).
 bool split_tuning_valid(int spl, int threads, int round_div, int arith) {
     return (spl == 1 || spl == 2 || spl == 4) && (threads == 128 || threads == 256 || threads == 512) && round_div >= 1 &&
            round_div <= 64 && (arith == 0 || arith == 1);
@@ -47,7 +48,14 @@ void launch_split_level(const Node *nodes, const uint32_t *ids, uint32_t count, 
     SHG_SPLIT_CASE(1, 128, 1) SHG_SPLIT_CASE(1, 256, 1) SHG_SPLIT_CASE(1, 512, 1)
     SHG_SPLIT_CASE(2, 128, 1) SHG_SPLIT_CASE(2, 256, 1) SHG_SPLIT_CASE(2, 512, 1)
     SHG_SPLIT_CASE(4, 128, 1) SHG_SPLIT_CASE(4, 256, 1) SHG_SPLIT_CASE(4, 512, 1)
+    // SIMDShockHash: its own split hash, so never the remix forms' fallback below
+    SHG_SPLIT_CASE(1, 128, 2) SHG_SPLIT_CASE(1, 256, 2) SHG_SPLIT_CASE(1, 512, 2)
+    SHG_SPLIT_CASE(2, 128, 2) SHG_SPLIT_CASE(2, 256, 2) SHG_SPLIT_CASE(2, 512, 2)
+    SHG_SPLIT_CASE(4, 128, 2) SHG_SPLIT_CASE(4, 256, 2) SHG_SPLIT_CASE(4, 512, 2)
 #undef SHG_SPLIT_CASE
+    if (t.arith == kSplitArithSimd)
+        return launch_split_t<2, 256, kSplitArithSimd>(nodes, ids, count, keys, codes, max_trials, err, work, kind_work,
+                                                       t.round_div, s);
     launch_split_t<2, 256, 0>(nodes, ids, count, keys, codes, max_trials, err, work, kind_work, t.round_div, s);
 }
 

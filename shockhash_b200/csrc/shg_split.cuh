@@ -26,6 +26,13 @@
 
 namespace shg {
 
+// The low 16 bits of a key's split hash under seed x (z = key + x): remix for ShockHash and
+// ShockHash2 (arithmetic forms 0 and 1), SIMDShockHash's fmix32 fold for kSplitArithSimd.
+template <int ARITH> __device__ __forceinline__ uint32_t split_r16(uint64_t z) {
+    if constexpr (ARITH == kSplitArithSimd) return simd_split_low16(z);
+    else return remix_low16(z);
+}
+
 template <int SPL, int THREADS> struct SplitSmem {
     static constexpr int kWarps = THREADS / 32;
     uint64_t keys[kMaxBucket];
@@ -36,7 +43,8 @@ template <int SPL, int THREADS> struct SplitSmem {
 
 // Counts of keys below each of NT thresholds, for SPL seeds, over keys [lo, hi).
 // ARITH 1 computes the same counts with remix_lo32_pipes and multiply-add-high counting (r < T is
-// the sign bit of r - T), trading integer-pipe instructions for multiply-pipe ones.
+// the sign bit of r - T), trading integer-pipe instructions for multiply-pipe ones. ARITH
+// kSplitArithSimd counts under SIMDShockHash's split hash.
 template <int NT, int SPL, int ARITH>
 __device__ __forceinline__ void count_range(const uint64_t *__restrict__ sk, uint32_t lo, uint32_t hi, uint64_t x0,
                                             const uint32_t T0, const uint32_t T1, const uint32_t T2,
@@ -61,8 +69,8 @@ __device__ __forceinline__ void count_range(const uint64_t *__restrict__ sk, uin
 #pragma unroll
             for (int s = 0; s < SPL; s++) {
                 const uint64_t x = x0 + (uint64_t)(s * 32);
-                const uint32_t r0 = remix_low16(k0 + x);
-                const uint32_t r1 = remix_low16(k1 + x);
+                const uint32_t r0 = split_r16<ARITH>(k0 + x);
+                const uint32_t r1 = split_r16<ARITH>(k1 + x);
 #pragma unroll
                 for (int t = 0; t < NT; t++) c[s][t] += (r0 < T[t]) + (r1 < T[t]);
             }
@@ -71,7 +79,7 @@ __device__ __forceinline__ void count_range(const uint64_t *__restrict__ sk, uin
             const uint64_t k0 = sk[i];
 #pragma unroll
             for (int s = 0; s < SPL; s++) {
-                const uint32_t r0 = remix_low16(k0 + x0 + (uint64_t)(s * 32));
+                const uint32_t r0 = split_r16<ARITH>(k0 + x0 + (uint64_t)(s * 32));
 #pragma unroll
                 for (int t = 0; t < NT; t++) c[s][t] += (r0 < T[t]);
             }
@@ -108,8 +116,8 @@ __device__ __forceinline__ void moments_range(const uint64_t *__restrict__ sk, u
 #pragma unroll
             for (int s = 0; s < SPL; s++) {
                 const uint64_t x = x0 + (uint64_t)(s * 32);
-                const uint32_t p0 = remix_low16(k0 + x) >> 14;
-                const uint32_t p1 = remix_low16(k1 + x) >> 14;
+                const uint32_t p0 = split_r16<ARITH>(k0 + x) >> 14;
+                const uint32_t p1 = split_r16<ARITH>(k1 + x) >> 14;
                 const uint32_t q0 = p0 * p0, q1 = p1 * p1;
                 c[s][0] += p0 + p1;
                 c[s][1] += q0 + q1;
@@ -120,7 +128,7 @@ __device__ __forceinline__ void moments_range(const uint64_t *__restrict__ sk, u
             const uint64_t k0 = sk[i];
 #pragma unroll
             for (int s = 0; s < SPL; s++) {
-                const uint32_t p0 = remix_low16(k0 + x0 + (uint64_t)(s * 32)) >> 14;
+                const uint32_t p0 = split_r16<ARITH>(k0 + x0 + (uint64_t)(s * 32)) >> 14;
                 c[s][0] += p0;
                 c[s][1] += p0 * p0;
                 c[s][2] += p0 * p0 * p0;
@@ -259,7 +267,7 @@ __device__ __forceinline__ void split_node(SplitSmem<SPL, THREADS> &sm, const No
     const uint32_t lo = min(m, threadIdx.x * chunk), hi = min(m, lo + chunk);
     uint64_t mine = 0;
     for (uint32_t i = lo; i < hi; i++) {
-        const uint32_t r = remix_low16(sm.keys[i] + x);
+        const uint32_t r = split_r16<ARITH>(sm.keys[i] + x);
         const uint32_t part = (r >= T[0]) + (r >= T[1]) + (r >= T[2]);
         mine += 1ull << (16 * part);
     }
@@ -279,7 +287,7 @@ __device__ __forceinline__ void split_node(SplitSmem<SPL, THREADS> &sm, const No
     const uint32_t unit = nd.unit;
     for (uint32_t i = lo; i < hi; i++) {
         const uint64_t k = sm.keys[i];
-        const uint32_t r = remix_low16(k + x);
+        const uint32_t r = split_r16<ARITH>(k + x);
         const uint32_t part = (r >= T[0]) + (r >= T[1]) + (r >= T[2]);
         const uint32_t dest = part * unit + (uint32_t)((run >> (16 * part)) & 0xFFFF);
         run += 1ull << (16 * part);

@@ -1,6 +1,7 @@
 // The reference's README example (README.md:41-47) compiled against the drop-in headers instead
 // of the reference's: prints "1 3 2 0". Then a ShockHash2<64> and a ShockHash2Flat<32> over 20000
-// keys, each checked to be a minimal perfect hash, and a ShockHash<16> over 128-bit hashes.
+// keys, each checked to be a minimal perfect hash, a ShockHash<16> over 128-bit hashes, and the
+// SIMD format (SIMDShockHash<30>, with and without rotation fitting).
 #include <algorithm>
 #include <iostream>
 #include <string>
@@ -8,6 +9,7 @@
 #include "shockhash_b200/ShockHash.h"
 #include "shockhash_b200/ShockHash2.h"
 #include "shockhash_b200/ShockHash2Flat.h"
+#include "shockhash_b200/SIMDShockHash.h"
 
 template <class F> static bool is_mphf(F &f, const std::vector<std::string> &keys) {
     std::vector<char> seen(keys.size(), 0);
@@ -52,5 +54,8 @@ int main() {
     std::cout << (ok ? "ShockHash hash128 ok" : "ShockHash hash128 FAIL") << std::endl;
     shockhash::ShockHash<30, true> hr(many, 2000);  // rotation fitting
     std::cout << (is_mphf(hr, many) ? "ShockHash rotation ok" : "ShockHash rotation FAIL") << std::endl;
+    shockhash::SIMDShockHash<30, false> hs(many, 2000);
+    shockhash::SIMDShockHash<30, true> hsr(many, 2000);
+    std::cout << (is_mphf(hs, many) && is_mphf(hsr, many) ? "SIMDShockHash ok" : "SIMDShockHash FAIL") << std::endl;
     return 0;
 }

@@ -7,7 +7,11 @@ inputs, runs the reference constructors and stores inputs and products as .npz f
 a SHA-256 manifest. The tests compare the CPU restatement (oracle/port) and the CUDA path against
 these files; they never need the reference sources at run time.
 
-Usage:  python tests/golden/make_golden.py
+The SIMDShockHash fixtures (simd_*, simdrot_*) come from the reference's SIMDShockHash.hpp compiled
+with -DSIMD (oracle/_ref/libshref_simd.so and its 8-lane twin in oracle/_ref/v4/; their products are
+the same for both lane counts, which tests/test_oracle.py checks).
+
+Usage:  python tests/golden/make_golden.py [core] [simd]     (no argument: both groups)
 """
 import hashlib
 import json
@@ -19,7 +23,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
-from oracle.bindings import RefLib  # noqa: E402
+from oracle.bindings import RefLib, RefSimdLib  # noqa: E402
 
 # (name, variant, leaf, n, bucket_size, seed)
 BUILDS = [
@@ -44,6 +48,23 @@ BUILDS = [
     ("rot_l33_b500", 3, 33, 5000, 500, 115),
     ("rot_l48_b2000", 3, 48, 6000, 2000, 116),
 ]
+# SIMDShockHash<leaf, rotation>: (name, rotation, leaf, n, bucket_size, seed)
+SIMD_BUILDS = [
+    ("simd_l30_b2000", 0, 30, 20000, 2000, 501),
+    ("simd_l8_b100", 0, 8, 5000, 100, 502),
+    ("simd_l40_b2000", 0, 40, 6000, 2000, 503),
+    ("simd_l16_b300", 0, 16, 9000, 300, 504),
+    ("simd_l2_b7", 0, 2, 1500, 7, 505),
+    ("simd_l33_b500", 0, 33, 4000, 500, 506),
+    ("simd_l48_b1000", 0, 48, 2000, 1000, 507),
+    ("simd_l30_tiny", 0, 30, 2, 2000, 508),
+    ("simdrot_l30_b2000", 1, 30, 20000, 2000, 511),
+    ("simdrot_l16_b100", 1, 16, 5000, 100, 512),
+    ("simdrot_l40_b2000", 1, 40, 8000, 2000, 513),
+    ("simdrot_l8_b50", 1, 8, 3000, 50, 514),
+    ("simdrot_l33_b500", 1, 33, 5000, 500, 515),
+    ("simdrot_l48_b2000", 1, 48, 6000, 2000, 516),
+]
 # (k, n, seed) for ShockHash2Flat<k>
 FLATS = [(16, 30000, 401), (32, 20000, 402), (64, 20003, 403), (100, 4100, 404), (8, 5000, 405)]
 LEAVES_SH2 = [(m, 40 if m <= 64 else 4) for m in list(range(2, 65)) + [80, 100, 128]]
@@ -57,9 +78,40 @@ def sha(path):
     return h.hexdigest()
 
 
-def main():
-    R = RefLib()
+def simd(manifest):
+    R = RefSimdLib()
+    for name, rot, leaf, n, b, seed in SIMD_BUILDS:
+        rng = np.random.default_rng(seed)
+        first = rng.integers(0, 2**64, size=n, dtype=np.uint64)
+        second = np.unique(rng.integers(0, 2**64, size=n + 8, dtype=np.uint64))[:n]
+        rng.shuffle(second)
+        r = R.build_hash(rot, leaf, first, second, b, 1)
+        q = r.query_hash(first, second)
+        path = os.path.join(HERE, name + ".npz")
+        np.savez_compressed(path, variant=6 if rot else 5, leaf=leaf, bucket_size=b, first=first, second=second,
+                            desc=r.desc, size_acc=r.size_acc, pos_acc=r.pos_acc, ribbon_keys=r.ribbon_keys,
+                            ribbon_bits=r.ribbon_bits, query=q, bits=r.bits, lanes=R.lanes)
+        manifest[name + ".npz"] = sha(path)
+        r.free()
+
+
+def main(groups):
+    mpath = os.path.join(HERE, "MANIFEST.json")
     manifest = {}
+    if os.path.exists(mpath):
+        with open(mpath) as fh:
+            manifest = json.load(fh)
+    if "simd" in groups:
+        simd(manifest)
+    if "core" in groups:
+        core(manifest)
+    with open(mpath, "w") as fh:
+        json.dump(manifest, fh, indent=1, sort_keys=True)
+    print(json.dumps(manifest, indent=1))
+
+
+def core(manifest):
+    R = RefLib()
     for name, variant, leaf, n, b, seed in BUILDS:
         rng = np.random.default_rng(seed)
         first = rng.integers(0, 2**64, size=n, dtype=np.uint64)
@@ -131,10 +183,7 @@ def main():
                         lengths=np.array([len(x) for x in strs], np.uint64), first=f, second=s,
                         murmur=R.murmur64(strs), readme_out=readme_out)
     manifest["strings.npz"] = sha(path)
-    with open(os.path.join(HERE, "MANIFEST.json"), "w") as fh:
-        json.dump(manifest, fh, indent=1, sort_keys=True)
-    print(json.dumps(manifest, indent=1))
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:] or ["core", "simd"])

@@ -1,4 +1,4 @@
-"""The C++ drop-in headers (include/shockhash_b200/ShockHash.h, ShockHash2.h, ShockHash2Flat.h)
+"""The C++ drop-in headers (include/shockhash_b200/ShockHash.h, ShockHash2.h, ShockHash2Flat.h, SIMDShockHash.h)
 compiled into the reference's README example (README.md:41-47) and linked against libshg.so."""
 import os
 import shutil
@@ -37,3 +37,4 @@ def test_dropin_readme_example(tmp_path):
     assert out[2] == "ShockHash2Flat ok"
     assert out[3] == "ShockHash hash128 ok"
     assert out[4] == "ShockHash rotation ok"
+    assert out[5] == "SIMDShockHash ok"

@@ -249,3 +249,93 @@ def test_elegant_pairing_of_raw_seeds_is_float_accurate():
     other = rng.integers(0, 1 << 24, size=(len(edges), 2000), dtype=np.uint64)
     ee = np.repeat(edges, 2000)
     assert accurate(ee, other.ravel()).all() and accurate(other.ravel(), ee).all()
+
+
+# ---------------------------------------------------------------- SIMDShockHash (SIMDShockHash.hpp)
+SIMD_FIXTURES = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "simd*.npz")))
+
+
+def simd_ref(lanes=None):
+    from oracle import bindings
+    path = bindings.SIMD_SO[lanes or 4]
+    if not os.path.exists(path):
+        pytest.skip("compiled SIMDShockHash oracle not available")
+    if lanes == 8 and not bindings.host_has_avx512():
+        pytest.skip("the 8-lane build needs an AVX-512 host")
+    return bindings.RefSimdLib(lanes)
+
+
+def fmix32(z):  # MurmurHash3's 32-bit finalizer, SIMDShockHash.hpp:76-83, on uint32 arrays
+    z = z.astype(np.uint32)
+    z ^= z >> np.uint32(16)
+    z = (z * np.uint32(0x85EBCA6B)).astype(np.uint32)
+    z ^= z >> np.uint32(13)
+    z = (z * np.uint32(0xC2B2AE35)).astype(np.uint32)
+    z ^= z >> np.uint32(16)
+    return z
+
+
+def test_simd_split_hash_restated(ref):
+    # remixAndRemap (SIMDShockHash.hpp:762-766): remap16 of fmix32(hi ^ lo), as the device computes it
+    R = simd_ref()
+    rng = np.random.default_rng(5)
+    x = rand_u64(rng, 20000)
+    with np.errstate(over="ignore"):
+        folded = fmix32((x >> np.uint64(32)).astype(np.uint32) ^ (x & np.uint64(0xFFFFFFFF)).astype(np.uint32))
+    for m in (2, 7, 100, 961, 2999):
+        want = ((folded.astype(np.uint64) & np.uint64(0xFFFF)) * np.uint64(m)) >> np.uint64(16)
+        assert np.array_equal(R.remix_and_remap(x, m).astype(np.uint64), want), m
+
+
+@pytest.mark.parametrize("rot,leaf,n,b", [(0, 8, 20000, 100), (0, 30, 20000, 2000), (1, 30, 12000, 2000),
+                                          (1, 40, 6000, 2000), (0, 2, 3000, 7), (1, 8, 3000, 50), (0, 33, 4000, 500)])
+def test_simd_ref_same_for_4_and_8_lanes(ref, rot, leaf, n, b):
+    # The format does not depend on the vector width: every seed search scans seeds in increasing
+    # order and keeps the first valid one, and the split hash folds each 64-bit lane on its own.
+    a, w = simd_ref(4), simd_ref(8)
+    assert (a.lanes, w.lanes) == (4, 8)
+    rng = np.random.default_rng(n + leaf + rot)
+    f, s = rand_u64(rng, n), unique_u64(rng, n)
+    ra, rw = a.build_hash(rot, leaf, f, s, b), w.build_hash(rot, leaf, f, s, b)
+    for k in ("desc", "size_acc", "pos_acc", "ribbon_keys", "ribbon_bits"):
+        assert np.array_equal(getattr(ra, k), getattr(rw, k)), k
+    assert np.array_equal(ra.query_hash(f, s), rw.query_hash(f, s))
+
+
+@pytest.mark.parametrize("name", SIMD_FIXTURES)
+def test_simd_ref_matches_golden(ref, name):
+    g = load(name)
+    R = simd_ref()
+    r = R.build_hash(int(g["variant"]) == 6, int(g["leaf"]), g["first"], g["second"], int(g["bucket_size"]), 2)
+    for k in ("desc", "size_acc", "pos_acc", "ribbon_keys", "ribbon_bits"):
+        assert np.array_equal(getattr(r, k), g[k]), k
+    assert np.array_equal(r.query_hash(g["first"], g["second"]), g["query"])
+    assert r.bits == int(g["bits"])
+
+
+@pytest.mark.parametrize("name", [n for n in SIMD_FIXTURES if n.startswith("simd_")])
+def test_port_simd_matches_golden(port, name):
+    # the restatement's variant 5 is SIMDShockHash<l, false>
+    g = load(name)
+    r = port.build_hash(5, int(g["leaf"]), g["first"], g["second"], int(g["bucket_size"]))
+    for k in ("desc", "size_acc", "pos_acc", "ribbon_keys", "ribbon_bits"):
+        assert np.array_equal(getattr(r, k), g[k]), k
+    assert np.array_equal(r.query_hash(g["first"], g["second"]), g["query"])
+
+
+@pytest.mark.parametrize("leaf,n,b", [(12, 6000, 150), (24, 9000, 700), (32, 6000, 900), (4, 2000, 11)])
+def test_port_simd_matches_ref_random(port, ref, leaf, n, b):
+    R = simd_ref()
+    rng = np.random.default_rng(7 * n + leaf)
+    f, s = rand_u64(rng, n), unique_u64(rng, n)
+    r, p = R.build_hash(0, leaf, f, s, b, 2), port.build_hash(5, leaf, f, s, b)
+    for k in ("desc", "size_acc", "pos_acc", "ribbon_keys", "ribbon_bits"):
+        assert np.array_equal(getattr(r, k), getattr(p, k)), k
+
+
+def test_simd_format_differs_from_shockhash(ref):
+    # same keys, same leaf size: SIMDShockHash<l> stores other seeds than ShockHash<l>
+    g = load("simd_l30_b2000")
+    r = ref.build_hash(1, 30, g["first"], g["second"], 2000, 1)
+    assert not np.array_equal(r.desc, g["desc"])
+    assert np.array_equal(r.size_acc, g["size_acc"])  # the same buckets

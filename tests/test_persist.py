@@ -57,6 +57,23 @@ def test_round_trip_rotation_fitting_golden(tmp_path):
     assert back.mphf().bits() == int(g["bits"])
 
 
+@pytest.mark.parametrize("name", ["simd_l30_b2000", "simd_l2_b7", "simd_l48_b1000", "simdrot_l30_b2000",
+                                  "simdrot_l40_b2000", "simdrot_l8_b50"])
+def test_round_trip_simd_golden(tmp_path, name):
+    # SIMDShockHash<l, rot>: the host query's own split hash and start seeds answer as the reference
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", name + ".npz"))
+    arrays = SimpleNamespace(size_acc=g["size_acc"], pos_acc=g["pos_acc"], desc=g["desc"],
+                             ribbon_keys=g["ribbon_keys"], ribbon_bits=g["ribbon_bits"])
+    variant, leaf = int(g["variant"]), int(g["leaf"])
+    res = shg.merge_shards(variant, leaf, [shard._arrays(arrays)], int(g["bucket_size"]))
+    path = str(tmp_path / "simd.shg")
+    res.save(path)
+    back = shg.load_result(path)
+    assert (back.params.variant, back.params.leaf_size) == (variant, leaf)
+    assert np.array_equal(back.mphf().query_hash(g["first"], g["second"]), g["query"])
+    assert back.mphf().bits() == int(g["bits"])
+
+
 def test_damaged_files_are_rejected(tmp_path, port):
     res, _, _, _ = _library_result(port, 2, 64, 5000, 2000, 5)
     path = str(tmp_path / "a.shg")
