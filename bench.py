@@ -19,8 +19,9 @@ Besides the headline line the GPU arm reports, on rank 0 at N=1:
   * cpu_baseline + parity: the reference CPU build of the same keys, its products compared word
     for word with the device build (descriptors, accumulators, retrieval input);
   * forms: the level schedule against the pipelined one and the per-leaf-launch form (1M keys),
-    the north-star size (100M keys), a Poisson serving stream, the device query of every key and
-    the device retrieval structure.
+    the SIMD format (SIMDShockHash<30>, 1M keys) against the reference's SIMD CPU build, the
+    north-star size (100M keys), a Poisson serving stream, the device query of every key and the
+    device retrieval structure.
 """
 import argparse
 import json
@@ -61,15 +62,24 @@ def _workload(args):
         CONFIG_NAME = (f"ShockHash2Flat<{LEAF}>, {args.n / 1e6:g}M uint64 keys (mt19937_64 seed {SEED}) as 8-byte "
                        "strings")
         return
-    name = "ShockHash2" if VARIANT == 2 else "ShockHash"
-    CONFIG_NAME = (f"{name}<{LEAF}> b={BUCKET}, {args.n / 1e6:g}M uint64 keys (mt19937_64 seed {SEED}) "
+    CONFIG_NAME = (f"{class_name(VARIANT, LEAF)} b={BUCKET}, {args.n / 1e6:g}M uint64 keys (mt19937_64 seed {SEED}) "
                    "hashed to 128-bit")
+
+
+def class_name(variant, leaf):
+    """The reference class a variant builds (shg_variant numbering)."""
+    return {1: f"ShockHash<{leaf}>", 2: f"ShockHash2<{leaf}>", 3: f"ShockHash<{leaf}, true>",
+            5: f"SIMDShockHash<{leaf}>", 6: f"SIMDShockHash<{leaf}, true>"}[variant]
+
+
+def is_simd(variant):
+    return variant in (5, 6)
 
 
 def config_dict(args):
     """The workload, identical in both arms' JSON lines."""
     return {"workload": CONFIG_NAME, "keys_per_gpu": args.n, "leaf_size": LEAF, "bucket_size": BUCKET,
-            "variant": "ShockHash2" if VARIANT == 2 else "ShockHash", "mode": MODES[args.mode],
+            "variant": class_name(VARIANT, LEAF).split("<")[0], "mode": MODES[args.mode],
             "key_encoding": "each uint64 key hashed as its 8-byte little-endian string (SpookyV2-128, seed 0)",
             "l2": "inputs (10M keys: 80 MB keys, 160 MB fingerprints, 240 MB partition buffers) exceed the 126 MB L2, "
                   "and a 256 MB buffer is written before every timed step, outside the timing",
@@ -141,14 +151,19 @@ def u64_as_strings(keys):
     return data, offs
 
 
-def cpu_reference(keys, threads, keep=False):
+def cpu_reference(keys, threads, keep=False, variant=None, leaf=None, bucket=None):
     """The reference CPU construction of `keys` (uint64, given to the reference's string constructor
     as 8-byte strings): (constructor seconds, kind, threads used, products or None). Uses
-    oracle/_ref; the C++ restatement oracle/_port (one thread) when that build is absent."""
+    oracle/_ref (SIMDShockHash: its SIMD build); the C++ restatement oracle/_port (one thread) when
+    that build is absent."""
     from oracle import bindings
+    variant, leaf, bucket = variant or VARIANT, leaf or LEAF, bucket or BUCKET
     if bindings.ref_available():
         data, offs = u64_as_strings(keys)
-        b, secs = bindings.RefLib().build_strings_packed_timed(VARIANT, LEAF, data, offs, BUCKET, threads)
+        if is_simd(variant):
+            b, secs = bindings.RefSimdLib().build_strings_packed_timed(variant == 6, leaf, data, offs, bucket, threads)
+        else:
+            b, secs = bindings.RefLib().build_strings_packed_timed(variant, leaf, data, offs, bucket, threads)
         if not keep:
             b.free()
             b = None
@@ -157,7 +172,7 @@ def cpu_reference(keys, threads, keep=False):
     data, offs = u64_as_strings(keys)
     first, second = lib.spooky128(bindings.split_strings(data, offs))
     t = time.perf_counter()
-    b = lib.build_hash(VARIANT, LEAF, first, second, BUCKET)
+    b = lib.build_hash(variant, leaf, first, second, bucket)
     dt = time.perf_counter() - t
     if not keep:
         b.free()
@@ -170,7 +185,7 @@ def ref_phase_split(n):
     (oracle/ref_stats.py in a subprocess, since the STATS build prints to stdout), or None."""
     from oracle import bindings
     helper = os.path.join(ROOT, "oracle", "ref_stats.py")
-    if not os.path.exists(bindings.STATS_SO):
+    if not os.path.exists(bindings.STATS_SO) or VARIANT not in (1, 2):
         return None
     try:
         out = subprocess.run([sys.executable, helper, "--n", str(n), "--variant", str(VARIANT), "--leaf", str(LEAF),
@@ -336,6 +351,34 @@ def timed_device_builds(eng, d_ptr, n, mode, flush, reps, warm=1):
     return statistics.mean(x.stage_ms["total"] for x in res), stages, res[-1]
 
 
+def simd_format_form(eng, d_ptr, keys, n, flush):
+    """SIMDShockHash<30> (the class the reference's SIMD benchmark builds as its ShockHash<30>; the leaf
+    and bucket size of configuration 1) on the first n keys of the stream: the device build, the
+    reference's SIMD CPU build of the same keys on all host threads, and a word-for-word comparison."""
+    import torch
+    import shockhash_b200 as shg
+    leaf, ms = 30, []
+    r = None
+    for it in range(4):  # one warm-up, then three timed builds
+        flush.zero_()
+        torch.cuda.synchronize()
+        if r is not None:
+            r.free()
+        r = eng.build_u64_device(shg.SIMDSHOCKHASH, leaf, d_ptr, n, BUCKET, shg.MODE_DEFAULT)
+        if it:
+            ms.append(r.stage_ms["total"])
+    dev = statistics.mean(ms) * 1e6 / n
+    dt, kind, cores, b = cpu_reference(keys[:n], os.cpu_count() or 1, keep=True, variant=shg.SIMDSHOCKHASH,
+                                       leaf=leaf)
+    out = {"class": f"SIMDShockHash<{leaf}> b={BUCKET}", "keys": n, "device_ns_per_key": round(dev, 3),
+           "stage_ms": {k: round(v, 3) for k, v in r.stage_ms.items()},
+           "cpu_reference_ns_per_key": round(dt * 1e9 / n, 3), "cpu_kind": kind, "cpu_cores": cores,
+           "vs_cpu_reference": round(dt * 1e9 / n / dev, 1), "parity": compare_products(r, b)}
+    b.free()
+    r.free()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -344,8 +387,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_KEYS)
     ap.add_argument("--mode", type=int, default=0)
-    ap.add_argument("--variant", type=int, default=VARIANT, choices=[1, 2, 4],
-                    help="1 ShockHash, 2 ShockHash2, 4 ShockHash2Flat (leaf = k; a profiling and C4 line)")
+    ap.add_argument("--variant", type=int, default=VARIANT, choices=[1, 2, 3, 4, 5, 6],
+                    help="1 ShockHash, 2 ShockHash2, 3 ShockHash with rotation fitting, 4 ShockHash2Flat (leaf = k; "
+                         "a profiling and C4 line), 5 SIMDShockHash, 6 SIMDShockHash with rotation fitting")
     ap.add_argument("--leaf", type=int, default=LEAF)
     ap.add_argument("--seed", type=int, default=SEED)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and parity leg")
@@ -381,8 +425,8 @@ def main():
     h_keys = torch.from_numpy(keys.view(np.int64)).pin_memory()
     eng = shg.Engine(local)
     peak_forms = {}
-    peaks = shg.split_peaks(local, detail=peak_forms)
-    leaf_peak, _ = shg.int_peak(local, 1 << 15, 1 if VARIANT == 1 else 2)
+    peaks = shg.split_peaks(local, detail=peak_forms, simd=is_simd(VARIANT))
+    leaf_peak, _ = shg.int_peak(local, 1 << 15, 2 if VARIANT == 2 else 1)
     lpeaks = shg.leaf_peaks(local) if VARIANT == 2 else None
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
 
@@ -520,6 +564,9 @@ def main():
                                                               and np.array_equal(rp.ribbon_bits, rl.ribbon_bits))}
             rp.free()
             rl.free()
+            if VARIANT == 2:  # the SIMD format beside the headline configuration
+                forms["simd_format"] = simd_format_form(eng, d_keys.data_ptr(), keys,
+                                                        min(n, int(os.environ.get("SHG_SIMD_SAMPLE", "1000000"))), flush)
         if ws == 1 and not args.no_forms:
             # operator() for every key of the build on the device (keys resident, SpookyV2 fused)
             dq = shg.DeviceMphf(r, local)

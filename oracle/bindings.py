@@ -153,6 +153,18 @@ class RefSimdLib(_Lib):
         b._strings = (data, offs)
         return b
 
+    def build_strings_packed_timed(self, rotation, leaf, data, offs, bucket_size=2000, threads=1):
+        """The constructor from packed string keys; returns (products, seconds of the call alone)."""
+        L = self.lib
+        L.refsimd_build_strings_timed.restype = _vp
+        L.refsimd_build_strings_timed.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_char_p, _vp, _sz, _sz, _sz,
+                                                  ctypes.POINTER(ctypes.c_double)]
+        secs = ctypes.c_double(0)
+        offs = np.ascontiguousarray(offs, dtype=np.uint64)
+        h = L.refsimd_build_strings_timed(int(rotation), leaf, data, _ptr(offs), len(offs) - 1, bucket_size, threads,
+                                          ctypes.byref(secs))
+        return self._built(h, leaf), float(secs.value)
+
     def query_strings(self, built, keys):
         data, offs = pack_strings(keys)
         out = np.zeros(len(keys), dtype=np.uint64)

@@ -179,6 +179,19 @@ void *refsimd_build_strings(int rotation, int leaf, const char *bytes, const uin
     return make_str(rotation, leaf, keys, bucket_size, threads);
 }
 
+// refsimd_build_strings with the wall time of the constructor call alone in *seconds (the key
+// strings are made before the clock starts, as benchmark/benchmark_construction.cpp:53-56 times).
+void *refsimd_build_strings_timed(int rotation, int leaf, const char *bytes, const uint64_t *offsets, size_t n,
+                                  size_t bucket_size, size_t threads, double *seconds) {
+    std::vector<std::string> keys;
+    keys.reserve(n);
+    for (size_t i = 0; i < n; i++) keys.emplace_back(bytes + offsets[i], offsets[i + 1] - offsets[i]);
+    const auto t0 = std::chrono::steady_clock::now();
+    RefBase *r = make_str(rotation, leaf, keys, bucket_size, threads);
+    *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return r;
+}
+
 void refsimd_free(void *h) { delete (RefBase *)h; }
 uint64_t refsimd_nbuckets(void *h) { return ((RefBase *)h)->nbuckets(); }
 uint64_t refsimd_desc_words(void *h) { return ((RefBase *)h)->desc_words(); }

@@ -1,16 +1,18 @@
 // Test infrastructure only (the oracle): restated stand-in for Agner Fog's vectorclass library
 // (VCL, Apache-2.0). The reference's submodule extlib/vectorclass is empty here and its revision is
-// unknown, so this header restates, as plain lane-wise C++ loops, only the classes and functions
-// that the reference's SIMDShockHash.hpp, shockhash/SimdUtils.h and TinyBinaryCuckooHashTable.h
-// (under -DSIMD) use, each with the meaning VCL documents:
+// unknown, so this header restates only the classes and functions that the reference's
+// SIMDShockHash.hpp, shockhash/SimdUtils.h and TinyBinaryCuckooHashTable.h (under -DSIMD) use, each
+// with the meaning VCL documents, on GCC vector extensions (so that, as with VCL, every operation
+// compiles to one or a few AVX2 / AVX-512 instructions):
 //   * VecNuq / VecNui / VecNq / VecNc: N lanes of uint64 / uint32 / int64 / int8 with wrap-around
 //     arithmetic (+, -, * keep the low bits), bitwise ops, shifts by a scalar count, comparisons
 //     that give a boolean vector, load/store of N lanes, extract;
 //   * construction from one scalar (broadcast), from N scalars, and between vectors of the same
 //     total width (a reinterpretation of the bytes, as VCL's conversion through the register type);
 //   * if_add(f, a, b) = a + (f ? b : 0); blend8/blend16<i...>(a, b) picks lane i of the
-//     concatenation a:b (i < 0 gives 0); lookup<n>(idx, table) = table[idx] (idx < n);
-//     a / const_uint(d) is exact unsigned division by the constant d;
+//     concatenation a:b; lookup<n>(idx, table) = table[idx] for n <= N, reading one vector of N
+//     entries from the table as VCL does (the reference pads its table for that,
+//     SIMDShockHash.hpp:97-104); a / const_uint(d) is exact unsigned division by the constant d;
 //   * horizontal_or, horizontal_find_first (-1 when no lane is set), horizontal_count and to_bits
 //     (lane i to bit i) on boolean vectors.
 // The two variable-shift intrinsics SimdUtils.h calls on its vectors (_mm{256,512}_{sllv,srlv}_epi64)
@@ -36,39 +38,35 @@
 
 namespace vcl_shim {
 
-template <int N> struct VBool {
-    bool b[N];
-    VBool() : b{} {}
-    friend VBool operator&(const VBool &x, const VBool &y) {
-        VBool r;
-        for (int i = 0; i < N; i++) r.b[i] = x.b[i] && y.b[i];
-        return r;
-    }
-    friend VBool operator|(const VBool &x, const VBool &y) {
-        VBool r;
-        for (int i = 0; i < N; i++) r.b[i] = x.b[i] || y.b[i];
-        return r;
-    }
+// Boolean vector of N lanes of S (a signed integer type): lane = -1 (true) or 0 (false), the
+// result of a GCC vector comparison.
+template <typename S, int N> struct VBool {
+    typedef S M __attribute__((vector_size(sizeof(S) * N)));
+    M m;
+    VBool() : m{} {}
+    explicit VBool(M x) : m(x) {}
+    friend VBool operator&(const VBool &x, const VBool &y) { return VBool(x.m & y.m); }
+    friend VBool operator|(const VBool &x, const VBool &y) { return VBool(x.m | y.m); }
     friend bool horizontal_or(const VBool &x) {
-        for (int i = 0; i < N; i++)
-            if (x.b[i]) return true;
-        return false;
+        S acc = 0;
+        for (int i = 0; i < N; i++) acc |= x.m[i];
+        return acc != 0;
     }
     friend int horizontal_find_first(const VBool &x) {
         for (int i = 0; i < N; i++)
-            if (x.b[i]) return i;
+            if (x.m[i]) return i;
         return -1;
     }
     friend uint32_t horizontal_count(const VBool &x) {
         uint32_t c = 0;
-        for (int i = 0; i < N; i++) c += x.b[i];
+        for (int i = 0; i < N; i++) c += x.m[i] != 0;
         return c;
     }
     friend auto to_bits(const VBool &x) {
         using Bits = std::conditional_t<(N <= 8), uint8_t, std::conditional_t<(N <= 16), uint16_t,
                      std::conditional_t<(N <= 32), uint32_t, uint64_t>>>;
         Bits r = 0;
-        for (int i = 0; i < N; i++) r |= (Bits)((Bits)x.b[i] << i);
+        for (int i = 0; i < N; i++) r |= (Bits)((Bits)(x.m[i] != 0) << i);
         return r;
     }
 };
@@ -76,9 +74,10 @@ template <int N> struct VBool {
 template <uint32_t d> struct Const_uint_t {};
 
 template <typename T, int N> struct Vec {
-    using elem = T;
-    static constexpr int lanes = N;
-    T v[N];
+    typedef T V __attribute__((vector_size(sizeof(T) * N)));
+    using S = std::make_signed_t<T>;
+    using Bool = VBool<S, N>;
+    V v;
 
     Vec() : v{} {}
     Vec(T s) {  // broadcast
@@ -88,23 +87,24 @@ template <typename T, int N> struct Vec {
     Vec(A... a) : v{(T)a...} {}
     template <typename U, int M, typename = std::enable_if_t<(sizeof(U) * M == sizeof(T) * N && !std::is_same_v<U, T>)>>
     explicit Vec(const Vec<U, M> &o) {  // same total width: reinterpret the bytes
-        std::memcpy(v, o.v, sizeof(v));
+        std::memcpy(&v, &o.v, sizeof(v));
+    }
+    static Vec raw(V x) {
+        Vec r;
+        r.v = x;
+        return r;
     }
 
     Vec &load(const void *p) {
-        std::memcpy(v, p, sizeof(v));
+        std::memcpy(&v, p, sizeof(v));
         return *this;
     }
-    void store(void *p) const { std::memcpy(p, v, sizeof(v)); }
+    void store(void *p) const { std::memcpy(p, &v, sizeof(v)); }
     T extract(int i) const { return v[i & (N - 1)]; }
     T operator[](int i) const { return v[i & (N - 1)]; }
 
-#define SHG_VCL_BINOP(OP)                                    \
-    friend Vec operator OP(const Vec &a, const Vec &b) {     \
-        Vec r;                                               \
-        for (int i = 0; i < N; i++) r.v[i] = (T)(a.v[i] OP b.v[i]); \
-        return r;                                            \
-    }                                                        \
+#define SHG_VCL_BINOP(OP)                                                                   \
+    friend Vec operator OP(const Vec &a, const Vec &b) { return raw(a.v OP b.v); }          \
     Vec &operator OP##=(const Vec &b) { return *this = *this OP b; }
     SHG_VCL_BINOP(+)
     SHG_VCL_BINOP(-)
@@ -113,24 +113,12 @@ template <typename T, int N> struct Vec {
     SHG_VCL_BINOP(|)
     SHG_VCL_BINOP(^)
 #undef SHG_VCL_BINOP
-    friend Vec operator>>(const Vec &a, int s) {
-        Vec r;
-        for (int i = 0; i < N; i++) r.v[i] = (T)(a.v[i] >> s);
-        return r;
-    }
-    friend Vec operator<<(const Vec &a, int s) {
-        Vec r;
-        for (int i = 0; i < N; i++) r.v[i] = (T)(a.v[i] << s);
-        return r;
-    }
+    friend Vec operator>>(const Vec &a, int s) { return raw(a.v >> s); }
+    friend Vec operator<<(const Vec &a, int s) { return raw(a.v << s); }
     Vec &operator>>=(int s) { return *this = *this >> s; }
     Vec &operator<<=(int s) { return *this = *this << s; }
-#define SHG_VCL_CMP(OP)                                      \
-    friend VBool<N> operator OP(const Vec &a, const Vec &b) { \
-        VBool<N> r;                                          \
-        for (int i = 0; i < N; i++) r.b[i] = a.v[i] OP b.v[i]; \
-        return r;                                            \
-    }
+#define SHG_VCL_CMP(OP)                                                                      \
+    friend Bool operator OP(const Vec &a, const Vec &b) { return Bool((typename Bool::M)(a.v OP b.v)); }
     SHG_VCL_CMP(==)
     SHG_VCL_CMP(!=)
     SHG_VCL_CMP(<)
@@ -140,44 +128,44 @@ template <typename T, int N> struct Vec {
 #undef SHG_VCL_CMP
     template <uint32_t d> friend Vec operator/(const Vec &a, Const_uint_t<d>) {
         static_assert(d != 0, "division by zero");
-        Vec r;
-        for (int i = 0; i < N; i++) r.v[i] = (T)(a.v[i] / d);
-        return r;
+        return raw(a.v / (T)d);
     }
-    friend Vec if_add(const VBool<N> &f, const Vec &a, const Vec &b) {
-        Vec r;
-        for (int i = 0; i < N; i++) r.v[i] = f.b[i] ? (T)(a.v[i] + b.v[i]) : a.v[i];
-        return r;
-    }
+    friend Vec if_add(const Bool &f, const Vec &a, const Vec &b) { return raw(a.v + (b.v & (V)f.m)); }
 };
 
-// lane k of the result = lane I_k of the concatenation a:b (I_k < 0 gives 0)
+// lane k of the result = lane I_k of the concatenation a:b
 template <int... I, typename T, int N>
 Vec<T, N> blend_lanes(const Vec<T, N> &a, const Vec<T, N> &b) {
     static_assert(sizeof...(I) == N, "one index per lane");
-    const int idx[N] = {I...};
-    Vec<T, N> r;
-    for (int k = 0; k < N; k++) r.v[k] = idx[k] < 0 ? (T)0 : idx[k] < N ? a.v[idx[k]] : b.v[idx[k] - N];
-    return r;
+    static_assert(((I >= 0 && I < 2 * N) && ...), "lane indexes of a:b");
+    return Vec<T, N>::raw(__builtin_shufflevector(a.v, b.v, I...));
 }
 
-// table[index] per lane, for indexes below n
+// table[index] per lane: one vector of N table entries permuted by the index (n <= N), as VCL's
+// lookup reads it; larger n gathers lane by lane
 template <int n, typename T, int N> Vec<T, N> lookup(const Vec<T, N> &index, const T *table) {
-    Vec<T, N> r;
-    for (int i = 0; i < N; i++) r.v[i] = table[index.v[i] < (T)n ? index.v[i] : (T)(n - 1)];
-    return r;
+    using V = typename Vec<T, N>::V;
+    if constexpr (n <= N) {
+        V t;
+        std::memcpy(&t, table, sizeof(t));
+        return Vec<T, N>::raw(__builtin_shuffle(t, index.v & (V)((T)(N - 1) + V{})));
+    } else {
+        Vec<T, N> r;
+        for (int i = 0; i < N; i++) r.v[i] = table[index.v[i] < (T)n ? index.v[i] : (T)(n - 1)];
+        return r;
+    }
 }
 
 // variable shifts of 64-bit lanes: a count of 64 or more gives 0 (VPSLLVQ / VPSRLVQ)
 template <int N> Vec<uint64_t, N> sllv64(const Vec<uint64_t, N> &x, const Vec<uint64_t, N> &c) {
-    Vec<uint64_t, N> r;
-    for (int i = 0; i < N; i++) r.v[i] = c.v[i] < 64 ? x.v[i] << c.v[i] : 0;
-    return r;
+    using V = typename Vec<uint64_t, N>::V;
+    const V lim = (uint64_t)64 + V{};
+    return Vec<uint64_t, N>::raw((x.v << (c.v & (lim - 1))) & (V)(c.v < lim));
 }
 template <int N> Vec<uint64_t, N> srlv64(const Vec<uint64_t, N> &x, const Vec<uint64_t, N> &c) {
-    Vec<uint64_t, N> r;
-    for (int i = 0; i < N; i++) r.v[i] = c.v[i] < 64 ? x.v[i] >> c.v[i] : 0;
-    return r;
+    using V = typename Vec<uint64_t, N>::V;
+    const V lim = (uint64_t)64 + V{};
+    return Vec<uint64_t, N>::raw((x.v >> (c.v & (lim - 1))) & (V)(c.v < lim));
 }
 
 } // namespace vcl_shim
@@ -194,8 +182,8 @@ using Vec8ui = vcl_shim::Vec<uint32_t, 8>;
 using Vec16ui = vcl_shim::Vec<uint32_t, 16>;
 using Vec32c = vcl_shim::Vec<int8_t, 32>;
 using Vec64c = vcl_shim::Vec<int8_t, 64>;
-using Vec8ib = vcl_shim::VBool<8>;
-using Vec16ib = vcl_shim::VBool<16>;
+using Vec8ib = Vec8ui::Bool;
+using Vec16ib = Vec16ui::Bool;
 
 template <int... I> inline Vec8ui blend8(const Vec8ui &a, const Vec8ui &b) { return vcl_shim::blend_lanes<I...>(a, b); }
 template <int... I> inline Vec16ui blend16(const Vec16ui &a, const Vec16ui &b) { return vcl_shim::blend_lanes<I...>(a, b); }

@@ -250,10 +250,16 @@ TUNING_PARAMS = ("split_seeds_per_lane", "split_threads", "split_round_div", "sp
 TUNING_FLAT = 4
 
 
-def split_peaks(device=0, iters=1 << 15, detail=None):
+def split_peaks(device=0, iters=1 << 15, detail=None, simd=False):
     """Measured evaluations/s of each split inner loop, keyed as SPLIT_KINDS: the faster of the two
     arithmetic forms the split kernel can run (split_arith 0 and 1), so the ceiling holds for both.
-    `detail`, a dict, receives both forms' rates per kind."""
+    `detail`, a dict, receives both forms' rates per kind. `simd`: the loops under SIMDShockHash's
+    split hash, which has one form."""
+    if simd:
+        out = {name: int_peak(device, iters, k)[0] for name, k in zip(SPLIT_KINDS, (17, 18, 19, 16))}
+        if detail is not None:
+            detail.update({name: {"simd": v} for name, v in out.items()})
+        return out
     plain, pipes = (3, 4, 5, 0), (10, 11, 12, 9)
     out = {}
     for name, a, b in zip(SPLIT_KINDS, plain, pipes):
