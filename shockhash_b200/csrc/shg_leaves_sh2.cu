@@ -366,7 +366,11 @@ __device__ __forceinline__ void sh2_leaf(const Src &src, uint32_t li, const uint
         const uint64_t s = S_proc + lane;
         const bool live = s < S;
         uint32_t mine = 0, mineA = 0, mineB = 0;
-        uint32_t ha0 = 0, ha1 = 0, hb0 = 0, hb1 = 0;  // first two partners on each side
+        // each lane's partners in scan order, in the union-find area (idle until this round's pair
+        // tests; [entry][lane], one column per lane): A side in entries 0..kPartners-1, B side after
+        constexpr uint32_t kPartners = MAXM / 4;
+        static_assert(2 * kPartners * 32 * sizeof(uint16_t) <= sizeof(sm.uf), "partner lists fit the union-find area");
+        uint16_t *const plist = reinterpret_cast<uint16_t *>(sm.uf);
         if (live) w_scan += cx.quad ? s + 1 : 1;  // mask pairs this raw seed is tested against
         if (live) {
             if (cx.quad) {
@@ -376,13 +380,11 @@ __device__ __forceinline__ void sh2_leaf(const Src &src, uint32_t li, const uint
                 const auto tA = ts.a, tB = ts.b;
                 auto visit = [&](uint64_t p, MaskPair<typename LeafCtx<MAXM>::Mask> w) {
                     if (p < s && (w.a | tB) == cx.full && float_accurate_elegant_seeds(p, s)) {
-                        ha0 = mineA == 0 ? (uint32_t)p : ha0;
-                        ha1 = mineA == 1 ? (uint32_t)p : ha1;
+                        if (mineA < kPartners) plist[mineA * 32 + lane] = (uint16_t)p;
                         mineA++;
                     }
                     if ((w.b | tA) == cx.full && float_accurate_elegant_seeds(s, p)) {
-                        hb0 = mineB == 0 ? (uint32_t)p : hb0;
-                        hb1 = mineB == 1 ? (uint32_t)p : hb1;
+                        if (mineB < kPartners) plist[(kPartners + mineB) * 32 + lane] = (uint16_t)p;
                         mineB++;
                     }
                 };
@@ -399,16 +401,28 @@ __device__ __forceinline__ void sh2_leaf(const Src &src, uint32_t li, const uint
                     const uint32_t full = cx.full;
                     uint64_t hq = 0;
                     uint32_t nh = 0, resume = 0;
-                    for (; p + 2 <= in_sm; p += 2) {
-                        const uint4 w = m2[p >> 1];
-                        const uint32_t z = min(min((w.x | tB) ^ full, (w.y | tA) ^ full),
-                                               min((w.z | tB) ^ full, (w.w | tA) ^ full));
-                        if (z == 0) {
-                            if (nh < 8) hq |= (uint64_t)(p >> 1) << (8 * nh);
-                            else if (nh == 8) resume = p;
-                            nh++;
+                    auto miss = [&](const uint4 &w) {  // 0 when a side of either seed covers the half table
+                        return min(min((w.x | tB) ^ full, (w.y | tA) ^ full), min((w.z | tB) ^ full, (w.w | tA) ^ full));
+                    };
+                    auto record = [&](uint32_t slot) {
+                        if (nh < 8) hq |= (uint64_t)slot << (8 * nh);
+                        else if (nh == 8) resume = 2 * slot;
+                        nh++;
+                    };
+                    // four 16-byte loads (eight raw seeds) in flight per step: the loads are
+                    // broadcasts, so latency, not bandwidth, sets this loop's speed
+                    for (; p + 8 <= in_sm; p += 8) {
+                        const uint4 w0 = m2[(p >> 1)], w1 = m2[(p >> 1) + 1], w2 = m2[(p >> 1) + 2], w3 = m2[(p >> 1) + 3];
+                        const uint32_t z0 = miss(w0), z1 = miss(w1), z2 = miss(w2), z3 = miss(w3);
+                        if (min(min(z0, z1), min(z2, z3)) == 0) {
+                            if (z0 == 0) record(p >> 1);
+                            if (z1 == 0) record((p >> 1) + 1);
+                            if (z2 == 0) record((p >> 1) + 2);
+                            if (z3 == 0) record((p >> 1) + 3);
                         }
                     }
+                    for (; p + 2 <= in_sm; p += 2)
+                        if (miss(m2[p >> 1]) == 0) record(p >> 1);
                     for (uint32_t h = 0; h < min(nh, 8u); h++) {
                         const uint32_t q = (uint32_t)((hq >> (8 * h)) & 0xFF) * 2;
                         const uint4 w = m2[q >> 1];
@@ -448,6 +462,30 @@ __device__ __forceinline__ void sh2_leaf(const Src &src, uint32_t li, const uint
                 }
                 for (; p < in_sm; p++) visit(p, sm.mask[p]);
                 uint64_t q = in_sm;
+                if constexpr (sizeof(typename LeafCtx<MAXM>::Mask) == 4) {
+                    // spilled masks (raw seeds from 256 on; q is even, so the 16-byte loads are
+                    // aligned): eight raw seeds' masks requested before any is tested
+                    const uint4 *g2 = reinterpret_cast<const uint4 *>(g.mask);
+                    const uint32_t full = cx.full;
+                    for (; q + 8 <= s + 1; q += 8) {
+                        uint4 w[4];
+#pragma unroll
+                        for (int t = 0; t < 4; t++) w[t] = g2[(q >> 1) + t];
+                        uint32_t z = 0xFFFFFFFFu;
+#pragma unroll
+                        for (int t = 0; t < 4; t++)
+                            z = min(z, min(min((w[t].x | tB) ^ full, (w[t].y | tA) ^ full),
+                                           min((w[t].z | tB) ^ full, (w[t].w | tA) ^ full)));
+                        if (z == 0) {  // rare: visit the eight seeds in order, reloading their masks
+#pragma unroll 1
+                            for (uint32_t t = 0; t < 4; t++) {
+                                const uint4 v = g2[(q >> 1) + t];
+                                visit(q + 2 * t, MaskPair<uint32_t>{v.x, v.y});
+                                visit(q + 2 * t + 1, MaskPair<uint32_t>{v.z, v.w});
+                            }
+                        }
+                    }
+                }
                 if constexpr (sizeof(typename LeafCtx<MAXM>::Mask) == 8) {  // spilled masks: same paired test
                     const uint64_t full = cx.full;
                     // eight raw seeds' masks requested before any is tested, so that eight L2 or DRAM
@@ -498,16 +536,16 @@ __device__ __forceinline__ void sh2_leaf(const Src &src, uint32_t li, const uint
         const uint32_t T = __shfl_sync(0xffffffffu, incl, take - 1);
         if (lane < take) {
             uint32_t pos = J + incl - mine;
-            if (cx.quad && mineA <= 2 && mineB <= 2) {
+            if (cx.quad && mineA <= kPartners && mineB <= kPartners) {
                 for (uint32_t t = 0; t < mineA; t++, pos++) {  // A side first: (a, s), a ascending
-                    cx.csa(pos) = t == 0 ? ha0 : ha1;
+                    cx.csa(pos) = plist[t * 32 + lane];
                     cx.csb(pos) = (uint32_t)s;
                 }
                 for (uint32_t t = 0; t < mineB; t++, pos++) {  // then B side: (s, b), b ascending
                     cx.csa(pos) = (uint32_t)s;
-                    cx.csb(pos) = t == 0 ? hb0 : hb1;
+                    cx.csb(pos) = plist[(kPartners + t) * 32 + lane];
                 }
-            } else if (cx.quad) {  // more than two partners on a side (rare): scan again
+            } else if (cx.quad) {  // more partners on a side than the lists hold (vanishingly rare): scan again
                 const auto tA = cx.maskA(s), tB = cx.maskB(s);
                 for (uint64_t a = 0; a < s && mine; a++)
                     if ((cx.maskA(a) | tB) == cx.full && float_accurate_elegant_seeds(a, s)) {
