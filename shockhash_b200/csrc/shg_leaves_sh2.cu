@@ -588,10 +588,18 @@ __device__ __forceinline__ void sh2_leaf(const Src &src, uint32_t li, const uint
                     if (k0 + 8 > m) v &= (1ull << (8 * (m - k0))) - 1;
                     return v;
                 };
+                // the candidate's cell words go to its own column of the union-find area (idle until
+                // the pair tests) for the second pass; the next word's loads are issued before this
+                // word's stores, which would otherwise hold them back
+                uint64_t *const uw = reinterpret_cast<uint64_t *>(sm.uf);  // [word][lane]
+                static_assert(MAXM / 8 * 32 * sizeof(uint64_t) <= sizeof(sm.uf), "cell words fit the union-find area");
                 uint64_t seen1 = 0, seen2 = 0;
+                uint64_t v_next = word_of(0);
 #pragma unroll 1
                 for (uint32_t w = 0; 8 * w < m; w++) {
-                    const uint64_t v = word_of(w);
+                    const uint64_t v = v_next;
+                    if (8 * (w + 1) < m) v_next = word_of(w + 1);
+                    uw[w * 32 + lane] = v;
                     if (row) row[w] = v;
                     const uint32_t kn = min(8u, m - 8 * w);
 #pragma unroll
@@ -607,7 +615,7 @@ __device__ __forceinline__ void sh2_leaf(const Src &src, uint32_t li, const uint
                 uint64_t iso0 = 0, iso1 = 0;
 #pragma unroll 1
                 for (uint32_t w = 0; 8 * w < m; w++) {
-                    const uint64_t v = word_of(w);
+                    const uint64_t v = uw[w * 32 + lane];
                     const uint32_t kn = min(8u, m - 8 * w);
                     uint64_t b8 = 0;
 #pragma unroll
