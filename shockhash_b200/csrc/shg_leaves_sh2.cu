@@ -120,9 +120,31 @@ template <int MAXM> struct LaneUF2 {
         if (MAXM <= 64 || r < 64) cyc0 |= 1ull << (r & 63);
         else cyc1 |= 1ull << (r & 63);
     }
+    // The roots of u and of v, both paths walked (and halved) in one loop so that their
+    // shared-memory loads overlap.
+    __device__ __forceinline__ void find2(uint32_t u, uint32_t v, uint32_t &ru, uint32_t &rv) {
+        for (;;) {
+            const uint32_t pu = par[u * 32 + lane], pv = par[v * 32 + lane];
+            const bool du = pu == u, dv = pv == v;
+            if (du && dv) break;
+            if (!du) {
+                const uint32_t g = par[pu * 32 + lane];
+                par[u * 32 + lane] = (uint8_t)g;
+                u = g;
+            }
+            if (!dv) {
+                const uint32_t g = par[pv * 32 + lane];
+                par[v * 32 + lane] = (uint8_t)g;
+                v = g;
+            }
+        }
+        ru = u;
+        rv = v;
+    }
     // Adds edge (u, v); false when a component would get a second cycle.
     __device__ __forceinline__ bool add(uint32_t u, uint32_t v) {
-        const uint32_t ru = find(u), rv = find(v);
+        uint32_t ru, rv;
+        find2(u, v, ru, rv);
         if (ru == rv) {
             if (cyc(ru)) return false;
             set_cyc(ru);
