@@ -222,8 +222,9 @@ shg_status shg_sh2_construct_leaves(shg_engine *e, const uint64_t *keys, const u
  * device image, held by every GPU that loads the library until the process exits; a leaf needing
  * more than 512 raw seeds or 512 candidates fails with SHG_ERR_TRIAL_LIMIT, a leaf outside 2..64
  * keys with SHG_ERR_ARG. The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress). All calls share the
- * array, so calls that overlap on the GPU (other streams, other host threads) race. */
+ * (cudaGetSymbolAddress, once per device); make that first call before any stream capture begins.
+ * All calls share the array, so calls that overlap on the GPU (other streams, other host threads)
+ * race. */
 shg_status shg_sh2_construct_leaves_noalloc(const uint64_t *d_keys, const uint64_t *d_leaf_offsets, uint64_t nleaves,
                                             uint64_t *d_seeds, uint8_t *d_bits, void *stream);
 

@@ -30,7 +30,7 @@ import sys
 
 import numpy as np
 
-from . import SHOCKHASH, SHOCKHASH2, TUNING_FLAT, Engine, keys_mt19937_64
+from . import SHOCKHASH, SHOCKHASH2, SIMDSHOCKHASH, TUNING_FLAT, Engine, keys_mt19937_64
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 TABLE = os.path.join(HERE, "tuning.tsv")
@@ -40,12 +40,15 @@ SPLIT_CANDIDATES = {"split_arith": (0, 1), "split_seeds_per_lane": (1, 2, 4), "s
 LEAF_CANDIDATES = {
     SHOCKHASH2: {"leaf_blocks_per_sm": (3, 4, 5, 6, 7, 8), "leaf_min_blocks": (4, 6, 8)},
     SHOCKHASH: {"leaf_blocks_per_sm": (4, 6, 8, 12, 16), "sh1_seeds_per_lane": (1, 2)},
+    SIMDSHOCKHASH: {"leaf_blocks_per_sm": (4, 6, 8, 12, 16), "sh1_seeds_per_lane": (1, 2)},
     TUNING_FLAT: {"leaf_blocks_per_sm": (1, 2, 3)},
 }
 # (variant, leaf size, keys): the benchmark configurations' searches
 CONFIGS = [(SHOCKHASH2, 64, 10_000_000), (SHOCKHASH, 30, 2_000_000), (SHOCKHASH, 40, 2_000_000),
+           (SIMDSHOCKHASH, 30, 2_000_000),
            (TUNING_FLAT, 100, 500_000)]
-NAMES = {SHOCKHASH: "ShockHash<{}>", SHOCKHASH2: "ShockHash2<{}>", TUNING_FLAT: "ShockHash2Flat<{}>"}
+NAMES = {SHOCKHASH: "ShockHash<{}>", SHOCKHASH2: "ShockHash2<{}>", SIMDSHOCKHASH: "SIMDShockHash<{}>",
+         TUNING_FLAT: "ShockHash2Flat<{}>"}
 
 
 class Tuner:
@@ -118,6 +121,8 @@ def tune_config(eng, variant, leaf, n, reps=3, min_gain=0.02, log=print):
         # the work-queue schedule (the default here): 256-thread blocks, at most 3 per SM
         split_c.pop("split_threads", None)
         leaf_c = {"leaf_blocks_per_sm": (1, 2, 3), "queue_lag_rounds": (0, 2, 4, 16, 32)}
+    if variant == SIMDSHOCKHASH:  # its split hash has one arithmetic form, chosen by the engine
+        split_c.pop("split_arith", None)
     if variant != TUNING_FLAT:
         params, _ = tu.descend(params, split_c, 0, min_gain)
     params, _ = tu.descend(params, leaf_c, 1, min_gain)
@@ -133,14 +138,17 @@ def tune_config(eng, variant, leaf, n, reps=3, min_gain=0.02, log=print):
 def write_table(results, path, device_name=""):
     lines = ["# Launch parameters of the search kernels per configuration, written by python -m shockhash_b200.tune",
              f"# on {device_name or 'a CUDA device'}, {datetime.date.today().isoformat()}. Columns: variant (1 ShockHash, "
-             "2 ShockHash2, 4 ShockHash2Flat) leaf name value.", "# Parameters change speed only; every result is identical."]
+             "2 ShockHash2, 4 ShockHash2Flat, 5 SIMDShockHash) leaf name value.",
+             "# Parameters change speed only; every result is identical."]
     for r in results:
         name = NAMES[r["variant"]].format(r["leaf"])
         d, t = r["default_ms"], r["tuned_ms"]
         lines.append(f"# {name}, {r['keys']} keys: splits {d['splits']} -> {t['splits']} ms, leaves {d['leaves']} -> "
                      f"{t['leaves']} ms (default -> tuned, best of the timed builds)")
         for k, v in r["params"].items():
-            if k.startswith("sh1_") and r["variant"] != SHOCKHASH:
+            if k.startswith("sh1_") and r["variant"] not in (SHOCKHASH, SIMDSHOCKHASH):
+                continue
+            if k == "split_arith" and r["variant"] == SIMDSHOCKHASH:
                 continue
             if k == "leaf_min_blocks" and (r["variant"] != SHOCKHASH2 or r["leaf"] > 64):
                 continue
