@@ -62,6 +62,31 @@ __global__ void k_bucket_count(const uint64_t *__restrict__ first, uint64_t n, u
     }
 }
 
+// The same counts with one shared-memory histogram per block (nb counters), flushed with one
+// global atomic per non-empty bucket: with a few thousand buckets every counter would otherwise take
+// about bucket_size contended global atomics. Each block counts a contiguous chunk of the keys.
+__global__ void __launch_bounds__(1024) k_bucket_count_smem(const uint64_t *__restrict__ first, uint64_t n, uint64_t nb,
+                                                            uint64_t nb_map, uint64_t b0, uint32_t *__restrict__ counts,
+                                                            uint32_t *__restrict__ err) {
+    extern __shared__ uint32_t hist[];
+    for (uint64_t b = threadIdx.x; b < nb; b += blockDim.x) hist[b] = 0;
+    __syncthreads();
+    const uint64_t lo = n * blockIdx.x / gridDim.x, hi = n * (blockIdx.x + 1) / gridDim.x;
+    for (uint64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+        const uint64_t b = remap128(first[i], nb_map) - b0;
+        if (b >= nb) {
+            atomicOr(err, kErrArg);
+            continue;
+        }
+        atomicAdd(&hist[b], 1u);
+    }
+    __syncthreads();
+    for (uint64_t b = threadIdx.x; b < nb; b += blockDim.x) {
+        const uint32_t c = hist[b];
+        if (c) atomicAdd(&counts[b], c);
+    }
+}
+
 // Exclusive scan of the bucket counts into bucket_size_acc (one block, sequential over chunks).
 __global__ void k_scan_counts(const uint32_t *__restrict__ counts, uint64_t nb, uint64_t *__restrict__ acc,
                               uint32_t *__restrict__ cursor, uint32_t *__restrict__ maxsz) {
@@ -114,6 +139,39 @@ __global__ void k_bucket_scatter(const uint64_t *__restrict__ first, uint64_t n,
         const uint64_t b = remap128(f, nb_map) - b0;
         if (b >= nb) continue;  // reported by k_bucket_count
         const uint32_t pos = atomicAdd(&cursor[b], 1u);
+        sfirst[pos] = f;
+        sidx[pos] = (uint32_t)(idx_base + i);
+    }
+}
+
+// The same scatter with the contention moved to shared memory: a block counts its chunk's keys per
+// bucket, reserves each non-empty bucket's range with one global atomic on the cursor, then places
+// its keys inside those ranges with shared-memory atomics. The order inside a bucket depends on
+// atomic order here as in k_bucket_scatter; k_bucket_sort orders each bucket by (first, input
+// index), so the products do not depend on it.
+__global__ void __launch_bounds__(1024) k_bucket_scatter_smem(const uint64_t *__restrict__ first, uint64_t n, uint64_t nb,
+                                                              uint64_t nb_map, uint64_t b0, uint32_t *__restrict__ cursor,
+                                                              uint64_t *__restrict__ sfirst, uint32_t *__restrict__ sidx,
+                                                              uint64_t idx_base) {
+    extern __shared__ uint32_t slot[];
+    for (uint64_t b = threadIdx.x; b < nb; b += blockDim.x) slot[b] = 0;
+    __syncthreads();
+    const uint64_t lo = n * blockIdx.x / gridDim.x, hi = n * (blockIdx.x + 1) / gridDim.x;
+    for (uint64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+        const uint64_t b = remap128(first[i], nb_map) - b0;
+        if (b < nb) atomicAdd(&slot[b], 1u);  // keys outside are reported by the count kernel
+    }
+    __syncthreads();
+    for (uint64_t b = threadIdx.x; b < nb; b += blockDim.x) {
+        const uint32_t c = slot[b];
+        if (c) slot[b] = atomicAdd(&cursor[b], c);  // this block's range of bucket b
+    }
+    __syncthreads();
+    for (uint64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+        const uint64_t f = first[i];
+        const uint64_t b = remap128(f, nb_map) - b0;
+        if (b >= nb) continue;
+        const uint32_t pos = atomicAdd(&slot[b], 1u);
         sfirst[pos] = f;
         sidx[pos] = (uint32_t)(idx_base + i);
     }
@@ -377,10 +435,32 @@ void launch_plan_expand(const uint64_t *acc, uint64_t nb, uint32_t rows, const u
                                                 lists, nodes, fixed_off, ids, singles);
 }
 
+// Blocks of the shared-memory partition kernels: as many 1024-thread blocks as fit each SM with nb
+// counters each, at most one per 4096 keys; 0 when nb counters do not fit one block's shared memory.
+static int partition_smem_blocks(uint64_t n, uint64_t nb, size_t &smem) {
+    constexpr uint64_t kMaxSmem = 200 * 1024;
+    smem = (size_t)nb * sizeof(uint32_t);
+    if (nb == 0 || smem > kMaxSmem) return 0;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int per_sm = (int)std::max<uint64_t>(1, std::min<uint64_t>(2, (228 * 1024) / (smem + 1024)));
+    return (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sms * per_sm, (n + 4095) / 4096));
+}
+
 void launch_bucket_count(const uint64_t *first, uint64_t n, uint64_t nb, uint64_t nb_map, uint64_t b0, uint32_t *counts,
                          uint32_t *err, cudaStream_t s) {
     cudaMemsetAsync(counts, 0, nb * sizeof(uint32_t), s);
-    if (n) k_bucket_count<<<grid_for(n, 256), 256, 0, s>>>(first, n, nb, nb_map, b0, counts, err);
+    if (!n) return;
+    size_t smem = 0;
+    const int blocks = partition_smem_blocks(n, nb, smem);
+    if (blocks) {
+        // the shared-memory limit is an attribute of the kernel on the current device: set it on every launch
+        cudaFuncSetAttribute(k_bucket_count_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_bucket_count_smem<<<blocks, 1024, smem, s>>>(first, n, nb, nb_map, b0, counts, err);
+    } else {
+        k_bucket_count<<<grid_for(n, 256), 256, 0, s>>>(first, n, nb, nb_map, b0, counts, err);
+    }
 }
 void launch_scan_counts(const uint32_t *counts, uint64_t nb, uint64_t *acc, uint32_t *cursor, uint32_t *maxsz,
                         cudaStream_t s) {
@@ -389,7 +469,15 @@ void launch_scan_counts(const uint32_t *counts, uint64_t nb, uint64_t *acc, uint
 }
 void launch_bucket_scatter(const uint64_t *first, uint64_t n, uint64_t nb, uint64_t nb_map, uint64_t b0, uint32_t *cursor,
                            uint64_t *sfirst, uint32_t *sidx, uint64_t idx_base, cudaStream_t s) {
-    if (n) k_bucket_scatter<<<grid_for(n, 256), 256, 0, s>>>(first, n, nb, nb_map, b0, cursor, sfirst, sidx, idx_base);
+    if (!n) return;
+    size_t smem = 0;
+    const int blocks = partition_smem_blocks(n, nb, smem);
+    if (blocks) {
+        cudaFuncSetAttribute(k_bucket_scatter_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_bucket_scatter_smem<<<blocks, 1024, smem, s>>>(first, n, nb, nb_map, b0, cursor, sfirst, sidx, idx_base);
+    } else {
+        k_bucket_scatter<<<grid_for(n, 256), 256, 0, s>>>(first, n, nb, nb_map, b0, cursor, sfirst, sidx, idx_base);
+    }
 }
 void launch_bucket_sort(const uint64_t *acc, uint64_t nb, const uint64_t *sfirst, const uint32_t *sidx,
                         const uint64_t *second, uint64_t *keys, cudaStream_t s) {
