@@ -81,15 +81,18 @@ template <int MAXM> struct Sh2Global {
     uint64_t *rows;       // [rcap][MAXM / 8]
     uint64_t *raw;        // [rawcap][MAXM / 8]: cells of every key (finder order) under raw seed s
     uint32_t rcap, rawcap;
-    __device__ void carve(uint8_t *base, uint32_t smax, uint32_t cmax) {
+    // row_rows / raw_rows: candidates and raw seeds whose cell rows are cached (beyond them the
+    // kernel recomputes cells from the keys)
+    __device__ void carve(uint8_t *base, uint32_t smax, uint32_t cmax, uint32_t row_rows = Sh2Cfg<MAXM>::ROWS,
+                          uint32_t raw_rows = Sh2Cfg<MAXM>::RAW_ROWS) {
         mask = (MaskPair<Mask> *)base;
         iso = (uint64_t *)(base + ((2ull * smax * sizeof(Mask) + 255) & ~255ull));
         csa = (uint32_t *)(iso + 2 * (uint64_t)cmax);
         csb = csa + cmax;
         rows = (uint64_t *)(csb + cmax);  // 8-byte aligned: cmax is even
-        rcap = cmax < Sh2Cfg<MAXM>::ROWS ? cmax : Sh2Cfg<MAXM>::ROWS;
+        rcap = cmax < row_rows ? cmax : row_rows;
         raw = rows + (uint64_t)rcap * (MAXM / 8);
-        rawcap = smax < Sh2Cfg<MAXM>::RAW_ROWS ? smax : Sh2Cfg<MAXM>::RAW_ROWS;
+        rawcap = smax < raw_rows ? smax : raw_rows;
     }
 };
 
@@ -232,6 +235,7 @@ struct NodeLeaves {
     const Node *nodes;
     const uint32_t *ids;
     uint64_t *codes;
+    static constexpr uint32_t kRowCache = 0;  // 0: the configuration's cell-row caches (Sh2Cfg)
     __device__ __forceinline__ bool get(uint32_t li, uint32_t &start, uint32_t &m, uint64_t *&code) const {
         const uint32_t id = ids[li];
         const Node nd = nodes[id];
@@ -245,6 +249,10 @@ struct NodeLeaves {
 template <int MAXM> struct OffsetLeaves {
     const uint64_t *offs;
     uint64_t *seeds;
+    // Cell-row caches of the no-allocation entry point, which uses this source: rows of the first
+    // 128 candidates and 192 raw seeds of a leaf, so that its fixed scratch array feeds about twice
+    // as many warps as with the engine's caches.
+    static constexpr uint32_t kRowCache = 1, kCandRows = 128, kRawRows = 192;
     __device__ __forceinline__ bool get(uint32_t li, uint32_t &start, uint32_t &m, uint64_t *&code) const {
         const uint64_t b = offs[li], e = offs[li + 1];
         if (e < b + 2 || e - b > (uint64_t)MAXM || e > 0xFFFFFFFFull) return false;
@@ -768,7 +776,8 @@ __global__ void __launch_bounds__(128, MINB) k_leaves_sh2_v2(Src src, uint32_t c
     const uint64_t gw = (uint64_t)blockIdx.x * WPB + warp;
     uint8_t *gbase = scratch + gw * scratch_per_warp;
     Sh2Global<MAXM> g;
-    g.carve(gbase, smax, cmax);
+    if constexpr (Src::kRowCache) g.carve(gbase, smax, cmax, Src::kCandRows, Src::kRawRows);
+    else g.carve(gbase, smax, cmax);
     LaneUF2<MAXM> uf{sm.uf, lane, 0, 0};
     LeafWork lw;
     for (;;) {
@@ -1063,11 +1072,14 @@ void launch_queue_t(const Node *nodes, const uint32_t *ids, const uint32_t *seq,
 } // namespace
 
 // Bytes of global scratch per warp for the given capacities (raw seeds, candidates).
-uint64_t sh2_scratch_bytes(uint32_t smax, uint32_t cmax, int max_leaf) {
-    const uint64_t rows = std::min<uint64_t>(cmax, max_leaf > 64 ? Sh2Cfg<128>::ROWS : Sh2Cfg<64>::ROWS);
-    const uint64_t raw = std::min<uint64_t>(smax, max_leaf > 64 ? Sh2Cfg<128>::RAW_ROWS : Sh2Cfg<64>::RAW_ROWS);
+// Bytes of one warp's scratch slice (Sh2Global::carve's layout); rows / raws cap the cached cell rows
+// (0: the configuration's caches).
+static uint64_t sh2_slice_bytes(uint32_t smax, uint32_t cmax, int max_leaf, uint32_t row_cap, uint32_t raw_cap) {
+    const uint64_t rows = std::min<uint64_t>(cmax, row_cap ? row_cap : max_leaf > 64 ? Sh2Cfg<128>::ROWS : Sh2Cfg<64>::ROWS);
+    const uint64_t raw = std::min<uint64_t>(smax, raw_cap ? raw_cap : max_leaf > 64 ? Sh2Cfg<128>::RAW_ROWS : Sh2Cfg<64>::RAW_ROWS);
     return 16ull * smax + 256 + 24ull * cmax + (rows + raw) * (max_leaf > 64 ? 128 : 64);
 }
+uint64_t sh2_scratch_bytes(uint32_t smax, uint32_t cmax, int max_leaf) { return sh2_slice_bytes(smax, cmax, max_leaf, 0, 0); }
 
 void launch_leaves_sh2_ctr(const Node *nodes, const uint32_t *ids, uint32_t count, const uint64_t *keys, uint64_t *codes,
                            uint8_t *rib_bits, uint8_t *scratch, uint64_t scratch_per_warp, uint32_t smax, uint32_t cmax,
@@ -1281,7 +1293,8 @@ extern "C" shg_status shg_sh2_construct_leaves_noalloc(const uint64_t *d_keys, c
     // counters start at zero on every call; the spill slices need no clearing (written before read)
     if ((st = cudaMemsetAsync(ctr, 0, sizeof(NoAllocCounters), s)) != cudaSuccess)
         return shg_set_error(SHG_ERR_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(st));
-    const uint64_t per_warp = (sh2_scratch_bytes(kNoAllocSmax, kNoAllocCmax, 64) + 255) & ~255ull;
+    const uint64_t per_warp = (sh2_slice_bytes(kNoAllocSmax, kNoAllocCmax, 64, OffsetLeaves<64>::kCandRows,
+                                               OffsetLeaves<64>::kRawRows) + 255) & ~255ull;
     const uint64_t warps = (kNoAllocScratchBytes - 256) / per_warp;
     const uint64_t blocks = std::min<uint64_t>(warps / 4, (nleaves + 3) / 4);
     const size_t smem = sizeof(Sh2Smem<64>) * 4;
