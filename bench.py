@@ -49,7 +49,7 @@ MODES = ["default (work queue for ShockHash2 with leaves of up to 64 keys, else 
 # kernel (the whole search: node keys read, retrieval bits and spilled leaf scratch written) and a
 # quarter-split level launch of the level schedule (node keys read once; the partition's writes
 # stay in L2).
-QUEUE_DRAM_BYTES_PER_KEY = (9_491_200 + 43_116_288) / 1_000_000
+QUEUE_DRAM_BYTES_PER_KEY = (13_114_880 + 81_113_856) / 1_000_000
 SPLIT_DRAM_BYTES_PER_KEY = (6_560_256 + 512) / 1_000_000
 
 
