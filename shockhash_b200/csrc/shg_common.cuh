@@ -136,8 +136,20 @@ SHG_HD bool float_accurate_elegant(uint64_t x, uint64_t y) {  // :93-96
 // skipped there. z = pair_elegant(x, y) lies in [f^2, (f + 1)^2 - 1] with f <= 2^24; sqrt(f^2) = f
 // is exact, and sqrt((f + 1)^2 - 1) stays more than 2^-26 below f + 1 while doubles near f are at
 // most 2^-28 apart, so the correctly rounded square root floors to f and unpairing is exact.
+#ifdef __CUDA_ARCH__
+// The square-root path out of line on the device: raw seeds of a leaf search stay far below 2^24 in
+// practice, and the leaf kernels test many seed pairs at many places, so inlining it would only
+// grow their code.
+static __device__ __noinline__ bool float_accurate_elegant_cold(uint64_t x, uint64_t y) {
+    return float_accurate_elegant(x, y);
+}
+#endif
 SHG_HD bool float_accurate_elegant_seeds(uint64_t x, uint64_t y) {
+#ifdef __CUDA_ARCH__
+    return (x | y) < (1ull << 24) || float_accurate_elegant_cold(x, y);
+#else
     return (x | y) < (1ull << 24) || float_accurate_elegant(x, y);
+#endif
 }
 
 // ------------------------------------------------------------------ leaf cell hashes

@@ -542,7 +542,7 @@ __device__ __forceinline__ void sh2_leaf(const Src &src, uint32_t li, const uint
                         }
                     }
                 }
-#pragma unroll 4
+#pragma unroll 1
                 for (; q <= s; q++) visit(q, g.mask[q]);
                 mine = mineA + mineB;
             } else {
