@@ -23,6 +23,7 @@
 #include <cstdint>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <cuda_runtime.h>
 #include "shg_common.cuh"
 #include "shg_internal.h"
@@ -623,7 +624,9 @@ __device__ __forceinline__ void sh2_leaf(const Src &src, uint32_t li, const uint
                 // word's stores, which would otherwise hold them back
                 uint64_t *const uw = reinterpret_cast<uint64_t *>(sm.uf);  // [word][lane]
                 static_assert(MAXM / 8 * 32 * sizeof(uint64_t) <= sizeof(sm.uf), "cell words fit the union-find area");
-                uint64_t seen1 = 0, seen2 = 0;
+                // cells are below (m + 1) / 2: 32-bit masks for leaves of up to 64 keys
+                using CMask = std::conditional_t<(MAXM <= 64), uint32_t, uint64_t>;
+                CMask seen1 = 0, seen2 = 0;
                 uint64_t v_next = word_of(0);
 #pragma unroll 1
                 for (uint32_t w = 0; 8 * w < m; w++) {
@@ -635,13 +638,13 @@ __device__ __forceinline__ void sh2_leaf(const Src &src, uint32_t li, const uint
 #pragma unroll
                     for (uint32_t t = 0; t < 8; t++) {
                         if (t < kn) {
-                            const uint64_t bit = 1ull << ((v >> (8 * t)) & 0xFF);
+                            const CMask bit = (CMask)1 << ((v >> (8 * t)) & 0xFF);
                             seen2 |= seen1 & bit;
                             seen1 |= bit;
                         }
                     }
                 }
-                const uint64_t single = seen1 & ~seen2;
+                const CMask single = seen1 & ~seen2;
                 uint64_t iso0 = 0, iso1 = 0;
 #pragma unroll 1
                 for (uint32_t w = 0; 8 * w < m; w++) {
