@@ -138,15 +138,16 @@ __global__ void __launch_bounds__(kPeakThreads) k_int_peak_sh1(uint64_t iters, u
 }
 
 // The arithmetic of the bipartite leaf search's raw-seed loop: remix, fastrange64 to the half
-// table, one bit into a 64-bit mask; two seeds per lane.
+// table (as the kernel computes it for a range below 2^32), one bit into a 64-bit mask; two seeds
+// per lane.
 __global__ void __launch_bounds__(kPeakThreads) k_int_peak_sh2(uint64_t iters, uint64_t half, unsigned long long *sink) {
     const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     uint64_t k0 = shg::remix(tid * 0x9E3779B97F4A7C15ULL), k1 = shg::remix(k0);
     const uint64_t x0 = 0x643e521ddbd2be98ULL + tid;
     uint64_t a0 = 0, a1 = 0;
     for (uint64_t i = 0; i < iters; i++) {
-        a0 |= 1ull << shg::fastrange64(shg::remix(k0 + x0 + i), half);
-        a1 |= 1ull << shg::fastrange64(shg::remix(k1 + x0 + i), half);
+        a0 |= 1ull << shg::fastrange64_32(shg::remix(k0 + x0 + i), (uint32_t)half);
+        a1 |= 1ull << shg::fastrange64_32(shg::remix(k1 + x0 + i), (uint32_t)half);
     }
     sink[tid] = a0 ^ a1;
 }

@@ -160,7 +160,18 @@ SHG_HD void sh1_cells(uint64_t key, uint64_t seed, uint32_t m, uint32_t &c1, uin
     c2 = fastrange32((uint32_t)(r >> 32), (m + 1) / 2) + m / 2;
 }
 // Bipartite half-table cell (ShockHash2-internal.h:100-102, 473-477).
-SHG_HD uint32_t half_hash(uint64_t key, uint64_t s, uint32_t half) { return (uint32_t)fastrange64(remix(key + s), half); }
+// fastrange64(word, p) for a range p below 2^32, exactly: with word = hi * 2^32 + lo,
+// floor(word * p / 2^64) = floor((hi * p + floor(lo * p / 2^32)) / 2^32), the dropped fraction
+// never carrying past an integer. Two 32-bit multiplies instead of a 64 x 64-bit high product.
+SHG_HD uint32_t fastrange64_32(uint64_t word, uint32_t p) {
+#ifdef __CUDA_ARCH__
+    const uint64_t a = (uint64_t)(uint32_t)(word >> 32) * p + __umulhi((uint32_t)word, p);
+    return (uint32_t)(a >> 32);
+#else
+    return (uint32_t)fastrange64(word, p);
+#endif
+}
+SHG_HD uint32_t half_hash(uint64_t key, uint64_t s, uint32_t half) { return fastrange64_32(remix(key + s), half); }
 // Cell of `key` under a bipartite candidate seed: the Basic finder's hash
 // (ShockHash2-internal.h:100-102), or QuadSplit's (elegant pair; even keys use seedA, odd keys
 // seedB, :473-477). The RecSplit leaves use QuadSplit from m = 10 on
