@@ -50,8 +50,8 @@ template <> struct Sh2Cfg<64> {
 };
 template <> struct Sh2Cfg<128> {
     using Mask = uint64_t;
-    static constexpr int SMS = 256;   // 17 KB of shared memory per warp: three 4-warp blocks per SM
-    static constexpr int CMS = 256;
+    static constexpr int SMS = 128;   // 12 KB of shared memory per warp: four 4-warp blocks per SM
+    static constexpr int CMS = 128;
     static constexpr int ISO_WORDS = 2;
     static constexpr uint32_t ROWS = 4096;
     static constexpr uint32_t RAW_ROWS = 1024;
