@@ -274,7 +274,9 @@ struct LeafWork {
 // global scratch `g` and union-find `uf` are reused from leaf to leaf. Errors set bits of *err.
 // L2: read the leaf's keys past L1 (the work-queue kernel, where another SM's partition may have
 // rewritten them after this SM cached the lines).
-template <int MAXM, class Src, bool L2 = false>
+// SIDE_WORDS: hash whole 8-key words that lie on one side of the leaf without per-key selects
+// (measured faster inside the work-queue kernel, slower in the level schedule's leaf kernel).
+template <int MAXM, class Src, bool L2 = false, bool SIDE_WORDS = false>
 __device__ __forceinline__ void sh2_leaf(const Src &src, uint32_t li, const uint64_t *__restrict__ keys,
                                          uint8_t *__restrict__ rib_bits, Sh2Smem<MAXM> &sm, Sh2Global<MAXM> &g,
                                          LaneUF2<MAXM> &uf, const int lane, const uint32_t smax, const uint32_t cmax,
@@ -377,14 +379,27 @@ __device__ __forceinline__ void sh2_leaf(const Src &src, uint32_t li, const uint
             // sm.keys[8w + 7] is in bounds, and the cells of keys past m are dropped)
             for (uint32_t k0 = 0; k0 < m; k0 += 8) {
                 uint64_t word = 0;
+                if (SIDE_WORDS && k0 + 8 <= m && (k0 + 8 <= sizeA || k0 >= sizeA)) {
+                    // the whole word inside the leaf and on one side (the same in every lane)
+                    Mask w8 = 0;
 #pragma unroll
-                for (uint32_t t = 0; t < 8; t++) {
-                    const uint32_t k = k0 + t;
-                    const uint32_t h = half_hash(sm.keys[k], s, half);
-                    const Mask bit = k < m ? (Mask)1 << h : (Mask)0;
-                    tA |= k < sizeA ? bit : (Mask)0;
-                    tB |= k < sizeA ? (Mask)0 : bit;
-                    word |= k < m ? (uint64_t)h << (8 * t) : 0ull;
+                    for (uint32_t t = 0; t < 8; t++) {
+                        const uint32_t h = half_hash(sm.keys[k0 + t], s, half);
+                        w8 |= (Mask)1 << h;
+                        word |= (uint64_t)h << (8 * t);
+                    }
+                    if (k0 + 8 <= sizeA) tA |= w8;
+                    else tB |= w8;
+                } else {
+#pragma unroll
+                    for (uint32_t t = 0; t < 8; t++) {
+                        const uint32_t k = k0 + t;
+                        const uint32_t h = half_hash(sm.keys[k], s, half);
+                        const Mask bit = k < m ? (Mask)1 << h : (Mask)0;
+                        tA |= k < sizeA ? bit : (Mask)0;
+                        tB |= k < sizeA ? (Mask)0 : bit;
+                        word |= k < m ? (uint64_t)h << (8 * t) : 0ull;
+                    }
                 }
                 if (rrow) rrow[k0 >> 3] = word;
             }
@@ -975,7 +990,7 @@ __device__ void write_bucket_out(uint32_t b, const uint64_t *__restrict__ acc, c
 __device__ __noinline__ void queue_leaf(const NodeLeaves &leaves, uint32_t li, const uint64_t *__restrict__ keys,
                                         uint8_t *__restrict__ rib_bits, Sh2Smem<64> &sm, Sh2Global<64> &g, LaneUF2<64> &uf,
                                         int lane, uint32_t smax, uint32_t cmax, uint32_t *__restrict__ err, LeafWork &lw) {
-    sh2_leaf<64, NodeLeaves, true>(leaves, li, keys, rib_bits, sm, g, uf, lane, smax, cmax, kQuadMinRecSplit, err, lw);
+    sh2_leaf<64, NodeLeaves, true, true>(leaves, li, keys, rib_bits, sm, g, uf, lane, smax, cmax, kQuadMinRecSplit, err, lw);
 }
 
 template <int SPL, int ARITH>
