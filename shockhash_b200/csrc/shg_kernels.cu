@@ -435,17 +435,18 @@ void launch_plan_expand(const uint64_t *acc, uint64_t nb, uint32_t rows, const u
                                                 lists, nodes, fixed_off, ids, singles);
 }
 
-// Blocks of the shared-memory partition kernels: as many 1024-thread blocks as fit each SM with nb
-// counters each, at most one per 4096 keys; 0 when nb counters do not fit one block's shared memory.
+// Blocks of the shared-memory partition kernels: two 1024-thread blocks per SM (a full SM of
+// threads, which the scattered writes need), at most one per 4096 keys; 0 when two blocks' nb
+// counters do not fit an SM's shared memory (above about 25,000 buckets, where the contention of the
+// global-atomic kernels is low anyway: 100M keys partition faster with them).
 static int partition_smem_blocks(uint64_t n, uint64_t nb, size_t &smem) {
-    constexpr uint64_t kMaxSmem = 200 * 1024;
+    constexpr uint64_t kMaxSmem = 100 * 1024;
     smem = (size_t)nb * sizeof(uint32_t);
     if (nb == 0 || smem > kMaxSmem) return 0;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int per_sm = (int)std::max<uint64_t>(1, std::min<uint64_t>(2, (228 * 1024) / (smem + 1024)));
-    return (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sms * per_sm, (n + 4095) / 4096));
+    return (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)sms * 2, (n + 4095) / 4096));
 }
 
 void launch_bucket_count(const uint64_t *first, uint64_t n, uint64_t nb, uint64_t nb_map, uint64_t b0, uint32_t *counts,
