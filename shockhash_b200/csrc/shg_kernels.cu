@@ -436,11 +436,11 @@ void launch_plan_expand(const uint64_t *acc, uint64_t nb, uint32_t rows, const u
 }
 
 // Blocks of the shared-memory partition kernels: two 1024-thread blocks per SM (a full SM of
-// threads, which the scattered writes need), at most one per 4096 keys; 0 when two blocks' nb
-// counters do not fit an SM's shared memory (above about 25,000 buckets, where the contention of the
-// global-atomic kernels is low anyway: 100M keys partition faster with them).
+// threads, which the scattered writes need), at most one per 4096 keys; 0 above 6,144 buckets, where
+// the global-atomic kernels were measured faster on B200 (partition of 4M / 10M / 16M keys:
+// 0.33 / 0.92 / 1.80 ms with these kernels, 0.56 / 1.04 / 1.46 ms without).
 static int partition_smem_blocks(uint64_t n, uint64_t nb, size_t &smem) {
-    constexpr uint64_t kMaxSmem = 100 * 1024;
+    constexpr uint64_t kMaxSmem = 6144 * sizeof(uint32_t);
     smem = (size_t)nb * sizeof(uint32_t);
     if (nb == 0 || smem > kMaxSmem) return 0;
     int dev = 0, sms = 148;
