@@ -21,7 +21,11 @@ Besides the headline line the GPU arm reports, on rank 0 at N=1:
   * forms: the level schedule against the pipelined one and the per-leaf-launch form (1M keys),
     the SIMD format (SIMDShockHash<30>, 1M keys) against the reference's SIMD CPU build, the
     north-star size (100M keys), a Poisson serving stream, the device query of every key and the
-    device retrieval structure.
+    device retrieval structure;
+  * forms.configs: the other configurations of the same path at stated sizes (ShockHash<30> over 1M
+    printable strings, ShockHash<40> over 100M keys, ShockHash2Flat<100> over 50M Zipf-length
+    strings), each with its leaf stage against its roofline and, on a bounded sample, the reference
+    CPU build of the same keys and a word-for-word comparison.
 """
 import argparse
 import json
@@ -379,6 +383,160 @@ def simd_format_form(eng, d_ptr, keys, n, flush):
     return out
 
 
+def synthetic_strings(kind, seed, n):
+    """Seeded synthetic string keys of a configuration's shape (numpy's PCG64 stream, packed as
+    (bytes, offsets[n+1])): "printable" = lengths uniform in 16..40, bytes uniform in 33..126;
+    "zipf" = lengths l in 8..200 with P(l) proportional to (l - 7)^-1.1 (Zipf(1.1) on the clipped
+    range, mean about 34 bytes), bytes uniform in 0..255."""
+    rng = np.random.default_rng(seed)
+    if kind == "printable":
+        lengths = rng.integers(16, 41, size=n, dtype=np.uint64)
+    else:
+        w = np.arange(1, 194, dtype=np.float64) ** -1.1
+        lengths = (8 + np.searchsorted(np.cumsum(w) / w.sum(), rng.random(n), side="right")).astype(np.uint64)
+        np.minimum(lengths, 200, out=lengths)
+    offs = np.zeros(n + 1, dtype=np.uint64)
+    np.cumsum(lengths, out=offs[1:])
+    total = int(offs[-1])
+    if kind == "printable":
+        data = rng.integers(33, 127, size=total, dtype=np.uint8).tobytes()
+    else:
+        data = rng.bytes(total)
+    return data, offs
+
+
+def config_forms(eng, dev, flush, with_cpu):
+    """The other configurations of the same path at stated sizes: device stage times, the leaf stage
+    against its roofline, and, where the reference's CPU build of the same keys finishes in seconds
+    on the host cores, its time and a word-for-word comparison with the device build.
+      c1: ShockHash<30, false>, b = 2000, 1M printable strings of 16..40 bytes (host strings in);
+      c3: ShockHash<40, false>, b = 2000, 100M uint64 keys (mt19937_64 seed 11, device-resident),
+          the CPU reference and the comparison on the first 200k keys;
+      c4: ShockHash2Flat<100>, 50M strings of Zipf(1.1) lengths 8..200 (host strings in), the
+          comparison on the first 20k keys."""
+    import torch
+    import shockhash_b200 as shg
+    threads = os.cpu_count() or 1
+    out = {}
+    bindings = None
+    if with_cpu:
+        from oracle import bindings
+        if not bindings.ref_available():
+            bindings = None
+
+    # c1
+    n1 = int(os.environ.get("SHG_C1_N", "1000000"))
+    data, offs = synthetic_strings("printable", 42, n1)
+    r, dev_ms, wall_ms = None, [], []
+    for it in range(4):  # one warm-up, then three timed builds
+        if r is not None:
+            r.free()
+        t0 = time.perf_counter()
+        r = eng.build_strings(shg.SHOCKHASH, 30, (data, offs), BUCKET)
+        if it:
+            wall_ms.append(1e3 * (time.perf_counter() - t0))
+            dev_ms.append(r.stage_ms["total"])
+    c1 = {"class": "ShockHash<30, false> b=2000", "keys": n1,
+          "input": "host strings, 16-40 printable bytes (numpy seed 42)",
+          "device_ns_per_key": round(statistics.mean(dev_ms) * 1e6 / n1, 3),
+          "wall_ns_per_key": round(statistics.mean(wall_ms) * 1e6 / n1, 3),
+          "stage_ms": {k: round(v, 3) for k, v in r.stage_ms.items()}}
+    if bindings:
+        b, secs = bindings.RefLib().build_strings_packed_timed(shg.SHOCKHASH, 30, data, offs, BUCKET, threads)
+        c1["cpu_reference_ns_per_key"] = round(secs * 1e9 / n1, 3)
+        c1["cpu_cores"] = threads
+        c1["vs_cpu_reference"] = round(secs * 1e9 / n1 / c1["device_ns_per_key"], 1)
+        c1["parity"] = {"keys": n1, **compare_products(r, b)}
+        b.free()
+    r.free()
+    out["c1_sh1_l30_strings"] = c1
+    del data, offs
+
+    # c3
+    n3 = int(os.environ.get("SHG_C3_N", "100000000"))
+    keys3 = shg.keys_mt19937_64(11, n3)
+    d3 = torch.from_numpy(keys3.view(np.int64)).to(dev)
+    peak1, _ = shg.int_peak(dev.index or 0, 1 << 15, 1)
+    res = []
+    for it in range(2):  # one warm-up, then one timed build
+        flush.zero_()
+        torch.cuda.synchronize()
+        rm = eng.build_u64_device(shg.SHOCKHASH, 40, d3.data_ptr(), n3, BUCKET)
+        if it:
+            res.append(_Summary(rm))
+        rm.free()
+    st = res[-1].stage_ms
+    rate = res[-1].work["leaf_evals"] / (st["leaves"] * 1e-3)
+    c3 = {"class": "ShockHash<40, false> b=2000", "keys": n3, "input": "device-resident uint64 keys (seed 11)",
+          "device_ns_per_key": round(st["total"] * 1e6 / n3, 3), "stage_ms": {k: round(v, 3) for k, v in st.items()},
+          "leaf_stage": {"evals_per_s_g": round(rate / 1e9, 3), "peak_g": round(peak1 / 1e9, 3),
+                         "frac": round(rate / peak1, 4),
+                         "note": "hash evaluations of the original leaf search per second vs the measured peak of "
+                                 "its coverage loop"}}
+    if bindings:
+        ns = min(n3, int(os.environ.get("SHG_C3_CPU_SAMPLE", "200000")))
+        dt, kind, cores, b = cpu_reference(keys3[:ns], threads, keep=True, variant=shg.SHOCKHASH, leaf=40)
+        rs = eng.build_u64_device(shg.SHOCKHASH, 40, d3.data_ptr(), ns, BUCKET)
+        c3["cpu_reference_ns_per_key"] = round(dt * 1e9 / ns, 3)
+        c3["cpu_sample"] = f"first {ns} keys, all {cores} host threads"
+        c3["vs_cpu_reference"] = round(dt * 1e9 / ns / c3["device_ns_per_key"], 1)
+        c3["parity"] = {"keys": ns, **compare_products(rs, b)}
+        rs.free()
+        b.free()
+    out["c3_sh1_l40_u64"] = c3
+    del d3, keys3
+    torch.cuda.empty_cache()
+
+    # c4
+    n4 = int(os.environ.get("SHG_C4_N", "50000000"))
+    data, offs = synthetic_strings("zipf", 23, n4)
+    lpeaks = shg.leaf_peaks(dev.index or 0, large=True)
+    f, wall_ms = None, []
+    for it in range(2):  # one warm-up, then one timed build
+        if f is not None:
+            f.free()
+        t0 = time.perf_counter()
+        f = eng.build_flat_strings(100, (data, offs))
+        if it:
+            wall_ms.append(1e3 * (time.perf_counter() - t0))
+    w = eng.last_work()["flat_leaves"]
+    counts = {"hash_evals": w["hash_evals"], "scan_tests": w["scan_tests"], "pair_tests": w["pair_tests"],
+              "uf_edges": w["uf_edges"]}
+    ceil_s = shg.leaf_ceiling_s(counts, lpeaks)
+    names = ("hash", "partition", "plan", "splits", "leaves", "encode", "copy_out", "total")
+    dq = f.device_query()
+    q = dq.query_strings((data, offs))
+    c4 = {"class": "ShockHash2Flat<100>", "keys": n4,
+          "input": f"host strings, Zipf(1.1) lengths 8..200 (numpy seed 23, mean {len(data) / n4:.1f} bytes)",
+          "wall_ns_per_key": round(statistics.mean(wall_ms) * 1e6 / n4, 3),
+          "device_ns_per_key": round(f.stage_ms[7] * 1e6 / n4, 3),
+          "stage_ms": {k: round(v, 3) for k, v in zip(names, f.stage_ms)},
+          "leaf_stage": {"ms": round(f.stage_ms[4], 3), "counts": counts, "ceiling_ms": round(ceil_s * 1e3, 3),
+                         "frac": round(ceil_s * 1e3 / f.stage_ms[4], 4)},
+          "device_query_ns_per_key": round(dq.last_kernel_ms() * 1e6 / n4, 4),
+          "device_query_is_permutation": bool(np.array_equal(np.sort(q), np.arange(n4, dtype=np.uint64)))}
+    dq.close()
+    f.free()
+    del q
+    if bindings:
+        ns = min(n4, int(os.environ.get("SHG_C4_CPU_SAMPLE", "20000")))
+        sd, so = data[:int(offs[ns])], offs[:ns + 1]
+        ref = bindings.RefLib().flat_build_strings(100, [sd[int(so[i]):int(so[i + 1])] for i in range(ns)])
+        fs = eng.build_flat_strings(100, (sd, so))
+        checks = {"thresholds_and_seeds": np.array_equal(fs.thresholds_and_seeds, ref["thresholds_and_seeds"]),
+                  "layer_bases": np.array_equal(fs.layer_bases, ref["layer_bases"]),
+                  "fallback_seeds": np.array_equal(fs.fallback_seeds, ref["fallback_seeds"]),
+                  "free_positions": np.array_equal(fs.free_positions, ref["free_positions"]),
+                  "ribbon_keys": np.array_equal(fs.ribbon_keys, ref["ribbon_keys"]),
+                  "ribbon_bits": np.array_equal(fs.ribbon_bits, ref["ribbon_bits"]),
+                  "query": np.array_equal(fs.query_strings((sd, so)), ref["query"])}
+        c4["parity"] = {"keys": ns, "against": "reference", "bit_exact": all(checks.values()),
+                        "compared": sorted(checks), "mismatch": sorted(k for k, v in checks.items() if not v)}
+        fs.free()
+    out["c4_flat100_zipf_strings"] = c4
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -398,6 +556,9 @@ def main():
                     help="keys of the north-star size leg (0 skips it)")
     ap.add_argument("--serve-requests", type=int, default=int(os.environ.get("SHG_SERVE_REQUESTS", "400")),
                     help="requests of the serving leg (0 skips it)")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other configurations' leg (ShockHash<30> strings, ShockHash<40> at 100M keys, "
+                         "ShockHash2Flat<100> at 50M strings)")
     ap.add_argument("--sharded", action="store_true",
                     help="build ONE structure over all ranks: every step exchanges the ranks' keys by bucket range "
                          "(device partition + NCCL all-to-all) and builds each rank's buckets on its GPU")
@@ -631,6 +792,12 @@ def main():
             eng = None
             torch.cuda.empty_cache()
             forms["serving"] = serve.run_stream(serve.poisson_stream(args.serve_requests, 200.0, 31), workers=2)
+        if ws == 1 and not args.no_forms and not args.no_configs:  # after serving, whose host-side
+            # request generation is sensitive to the host memory these large key sets take
+            ceng = eng if eng is not None else shg.Engine(local)
+            forms["configs"] = config_forms(ceng, dev, flush, not args.no_cpu)
+            if ceng is not eng:
+                ceng.close()
         line = {
             "metric": METRIC, "value": round(ms * 1e6 / total_keys, 3), "unit": "ns/key", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": False,

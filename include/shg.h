@@ -384,7 +384,8 @@ int shg_int_peak(int device, uint64_t iters, double *evals_per_s, double *ms);
  * 9 / 10 / 11 / 12 = kinds 0 / 3 / 4 / 5 with the split kernel's pipe-split arithmetic
  * (tuning parameter split_arith 1), 13 / 14 / 15 = kinds 6 / 7 / 8 for bipartite leaves of more
  * than 64 keys (64-bit masks, 100-edge tests), 16 / 17 / 18 / 19 = kinds 0 / 3 / 4 / 5 under
- * SIMDShockHash's split hash (SIMDShockHash.hpp:762-766). */
+ * SIMDShockHash's split hash (SIMDShockHash.hpp:762-766), 20 = kind 13 with the other form of the
+ * mask test ((a | t) == full instead of (~t & ~a) == 0; the faster of 13 and 20 bounds the scan). */
 int shg_int_peak_kind(int device, int kind, uint64_t iters, double *evals_per_s, double *ms);
 
 /* Work counts of the engine's last RecSplit build beyond shg_result.work (measurement utility, no

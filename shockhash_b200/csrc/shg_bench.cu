@@ -244,10 +244,10 @@ int shg_int_peak(int device, uint64_t iters, double *evals_per_s, double *ms_out
 // 2 = bipartite leaf hashing, 3..5 = split compare-and-count with 1..3 thresholds, 6..8 = bipartite
 // candidate scan, pair filter and pseudoforest edges, 9..12 = kinds 0 and 3..5 with the split
 // kernel's pipe-split arithmetic, 13..15 = kinds 6..8 for leaves of more than 64 keys, 16..19 = kinds
-// 0 and 3..5 under SIMDShockHash's split hash).
+// 0 and 3..5 under SIMDShockHash's split hash, 20 = kind 13 with the other form of the mask test).
 int shg_int_peak_kind(int device, int kind, uint64_t iters, double *evals_per_s, double *ms_out) {
     if (kind == 0) return shg_int_peak(device, iters, evals_per_s, ms_out);
-    if (kind < 1 || kind > 19) return SHG_ERR_ARG;
+    if (kind < 1 || kind > 20) return SHG_ERR_ARG;
     if (cudaSetDevice(device) != cudaSuccess) return SHG_ERR_CUDA;
     cudaDeviceProp prop;
     cudaGetDeviceProperties(&prop, device);
@@ -280,6 +280,8 @@ int shg_int_peak_kind(int device, int kind, uint64_t iters, double *evals_per_s,
             k_int_peak_simd<2><<<blocks, kPeakThreads>>>(it, 21846, 43691, 65536, sink);
         else if (kind == 19)
             k_int_peak_simd<3><<<blocks, kPeakThreads>>>(it, 16384, 32768, 49152, sink);
+        else if (kind == 20)
+            shg::launch_sh2_op_peak(6, blocks, it, sink);
         else if (kind >= 13)  // the same for leaves of more than 64 keys (100 edges per iteration)
             shg::launch_sh2_op_peak(kind - 10, blocks, kind == 15 ? it / 100 + 1 : it, sink);
         else {  // 9: quarter moments, 10..12: 1..3 thresholds, with the split kernel's pipe-split arithmetic
@@ -306,6 +308,8 @@ int shg_int_peak_kind(int device, int kind, uint64_t iters, double *evals_per_s,
     } else if (kind >= 13 && kind <= 15) {
         per_iter = shg::sh2_op_peak_per_iter(kind - 10);
         if (kind == 15) timed_iters = iters / 100 + 1;
+    } else if (kind == 20) {
+        per_iter = shg::sh2_op_peak_per_iter(6);
     }
     *evals_per_s = per_iter * (double)timed_iters * blocks * kPeakThreads / (ms * 1e-3);
     if (ms_out) *ms_out = ms;

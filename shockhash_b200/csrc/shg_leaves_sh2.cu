@@ -18,7 +18,9 @@
 //      a cycle flag per root over the cached cell rows); fewer than 32 wait for the next batch,
 //      and the first passing survivor in queue order is the answer.
 // Candidate and raw-seed state live in shared memory; indices past its capacity spill to a
-// per-warp slice of global scratch, which also holds the cell rows.
+// per-warp slice of global scratch, which also holds the cell rows. For leaves of more than 64
+// keys, whose raw seeds run into the thousands, step 2 streams the spilled masks of earlier rounds
+// through a shared-memory ring (cp.async, two chunks of 32 ahead) instead of loading them per lane.
 #include <algorithm>
 #include <cstdint>
 #include <mutex>
@@ -47,6 +49,7 @@ template <> struct Sh2Cfg<64> {
     static constexpr int ISO_WORDS = 1;
     static constexpr uint32_t ROWS = 2048;  // candidates whose cell rows are cached in global scratch
     static constexpr uint32_t RAW_ROWS = 2048;  // raw seeds whose cell rows are cached
+    static constexpr int RING = 0;  // staging buffers of 32 spilled masks (none: leaves this small rarely spill)
 };
 template <> struct Sh2Cfg<128> {
     using Mask = uint64_t;
@@ -55,7 +58,22 @@ template <> struct Sh2Cfg<128> {
     static constexpr int ISO_WORDS = 2;
     static constexpr uint32_t ROWS = 4096;
     static constexpr uint32_t RAW_ROWS = 1024;
+    static constexpr int RING = 3;  // staging buffers of 32 spilled masks: two chunks in flight while one is tested
 };
+
+// Shared-memory ring through which a warp streams spilled raw-seed masks (R buffers of 32 pairs).
+template <class M, int R> struct MaskRing {
+    MaskPair<M> e[R][32];
+};
+template <class M> struct MaskRing<M, 0> {};
+
+// 16-byte global -> shared copies that bypass registers and L1 (cp.async), grouped per thread.
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gsrc) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 template <int MAXM> struct alignas(16) Sh2Smem {  // 16-byte aligned per warp: the masks are read 16 bytes at a time
     using C = Sh2Cfg<MAXM>;
@@ -70,6 +88,7 @@ template <int MAXM> struct alignas(16) Sh2Smem {  // 16-byte aligned per warp: t
     uint8_t c1[MAXM], c2[MAXM];                  // retrieval cuckoo insertion
     int16_t cell[MAXM];
     uint8_t xr[MAXM];
+    MaskRing<typename C::Mask, C::RING> ring;
 };
 
 // Per-warp global scratch (L2-resident in practice): what does not fit shared memory, and the
@@ -418,96 +437,150 @@ __device__ __forceinline__ void sh2_leaf(const Src &src, uint32_t li, const uint
         static_assert(2 * kPartners * 32 * sizeof(uint16_t) <= sizeof(sm.uf), "partner lists fit the union-find area");
         uint16_t *const plist = reinterpret_cast<uint16_t *>(sm.uf);
         if (live) w_scan += cx.quad ? s + 1 : 1;  // mask pairs this raw seed is tested against
-        if (live) {
-            if (cx.quad) {
-                // one pass over the earlier raw seeds p <= s: A-side pairs (p, s) for p < s and
-                // B-side pairs (s, p) for p <= s (candidatesA/B.filter, ShockHash2-internal.h:446-465)
-                const auto ts = cx.mp(s);
-                const auto tA = ts.a, tB = ts.b;
-                auto visit = [&](uint64_t p, MaskPair<typename LeafCtx<MAXM>::Mask> w) {
-                    if (p < s && (w.a | tB) == cx.full && float_accurate_elegant_seeds(p, s)) {
-                        if (mineA < kPartners) plist[mineA * 32 + lane] = (uint16_t)p;
-                        mineA++;
-                    }
-                    if ((w.b | tA) == cx.full && float_accurate_elegant_seeds(s, p)) {
-                        if (mineB < kPartners) plist[(kPartners + mineB) * 32 + lane] = (uint16_t)p;
-                        mineB++;
-                    }
+        // one pass over the earlier raw seeds p <= s: A-side pairs (p, s) for p < s and B-side pairs
+        // (s, p) for p <= s (candidatesA/B.filter, ShockHash2-internal.h:446-465), in three parts:
+        // the masks in shared memory (each lane alone), the spilled masks of earlier rounds (the
+        // warp streams them through a shared-memory ring), and the rest up to s (each lane alone)
+        using RMask = typename LeafCtx<MAXM>::Mask;
+        const MaskPair<RMask> ts = live && cx.quad ? cx.mp(s) : MaskPair<RMask>{0, 0};
+        const RMask tA = ts.a, tB = ts.b;
+        // a side of raw seed p pairs with s when it covers every cell s's other side leaves empty:
+        // (w.a | tB) == full  <=>  (nB & ~w.a) == 0 (masks hold no bits past the half table)
+        const RMask nA = ~tA & cx.full, nB = ~tB & cx.full;
+        const uint32_t in_sm = (uint32_t)min(s + 1, (uint64_t)Sh2Cfg<MAXM>::SMS);
+        auto visit = [&](uint64_t p, MaskPair<RMask> w) {
+            if (p < s && (w.a | tB) == cx.full && float_accurate_elegant_seeds(p, s)) {
+                if (mineA < kPartners) plist[mineA * 32 + lane] = (uint16_t)p;
+                mineA++;
+            }
+            if ((w.b | tA) == cx.full && float_accurate_elegant_seeds(s, p)) {
+                if (mineB < kPartners) plist[(kPartners + mineB) * 32 + lane] = (uint16_t)p;
+                mineB++;
+            }
+        };
+        if (live && cx.quad) {
+            uint32_t p = 0;
+            if constexpr (sizeof(typename LeafCtx<MAXM>::Mask) == 4) {
+                // two raw seeds per 16-byte load; one combined test rejects the common case
+                // that neither side of either seed covers the half table. A hit only
+                // appends its 16-byte slot (p / 2 < 128) to a register queue of up to 8;
+                // the hits are visited after the loop, in the same ascending order, so the
+                // loop itself stays free of the recording path. Past 8 hits the scan
+                // resumes, visiting directly, from the 9th hit's slot on.
+                const uint4 *m2 = reinterpret_cast<const uint4 *>(sm.mask);
+                const uint32_t full = cx.full;
+                uint64_t hq = 0;
+                uint32_t nh = 0, resume = 0;
+                auto miss = [&](const uint4 &w) {  // 0 when a side of either seed covers the half table
+                    return min(min((w.x | tB) ^ full, (w.y | tA) ^ full), min((w.z | tB) ^ full, (w.w | tA) ^ full));
                 };
-                const uint32_t in_sm = (uint32_t)min(s + 1, (uint64_t)Sh2Cfg<MAXM>::SMS);
-                uint32_t p = 0;
-                if constexpr (sizeof(typename LeafCtx<MAXM>::Mask) == 4) {
-                    // two raw seeds per 16-byte load; one combined test rejects the common case
-                    // that neither side of either seed covers the half table. A hit only
-                    // appends its 16-byte slot (p / 2 < 128) to a register queue of up to 8;
-                    // the hits are visited after the loop, in the same ascending order, so the
-                    // loop itself stays free of the recording path. Past 8 hits the scan
-                    // resumes, visiting directly, from the 9th hit's slot on.
-                    const uint4 *m2 = reinterpret_cast<const uint4 *>(sm.mask);
-                    const uint32_t full = cx.full;
-                    uint64_t hq = 0;
-                    uint32_t nh = 0, resume = 0;
-                    auto miss = [&](const uint4 &w) {  // 0 when a side of either seed covers the half table
-                        return min(min((w.x | tB) ^ full, (w.y | tA) ^ full), min((w.z | tB) ^ full, (w.w | tA) ^ full));
-                    };
-                    auto record = [&](uint32_t slot) {
-                        if (nh < 8) hq |= (uint64_t)slot << (8 * nh);
-                        else if (nh == 8) resume = 2 * slot;
-                        nh++;
-                    };
-                    // four 16-byte loads (eight raw seeds) in flight per step: the loads are
-                    // broadcasts, so latency, not bandwidth, sets this loop's speed
-                    for (; p + 8 <= in_sm; p += 8) {
-                        const uint4 w0 = m2[(p >> 1)], w1 = m2[(p >> 1) + 1], w2 = m2[(p >> 1) + 2], w3 = m2[(p >> 1) + 3];
-                        const uint32_t z0 = miss(w0), z1 = miss(w1), z2 = miss(w2), z3 = miss(w3);
-                        if (min(min(z0, z1), min(z2, z3)) == 0) {
-                            if (z0 == 0) record(p >> 1);
-                            if (z1 == 0) record((p >> 1) + 1);
-                            if (z2 == 0) record((p >> 1) + 2);
-                            if (z3 == 0) record((p >> 1) + 3);
+                auto record = [&](uint32_t slot) {
+                    if (nh < 8) hq |= (uint64_t)slot << (8 * nh);
+                    else if (nh == 8) resume = 2 * slot;
+                    nh++;
+                };
+                // four 16-byte loads (eight raw seeds) in flight per step: the loads are
+                // broadcasts, so latency, not bandwidth, sets this loop's speed
+                for (; p + 8 <= in_sm; p += 8) {
+                    const uint4 w0 = m2[(p >> 1)], w1 = m2[(p >> 1) + 1], w2 = m2[(p >> 1) + 2], w3 = m2[(p >> 1) + 3];
+                    const uint32_t z0 = miss(w0), z1 = miss(w1), z2 = miss(w2), z3 = miss(w3);
+                    if (min(min(z0, z1), min(z2, z3)) == 0) {
+                        if (z0 == 0) record(p >> 1);
+                        if (z1 == 0) record((p >> 1) + 1);
+                        if (z2 == 0) record((p >> 1) + 2);
+                        if (z3 == 0) record((p >> 1) + 3);
+                    }
+                }
+                for (; p + 2 <= in_sm; p += 2)
+                    if (miss(m2[p >> 1]) == 0) record(p >> 1);
+                for (uint32_t h = 0; h < min(nh, 8u); h++) {
+                    const uint32_t q = (uint32_t)((hq >> (8 * h)) & 0xFF) * 2;
+                    const uint4 w = m2[q >> 1];
+                    visit(q, MaskPair<uint32_t>{w.x, w.y});
+                    visit(q + 1, MaskPair<uint32_t>{w.z, w.w});
+                }
+                if (nh > 8) {
+                    for (uint32_t q = resume; q + 2 <= in_sm; q += 2) {
+                        const uint4 w = m2[q >> 1];
+                        const uint32_t z = min(min((w.x | tB) ^ full, (w.y | tA) ^ full),
+                                               min((w.z | tB) ^ full, (w.w | tA) ^ full));
+                        if (z == 0) {
+                            visit(q, MaskPair<uint32_t>{w.x, w.y});
+                            visit(q + 1, MaskPair<uint32_t>{w.z, w.w});
                         }
                     }
-                    for (; p + 2 <= in_sm; p += 2)
-                        if (miss(m2[p >> 1]) == 0) record(p >> 1);
-                    for (uint32_t h = 0; h < min(nh, 8u); h++) {
-                        const uint32_t q = (uint32_t)((hq >> (8 * h)) & 0xFF) * 2;
-                        const uint4 w = m2[q >> 1];
-                        visit(q, MaskPair<uint32_t>{w.x, w.y});
-                        visit(q + 1, MaskPair<uint32_t>{w.z, w.w});
+                }
+            }
+            if constexpr (sizeof(typename LeafCtx<MAXM>::Mask) == 8) {
+                // one raw seed per 16-byte load, two per round; a tight scan finds the next
+                // pair in which some side covers the half table, and only then records it
+                for (;;) {
+                    MaskPair<uint64_t> w{0, 0}, v{0, 0};
+                    for (; p + 2 <= in_sm; p += 2) {
+                        w = sm.mask[p];
+                        v = sm.mask[p + 1];
+                        if (((nB & ~w.a) == 0) | ((nA & ~w.b) == 0) | ((nB & ~v.a) == 0) | ((nA & ~v.b) == 0))
+                            break;
                     }
-                    if (nh > 8) {
-                        for (uint32_t q = resume; q + 2 <= in_sm; q += 2) {
-                            const uint4 w = m2[q >> 1];
-                            const uint32_t z = min(min((w.x | tB) ^ full, (w.y | tA) ^ full),
-                                                   min((w.z | tB) ^ full, (w.w | tA) ^ full));
-                            if (z == 0) {
-                                visit(q, MaskPair<uint32_t>{w.x, w.y});
-                                visit(q + 1, MaskPair<uint32_t>{w.z, w.w});
+                    if (p + 2 > in_sm) break;
+                    visit(p, w);
+                    visit(p + 1, v);
+                    p += 2;
+                }
+            }
+            for (; p < in_sm; p++) visit(p, sm.mask[p]);
+        }
+        uint64_t spill0 = in_sm;  // where each lane's own pass over the spilled masks starts
+        if constexpr (Sh2Cfg<MAXM>::RING > 0) {
+            constexpr int R = Sh2Cfg<MAXM>::RING;
+            constexpr uint64_t lo = Sh2Cfg<MAXM>::SMS;
+            if (cx.quad && S_proc > lo) {
+                // raw seeds lo..S_proc-1 lie below every lane's s and their masks are in global
+                // scratch: the warp copies them 32 at a time (one 16-byte pair per lane, coalesced)
+                // into the ring, R - 1 chunks ahead of the one being tested, and every lane tests
+                // its own seed against each pair with shared-memory broadcasts, so the loop waits on
+                // no global load; hits are visited in ascending order as before
+                const uint64_t hi = S_proc;
+                const uint32_t nch = (uint32_t)((hi - lo + 31) / 32);
+                auto issue = [&](uint32_t c) {
+                    const uint64_t p = lo + 32ull * c + lane;
+                    if (c < nch && p < hi) cp_async16(&sm.ring.e[c % R][lane], &g.mask[p]);
+                    cp_async_commit();  // one group per chunk in every lane, empty ones included
+                };
+#pragma unroll
+                for (int c = 0; c < R - 1; c++) issue(c);
+                for (uint32_t c = 0; c < nch; c++) {
+                    cp_async_wait<R - 2>();  // this lane's copies of chunk c have landed
+                    __syncwarp();            // and every lane's; all are done testing chunk c - 1
+                    issue(c + R - 1);        // into the buffer chunk c - 1 used
+                    if (live) {
+                        const MaskPair<uint64_t> *buf = sm.ring.e[c % R];
+                        const uint64_t c0 = lo + 32ull * c;
+                        const uint32_t cnt = (uint32_t)min((uint64_t)32, hi - c0);
+                        uint32_t t = 0;
+                        for (; t + 8 <= cnt; t += 8) {
+                            MaskPair<uint64_t> w8[8];
+#pragma unroll
+                            for (int u = 0; u < 8; u++) w8[u] = buf[t + u];
+                            bool any = false;
+#pragma unroll
+                            for (int u = 0; u < 8; u++) any |= ((nB & ~w8[u].a) == 0) | ((nA & ~w8[u].b) == 0);
+                            if (any) {
+#pragma unroll 1
+                                for (uint32_t u = 0; u < 8; u++) visit(c0 + t + u, buf[t + u]);
                             }
                         }
+                        for (; t < cnt; t++) visit(c0 + t, buf[t]);
                     }
                 }
-                if constexpr (sizeof(typename LeafCtx<MAXM>::Mask) == 8) {
-                    // one raw seed per 16-byte load, two per round; a tight scan finds the next
-                    // pair in which some side covers the half table, and only then records it
-                    const uint64_t full = cx.full;
-                    for (;;) {
-                        MaskPair<uint64_t> w{0, 0}, v{0, 0};
-                        for (; p + 2 <= in_sm; p += 2) {
-                            w = sm.mask[p];
-                            v = sm.mask[p + 1];
-                            if ((((w.a | tB) ^ full) == 0) | (((w.b | tA) ^ full) == 0) | (((v.a | tB) ^ full) == 0) |
-                                (((v.b | tA) ^ full) == 0))
-                                break;
-                        }
-                        if (p + 2 > in_sm) break;
-                        visit(p, w);
-                        visit(p + 1, v);
-                        p += 2;
-                    }
-                }
-                for (; p < in_sm; p++) visit(p, sm.mask[p]);
-                uint64_t q = in_sm;
+                cp_async_wait<0>();
+                __syncwarp();
+                spill0 = hi;
+            }
+        }
+        if (live) {
+            if (cx.quad) {
+                uint64_t q = spill0;
                 if constexpr (sizeof(typename LeafCtx<MAXM>::Mask) == 4) {
                     // spilled masks (raw seeds from 256 on; q is even, so the 16-byte loads are
                     // aligned): eight raw seeds' masks requested before any is tested
@@ -533,7 +606,6 @@ __device__ __forceinline__ void sh2_leaf(const Src &src, uint32_t li, const uint
                     }
                 }
                 if constexpr (sizeof(typename LeafCtx<MAXM>::Mask) == 8) {  // spilled masks: same paired test
-                    const uint64_t full = cx.full;
                     // eight raw seeds' masks requested before any is tested, so that eight L2 or DRAM
                     // loads are in flight per warp instead of two (these loads dominate large leaves)
                     for (; q + 8 <= s + 1; q += 8) {
@@ -542,7 +614,7 @@ __device__ __forceinline__ void sh2_leaf(const Src &src, uint32_t li, const uint
                         for (int t = 0; t < 8; t++) w8[t] = g.mask[q + t];
                         bool any = false;
 #pragma unroll
-                        for (int t = 0; t < 8; t++) any |= (((w8[t].a | tB) ^ full) == 0) | (((w8[t].b | tA) ^ full) == 0);
+                        for (int t = 0; t < 8; t++) any |= ((nB & ~w8[t].a) == 0) | ((nA & ~w8[t].b) == 0);
                         if (any) {
 #pragma unroll 1
                             for (uint32_t t = 0; t < 8; t++) visit(q + t, g.mask[q + t]);
@@ -550,8 +622,7 @@ __device__ __forceinline__ void sh2_leaf(const Src &src, uint32_t li, const uint
                     }
                     for (; q + 2 <= s + 1; q += 2) {
                         const MaskPair<uint64_t> w = g.mask[q], v = g.mask[q + 1];
-                        const bool any = (((w.a | tB) ^ full) == 0) | (((w.b | tA) ^ full) == 0) |
-                                         (((v.a | tB) ^ full) == 0) | (((v.b | tA) ^ full) == 0);
+                        const bool any = ((nB & ~w.a) == 0) | ((nA & ~w.b) == 0) | ((nB & ~v.a) == 0) | ((nA & ~v.b) == 0);
                         if (any) {
                             visit(q, w);
                             visit(q + 1, v);
@@ -1106,7 +1177,7 @@ void launch_leaves_sh2_ctr(const Node *nodes, const uint32_t *ids, uint32_t coun
     if (!count) return;
     cudaMemsetAsync(ctr, 0, sizeof(unsigned int), s);
     if (max_leaf > 64)
-        launch_v2<128, 1>(nodes, ids, count, keys, codes, rib_bits, scratch, scratch_per_warp, smax, cmax, err, work, ctr, grid,
+        launch_v2<128, 4>(nodes, ids, count, keys, codes, rib_bits, scratch, scratch_per_warp, smax, cmax, err, work, ctr, grid,
                           s, quad_min);
     else if (minb == 4)
         launch_v2<64, 4>(nodes, ids, count, keys, codes, rib_bits, scratch, scratch_per_warp, smax, cmax, err, work, ctr, grid,
@@ -1167,7 +1238,9 @@ void launch_tree_queue(const Node *nodes, const uint32_t *ids, const uint32_t *s
 //           (two pairs per 16-byte broadcast load, as the 64-key scan);
 //   kind 1: isolated-key filter of one candidate pair (two 64-bit masks from shared memory);
 //   kind 2: one pseudoforest edge of a 64-key leaf (LaneUF2::add on shared-memory parents; each
-//           test initialises the parents and adds 64 edges).
+//           test initialises the parents and adds 64 edges);
+//   kind 3: kind 0 for 64-bit masks with the test written as (a | t) == full, the form the scan
+//           used before its complement form (~t & ~a) == 0; the faster of the two bounds the scan.
 namespace {
 // W = 64: the loops of leaves of up to 64 keys (32-bit half masks, two raw seeds per 16-byte load,
 // one isolated-key word, 64-edge tests); W = 128: of larger leaves (64-bit half masks, one raw seed
@@ -1200,7 +1273,16 @@ __global__ void __launch_bounds__(256) k_sh2_op_peak(uint64_t iters, unsigned lo
         }
         acc = hits;
     } else if (KIND == 0) {
-        const uint64_t tA = remix(tid), tB = remix(tA), full = ~0ull;
+        const uint64_t tA = remix(tid), tB = remix(tA), full = (1ull << 50) - 1, nA = ~tA & full, nB = ~tB & full;
+        uint32_t hits = 0;
+        for (uint64_t i = 0; i < iters; i++) {
+            const uint4 w = masks[i & 127];
+            const uint64_t a = (uint64_t)w.y << 32 | w.x, b = (uint64_t)w.w << 32 | w.z;
+            hits += ((nB & ~a) == 0) | ((nA & ~b) == 0);  // the scan's complement form
+        }
+        acc = hits;
+    } else if (KIND == 3) {  // the same test as (a | t) == full, full a value the compiler cannot fold
+        const uint64_t tA = remix(tid), tB = remix(tA), full = ~0ull >> (14 + (tid >> 62));
         uint32_t hits = 0;
         for (uint64_t i = 0; i < iters; i++) {
             const uint4 w = masks[i & 127];
@@ -1238,9 +1320,10 @@ __global__ void __launch_bounds__(256) k_sh2_op_peak(uint64_t iters, unsigned lo
 }  // namespace
 
 // Operations per launch thread and iteration: kinds 0..2 for leaves of up to 64 keys (2 scan tests,
-// 1 pair filter, 64 edges), kinds 3..5 for larger leaves (1 scan test, 1 pair filter, 100 edges).
+// 1 pair filter, 64 edges), kinds 3..5 for larger leaves (1 scan test, 1 pair filter, 100 edges),
+// kind 6 the larger leaves' scan test in its other form (1 scan test).
 int sh2_op_peak_per_iter(int kind) {
-    static const int per[6] = {2, 1, 64, 1, 1, 100};
+    static const int per[7] = {2, 1, 64, 1, 1, 100, 1};
     return per[kind];
 }
 void launch_sh2_op_peak(int kind, int blocks, uint64_t iters, unsigned long long *sink) {
@@ -1250,6 +1333,7 @@ void launch_sh2_op_peak(int kind, int blocks, uint64_t iters, unsigned long long
         case 2: k_sh2_op_peak<2, 64><<<blocks, 256>>>(iters, sink); break;
         case 3: k_sh2_op_peak<0, 128><<<blocks, 256>>>(iters, sink); break;
         case 4: k_sh2_op_peak<1, 128><<<blocks, 256>>>(iters, sink); break;
+        case 6: k_sh2_op_peak<3, 128><<<blocks, 256>>>(iters, sink); break;
         default: k_sh2_op_peak<2, 128><<<blocks, 256>>>(iters, sink); break;
     }
 }
