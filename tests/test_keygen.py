@@ -64,3 +64,23 @@ def test_zipf_strings(port):
     keys = bindings.split_strings(d, o)
     assert len(set(keys)) == n
     assert 0 in np.frombuffer(d, dtype=np.uint8)  # NUL bytes occur
+
+
+def test_bench_synthetic_strings_follow_the_configuration_shapes():
+    """bench.py's stand-ins for the string configurations (numpy streams, used by its GPU leg):
+    the same lengths, byte ranges and length distribution as the oracle's generators define."""
+    import bench
+    d, o = bench.synthetic_strings("printable", 42, 20_000)
+    lens = np.diff(o.astype(np.int64))
+    assert lens.min() >= 16 and lens.max() <= 40 and len(set(lens.tolist())) == 25
+    arr = np.frombuffer(d, dtype=np.uint8)
+    assert arr.min() >= 33 and arr.max() <= 126 and len(d) == int(o[-1])
+    n = 200_000
+    d, o = bench.synthetic_strings("zipf", 23, n)
+    lens = np.diff(o.astype(np.int64))
+    assert lens.min() >= 8 and lens.max() <= 200 and len(d) == int(o[-1])
+    w = np.arange(1, 194, dtype=np.float64) ** -1.1
+    assert abs((lens == 8).mean() - w[0] / w.sum()) < 0.01
+    assert abs(lens.mean() - (np.arange(8, 201) * w).sum() / w.sum()) < 1.0
+    d2, o2 = bench.synthetic_strings("zipf", 23, n)
+    assert d2 == d and np.array_equal(o2, o)
