@@ -424,6 +424,14 @@ def config_forms(eng, dev, flush, with_cpu):
         if not bindings.ref_available():
             bindings = None
 
+    peak1, _ = shg.int_peak(dev.index or 0, 1 << 15, 1)  # the original leaf search's coverage loop
+
+    def sh1_leaf_stage(stage_ms, work):
+        rate = work["leaf_evals"] / (stage_ms["leaves"] * 1e-3)
+        return {"evals_per_s_g": round(rate / 1e9, 3), "peak_g": round(peak1 / 1e9, 3), "frac": round(rate / peak1, 4),
+                "note": "hash evaluations of the original leaf search per second vs the measured peak of its "
+                        "coverage loop"}
+
     # c1
     n1 = int(os.environ.get("SHG_C1_N", "1000000"))
     data, offs = synthetic_strings("printable", 42, n1)
@@ -440,7 +448,8 @@ def config_forms(eng, dev, flush, with_cpu):
           "input": "host strings, 16-40 printable bytes (numpy seed 42)",
           "device_ns_per_key": round(statistics.mean(dev_ms) * 1e6 / n1, 3),
           "wall_ns_per_key": round(statistics.mean(wall_ms) * 1e6 / n1, 3),
-          "stage_ms": {k: round(v, 3) for k, v in r.stage_ms.items()}}
+          "stage_ms": {k: round(v, 3) for k, v in r.stage_ms.items()},
+          "leaf_stage": sh1_leaf_stage(r.stage_ms, r.work)}
     if bindings:
         b, secs = bindings.RefLib().build_strings_packed_timed(shg.SHOCKHASH, 30, data, offs, BUCKET, threads)
         c1["cpu_reference_ns_per_key"] = round(secs * 1e9 / n1, 3)
@@ -456,7 +465,6 @@ def config_forms(eng, dev, flush, with_cpu):
     n3 = int(os.environ.get("SHG_C3_N", "100000000"))
     keys3 = shg.keys_mt19937_64(11, n3)
     d3 = torch.from_numpy(keys3.view(np.int64)).to(dev)
-    peak1, _ = shg.int_peak(dev.index or 0, 1 << 15, 1)
     res = []
     for it in range(2):  # one warm-up, then one timed build
         flush.zero_()
@@ -466,13 +474,9 @@ def config_forms(eng, dev, flush, with_cpu):
             res.append(_Summary(rm))
         rm.free()
     st = res[-1].stage_ms
-    rate = res[-1].work["leaf_evals"] / (st["leaves"] * 1e-3)
     c3 = {"class": "ShockHash<40, false> b=2000", "keys": n3, "input": "device-resident uint64 keys (seed 11)",
           "device_ns_per_key": round(st["total"] * 1e6 / n3, 3), "stage_ms": {k: round(v, 3) for k, v in st.items()},
-          "leaf_stage": {"evals_per_s_g": round(rate / 1e9, 3), "peak_g": round(peak1 / 1e9, 3),
-                         "frac": round(rate / peak1, 4),
-                         "note": "hash evaluations of the original leaf search per second vs the measured peak of "
-                                 "its coverage loop"}}
+          "leaf_stage": sh1_leaf_stage(st, res[-1].work)}
     if bindings:
         ns = min(n3, int(os.environ.get("SHG_C3_CPU_SAMPLE", "200000")))
         dt, kind, cores, b = cpu_reference(keys3[:ns], threads, keep=True, variant=shg.SHOCKHASH, leaf=40)
