@@ -83,7 +83,17 @@ __device__ bool cuckoo_insert(int16_t *cell, uint8_t *xr, int e, uint32_t c1, ui
 }
 
 // ------------------------------------------------------------------ original ShockHash leaves
+// Seeds that pass the coverage test queue up (in seed order) until kSh1Drain of them wait, and are
+// then tested for the pseudoforest property side by side, one per lane: tested one round at a
+// time, a round's one or two passing seeds ran the union-find while the other lanes waited.
+#ifndef SHG_SH1_DRAIN
+#define SHG_SH1_DRAIN 4
+#endif
+constexpr uint32_t kSh1Drain = SHG_SH1_DRAIN;
+constexpr uint32_t kSh1Queue = kSh1Drain + 64;  // fewer than kSh1Drain wait, plus one round's 32 x SPL (SPL <= 2)
+
 struct Sh1WarpSmem {
+    uint64_t q[kSh1Queue];  // coverage-passing seed offsets, ascending
     uint64_t keys[64];
     uint64_t fkeys[64];  // rotation fitting: even keys in order, odd keys from the back
     uint8_t uf[64 * 32];
@@ -283,6 +293,20 @@ __global__ void __launch_bounds__(kLeafWarps * 32) k_leaves_sh1(const Node *__re
             }
             return ok;
         };
+        // queued survivors, tested 32 at a time in queue (= seed) order: the first passing one is
+        // the smallest passing seed, as every smaller seed failed coverage or an earlier test
+        const unsigned below = (1u << lane) - 1;
+        uint32_t nq = 0;
+        auto drain = [&]() {
+            for (uint32_t q0 = 0; q0 < nq && found == ~0ull; q0 += 32) {
+                const uint64_t off = q0 + lane < nq ? sm.q[q0 + lane] : ~0ull;
+                const bool pass = off != ~0ull && pseudoforest(seed0 + off);
+                const unsigned bal = __ballot_sync(0xffffffffu, pass);
+                if (bal) found = __shfl_sync(0xffffffffu, off, __ffs(bal) - 1);
+            }
+            nq = 0;
+            __syncwarp();  // the queue's slots are read before the next round refills them
+        };
         // SPL seeds per lane (x, x + 32, ...): one shared-memory key read feeds SPL evaluations.
         for (uint64_t base = 0; base < cap && found == ~0ull; base += 32 * SPL) {
             uint32_t c1m[SPL], c2m[SPL];
@@ -306,15 +330,15 @@ __global__ void __launch_bounds__(kLeafWarps * 32) k_leaves_sh1(const Node *__re
             if (__any_sync(0xffffffffu, any)) {
 #pragma unroll
                 for (int t = 0; t < SPL; t++) {  // seeds in order: all lanes' x + 32 t before x + 32 (t + 1)
-                    bool pass = ok[t] && pseudoforest(seed0 + base + lane + 32 * t);
-                    const unsigned bal = __ballot_sync(0xffffffffu, pass);
-                    if (bal) {
-                        found = base + 32 * t + (__ffs(bal) - 1);
-                        break;
-                    }
+                    const unsigned bal = __ballot_sync(0xffffffffu, ok[t]);
+                    if (ok[t]) sm.q[nq + __popc(bal & below)] = base + 32 * t + lane;
+                    nq += __popc(bal);
                 }
+                __syncwarp();
+                if (nq >= kSh1Drain) drain();
             }
         }
+        if (found == ~0ull && nq) drain();  // the last survivors, at the trial limit
         if (found == ~0ull || found >= cap) {
             if (lane == 0) atomicOr(err, kErrTrialLimit);
             continue;
