@@ -507,14 +507,14 @@ def config_forms(eng, dev, flush, with_cpu):
     counts = {"hash_evals": w["hash_evals"], "scan_tests": w["scan_tests"], "pair_tests": w["pair_tests"],
               "uf_edges": w["uf_edges"]}
     ceil_s = shg.leaf_ceiling_s(counts, lpeaks)
-    names = ("hash", "partition", "plan", "splits", "leaves", "encode", "copy_out", "total")
+    names = ("hash", "layers", "fallback_build", "assign", "leaves", "copy_out", None, "total")  # shg_flat_result
     dq = f.device_query()
     q = dq.query_strings((data, offs))
     c4 = {"class": "ShockHash2Flat<100>", "keys": n4,
           "input": f"host strings, Zipf(1.1) lengths 8..200 (numpy seed 23, mean {len(data) / n4:.1f} bytes)",
           "wall_ns_per_key": round(statistics.mean(wall_ms) * 1e6 / n4, 3),
           "device_ns_per_key": round(f.stage_ms[7] * 1e6 / n4, 3),
-          "stage_ms": {k: round(v, 3) for k, v in zip(names, f.stage_ms)},
+          "stage_ms": {k: round(v, 3) for k, v in zip(names, f.stage_ms) if k},
           "leaf_stage": {"ms": round(f.stage_ms[4], 3), "counts": counts, "ceiling_ms": round(ceil_s * 1e3, 3),
                          "frac": round(ceil_s * 1e3 / f.stage_ms[4], 4)},
           "device_query_ns_per_key": round(dq.last_kernel_ms() * 1e6 / n4, 4),

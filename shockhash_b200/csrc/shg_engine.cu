@@ -16,6 +16,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 #include <dlfcn.h>
 #include <cuda_runtime.h>
@@ -896,7 +897,24 @@ shg_status build_flat(shg_engine *e, uint64_t k, const char *bytes, const uint64
     if (nfb) {
         std::vector<uint64_t> idx(nfb), last(nfb), vals(nfb);
         CU(cudaMemcpy(idx.data(), e->f_list.p, nfb * 8, cudaMemcpyDeviceToHost));
-        std::sort(idx.begin(), idx.end());
+        {  // input order: the device listed them in any order; key indices are below 2^32, so two
+           // 16-bit counting passes sort them
+            std::vector<uint64_t> tmp(nfb);
+            std::vector<uint64_t> cnt(1 << 16);
+            for (int pass = 0; pass < 2; pass++) {
+                const int sh = 16 * pass;
+                std::fill(cnt.begin(), cnt.end(), 0);
+                for (uint64_t v : idx) cnt[(v >> sh) & 0xFFFF]++;
+                uint64_t sum = 0;
+                for (uint64_t &c : cnt) {
+                    const uint64_t x = c;
+                    c = sum;
+                    sum += x;
+                }
+                for (uint64_t v : idx) tmp[cnt[(v >> sh) & 0xFFFF]++] = v;
+                idx.swap(tmp);
+            }
+        }
         // re-mixed hashes of the fallback keys, gathered on the device
         CU(e->f_tmp.ensure(nfb * 8));
         CU(e->f_tmp2.ensure(nfb * 8));
@@ -904,20 +922,39 @@ shg_status build_flat(shg_engine *e, uint64_t k, const char *bytes, const uint64
         flat_launch_gather(e->f_tmp.as<uint64_t>(), e->f_last.as<uint64_t>(), nfb, e->f_tmp2.as<uint64_t>(), s);
         CU(cudaMemcpyAsync(last.data(), e->f_tmp2.p, nfb * 8, cudaMemcpyDeviceToHost, s));
         CU(cudaStreamSynchronize(s));
-        std::string qb;
-        std::vector<uint64_t> qo{0};
-        for (uint64_t h : last) {
-            qb += std::to_string(h);
-            qo.push_back(qb.size());
+        // each fallback key is the decimal string of its re-mixed hash, queried through the fallback
+        // PHF (a read-only host object) on the host's threads, a contiguous range each
+        const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+        const uint64_t nt = std::max<uint64_t>(1, std::min<uint64_t>(hw, nfb / 16384));
+        std::vector<shg_status> tst(nt, SHG_OK);
+        auto query_range = [&](uint64_t t) {
+            const uint64_t j0 = nfb * t / nt, j1 = nfb * (t + 1) / nt;
+            std::string qb;
+            std::vector<uint64_t> qo{0};
+            for (uint64_t j = j0; j < j1; j++) {
+                qb += std::to_string(last[j]);
+                qo.push_back(qb.size());
+            }
+            std::vector<uint64_t> phf(j1 - j0);
+            tst[t] = shg_mphf_query_strings(fbq, qb.data(), qo.data(), j1 - j0, phf.data());
+            for (uint64_t j = j0; j < j1 && tst[t] == SHG_OK; j++) {
+                const uint64_t q = phf[j - j0];
+                if (q >= free_positions.size()) {
+                    tst[t] = SHG_ERR_CUDA;
+                    break;
+                }
+                const uint64_t b = free_positions[q];  // select1(phf + 1) - phf (:295)
+                vals[j] = b < nbuckets ? b : ~1ull;    // keys past the last full bucket are not searched
+            }
+        };
+        {
+            std::vector<std::thread> pool;
+            for (uint64_t t = 1; t < nt; t++) pool.emplace_back(query_range, t);
+            query_range(0);
+            for (auto &th : pool) th.join();
         }
-        std::vector<uint64_t> phf(nfb);
-        shg_status st = shg_mphf_query_strings(fbq, qb.data(), qo.data(), nfb, phf.data());
-        if (st) return fail(st, "fallback query");
-        for (uint64_t j = 0; j < nfb; j++) {
-            if (phf[j] >= free_positions.size()) return fail(SHG_ERR_CUDA, "fallback value outside the free positions");
-            const uint64_t b = free_positions[phf[j]];  // select1(phf + 1) - phf (:295)
-            vals[j] = b < nbuckets ? b : ~1ull;         // keys past the last full bucket are not searched
-        }
+        for (shg_status qs : tst)
+            if (qs) return fail(qs, qs == SHG_ERR_CUDA ? "fallback value outside the free positions" : "fallback query");
         CU(cudaMemcpyAsync(e->f_tmp2.p, vals.data(), nfb * 8, cudaMemcpyHostToDevice, s));
         flat_launch_set_buckets(e->f_tmp.as<uint64_t>(), e->f_tmp2.as<uint64_t>(), nfb, e->f_bucket.as<uint64_t>(), s);
     }
