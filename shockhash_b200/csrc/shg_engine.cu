@@ -135,6 +135,9 @@ struct shg_engine {
     cudaEvent_t chunk_ev[kMaxChunks] = {};
     cudaEvent_t join_ev = nullptr;
     int pipe_chunks = 8;
+    // pinned staging of large copies from pageable host memory (h2d_from_host), made on first use
+    void *stage[2] = {nullptr, nullptr};
+    cudaEvent_t stage_ev[2] = {};
     unsigned long long split_kind[4] = {};  // of the last build (shg_engine_last_work)
     uint64_t split_launches = 0, leaf_scan = 0;
     unsigned long long flat_work[5] = {};  // leaf work of the last ShockHash2Flat build (shg_engine_last_work)
@@ -185,6 +188,13 @@ struct shg_engine {
         for (auto &e : chunk_ev)
             if (e) cudaEventDestroy(e);
         if (join_ev) cudaEventDestroy(join_ev);
+        for (int i = 0; i < 2; i++) {
+            if (stage_ev[i]) {
+                cudaEventSynchronize(stage_ev[i]);
+                cudaEventDestroy(stage_ev[i]);
+            }
+            if (stage[i]) cudaFreeHost(stage[i]);
+        }
         if (stream2) cudaStreamDestroy(stream2);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -193,6 +203,45 @@ struct shg_engine {
 shg_status hash_strings_into(shg_engine *e, const char *bytes, const uint64_t *offsets, uint64_t n, float &ms);
 
 namespace {
+
+// Host-to-device copy of `bytes` from host memory that may be pageable. A pageable source of at
+// least two staging buffers goes through the engine's two pinned buffers of kStageBytes: host
+// threads fill one while the copy engine drains the other (a copy straight from pageable memory ran
+// at about 11 GB/s). The source may be reused when this returns; the device copy is ordered on s.
+constexpr size_t kStageBytes = 64ull << 20;
+shg_status h2d_from_host(shg_engine *e, void *dst, const void *src, size_t bytes, cudaStream_t s) {
+    if (!bytes) return SHG_OK;
+    cudaPointerAttributes attr{};
+    const bool pinned = cudaPointerGetAttributes(&attr, src) == cudaSuccess && attr.type == cudaMemoryTypeHost;
+    cudaGetLastError();  // a pageable pointer may leave an error behind on some drivers
+    if (pinned || bytes < 2 * kStageBytes) {
+        CU(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+        return SHG_OK;
+    }
+    for (int i = 0; i < 2; i++) {
+        if (!e->stage[i]) CU(cudaHostAlloc(&e->stage[i], kStageBytes, cudaHostAllocDefault));
+        if (!e->stage_ev[i]) CU(cudaEventCreateWithFlags(&e->stage_ev[i], cudaEventDisableTiming));
+    }
+    const unsigned nt = std::min(8u, std::max(1u, std::thread::hardware_concurrency()));
+    for (size_t off = 0, c = 0; off < bytes; off += kStageBytes, c++) {
+        const size_t len = std::min(kStageBytes, bytes - off);
+        const int b = (int)(c & 1);
+        CU(cudaEventSynchronize(e->stage_ev[b]));  // the copy that last read this buffer is done
+        char *d = (char *)e->stage[b];
+        const char *from = (const char *)src + off;
+        auto part = [&](unsigned t) {
+            const size_t a = len * t / nt, z = len * (t + 1) / nt;
+            memcpy(d + a, from + a, z - a);
+        };
+        std::vector<std::thread> pool;
+        for (unsigned t = 1; t < nt; t++) pool.emplace_back(part, t);
+        part(0);
+        for (auto &th : pool) th.join();
+        CU(cudaMemcpyAsync((char *)dst + off, d, len, cudaMemcpyHostToDevice, s));
+        CU(cudaEventRecord(e->stage_ev[b], s));
+    }
+    return SHG_OK;
+}
 
 PinnedBlock *acquire_pinned(shg_engine *e, size_t bytes, int refs = 1) {
     std::lock_guard<std::mutex> lock(g_pool_mu);
@@ -781,8 +830,8 @@ shg_status build_flat(shg_engine *e, uint64_t k, const char *bytes, const uint64
     CU(e->f_thr.ensure(std::max<uint64_t>(nbuckets, 1)));
     CU(e->f_mapping.ensure(fc.threshold_range * 4 + 4));
     CU(e->f_lb.ensure(4 * 8));
-    if (nbytes) CU(cudaMemcpyAsync(e->f_bytes.p, bytes, nbytes, cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(e->f_offs.p, offsets, (n + 1) * 8, cudaMemcpyHostToDevice, s));
+    if (shg_status cs = h2d_from_host(e, e->f_bytes.p, bytes, nbytes, s)) return cs;
+    if (shg_status cs = h2d_from_host(e, e->f_offs.p, offsets, (n + 1) * 8, s)) return cs;
     CU(cudaMemcpyAsync(e->f_mapping.p, fc.mapping.data(), fc.threshold_range * 4, cudaMemcpyHostToDevice, s));
     CU(cudaMemsetAsync(e->f_thr.p, 0, std::max<uint64_t>(nbuckets, 1), s));  // thresholdsAndSeeds starts zeroed
     flat_launch_murmur(e->f_bytes.as<uint8_t>(), e->f_offs.as<uint64_t>(), n, e->f_mhc0.as<uint64_t>(), s);
@@ -1248,8 +1297,8 @@ shg_status shg_build_hash128(shg_engine *e, const shg_params *p, const uint64_t 
     CU(e->first.ensure(std::max<uint64_t>(n, 1) * 8));
     CU(e->second.ensure(std::max<uint64_t>(n, 1) * 8));
     if (n) {
-        CU(cudaMemcpyAsync(e->first.p, first, n * 8, cudaMemcpyHostToDevice, e->stream));
-        CU(cudaMemcpyAsync(e->second.p, second, n * 8, cudaMemcpyHostToDevice, e->stream));
+        if (shg_status cs = h2d_from_host(e, e->first.p, first, n * 8, e->stream)) return cs;
+        if (shg_status cs = h2d_from_host(e, e->second.p, second, n * 8, e->stream)) return cs;
     }
     return build_core(e, p, e->first.as<uint64_t>(), e->second.as<uint64_t>(), n, out, 0.f);
 }
@@ -1264,8 +1313,8 @@ shg_status shg_build_shard_hash128(shg_engine *e, const shg_params *p, const uin
     CU(e->first.ensure(std::max<uint64_t>(n, 1) * 8));
     CU(e->second.ensure(std::max<uint64_t>(n, 1) * 8));
     if (n) {
-        CU(cudaMemcpyAsync(e->first.p, first, n * 8, cudaMemcpyHostToDevice, e->stream));
-        CU(cudaMemcpyAsync(e->second.p, second, n * 8, cudaMemcpyHostToDevice, e->stream));
+        if (shg_status cs = h2d_from_host(e, e->first.p, first, n * 8, e->stream)) return cs;
+        if (shg_status cs = h2d_from_host(e, e->second.p, second, n * 8, e->stream)) return cs;
     }
     const ShardSpec shard{nb_global, b0, b1};
     return build_batch(e, p, e->first.as<uint64_t>(), e->second.as<uint64_t>(), std::vector<uint64_t>{n}, out, 0.f, &shard);
@@ -1536,7 +1585,7 @@ shg_status shg_build_u64(shg_engine *e, const shg_params *p, const uint64_t *key
     if (st) return st;
     CU(cudaSetDevice(e->device));
     CU(e->in_keys.ensure(std::max<uint64_t>(n, 1) * 8));
-    if (n) CU(cudaMemcpyAsync(e->in_keys.p, keys, n * 8, cudaMemcpyHostToDevice, e->stream));
+    if (shg_status cs = h2d_from_host(e, e->in_keys.p, keys, n * 8, e->stream)) return cs;
     float ms = 0;
     st = timed_hash_u64(e, e->in_keys.as<uint64_t>(), n, ms);
     if (st) return st;
@@ -1576,8 +1625,8 @@ shg_status hash_strings_into(shg_engine *e, const char *bytes, const uint64_t *o
     CU(e->in_offsets.ensure((n + 1) * 8));
     CU(e->first.ensure(std::max<uint64_t>(n, 1) * 8));
     CU(e->second.ensure(std::max<uint64_t>(n, 1) * 8));
-    if (nbytes) CU(cudaMemcpyAsync(e->in_bytes.p, bytes, nbytes, cudaMemcpyHostToDevice, e->stream));
-    CU(cudaMemcpyAsync(e->in_offsets.p, offsets, (n + 1) * 8, cudaMemcpyHostToDevice, e->stream));
+    if (shg_status cs = h2d_from_host(e, e->in_bytes.p, bytes, nbytes, e->stream)) return cs;
+    if (shg_status cs = h2d_from_host(e, e->in_offsets.p, offsets, (n + 1) * 8, e->stream)) return cs;
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
