@@ -209,6 +209,21 @@ namespace {
 // threads fill one while the copy engine drains the other (a copy straight from pageable memory ran
 // at about 11 GB/s). The source may be reused when this returns; the device copy is ordered on s.
 constexpr size_t kStageBytes = 64ull << 20;
+
+// fn(0) .. fn(nt - 1) on nt host threads (this one included); the parts a thread could not be
+// started for run on this thread, so no exception leaves through the C ABI.
+template <class F> void run_parts(unsigned nt, F &fn) {
+    std::vector<std::thread> pool;
+    unsigned started = 1;
+    try {
+        for (unsigned t = 1; t < nt; t++, started++) pool.emplace_back(fn, t);
+    } catch (...) {
+    }
+    fn(0u);
+    for (unsigned t = started; t < nt; t++) fn(t);
+    for (auto &th : pool) th.join();
+}
+
 shg_status h2d_from_host(shg_engine *e, void *dst, const void *src, size_t bytes, cudaStream_t s) {
     if (!bytes) return SHG_OK;
     cudaPointerAttributes attr{};
@@ -219,7 +234,12 @@ shg_status h2d_from_host(shg_engine *e, void *dst, const void *src, size_t bytes
         return SHG_OK;
     }
     for (int i = 0; i < 2; i++) {
-        if (!e->stage[i]) CU(cudaHostAlloc(&e->stage[i], kStageBytes, cudaHostAllocDefault));
+        if (!e->stage[i] && cudaHostAlloc(&e->stage[i], kStageBytes, cudaHostAllocDefault) != cudaSuccess) {
+            e->stage[i] = nullptr;  // no pinned memory to spare: copy directly
+            cudaGetLastError();
+            CU(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+            return SHG_OK;
+        }
         if (!e->stage_ev[i]) CU(cudaEventCreateWithFlags(&e->stage_ev[i], cudaEventDisableTiming));
     }
     const unsigned nt = std::min(8u, std::max(1u, std::thread::hardware_concurrency()));
@@ -233,10 +253,7 @@ shg_status h2d_from_host(shg_engine *e, void *dst, const void *src, size_t bytes
             const size_t a = len * t / nt, z = len * (t + 1) / nt;
             memcpy(d + a, from + a, z - a);
         };
-        std::vector<std::thread> pool;
-        for (unsigned t = 1; t < nt; t++) pool.emplace_back(part, t);
-        part(0);
-        for (auto &th : pool) th.join();
+        run_parts(nt, part);
         CU(cudaMemcpyAsync((char *)dst + off, d, len, cudaMemcpyHostToDevice, s));
         CU(cudaEventRecord(e->stage_ev[b], s));
     }
@@ -996,12 +1013,8 @@ shg_status build_flat(shg_engine *e, uint64_t k, const char *bytes, const uint64
                 vals[j] = b < nbuckets ? b : ~1ull;    // keys past the last full bucket are not searched
             }
         };
-        {
-            std::vector<std::thread> pool;
-            for (uint64_t t = 1; t < nt; t++) pool.emplace_back(query_range, t);
-            query_range(0);
-            for (auto &th : pool) th.join();
-        }
+        auto query_part = [&](unsigned t) { query_range(t); };
+        run_parts((unsigned)nt, query_part);
         for (shg_status qs : tst)
             if (qs) return fail(qs, qs == SHG_ERR_CUDA ? "fallback value outside the free positions" : "fallback query");
         CU(cudaMemcpyAsync(e->f_tmp2.p, vals.data(), nfb * 8, cudaMemcpyHostToDevice, s));
